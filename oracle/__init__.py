@@ -1,0 +1,92 @@
+"""CPU oracle for the periodic DMK evaluate path (test infrastructure only).
+
+The product never imports this package.  Tests, the smoke check and the
+CPU-baseline leg of bench.py load it as the checker.  It wraps
+``oracle/_build/liboracle.so`` (built by ``make -C oracle``), a CPU restatement
+of the reference evaluate path plus a direct Ewald sum.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-C", _HERE], check=True, stdout=subprocess.DEVNULL)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        d = ctypes.POINTER(ctypes.c_double)
+        _lib.oracle_evaluate.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, d, d]
+        _lib.oracle_evaluate.restype = ctypes.c_int
+        _lib.oracle_plan_stats.argtypes = [d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+        _lib.oracle_plan_stats.restype = ctypes.c_int
+        _lib.oracle_ewald_direct.argtypes = [d, ctypes.c_int, d, d, ctypes.c_double, d, d]
+        _lib.oracle_ewald_direct.restype = ctypes.c_int
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _cell(cell):
+    """cell: 3x3 array whose COLUMNS are lattice vectors -> cell[j*3+i] layout."""
+    c = np.asarray(cell, dtype=np.float64)
+    return np.ascontiguousarray(c.T).reshape(-1)
+
+
+def evaluate(cell, pos, q, n_digits=6, n_per_leaf=300, nz=4, with_far=True, components=False):
+    """Oracle potentials.  pos: (N,3) Cartesian, q: (N,).
+
+    Returns pot (N,) or, with components=True, (pot, dict(near, mid, self, far)).
+    """
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    n = len(q)
+    pot = np.zeros(n)
+    comp = np.zeros(4 * n)
+    c = _cell(cell)
+    rc = lib().oracle_evaluate(_dp(c), n, _dp(pos), _dp(q), n_digits, n_per_leaf, nz,
+                               1 if with_far else 0, _dp(pot), _dp(comp))
+    if rc != 0:
+        raise RuntimeError("oracle_evaluate failed")
+    if components:
+        comp = comp.reshape(4, n)
+        return pot, dict(near=comp[0], mid=comp[1], self=comp[2], far=comp[3])
+    return pot
+
+
+def plan_stats(cell, pos, n_digits=6, n_per_leaf=300, nz=4):
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    out = (ctypes.c_longlong * 10)()
+    c = _cell(cell)
+    if lib().oracle_plan_stats(_dp(c), len(pos), _dp(pos), n_digits, n_per_leaf, nz, out) != 0:
+        raise RuntimeError("oracle_plan_stats failed")
+    keys = ["n_all", "nboxes", "nlevels", "n_target_leaves", "n_pw_boxes", "n_c2proxy_work",
+            "n_list1", "ms", "mt", "mu"]
+    return dict(zip(keys, list(out)))
+
+
+def ewald_direct(cell, pos, q, s=5.0):
+    """Direct Ewald sum: returns (potentials, energy)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    pot = np.zeros(len(q))
+    e = np.zeros(1)
+    c = _cell(cell)
+    if lib().oracle_ewald_direct(_dp(c), len(q), _dp(pos), _dp(q), s, _dp(pot), _dp(e)) != 0:
+        raise RuntimeError("oracle_ewald_direct failed")
+    return pot, float(e[0])

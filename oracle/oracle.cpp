@@ -1,0 +1,523 @@
+// ORACLE — test infrastructure only.  Nothing in the product links, imports or
+// calls this file; only tests/, the smoke check and the CPU-baseline leg of
+// bench.py load it, as the checker.
+//
+// A CPU restatement (FP64, OpenMP) of the reference's evaluate path for one
+// periodic tree, written as plain per-box loops that follow the reference's
+// stage structure:
+//   charge gather + sort                cpp/src/periodic_dmk.cpp:164-169, cpp/src/dmk/pbc_tree.cpp:1807-1821
+//   upward: charge -> proxy moments     cpp/src/dmk/pbc_tree.cpp:1152-1163, cpp/src/dmk/proxy.cpp:153-212
+//   upward: child -> parent (c2p)       cpp/src/dmk/pbc_tree.cpp:1166-1185, cpp/src/dmk/tensorprod.cpp:39-75
+//   outgoing plane waves                cpp/src/dmk/pbc_tree.cpp:1208-1249, cpp/src/dmk/proxy.cpp:42-90
+//   shift + pw -> proxy + p2c + eval    cpp/src/dmk/pbc_tree.cpp:1251-1440, cpp/src/dmk/planewave.cpp:49-105,
+//                                       cpp/src/dmk/proxy.cpp:307-448
+//   residual near field                 cpp/src/dmk/pbc_tree.cpp:1442-1681, cpp/include/dmk/vector_kernels.hpp:354-421
+//   self correction + desort            cpp/src/dmk/pbc_tree.cpp:1759-1805
+//   periodic far field                  cpp/src/dmk/pbc.cpp:359-541
+// Differences from the reference, both exact up to rounding:
+//   * the far field is the exact reciprocal-lattice sum over the same modes and
+//     weights (the reference uses a NUFFT at tolerance eps/4);
+//   * the near field masks pairs by distance instead of culling them by box
+//     contact geometry first (culled pairs all have r >= b and contribute 0).
+// The tree, lists and tables come from the host plan builder.
+//
+// Also: a direct O(N^2) Ewald sum (cpp/src/ewald_nufft.cpp:777-910) as the
+// independent physics check.
+#include <omp.h>
+
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <vector>
+
+#include "../periodicdmk_b200/csrc/host/plan.hpp"
+
+using pdmkb::cplx;
+using pdmkb::Plan;
+
+namespace {
+
+// out(a,b,c) (+)= sum_{ijk} Ux(a,i) Uy(b,j) Uz(c,k) in(i,j,k), x fastest.
+// U_d(a,i) = m[d][a + no*i] (column-major no x ni).
+template <typename Tin, typename Tm, typename Tout>
+void separable(int ni, int no, const Tin* in, const Tm* mx, const Tm* my, const Tm* mz, Tout* out) {
+    using T = decltype(Tin() * Tm());
+    std::vector<T> t1((size_t)no * ni * ni), t2((size_t)no * no * ni);
+    for (int k = 0; k < ni; ++k)
+        for (int j = 0; j < ni; ++j)
+            for (int a = 0; a < no; ++a) {
+                T s = T(0);
+                for (int i = 0; i < ni; ++i) s += mx[a + (size_t)no * i] * in[i + (size_t)ni * (j + (size_t)ni * k)];
+                t1[a + (size_t)no * (j + (size_t)ni * k)] = s;
+            }
+    for (int k = 0; k < ni; ++k)
+        for (int b = 0; b < no; ++b)
+            for (int a = 0; a < no; ++a) {
+                T s = T(0);
+                for (int j = 0; j < ni; ++j) s += my[b + (size_t)no * j] * t1[a + (size_t)no * (j + (size_t)ni * k)];
+                t2[a + (size_t)no * (b + (size_t)no * k)] = s;
+            }
+    for (int c = 0; c < no; ++c)
+        for (int b = 0; b < no; ++b)
+            for (int a = 0; a < no; ++a) {
+                T s = T(0);
+                for (int k = 0; k < ni; ++k) s += mz[c + (size_t)no * k] * t2[a + (size_t)no * (b + (size_t)no * k)];
+                out[a + (size_t)no * (b + (size_t)no * c)] += s;
+            }
+}
+
+void cheb(int p, double x, double* t) {
+    t[0] = 1.0;
+    if (p > 1) t[1] = x;
+    for (int a = 2; a < p; ++a) t[a] = 2.0 * x * t[a - 1] - t[a - 2];
+}
+
+struct Components {
+    std::vector<double> near, mid, self, far;  // user order
+};
+
+void oracle_eval(const Plan& P, const double* q_user, Components& C, bool do_far) {
+    const int p = P.p, n = P.n_pw, n2 = P.n_pw2, M = P.n_modes;
+    const size_t ncoef = (size_t)p * p * p;
+    const int N = P.n_src;
+    std::vector<double> qs(P.n_all);
+    for (int i = 0; i < P.n_all; ++i) qs[i] = q_user[P.src_charge_idx[i]];
+
+    // ---- upward: proxy moments
+    std::vector<double> up((size_t)P.n_proxy_up * ncoef, 0.0);
+    {
+        // group work by centre box so each centre is written by one thread
+        std::vector<std::vector<int>> by_center(P.nboxes);
+        for (int w = 0; w < (int)P.c2proxy_work.size(); ++w) by_center[P.c2proxy_work[w].center_box].push_back(w);
+        std::vector<int> centers;
+        for (int b = 0; b < P.nboxes; ++b)
+            if (!by_center[b].empty()) centers.push_back(b);
+#pragma omp parallel for schedule(dynamic)
+        for (int ci = 0; ci < (int)centers.size(); ++ci) {
+            const int cb = centers[ci];
+            double* M3 = &up[P.proxy_up_off[cb]];
+            std::vector<double> tx(p), ty(p), tz(p);
+            for (int w : by_center[cb]) {
+                const auto& W = P.c2proxy_work[w];
+                const double sc = 2.0 / P.boxsize[W.level];
+                const double* c = &P.centers[3 * cb];
+                for (int s = P.src_start[W.src_box]; s < P.src_start[W.src_box] + P.src_count[W.src_box]; ++s) {
+                    const double* x = &P.src_sorted[3 * (size_t)s];
+                    cheb(p, sc * (x[0] - c[0]), tx.data());
+                    cheb(p, sc * (x[1] - c[1]), ty.data());
+                    cheb(p, sc * (x[2] - c[2]), tz.data());
+                    for (int k = 0; k < p; ++k)
+                        for (int j = 0; j < p; ++j) {
+                            const double f = qs[s] * ty[j] * tz[k];
+                            double* row = M3 + (size_t)p * (j + (size_t)p * k);
+                            for (int i = 0; i < p; ++i) row[i] += f * tx[i];
+                        }
+                }
+            }
+        }
+    }
+    // ---- upward: children -> parent, bottom-up
+    {
+        std::vector<double> c2p((size_t)8 * 3 * p * p);
+        for (int c = 0; c < 8; ++c)
+            for (int d = 0; d < 3; ++d)
+                for (int a = 0; a < p; ++a)
+                    for (int i = 0; i < p; ++i)
+                        c2p[((size_t)c * 3 + d) * p * p + a + (size_t)p * i] =
+                            P.p2c[((size_t)c * 3 + d) * p * p + i + (size_t)p * a];
+        for (int l = P.nlevels - 1; l >= 0; --l) {
+            const auto& LB = P.level_boxes[l];
+#pragma omp parallel for schedule(dynamic)
+            for (int bi = 0; bi < (int)LB.size(); ++bi) {
+                const int b = LB[bi];
+                if (!P.has_proxy_from_children[b]) continue;
+                for (int c = 0; c < 8; ++c) {
+                    const int ch = P.children[b][c];
+                    if (ch < 0 || !(P.src_count[ch] > 0 && P.ifpwexp[ch])) continue;
+                    const double* m = &c2p[(size_t)c * 3 * p * p];
+                    separable<double, double, double>(p, p, &up[P.proxy_up_off[ch]], m, m + p * p, m + 2 * p * p,
+                                                      &up[P.proxy_up_off[b]]);
+                }
+            }
+        }
+    }
+    // ---- outgoing plane waves
+    std::vector<cplx> pw((size_t)P.n_pw_exp * M, cplx(0));
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < P.nboxes; ++b) {
+        if (P.pw_off[b] < 0) continue;
+        const auto& T = P.lev[P.depth[b]];
+        // out(k1,k2,k3) = sum poly2pw(k1,m1) poly2pw(k2,m2) poly2pw(k3,m3) proxy(m1,m2,m3),
+        // k3 restricted to the half-space (first n2 z-frequencies).
+        {
+            const double* in = &up[P.proxy_up_off[b]];
+            std::vector<cplx> t1((size_t)n * p * p), t2((size_t)n * n * p);
+            for (int k = 0; k < p; ++k)
+                for (int j = 0; j < p; ++j)
+                    for (int a = 0; a < n; ++a) {
+                        cplx s(0);
+                        for (int i = 0; i < p; ++i) s += T.poly2pw[a + (size_t)n * i] * in[i + (size_t)p * (j + (size_t)p * k)];
+                        t1[a + (size_t)n * (j + (size_t)p * k)] = s;
+                    }
+            for (int k = 0; k < p; ++k)
+                for (int bb = 0; bb < n; ++bb)
+                    for (int a = 0; a < n; ++a) {
+                        cplx s(0);
+                        for (int j = 0; j < p; ++j) s += T.poly2pw[bb + (size_t)n * j] * t1[a + (size_t)n * (j + (size_t)p * k)];
+                        t2[a + (size_t)n * (bb + (size_t)n * k)] = s;
+                    }
+            cplx* out = &pw[P.pw_off[b]];
+            for (int c = 0; c < n2; ++c)
+                for (int bb = 0; bb < n; ++bb)
+                    for (int a = 0; a < n; ++a) {
+                        cplx s(0);
+                        for (int k = 0; k < p; ++k) s += T.poly2pw[c + (size_t)n * k] * t2[a + (size_t)n * (bb + (size_t)n * k)];
+                        out[a + (size_t)n * (bb + (size_t)n * c)] = s;
+                    }
+        }
+    }
+    // ---- downward: per level, shift + pw->proxy + parent->child
+    std::vector<double> down((size_t)P.n_proxy_down * ncoef, 0.0);
+    for (int l = 0; l < P.nlevels; ++l) {
+        const auto& T = P.lev[l];
+        const double bs = P.boxsize[l];
+        const auto& LB = P.level_boxes[l];
+#pragma omp parallel for schedule(dynamic)
+        for (int bi = 0; bi < (int)LB.size(); ++bi) {
+            const int b = LB[bi];
+            const bool has_output = P.trg_count[b] > 0;
+            if (!(P.ifpwexp[b] && P.src_count[b] + P.trg_count[b] > 0 && has_output)) continue;
+            std::vector<cplx> pin((size_t)M, cplx(0));
+            // self term (stencil 13) then colleagues
+            auto add_shift = [&](int src_box, int st) {
+                const cplx* po = &pw[P.pw_off[src_box]];
+                const double* re = &T.shift[(size_t)st * 2 * M];
+                const double* im = re + M;
+                for (int m = 0; m < M; ++m) pin[m] += po[m] * cplx(re[m], im[m]);
+            };
+            add_shift(b, 13);
+            for (int ind = 0; ind < 27; ++ind) {
+                const int nb = P.colleagues[b][ind];
+                if (nb < 0 || nb == b) continue;
+                if (P.is_leaf[b] && P.is_leaf[nb]) continue;
+                if (P.pw_off[nb] < 0) continue;
+                int st = 0, stride = 1;
+                for (int d = 0; d < 3; ++d) {
+                    const int kd = (int)std::lround((P.centers[3 * b + d] - P.centers[3 * nb + d]) / bs) + 1;
+                    st += kd * stride;
+                    stride *= 3;
+                }
+                add_shift(nb, st);
+            }
+            // proxy_down += 2 Re sum pw2poly(m1,a) pw2poly(m2,b) w(m3) pw2poly(m3,c) pin(m1,m2,m3)
+            std::vector<cplx> t1((size_t)p * n * n2), t2((size_t)p * p * n2);
+            for (int m3 = 0; m3 < n2; ++m3)
+                for (int m2 = 0; m2 < n; ++m2)
+                    for (int a = 0; a < p; ++a) {
+                        cplx s(0);
+                        for (int m1 = 0; m1 < n; ++m1) s += T.pw2poly[m1 + (size_t)n * a] * pin[m1 + (size_t)n * (m2 + (size_t)n * m3)];
+                        t1[a + (size_t)p * (m2 + (size_t)n * m3)] = s;
+                    }
+            for (int m3 = 0; m3 < n2; ++m3)
+                for (int bb = 0; bb < p; ++bb)
+                    for (int a = 0; a < p; ++a) {
+                        cplx s(0);
+                        for (int m2 = 0; m2 < n; ++m2) s += T.pw2poly[m2 + (size_t)n * bb] * t1[a + (size_t)p * (m2 + (size_t)n * m3)];
+                        t2[a + (size_t)p * (bb + (size_t)p * m3)] = s;
+                    }
+            double* dn = &down[P.proxy_down_off[b]];
+            for (int c = 0; c < p; ++c)
+                for (int bb = 0; bb < p; ++bb)
+                    for (int a = 0; a < p; ++a) {
+                        cplx s(0);
+                        for (int m3 = 0; m3 < n2; ++m3) {
+                            const double w = m3 >= n / 2 ? 0.5 : 1.0;
+                            s += w * T.pw2poly[m3 + (size_t)n * c] * t2[a + (size_t)p * (bb + (size_t)p * m3)];
+                        }
+                        dn[a + (size_t)p * (bb + (size_t)p * c)] += 2.0 * s.real();
+                    }
+            if (!P.iftensprodeval[b]) {
+                for (int c = 0; c < 8; ++c) {
+                    const int ch = P.children[b][c];
+                    if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch])) continue;
+                    const double* m = &P.p2c[(size_t)c * 3 * p * p];
+                    separable<double, double, double>(p, p, dn, m, m + p * p, m + 2 * p * p, &down[P.proxy_down_off[ch]]);
+                }
+            }
+        }
+    }
+    // ---- proxy -> targets at leaves
+    std::vector<double> mid_sorted(N, 0.0), near_sorted(N, 0.0);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < P.nboxes; ++b) {
+        if (!P.iftensprodeval[b] || P.trg_count[b] == 0) continue;
+        const double sc = 2.0 / P.boxsize[P.depth[b]];
+        const double* c = &P.centers[3 * b];
+        const double* cf = &down[P.proxy_down_off[b]];
+        std::vector<double> tx(p), ty(p), tz(p);
+        for (int t = P.trg_start[b]; t < P.trg_start[b] + P.trg_count[b]; ++t) {
+            const double* x = &P.trg_sorted[3 * (size_t)t];
+            cheb(p, sc * (x[0] - c[0]), tx.data());
+            cheb(p, sc * (x[1] - c[1]), ty.data());
+            cheb(p, sc * (x[2] - c[2]), tz.data());
+            double s = 0;
+            for (int k = 0; k < p; ++k)
+                for (int j = 0; j < p; ++j) {
+                    double r = 0;
+                    const double* row = cf + (size_t)p * (j + (size_t)p * k);
+                    for (int i = 0; i < p; ++i) r += row[i] * tx[i];
+                    s += r * ty[j] * tz[k];
+                }
+            mid_sorted[t] += s;
+        }
+    }
+    // ---- residual near field
+    const std::vector<double>& cf = P.resid;
+    const int nc = (int)cf.size();
+#pragma omp parallel for schedule(dynamic)
+    for (int wi = 0; wi < (int)P.direct_work.size(); ++wi) {
+        const int tb = P.direct_work[wi];
+        if (P.trg_count[tb] == 0) continue;
+        const int tl = P.depth[tb];
+        for (int li = P.list1_start[tb]; li < P.list1_start[tb + 1]; ++li) {
+            const int sb = P.list1[li];
+            int sl = P.depth[sb];
+            double bsize = P.boxsize[sl];
+            if (P.ifpwexp[sb] && sb == tb)
+                bsize /= 2.0;
+            else if (sl < tl)
+                bsize = P.boxsize[tl];
+            const double d2max = bsize * bsize, rsc = 2.0 / bsize, cen = -bsize / 2.0;
+            for (int t = P.trg_start[tb]; t < P.trg_start[tb] + P.trg_count[tb]; ++t) {
+                const double* x = &P.trg_sorted[3 * (size_t)t];
+                double acc = 0;
+                for (int s = P.src_start[sb]; s < P.src_start[sb] + P.src_count[sb]; ++s) {
+                    const double* y = &P.src_sorted[3 * (size_t)s];
+                    const double dx = x[0] - y[0], dy = x[1] - y[1], dz = x[2] - y[2];
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (!(r2 > 1e-30 && r2 < d2max)) continue;
+                    const double r = std::sqrt(r2);
+                    const double xm = (r + cen) * rsc;
+                    double pv = cf[nc - 1];
+                    for (int i = nc - 2; i >= 0; --i) pv = pv * xm + cf[i];
+                    acc += qs[s] * pv / r;
+                }
+                near_sorted[t] += acc;
+            }
+        }
+    }
+    // ---- self correction and desort
+    C.near.assign(N, 0.0);
+    C.mid.assign(N, 0.0);
+    C.self.assign(N, 0.0);
+    C.far.assign(N, 0.0);
+    for (int b = 0; b < P.nboxes; ++b) {
+        if (!P.is_leaf[b] || P.trg_count[b] == 0) continue;
+        const double w0 = P.w0[P.depth[b] + P.ifpwexp[b]];
+        for (int t = P.trg_start[b]; t < P.trg_start[b] + P.trg_count[b]; ++t) {
+            const int u = P.trg_perm[t];
+            C.self[u] = -w0 * q_user[u];
+            C.near[u] = near_sorted[t];
+            C.mid[u] = mid_sorted[t];
+        }
+    }
+    if (!do_far) return;
+    // ---- far field: exact sum over the (ms, mt, mu) modes with nonzero weight
+    const double twopi = 2.0 * M_PI;
+    std::vector<double> X(N), Y(N), Z(N);
+    for (int i = 0; i < N; ++i) {
+        const double* r = &P.r_user[3 * (size_t)i];
+        X[i] = twopi * (P.umatinv[0] * r[0] + P.umatinv[3] * r[1] + P.umatinv[6] * r[2]);
+        Y[i] = twopi * (P.umatinv[4] * r[1] + P.umatinv[7] * r[2]);
+        Z[i] = twopi * (P.umatinv[8] * r[2]);
+    }
+    struct Mode {
+        int i, j, k;
+        double w;
+    };
+    std::vector<Mode> modes;
+    {
+        size_t idx = 0;
+        for (int k = -P.mu / 2; k <= (P.mu - 1) / 2; ++k)
+            for (int j = -P.mt / 2; j <= (P.mt - 1) / 2; ++j)
+                for (int i = -P.ms / 2; i <= (P.ms - 1) / 2; ++i, ++idx)
+                    if (P.ff_weights[idx] != 0.0) modes.push_back({i, j, k, P.ff_weights[idx]});
+    }
+    const int nm = (int)modes.size();
+    std::vector<cplx> S(nm, cplx(0));
+#pragma omp parallel for schedule(static)
+    for (int m = 0; m < nm; ++m) {
+        cplx s(0);
+        for (int l = 0; l < N; ++l) {
+            const double ph = modes[m].i * X[l] + modes[m].j * Y[l] + modes[m].k * Z[l];
+            s += q_user[l] * cplx(std::cos(ph), -std::sin(ph));
+        }
+        S[m] = s * modes[m].w;
+    }
+#pragma omp parallel for schedule(static)
+    for (int l = 0; l < N; ++l) {
+        double u = 0;
+        for (int m = 0; m < nm; ++m) {
+            const double ph = modes[m].i * X[l] + modes[m].j * Y[l] + modes[m].k * Z[l];
+            u += S[m].real() * std::cos(ph) - S[m].imag() * std::sin(ph);
+        }
+        C.far[l] = u;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Evaluate potentials with the oracle.  comp (optional, 4*N): near | mid | self | far.
+// Returns 0 on success, -1 on error (message on stderr).
+int oracle_evaluate(const double* cell, int n, const double* pos, const double* q, int n_digits, int n_per_leaf,
+                    int nz, int with_far, double* pot, double* comp) {
+    try {
+        Plan P = pdmkb::build_plan(cell, n, pos, n_digits, n_per_leaf, nz);
+        Components C;
+        oracle_eval(P, q, C, with_far != 0);
+        for (int i = 0; i < n; ++i) pot[i] = C.near[i] + C.mid[i] + C.self[i] + C.far[i];
+        if (comp) {
+            std::memcpy(comp, C.near.data(), n * sizeof(double));
+            std::memcpy(comp + n, C.mid.data(), n * sizeof(double));
+            std::memcpy(comp + 2 * (size_t)n, C.self.data(), n * sizeof(double));
+            std::memcpy(comp + 3 * (size_t)n, C.far.data(), n * sizeof(double));
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_evaluate: %s\n", e.what());
+        return -1;
+    }
+}
+
+// Plan statistics for tests: out[0..9] = n_all, nboxes, nlevels, n_target_leaves,
+// n_pw_boxes, n_c2proxy_work, list1 total, ms, mt, mu.
+int oracle_plan_stats(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz,
+                      long long* out) {
+    try {
+        Plan P = pdmkb::build_plan(cell, n, pos, n_digits, n_per_leaf, nz);
+        int nlt = 0;
+        for (int b = 0; b < P.nboxes; ++b)
+            if (P.is_leaf[b] && P.trg_count[b] > 0) nlt++;
+        out[0] = P.n_all;
+        out[1] = P.nboxes;
+        out[2] = P.nlevels;
+        out[3] = nlt;
+        out[4] = P.n_pw_exp;
+        out[5] = (long long)P.c2proxy_work.size();
+        out[6] = (long long)P.list1.size();
+        out[7] = P.ms;
+        out[8] = P.mt;
+        out[9] = P.mu;
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_plan_stats: %s\n", e.what());
+        return -1;
+    }
+}
+
+// Direct Ewald sum (neutral-gauge potentials, k = 0 dropped).  cell[j*3+i] =
+// component i of lattice vector j; pos[3*i+d].  s sets the accuracy
+// (erfc(s), exp(-s^2)).  energy = 1/2 sum q phi - pi Q^2 / (2 V alpha^2).
+int oracle_ewald_direct(const double* cell, int n, const double* pos, const double* q, double s, double* pot,
+                        double* energy) {
+    const double* a0 = cell;
+    const double* a1 = cell + 3;
+    const double* a2 = cell + 6;
+    auto cross = [](const double* u, const double* v, double* w) {
+        w[0] = u[1] * v[2] - u[2] * v[1];
+        w[1] = u[2] * v[0] - u[0] * v[2];
+        w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+    double c12[3], c20[3], c01[3];
+    cross(a1, a2, c12);
+    cross(a2, a0, c20);
+    cross(a0, a1, c01);
+    const double V = std::fabs(dot(a0, c12));
+    if (V <= 0) return -1;
+    const double alpha = std::pow(n * M_PI * M_PI * M_PI / (V * V), 1.0 / 6.0);
+    const double rcut = s / alpha, kmax = 2.0 * s * alpha;
+    const double h[3] = {V / std::sqrt(dot(c12, c12)), V / std::sqrt(dot(c20, c20)), V / std::sqrt(dot(c01, c01))};
+    int nmax[3];
+    for (int d = 0; d < 3; ++d) nmax[d] = (int)std::ceil(rcut / h[d]);
+    // reciprocal vectors b_d = 2 pi (a_{d+1} x a_{d+2}) / V
+    double b[3][3];
+    for (int d = 0; d < 3; ++d) {
+        b[0][d] = 2 * M_PI * c12[d] / V;
+        b[1][d] = 2 * M_PI * c20[d] / V;
+        b[2][d] = 2 * M_PI * c01[d] / V;
+    }
+    // reciprocal-lattice heights: 2 pi / |a_d| along b_d directions
+    int mmax[3];
+    for (int d = 0; d < 3; ++d) {
+        const double* ad = cell + 3 * d;
+        mmax[d] = (int)std::ceil(kmax * std::sqrt(dot(ad, ad)) / (2 * M_PI));
+    }
+    std::vector<double> phi(n, 0.0);
+    const double rc2 = rcut * rcut;
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < n; ++i) {
+        double acc = 0;
+        for (int j = 0; j < n; ++j)
+            for (int n0 = -nmax[0]; n0 <= nmax[0]; ++n0)
+                for (int n1 = -nmax[1]; n1 <= nmax[1]; ++n1)
+                    for (int n2 = -nmax[2]; n2 <= nmax[2]; ++n2) {
+                        if (i == j && n0 == 0 && n1 == 0 && n2 == 0) continue;
+                        double dr[3];
+                        for (int d = 0; d < 3; ++d)
+                            dr[d] = pos[3 * i + d] - pos[3 * j + d] + n0 * a0[d] + n1 * a1[d] + n2 * a2[d];
+                        const double r2 = dot(dr, dr);
+                        if (r2 > rc2) continue;
+                        const double r = std::sqrt(r2);
+                        acc += q[j] * std::erfc(alpha * r) / r;
+                    }
+        phi[i] = acc;
+    }
+    const double km2 = kmax * kmax, inv4a2 = 1.0 / (4 * alpha * alpha), pref = 4 * M_PI / V;
+    std::vector<std::array<double, 4>> ks;
+    for (int m3 = -mmax[2]; m3 <= mmax[2]; ++m3)
+        for (int m2 = -mmax[1]; m2 <= mmax[1]; ++m2)
+            for (int m1 = -mmax[0]; m1 <= mmax[0]; ++m1) {
+                if (!m1 && !m2 && !m3) continue;
+                double kv[3];
+                for (int d = 0; d < 3; ++d) kv[d] = m1 * b[0][d] + m2 * b[1][d] + m3 * b[2][d];
+                const double k2 = dot(kv, kv);
+                if (k2 > km2) continue;
+                ks.push_back({kv[0], kv[1], kv[2], pref * std::exp(-k2 * inv4a2) / k2});
+            }
+    const int nk = (int)ks.size();
+    std::vector<cplx> S(nk);
+#pragma omp parallel for schedule(static)
+    for (int m = 0; m < nk; ++m) {
+        cplx s(0);
+        for (int j = 0; j < n; ++j) {
+            const double ph = ks[m][0] * pos[3 * j] + ks[m][1] * pos[3 * j + 1] + ks[m][2] * pos[3 * j + 2];
+            s += q[j] * cplx(std::cos(ph), -std::sin(ph));
+        }
+        S[m] = s * ks[m][3];
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        double acc = 0;
+        for (int m = 0; m < nk; ++m) {
+            const double ph = ks[m][0] * pos[3 * i] + ks[m][1] * pos[3 * i + 1] + ks[m][2] * pos[3 * i + 2];
+            acc += S[m].real() * std::cos(ph) - S[m].imag() * std::sin(ph);
+        }
+        phi[i] += acc - 2.0 * alpha / std::sqrt(M_PI) * q[i];
+    }
+    double E = 0, Q = 0;
+    for (int i = 0; i < n; ++i) {
+        pot[i] = phi[i];
+        E += q[i] * phi[i];
+        Q += q[i];
+    }
+    if (energy) *energy = 0.5 * E - M_PI * Q * Q / (2 * V * alpha * alpha);
+    return 0;
+}
+
+}  // extern "C"
