@@ -1,0 +1,101 @@
+/* C ABI of the B200 periodic DMK library (libpdmk_b200.so).
+ *
+ * The first block replaces, symbol for symbol, the reference's
+ * cpp/include/pdmk/pdmk_capi.h:20-51 (exported from libpdmk_jl.so and bound by
+ * julia/PeriodicDMK/src/PeriodicDMK.jl:120-126,135-137,172-181,198-209):
+ * same names, argument order, layouts and return conventions.
+ *   - cell_3x3: column-major 3x3, cell[i + 3*j] = component i of lattice vector j
+ *   - positions_3xN: column-major 3xN, positions[d + 3*i] = coordinate d of point i
+ *   - int-returning calls: 0 on success, -1 on a null handle or an exception
+ *     (message on stderr), -2 on a CUDA error reported by the device.
+ *   - create calls return NULL on error (message on stderr).
+ *   - the caller owns all buffers; the library owns a handle until destroy.
+ * The second block is additive (no reference counterpart, same conventions).
+ */
+#ifndef PDMK_CAPI_H
+#define PDMK_CAPI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference entry points ------------------------------------------- */
+
+/* Ewald summation reference (replaces cpp/include/pdmk/pdmk_capi.h:23-28;
+ * reference implementation cpp/src/ewald_nufft.cpp:445-654).  Host code, not
+ * the accelerated path.  s sets the accuracy: erfc(s) ~ exp(-s^2). */
+int pdmk_ewald_nufft(const double* cell_3x3, int N, const double* positions_3xN, const double* charges, double s,
+                     double* potentials_out, double* energy_out);
+
+/* Cubic cover of a cell (replaces cpp/include/pdmk/pdmk_capi.h:32-35;
+ * reference cpp/src/cubic_cover_optimizer.cpp:33-89).  Returns 1 for nz <= 0. */
+int pdmk_optimize_cubic_cover(const double* cell_3x3, int nz, int* m_out, int* n_out, int* p_out, double* e1_out,
+                              double* e2_out, double* e3_out, double* s_out, double* cost_out);
+
+/* Build a tree (replaces cpp/include/pdmk/pdmk_capi.h:39-41 / :45-47,
+ * cpp/src/pdmk_capi.cpp:48-59).  The tree is built on the host and uploaded to
+ * the current CUDA device. */
+void* pdmk_create_double(const double* cell_3x3, int N, const double* positions_3xN, int n_digits, int n_per_leaf,
+                         int nz);
+void* pdmk_create_float(const double* cell_3x3, int N, const double* positions_3xN, int n_digits, int n_per_leaf,
+                        int nz);
+
+/* Evaluate potentials for N charges in user order (replaces
+ * cpp/include/pdmk/pdmk_capi.h:40-43 / :46-49, cpp/src/pdmk_capi.cpp:61-77).
+ * N and positions_3xN are ignored, as in the reference. */
+int pdmk_evaluate_double(void* h, int N, const double* positions_3xN, const double* charges, double* pot_out);
+int pdmk_evaluate_float(void* h, int N, const double* positions_3xN, const double* charges, float* pot_out);
+
+void pdmk_destroy_double(void* h);
+void pdmk_destroy_float(void* h);
+
+/* ---- additive entry points (no reference counterpart) ----------------- */
+
+/* evaluate with a device-time breakdown: timing[0..3] = nufft_ms, dmk_ms,
+ * direct_ms, build_ms (the fields of the reference's EvalTiming). */
+int pdmk_evaluate_timed_double(void* h, int N, const double* positions_3xN, const double* charges, double* pot_out,
+                               double* timing4);
+int pdmk_evaluate_timed_float(void* h, int N, const double* positions_3xN, const double* charges, float* pot_out,
+                              double* timing4);
+
+/* k charge vectors on one tree: charges_Nxk[i + N*c], pot_Nxk[i + N*c]. */
+int pdmk_evaluate_multi_double(void* h, int N, int k, const double* charges_Nxk, double* pot_Nxk);
+int pdmk_evaluate_multi_float(void* h, int N, int k, const double* charges_Nxk, float* pot_Nxk);
+
+/* Device-resident evaluate: charges_dev / pot_dev are device pointers (N
+ * doubles for the double tree; charges double and pot float for the float
+ * tree) on the tree's device.  The call returns after the work completes. */
+int pdmk_evaluate_device_double(void* h, const double* charges_dev, double* pot_dev);
+int pdmk_evaluate_device_float(void* h, const double* charges_dev, float* pot_dev);
+
+/* The two parts of the potential in user order: the tree part (near field +
+ * plane-wave levels - self term) and the periodic far field. */
+int pdmk_evaluate_parts_double(void* h, const double* charges, double* tree_part, double* far_part);
+
+/* Tree facts: out[0..11] = N, n_all (originals + images), boxes, levels,
+ * target leaves, expansion order p, plane waves per axis, kernel launches per
+ * evaluate, device bytes, far-field modes (ms, mt, mu product), near-field
+ * box pairs, plane-wave boxes. */
+int pdmk_info_double(void* h, int64_t* out12);
+int pdmk_info_float(void* h, int64_t* out12);
+
+/* Stage times of the most recent evaluate of a double tree: out8[0..7] =
+ * dmk_ms, near_ms (residual near-field kernel), nufft_ms, finalize_ms,
+ * total_ms, near-field pairs after the reference's contact-geometry cull,
+ * near-field pairs before it, residual polynomial length. */
+int pdmk_stage_times_double(void* h, double* out8);
+
+/* Measured FMA throughput of the current device in TFLOP/s (fp64 != 0: FP64,
+ * else FP32), 2 flops per FMA; the denominator of CUDA-core rooflines. */
+int pdmk_fma_peak(int fp64, double* tflops);
+
+/* Last error message of the calling thread ("" if none). */
+const char* pdmk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDMK_CAPI_H */

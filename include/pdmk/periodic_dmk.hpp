@@ -1,0 +1,67 @@
+// Public C++ API: build-once / evaluate-many periodic Laplace (Coulomb) solver.
+//
+// Drop-in for the reference's PeriodicDMKTreeT<Real, DIM>
+// (cpp/include/pdmk/periodic_dmk.hpp:17-60): same constructor arguments,
+// evaluate / evaluate_timed semantics, n_points(), cube_size(); non-copyable,
+// non-movable, not thread-safe.  Construction builds the tree on the host and
+// uploads it to the current CUDA device; evaluate runs on that GPU.
+//   Real = double : plain path, FP64 throughout.
+//   Real = float  : mixed-precision path (FP32 near field and transforms where
+//                   the error budget allows, FP64 far field and accumulation),
+//                   float output as in the reference.
+// Only DIM = 3 is provided (the reference's 2D and quasi-periodic paths are
+// not part of this build).
+#pragma once
+#include <array>
+#include <memory>
+#include <optional>
+#include <vector>
+
+#include "eval_timing.hpp"
+#include "types.hpp"
+
+namespace pdmk {
+
+template <typename Real = double, int DIM = 3>
+class PeriodicDMKTreeT {
+    static_assert(DIM == 3, "only DIM = 3 is supported");
+
+  public:
+    using scalar_type = Real;
+
+    PeriodicDMKTreeT(const MatND<DIM>& cell_matrix, const std::vector<VecND<DIM>>& positions, int n_digits = 6,
+                     int n_per_leaf = 300, int nz = 4, std::optional<std::array<double, DIM>> bloch = std::nullopt);
+    ~PeriodicDMKTreeT();
+    PeriodicDMKTreeT(const PeriodicDMKTreeT&) = delete;
+    PeriodicDMKTreeT& operator=(const PeriodicDMKTreeT&) = delete;
+    PeriodicDMKTreeT(PeriodicDMKTreeT&&) = delete;
+    PeriodicDMKTreeT& operator=(PeriodicDMKTreeT&&) = delete;
+
+    /// Periodic Coulomb potentials sum'_{j,n} q_j / |x_i - x_j - R_n| at the
+    /// stored positions (neutral gauge: the k = 0 mode is dropped).
+    /// Throws std::invalid_argument if charges.size() != n_points().
+    std::vector<Real> evaluate(const std::vector<double>& charges);
+    /// Same, with a three-way device-time breakdown.
+    std::vector<Real> evaluate_timed(const std::vector<double>& charges, EvalTiming& timing);
+    /// k charge vectors on the same tree: charges is N x k column-major
+    /// (charges[i + N*c]); returns N x k column-major potentials.
+    std::vector<Real> evaluate_multi(const std::vector<double>& charges, int k);
+
+    int n_points() const { return n_src_; }
+    double cube_size() const { return rc_; }
+
+    struct Impl;
+    Impl* impl() { return p_.get(); }
+
+  private:
+    std::unique_ptr<Impl> p_;
+    int n_src_;
+    double rc_;
+};
+
+using PeriodicDMKTree = PeriodicDMKTreeT<double, 3>;
+
+extern template class PeriodicDMKTreeT<double, 3>;
+extern template class PeriodicDMKTreeT<float, 3>;
+
+}  // namespace pdmk

@@ -30,11 +30,19 @@ def lib():
         _lib.oracle_evaluate.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, d, d]
         _lib.oracle_evaluate.restype = ctypes.c_int
+        _lib.oracle_evaluate2.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, d, d]
+        _lib.oracle_evaluate2.restype = ctypes.c_int
         _lib.oracle_plan_stats.argtypes = [d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
         _lib.oracle_plan_stats.restype = ctypes.c_int
         _lib.oracle_ewald_direct.argtypes = [d, ctypes.c_int, d, d, ctypes.c_double, d, d]
         _lib.oracle_ewald_direct.restype = ctypes.c_int
+        _lib.oracle_pswf.argtypes = [ctypes.c_double, ctypes.c_int, d, d, d]
+        _lib.oracle_legendre.argtypes = [ctypes.c_int, d, d]
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.oracle_plan_images.argtypes = [d, ctypes.c_int, d, ctypes.c_int, d, d, ip, d, d, ip, ctypes.c_long]
+        _lib.oracle_plan_images.restype = ctypes.c_long
     return _lib
 
 
@@ -48,10 +56,12 @@ def _cell(cell):
     return np.ascontiguousarray(c.T).reshape(-1)
 
 
-def evaluate(cell, pos, q, n_digits=6, n_per_leaf=300, nz=4, with_far=True, components=False):
+def evaluate(cell, pos, q, n_digits=6, n_per_leaf=300, nz=4, with_far=True, components=False, fast_far=False):
     """Oracle potentials.  pos: (N,3) Cartesian, q: (N,).
 
-    Returns pot (N,) or, with components=True, (pot, dict(near, mid, self, far)).
+    The far field is the exact reciprocal-lattice sum unless fast_far=True (CPU
+    NUFFT, used for CPU timing only).  Returns pot (N,) or, with
+    components=True, (pot, dict(near, mid, self, far)).
     """
     pos = np.ascontiguousarray(pos, dtype=np.float64)
     q = np.ascontiguousarray(q, dtype=np.float64)
@@ -59,8 +69,8 @@ def evaluate(cell, pos, q, n_digits=6, n_per_leaf=300, nz=4, with_far=True, comp
     pot = np.zeros(n)
     comp = np.zeros(4 * n)
     c = _cell(cell)
-    rc = lib().oracle_evaluate(_dp(c), n, _dp(pos), _dp(q), n_digits, n_per_leaf, nz,
-                               1 if with_far else 0, _dp(pot), _dp(comp))
+    rc = lib().oracle_evaluate2(_dp(c), n, _dp(pos), _dp(q), n_digits, n_per_leaf, nz,
+                                1 if with_far else 0, 1 if fast_far else 0, _dp(pot), _dp(comp))
     if rc != 0:
         raise RuntimeError("oracle_evaluate failed")
     if components:
@@ -90,3 +100,34 @@ def ewald_direct(cell, pos, q, s=5.0):
     if lib().oracle_ewald_direct(_dp(c), len(q), _dp(pos), _dp(q), s, _dp(pot), _dp(e)) != 0:
         raise RuntimeError("oracle_ewald_direct failed")
     return pot, float(e[0])
+
+
+def pswf(beta, x):
+    """Host PSWF psi_0^beta(x) and moments (c0, c1, c2/c0, c4) of the product's plan builder."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    psi = np.zeros_like(x)
+    m = np.zeros(4)
+    lib().oracle_pswf(beta, len(x), _dp(x), _dp(psi), _dp(m))
+    return psi, m
+
+
+def legendre(n):
+    x, w = np.zeros(n), np.zeros(n)
+    lib().oracle_legendre(n, _dp(x), _dp(w))
+    return x, w
+
+
+def plan_images(cell, pos, nz=4):
+    """(umat, qmat, mgrid, xgrid0, rc, img_src_idx) of the product's host plan."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    c = _cell(cell)
+    umat, qmat, xg, rc = np.zeros(9), np.zeros(9), np.zeros(3), np.zeros(1)
+    mg = np.zeros(3, dtype=np.int32)
+    cap = 60 * len(pos)
+    idx = np.zeros(cap, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    n = lib().oracle_plan_images(_dp(c), len(pos), _dp(pos), nz, _dp(umat), _dp(qmat), mg.ctypes.data_as(ip),
+                                 _dp(xg), _dp(rc), idx.ctypes.data_as(ip), cap)
+    if n < 0:
+        raise RuntimeError("oracle_plan_images failed")
+    return umat, qmat, mg, xg, float(rc[0]), idx[:n]

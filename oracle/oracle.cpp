@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "../periodicdmk_b200/csrc/host/plan.hpp"
+#include "../periodicdmk_b200/csrc/host/pswf.hpp"
 
 using pdmkb::cplx;
 using pdmkb::Plan;
@@ -79,7 +80,9 @@ struct Components {
     std::vector<double> near, mid, self, far;  // user order
 };
 
-void oracle_eval(const Plan& P, const double* q_user, Components& C, bool do_far) {
+void far_nufft(const Plan& P, const double* q_user, std::vector<double>& far);
+
+void oracle_eval(const Plan& P, const double* q_user, Components& C, bool do_far, bool fast_far) {
     const int p = P.p, n = P.n_pw, n2 = P.n_pw2, M = P.n_modes;
     const size_t ncoef = (size_t)p * p * p;
     const int N = P.n_src;
@@ -325,6 +328,10 @@ void oracle_eval(const Plan& P, const double* q_user, Components& C, bool do_far
         }
     }
     if (!do_far) return;
+    if (fast_far) {
+        far_nufft(P, q_user, C.far);
+        return;
+    }
     // ---- far field: exact sum over the (ms, mt, mu) modes with nonzero weight
     const double twopi = 2.0 * M_PI;
     std::vector<double> X(N), Y(N), Z(N);
@@ -368,18 +375,177 @@ void oracle_eval(const Plan& P, const double* q_user, Components& C, bool do_far
     }
 }
 
+// Far field by a CPU NUFFT (for the CPU timing baseline only; the exact sum
+// above is the parity reference).  Exponential-of-semicircle kernel
+// phi(z) = exp(b (sqrt(1 - z^2) - 1)), width W, b = 2.30 W, 2x oversampled
+// grid; the small grid is transformed to and from the mode box by separable
+// direct DFTs.
+void far_nufft(const Plan& P, const double* q, std::vector<double>& far) {
+    const int N = P.n_src;
+    int W = (int)std::ceil(-std::log10(P.dp.eps / 4.0)) + 1;
+    W = std::min(14, std::max(4, W));
+    const double beta = 2.30 * W;
+    const int m[3] = {P.ms, P.mt, P.mu};
+    int ng[3];
+    for (int d = 0; d < 3; ++d) ng[d] = std::max(2 * m[d], 2 * W) + (std::max(2 * m[d], 2 * W) & 1);
+    const double twopi = 2.0 * M_PI;
+    const size_t G = (size_t)ng[0] * ng[1] * ng[2];
+    auto kern = [&](double z) { return z * z < 1.0 ? std::exp(beta * (std::sqrt(1.0 - z * z) - 1.0)) : 0.0; };
+    std::vector<std::array<int, 3>> l0(N);
+    std::vector<double> kv((size_t)N * 3 * W);
+    for (int i = 0; i < N; ++i) {
+        const double* r = &P.r_user[3 * (size_t)i];
+        const double s[3] = {P.umatinv[0] * r[0] + P.umatinv[3] * r[1] + P.umatinv[6] * r[2],
+                             P.umatinv[4] * r[1] + P.umatinv[7] * r[2], P.umatinv[8] * r[2]};
+        for (int d = 0; d < 3; ++d) {
+            const double t = (s[d] - std::floor(s[d])) * ng[d];
+            l0[i][d] = (int)std::ceil(t - 0.5 * W);
+            for (int a = 0; a < W; ++a) kv[((size_t)i * 3 + d) * W + a] = kern((t - (l0[i][d] + a)) / (0.5 * W));
+        }
+    }
+    auto wrap = [](int i, int n) { i %= n; return i < 0 ? i + n : i; };
+    // spread (per-thread grids, then reduce)
+    std::vector<double> grid(G, 0.0);
+#pragma omp parallel
+    {
+        std::vector<double> g(G, 0.0);
+#pragma omp for schedule(static)
+        for (int i = 0; i < N; ++i) {
+            const double* kx = &kv[((size_t)i * 3 + 0) * W];
+            const double* ky = &kv[((size_t)i * 3 + 1) * W];
+            const double* kz = &kv[((size_t)i * 3 + 2) * W];
+            for (int a = 0; a < W; ++a) {
+                const size_t ia = (size_t)wrap(l0[i][0] + a, ng[0]) * ng[1];
+                for (int b = 0; b < W; ++b) {
+                    const size_t ib = (ia + wrap(l0[i][1] + b, ng[1])) * ng[2];
+                    const double f = q[i] * kx[a] * ky[b];
+                    for (int c = 0; c < W; ++c) g[ib + wrap(l0[i][2] + c, ng[2])] += f * kz[c];
+                }
+            }
+        }
+#pragma omp critical
+        for (size_t k = 0; k < G; ++k) grid[k] += g[k];
+    }
+    // kernel Fourier transforms on each axis
+    std::vector<double> gx(200), gw(200);
+    pdmkb::gauss_legendre(200, gx.data(), gw.data());
+    auto phihat = [&](int d, int k) {
+        const double alpha = 0.5 * W * twopi / ng[d];
+        double s = 0;
+        for (int i = 0; i < 200; ++i) s += gw[i] * kern(gx[i]) * std::cos(k * alpha * gx[i]);
+        return alpha * s;
+    };
+    // forward separable DFT: grid (l1,l2,l3) -> B(k1,k2,k3) for k_d in [-m_d/2, (m_d-1)/2]
+    std::vector<cplx> e[3];
+    for (int d = 0; d < 3; ++d) {
+        e[d].resize((size_t)m[d] * ng[d]);
+        for (int k = 0; k < m[d]; ++k)
+            for (int l = 0; l < ng[d]; ++l) {
+                const double ph = -twopi * (double)(k - m[d] / 2) * l / ng[d];
+                e[d][(size_t)k * ng[d] + l] = cplx(std::cos(ph), std::sin(ph));
+            }
+    }
+    // layout grid[(l1*n2 + l2)*n3 + l3]
+    std::vector<cplx> b1((size_t)m[0] * ng[1] * ng[2]), b2((size_t)m[0] * m[1] * ng[2]), b3((size_t)m[0] * m[1] * m[2]);
+#pragma omp parallel for collapse(2)
+    for (int k1 = 0; k1 < m[0]; ++k1)
+        for (int l2 = 0; l2 < ng[1]; ++l2)
+            for (int l3 = 0; l3 < ng[2]; ++l3) {
+                cplx s(0);
+                for (int l1 = 0; l1 < ng[0]; ++l1) s += e[0][(size_t)k1 * ng[0] + l1] * grid[((size_t)l1 * ng[1] + l2) * ng[2] + l3];
+                b1[((size_t)k1 * ng[1] + l2) * ng[2] + l3] = s;
+            }
+#pragma omp parallel for collapse(2)
+    for (int k1 = 0; k1 < m[0]; ++k1)
+        for (int k2 = 0; k2 < m[1]; ++k2)
+            for (int l3 = 0; l3 < ng[2]; ++l3) {
+                cplx s(0);
+                for (int l2 = 0; l2 < ng[1]; ++l2) s += e[1][(size_t)k2 * ng[1] + l2] * b1[((size_t)k1 * ng[1] + l2) * ng[2] + l3];
+                b2[((size_t)k1 * m[1] + k2) * ng[2] + l3] = s;
+            }
+    const double H = twopi * twopi * twopi / ((double)ng[0] * ng[1] * ng[2]);
+    std::vector<double> ph[3];
+    for (int d = 0; d < 3; ++d) {
+        ph[d].resize(m[d]);
+        for (int k = 0; k < m[d]; ++k) ph[d][k] = phihat(d, k - m[d] / 2);
+    }
+#pragma omp parallel for collapse(2)
+    for (int k1 = 0; k1 < m[0]; ++k1)
+        for (int k2 = 0; k2 < m[1]; ++k2)
+            for (int k3 = 0; k3 < m[2]; ++k3) {
+                cplx s(0);
+                for (int l3 = 0; l3 < ng[2]; ++l3) s += e[2][(size_t)k3 * ng[2] + l3] * b2[((size_t)k1 * m[1] + k2) * ng[2] + l3];
+                // ff_weights layout: k3 slowest, k1 fastest
+                const double w = P.ff_weights[((size_t)k3 * m[1] + k2) * m[0] + k1];
+                const double Ps = ph[0][k1] * ph[1][k2] * ph[2][k3];
+                b3[((size_t)k1 * m[1] + k2) * m[2] + k3] = s * (w * H * H / (Ps * Ps));
+            }
+    // inverse separable DFT back to the grid (real part)
+#pragma omp parallel for collapse(2)
+    for (int k1 = 0; k1 < m[0]; ++k1)
+        for (int k2 = 0; k2 < m[1]; ++k2)
+            for (int l3 = 0; l3 < ng[2]; ++l3) {
+                cplx s(0);
+                for (int k3 = 0; k3 < m[2]; ++k3) s += std::conj(e[2][(size_t)k3 * ng[2] + l3]) * b3[((size_t)k1 * m[1] + k2) * m[2] + k3];
+                b2[((size_t)k1 * m[1] + k2) * ng[2] + l3] = s;
+            }
+#pragma omp parallel for collapse(2)
+    for (int k1 = 0; k1 < m[0]; ++k1)
+        for (int l2 = 0; l2 < ng[1]; ++l2)
+            for (int l3 = 0; l3 < ng[2]; ++l3) {
+                cplx s(0);
+                for (int k2 = 0; k2 < m[1]; ++k2) s += std::conj(e[1][(size_t)k2 * ng[1] + l2]) * b2[((size_t)k1 * m[1] + k2) * ng[2] + l3];
+                b1[((size_t)k1 * ng[1] + l2) * ng[2] + l3] = s;
+            }
+#pragma omp parallel for collapse(2)
+    for (int l1 = 0; l1 < ng[0]; ++l1)
+        for (int l2 = 0; l2 < ng[1]; ++l2)
+            for (int l3 = 0; l3 < ng[2]; ++l3) {
+                cplx s(0);
+                for (int k1 = 0; k1 < m[0]; ++k1) s += std::conj(e[0][(size_t)k1 * ng[0] + l1]) * b1[((size_t)k1 * ng[1] + l2) * ng[2] + l3];
+                grid[((size_t)l1 * ng[1] + l2) * ng[2] + l3] = s.real();
+            }
+    far.assign(N, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; ++i) {
+        const double* kx = &kv[((size_t)i * 3 + 0) * W];
+        const double* ky = &kv[((size_t)i * 3 + 1) * W];
+        const double* kz = &kv[((size_t)i * 3 + 2) * W];
+        double u = 0;
+        for (int a = 0; a < W; ++a) {
+            const size_t ia = (size_t)wrap(l0[i][0] + a, ng[0]) * ng[1];
+            for (int b = 0; b < W; ++b) {
+                const size_t ib = (ia + wrap(l0[i][1] + b, ng[1])) * ng[2];
+                double sc = 0;
+                for (int c = 0; c < W; ++c) sc += kz[c] * grid[ib + wrap(l0[i][2] + c, ng[2])];
+                u += kx[a] * ky[b] * sc;
+            }
+        }
+        far[i] = u;
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+int oracle_evaluate2(const double* cell, int n, const double* pos, const double* q, int n_digits, int n_per_leaf,
+                     int nz, int with_far, int fast_far, double* pot, double* comp);
 
 // Evaluate potentials with the oracle.  comp (optional, 4*N): near | mid | self | far.
 // Returns 0 on success, -1 on error (message on stderr).
 int oracle_evaluate(const double* cell, int n, const double* pos, const double* q, int n_digits, int n_per_leaf,
                     int nz, int with_far, double* pot, double* comp) {
+    return oracle_evaluate2(cell, n, pos, q, n_digits, n_per_leaf, nz, with_far, 0, pot, comp);
+}
+
+// with_far: 0 none, 1 far field; fast_far: 0 exact reciprocal sum, 1 CPU NUFFT.
+int oracle_evaluate2(const double* cell, int n, const double* pos, const double* q, int n_digits, int n_per_leaf,
+                     int nz, int with_far, int fast_far, double* pot, double* comp) {
     try {
         Plan P = pdmkb::build_plan(cell, n, pos, n_digits, n_per_leaf, nz);
         Components C;
-        oracle_eval(P, q, C, with_far != 0);
+        oracle_eval(P, q, C, with_far != 0, fast_far != 0);
         for (int i = 0; i < n; ++i) pot[i] = C.near[i] + C.mid[i] + C.self[i] + C.far[i];
         if (comp) {
             std::memcpy(comp, C.near.data(), n * sizeof(double));
@@ -416,6 +582,43 @@ int oracle_plan_stats(const double* cell, int n, const double* pos, int n_digits
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "oracle_plan_stats: %s\n", e.what());
+        return -1;
+    }
+}
+
+// Host PSWF and quadrature of the product (checked against golden vectors).
+int oracle_pswf(double beta, int nx, const double* x, double* psi, double* moments4) {
+    pdmkb::Pswf0 pf(beta);
+    for (int i = 0; i < nx; ++i) psi[i] = pf(x[i]);
+    pf.moments(moments4[0], moments4[1], moments4[2], moments4[3]);
+    return 0;
+}
+
+int oracle_legendre(int n, double* x, double* w) {
+    pdmkb::gauss_legendre(n, x, w);
+    return 0;
+}
+
+// Geometry of the host plan (for comparison with the reference's own image
+// layout): returns the image count; fills umat, qmat, mgrid, xgrid0, rc and up
+// to cap image source indices.
+long oracle_plan_images(const double* cell, int n, const double* pos, int nz, double* umat, double* qmat, int* mgrid,
+                        double* xgrid0, double* rc, int* img_idx, long cap) {
+    try {
+        Plan P = pdmkb::build_plan(cell, n, pos, 6, 1 << 30, nz);
+        for (int i = 0; i < 9; ++i) {
+            umat[i] = P.umat[i];
+            qmat[i] = P.qmat[i];
+        }
+        for (int d = 0; d < 3; ++d) {
+            mgrid[d] = P.mgrid[d];
+            xgrid0[d] = P.xgrid0[d];
+        }
+        *rc = P.rc;
+        for (long i = 0; i < (long)P.img_src_idx.size() && i < cap; ++i) img_idx[i] = P.img_src_idx[i];
+        return (long)P.img_src_idx.size();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_plan_images: %s\n", e.what());
         return -1;
     }
 }

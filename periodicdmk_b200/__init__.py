@@ -1,0 +1,269 @@
+"""B200-native periodic DMK (3D Laplace / Coulomb) evaluate path.
+
+Python mirror of the reference's build-once / evaluate-many interface
+(``PeriodicDMKTreeT`` in cpp/include/pdmk/periodic_dmk.hpp:17-60 and the Julia
+``PDMKSolver`` in julia/PeriodicDMK/src/PeriodicDMK.jl:90-211), bound to the
+C ABI of ``lib/libpdmk_b200.so`` (include/pdmk/pdmk_capi.h).  Every evaluate
+runs on the GPU; there is no CPU fallback: if the library cannot be loaded,
+or CUDA is unavailable, the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["PeriodicDMKTree", "library", "library_path", "ewald", "optimize_cubic_cover", "EXPORTED_SYMBOLS"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "lib", "libpdmk_b200.so")
+_lib = None
+
+# Every entry point declared in include/pdmk/pdmk_capi.h.
+EXPORTED_SYMBOLS = [
+    "pdmk_ewald_nufft", "pdmk_optimize_cubic_cover",
+    "pdmk_create_double", "pdmk_create_float",
+    "pdmk_evaluate_double", "pdmk_evaluate_float",
+    "pdmk_destroy_double", "pdmk_destroy_float",
+    "pdmk_evaluate_timed_double", "pdmk_evaluate_timed_float",
+    "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
+    "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
+    "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
+    "pdmk_stage_times_double", "pdmk_fma_peak", "pdmk_last_error",
+]
+
+_D = ctypes.POINTER(ctypes.c_double)
+_F = ctypes.POINTER(ctypes.c_float)
+_I64 = ctypes.POINTER(ctypes.c_int64)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def library():
+    """Load libpdmk_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError("libpdmk_b200.so not built: run `python -m periodicdmk_b200.build` (%s)" % _LIB_PATH)
+    lib = ctypes.CDLL(_LIB_PATH)
+    v = ctypes.c_void_p
+    lib.pdmk_create_double.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.pdmk_create_double.restype = v
+    lib.pdmk_create_float.argtypes = lib.pdmk_create_double.argtypes
+    lib.pdmk_create_float.restype = v
+    lib.pdmk_evaluate_double.argtypes = [v, ctypes.c_int, _D, _D, _D]
+    lib.pdmk_evaluate_float.argtypes = [v, ctypes.c_int, _D, _D, _F]
+    lib.pdmk_evaluate_timed_double.argtypes = [v, ctypes.c_int, _D, _D, _D, _D]
+    lib.pdmk_evaluate_timed_float.argtypes = [v, ctypes.c_int, _D, _D, _F, _D]
+    lib.pdmk_evaluate_multi_double.argtypes = [v, ctypes.c_int, ctypes.c_int, _D, _D]
+    lib.pdmk_evaluate_multi_float.argtypes = [v, ctypes.c_int, ctypes.c_int, _D, _F]
+    lib.pdmk_evaluate_device_double.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pdmk_evaluate_device_float.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pdmk_evaluate_parts_double.argtypes = [v, _D, _D, _D]
+    lib.pdmk_info_double.argtypes = [v, _I64]
+    lib.pdmk_info_float.argtypes = [v, _I64]
+    for f in ("pdmk_evaluate_double", "pdmk_evaluate_float", "pdmk_evaluate_timed_double",
+              "pdmk_evaluate_timed_float", "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
+              "pdmk_evaluate_device_double", "pdmk_evaluate_device_float", "pdmk_evaluate_parts_double",
+              "pdmk_info_double", "pdmk_info_float"):
+        getattr(lib, f).restype = ctypes.c_int
+    lib.pdmk_destroy_double.argtypes = [v]
+    lib.pdmk_destroy_double.restype = None
+    lib.pdmk_destroy_float.argtypes = [v]
+    lib.pdmk_destroy_float.restype = None
+    lib.pdmk_ewald_nufft.argtypes = [_D, ctypes.c_int, _D, _D, ctypes.c_double, _D, _D]
+    lib.pdmk_ewald_nufft.restype = ctypes.c_int
+    lib.pdmk_optimize_cubic_cover.argtypes = [_D, ctypes.c_int, _I, _I, _I, _D, _D, _D, _D, _D]
+    lib.pdmk_optimize_cubic_cover.restype = ctypes.c_int
+    lib.pdmk_stage_times_double.argtypes = [v, _D]
+    lib.pdmk_stage_times_double.restype = ctypes.c_int
+    lib.pdmk_fma_peak.argtypes = [ctypes.c_int, _D]
+    lib.pdmk_fma_peak.restype = ctypes.c_int
+    lib.pdmk_last_error.argtypes = []
+    lib.pdmk_last_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _last_error():
+    return library().pdmk_last_error().decode(errors="replace")
+
+
+def _ptr(a, t=_D):
+    return a.ctypes.data_as(t)
+
+
+def _cell_colmajor(cell):
+    """3x3 with lattice vectors as COLUMNS -> column-major flat (cell[i + 3*j])."""
+    c = np.asarray(cell, dtype=np.float64)
+    if c.shape != (3, 3):
+        raise ValueError("cell must be 3x3 (columns = lattice vectors)")
+    return np.ascontiguousarray(c.T).reshape(-1)
+
+
+class PeriodicDMKTree:
+    """Build-once / evaluate-many periodic Coulomb solver on one GPU.
+
+    cell: 3x3, columns are the lattice vectors.  positions: (N, 3) Cartesian.
+    precision: "double" (plain FP64 path) or "float" (mixed-precision path,
+    float output), as the reference's double / float instantiations.
+    """
+
+    INFO_KEYS = ["n_points", "n_all", "n_boxes", "n_levels", "n_target_leaves", "p", "n_pw",
+                 "launches_per_evaluate", "device_bytes", "far_modes", "near_pairs", "pw_boxes"]
+
+    def __init__(self, cell, positions, n_digits=6, n_per_leaf=300, nz=4, precision="double"):
+        if precision not in ("double", "float"):
+            raise ValueError("precision must be 'double' or 'float'")
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        if pos.ndim != 2 or pos.shape[1] != 3:
+            raise ValueError("positions must be (N, 3)")
+        self._lib = library()
+        self.precision = precision
+        self.N = pos.shape[0]
+        c = _cell_colmajor(cell)
+        create = self._lib.pdmk_create_double if precision == "double" else self._lib.pdmk_create_float
+        self._h = create(_ptr(c), self.N, _ptr(pos), int(n_digits), int(n_per_leaf), int(nz))
+        if not self._h:
+            raise RuntimeError("pdmk_create failed: " + _last_error())
+        self.n_digits = n_digits
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("%s failed (code %d): %s" % (what, rc, _last_error()))
+
+    def _charges(self, charges):
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        if q.shape != (self.N,):
+            raise ValueError("charges must have shape (%d,)" % self.N)
+        return q
+
+    @property
+    def dtype(self):
+        return np.float64 if self.precision == "double" else np.float32
+
+    def evaluate(self, charges):
+        q = self._charges(charges)
+        out = np.empty(self.N, dtype=self.dtype)
+        dummy = np.zeros(3, dtype=np.float64)
+        if self.precision == "double":
+            rc = self._lib.pdmk_evaluate_double(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(out))
+        else:
+            rc = self._lib.pdmk_evaluate_float(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(out, _F))
+        self._check(rc, "pdmk_evaluate")
+        return out
+
+    def evaluate_timed(self, charges):
+        """Returns (potentials, {"nufft_ms", "dmk_ms", "direct_ms", "build_ms"})."""
+        q = self._charges(charges)
+        out = np.empty(self.N, dtype=self.dtype)
+        t = np.zeros(4)
+        dummy = np.zeros(3, dtype=np.float64)
+        if self.precision == "double":
+            rc = self._lib.pdmk_evaluate_timed_double(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(out), _ptr(t))
+        else:
+            rc = self._lib.pdmk_evaluate_timed_float(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(out, _F), _ptr(t))
+        self._check(rc, "pdmk_evaluate_timed")
+        return out, dict(nufft_ms=t[0], dmk_ms=t[1], direct_ms=t[2], build_ms=t[3])
+
+    def evaluate_multi(self, charges):
+        """charges: (N, k) -> potentials (N, k)."""
+        q = np.asarray(charges, dtype=np.float64)
+        if q.ndim != 2 or q.shape[0] != self.N:
+            raise ValueError("charges must be (N, k)")
+        k = q.shape[1]
+        qc = np.ascontiguousarray(q.T)  # column-major N x k
+        out = np.empty((k, self.N), dtype=self.dtype)
+        if self.precision == "double":
+            rc = self._lib.pdmk_evaluate_multi_double(self._h, self.N, k, _ptr(qc), _ptr(out))
+        else:
+            rc = self._lib.pdmk_evaluate_multi_float(self._h, self.N, k, _ptr(qc), _ptr(out, _F))
+        self._check(rc, "pdmk_evaluate_multi")
+        return out.T
+
+    def evaluate_device(self, q_ptr, pot_ptr):
+        """Device-resident evaluate on raw device pointers (e.g. torch .data_ptr())."""
+        f = self._lib.pdmk_evaluate_device_double if self.precision == "double" else \
+            self._lib.pdmk_evaluate_device_float
+        self._check(f(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(pot_ptr)), "pdmk_evaluate_device")
+
+    def evaluate_parts(self, charges):
+        """(tree part, far-field part), both user order; double trees only."""
+        if self.precision != "double":
+            raise RuntimeError("evaluate_parts is provided for double trees")
+        q = self._charges(charges)
+        a = np.empty(self.N)
+        b = np.empty(self.N)
+        self._check(self._lib.pdmk_evaluate_parts_double(self._h, _ptr(q), _ptr(a), _ptr(b)),
+                    "pdmk_evaluate_parts")
+        return a, b
+
+    def info(self):
+        out = np.zeros(12, dtype=np.int64)
+        f = self._lib.pdmk_info_double if self.precision == "double" else self._lib.pdmk_info_float
+        self._check(f(self._h, _ptr(out, _I64)), "pdmk_info")
+        return dict(zip(self.INFO_KEYS, [int(x) for x in out]))
+
+    STAGE_KEYS = ["dmk_ms", "near_ms", "nufft_ms", "finalize_ms", "total_ms", "near_pairs_culled",
+                  "near_pairs_nominal", "near_ncoef"]
+
+    def stage_times(self):
+        """Stage times of the most recent evaluate (double trees)."""
+        out = np.zeros(8)
+        self._check(self._lib.pdmk_stage_times_double(self._h, _ptr(out)), "pdmk_stage_times")
+        return dict(zip(self.STAGE_KEYS, out.tolist()))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            (self._lib.pdmk_destroy_double if self.precision == "double" else self._lib.pdmk_destroy_float)(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def ewald(cell, positions, charges, s=4.8):
+    """Ewald reference through the C ABI (host code).  Returns (potentials, energy)."""
+    lib = library()
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    q = np.ascontiguousarray(charges, dtype=np.float64)
+    pot = np.empty(len(q))
+    e = np.zeros(1)
+    c = _cell_colmajor(cell)
+    rc = lib.pdmk_ewald_nufft(_ptr(c), len(q), _ptr(pos), _ptr(q), float(s), _ptr(pot), _ptr(e))
+    if rc != 0:
+        raise RuntimeError("pdmk_ewald_nufft failed: " + _last_error())
+    return pot, float(e[0])
+
+
+def optimize_cubic_cover(cell, nz=4):
+    lib = library()
+    c = _cell_colmajor(cell)
+    m, n, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    e1, e2, e3 = np.zeros(3), np.zeros(3), np.zeros(3)
+    s, cost = np.zeros(1), np.zeros(1)
+    rc = lib.pdmk_optimize_cubic_cover(_ptr(c), int(nz), ctypes.byref(m), ctypes.byref(n), ctypes.byref(p),
+                                       _ptr(e1), _ptr(e2), _ptr(e3), _ptr(s), _ptr(cost))
+    if rc != 0:
+        raise RuntimeError("pdmk_optimize_cubic_cover failed (code %d)" % rc)
+    return dict(m=m.value, n=n.value, p=p.value, e1=e1, e2=e2, e3=e3, s=float(s[0]), cost=float(cost[0]))
+
+
+def fma_peak_tflops(fp64=True):
+    """Measured FMA throughput of the current CUDA device (TFLOP/s)."""
+    out = np.zeros(1)
+    if library().pdmk_fma_peak(1 if fp64 else 0, _ptr(out)) != 0:
+        raise RuntimeError("pdmk_fma_peak failed: " + _last_error())
+    return float(out[0])

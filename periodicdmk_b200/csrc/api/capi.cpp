@@ -1,0 +1,380 @@
+// extern "C" boundary of libpdmk_b200.so.  See include/pdmk/pdmk_capi.h for the
+// contract; each entry cites the reference interface it replaces there.
+#include "pdmk/pdmk_capi.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "impl.hpp"
+#include "pdmk/periodic_dmk.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const char* where, const char* what) {
+    g_last_error = std::string(where) + ": " + what;
+    std::fprintf(stderr, "%s\n", g_last_error.c_str());
+}
+
+// CUDA failures surface as std::runtime_error whose message starts with
+// "CUDA error" / "cuFFT error"; they map to -2.
+int fail(const char* where, const std::exception& e) {
+    set_error(where, e.what());
+    const std::string m = e.what();
+    return (m.rfind("CUDA error", 0) == 0 || m.rfind("cuFFT error", 0) == 0) ? -2 : -1;
+}
+
+pdmk::Mat3 to_mat3(const double* c) {
+    pdmk::Mat3 h;
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) h[j][i] = c[i + 3 * j];
+    return h;
+}
+
+std::vector<pdmk::Vec3> to_positions(const double* p, int n) {
+    std::vector<pdmk::Vec3> v(n);
+    for (int i = 0; i < n; ++i) v[i] = {p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+    return v;
+}
+
+template <typename Real>
+void* create_impl(const double* cell, int n, const double* pos, int nd, int npl, int nz) {
+    try {
+        if (!cell || !pos) throw std::invalid_argument("null cell or positions");
+        if (n <= 0) throw std::invalid_argument("N must be positive");
+        g_last_error.clear();
+        return new pdmk::PeriodicDMKTreeT<Real, 3>(to_mat3(cell), to_positions(pos, n), nd, npl, nz);
+    } catch (const std::exception& e) {
+        set_error("pdmk_create", e.what());
+        return nullptr;
+    }
+}
+
+template <typename Real, typename Out>
+int evaluate_impl(void* h, const double* q, Out* pot, double* timing4) {
+    if (!h) {
+        set_error("pdmk_evaluate", "null handle");
+        return -1;
+    }
+    try {
+        if (!q || !pot) throw std::invalid_argument("null charges or output");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
+        const int n = t->n_points();
+        std::vector<double> qv(q, q + n);
+        pdmk::EvalTiming tm;
+        auto r = t->evaluate_timed(qv, tm);
+        for (int i = 0; i < n; ++i) pot[i] = (Out)r[i];
+        if (timing4) {
+            timing4[0] = tm.nufft_ms;
+            timing4[1] = tm.dmk_ms;
+            timing4[2] = tm.direct_ms;
+            timing4[3] = tm.build_ms;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate", e);
+    }
+}
+
+template <typename Real, typename Out>
+int evaluate_multi_impl(void* h, int k, const double* q, Out* pot) {
+    if (!h) {
+        set_error("pdmk_evaluate_multi", "null handle");
+        return -1;
+    }
+    try {
+        if (!q || !pot) throw std::invalid_argument("null charges or output");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
+        const size_t n = (size_t)t->n_points();
+        if (k <= 0) throw std::invalid_argument("k must be positive");
+        std::vector<double> qv(q, q + n * k);
+        auto r = t->evaluate_multi(qv, k);
+        for (size_t i = 0; i < n * k; ++i) pot[i] = (Out)r[i];
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_multi", e);
+    }
+}
+
+template <typename Real>
+int info_impl(void* h, int64_t* out) {
+    if (!h || !out) {
+        set_error("pdmk_info", "null handle or output");
+        return -1;
+    }
+    auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
+    auto* im = t->impl();
+    const pdmkb::Plan& P = *im->plan;
+    int nlt = 0;
+    for (int b = 0; b < P.nboxes; ++b)
+        if (P.is_leaf[b] && P.trg_count[b] > 0) nlt++;
+    out[0] = P.n_src;
+    out[1] = P.n_all;
+    out[2] = P.nboxes;
+    out[3] = P.nlevels;
+    out[4] = nlt;
+    out[5] = P.p;
+    out[6] = P.n_pw;
+    out[7] = im->dev->launches_per_evaluate();
+    out[8] = (int64_t)im->dev->device_bytes();
+    out[9] = (int64_t)P.ms * P.mt * P.mu;
+    out[10] = (int64_t)P.list1.size();
+    out[11] = P.n_pw_exp;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pdmk_last_error(void) { return g_last_error.c_str(); }
+
+void* pdmk_create_double(const double* cell, int N, const double* pos, int nd, int npl, int nz) {
+    return create_impl<double>(cell, N, pos, nd, npl, nz);
+}
+void* pdmk_create_float(const double* cell, int N, const double* pos, int nd, int npl, int nz) {
+    return create_impl<float>(cell, N, pos, nd, npl, nz);
+}
+int pdmk_evaluate_double(void* h, int, const double*, const double* q, double* pot) {
+    return evaluate_impl<double, double>(h, q, pot, nullptr);
+}
+int pdmk_evaluate_float(void* h, int, const double*, const double* q, float* pot) {
+    return evaluate_impl<float, float>(h, q, pot, nullptr);
+}
+int pdmk_evaluate_timed_double(void* h, int, const double*, const double* q, double* pot, double* t4) {
+    return evaluate_impl<double, double>(h, q, pot, t4);
+}
+int pdmk_evaluate_timed_float(void* h, int, const double*, const double* q, float* pot, double* t4) {
+    return evaluate_impl<float, float>(h, q, pot, t4);
+}
+int pdmk_evaluate_multi_double(void* h, int, int k, const double* q, double* pot) {
+    return evaluate_multi_impl<double, double>(h, k, q, pot);
+}
+int pdmk_evaluate_multi_float(void* h, int, int k, const double* q, float* pot) {
+    return evaluate_multi_impl<float, float>(h, k, q, pot);
+}
+void pdmk_destroy_double(void* h) { delete static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h); }
+void pdmk_destroy_float(void* h) { delete static_cast<pdmk::PeriodicDMKTreeT<float, 3>*>(h); }
+
+int pdmk_evaluate_device_double(void* h, const double* q_dev, double* pot_dev) {
+    if (!h) {
+        set_error("pdmk_evaluate_device", "null handle");
+        return -1;
+    }
+    try {
+        if (!q_dev || !pot_dev) throw std::invalid_argument("null device pointer");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h);
+        auto* dv = t->impl()->dev.get();
+        dv->evaluate_device(q_dev, pot_dev, nullptr);
+        PDMK_CUDA_CHECK(cudaStreamSynchronize(dv->stream()));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_device", e);
+    }
+}
+
+int pdmk_evaluate_device_float(void* h, const double* q_dev, float* pot_dev) {
+    (void)q_dev;
+    (void)pot_dev;
+    if (!h) {
+        set_error("pdmk_evaluate_device", "null handle");
+        return -1;
+    }
+    set_error("pdmk_evaluate_device_float", "not available for this tree type");
+    return -1;
+}
+
+int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, double* far_part) {
+    if (!h) {
+        set_error("pdmk_evaluate_parts", "null handle");
+        return -1;
+    }
+    try {
+        if (!q || !tree_part || !far_part) throw std::invalid_argument("null buffer");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h);
+        t->impl()->dev->evaluate_parts_host(q, tree_part, far_part);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_parts", e);
+    }
+}
+
+int pdmk_info_double(void* h, int64_t* out) { return info_impl<double>(h, out); }
+
+int pdmk_stage_times_double(void* h, double* out8) {
+    if (!h || !out8) {
+        set_error("pdmk_stage_times", "null handle or output");
+        return -1;
+    }
+    try {
+        auto* dv = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h)->impl()->dev.get();
+        const pdmkb::StageTimes t = dv->last_times();
+        out8[0] = t.dmk_ms;
+        out8[1] = t.near_ms;
+        out8[2] = t.nufft_ms;
+        out8[3] = t.finalize_ms;
+        out8[4] = t.dmk_ms + t.direct_ms + t.nufft_ms;
+        out8[5] = (double)dv->near_pairs_culled();
+        out8[6] = (double)dv->near_pairs_nominal();
+        out8[7] = (double)dv->near_coeffs();
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_stage_times", e);
+    }
+}
+
+int pdmk_fma_peak(int fp64, double* tflops) {
+    try {
+        if (!tflops) throw std::invalid_argument("null output");
+        *tflops = pdmkb::dev::fma_probe_tflops(fp64 != 0);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_fma_peak", e);
+    }
+}
+int pdmk_info_float(void* h, int64_t* out) { return info_impl<float>(h, out); }
+
+// ---------------------------------------------------------------------------
+// Ewald reference (host).  Real-space erfc sum over lattice shells within
+// r_cut = s/alpha plus the reciprocal Gaussian sum over |k| <= 2 s alpha, self
+// term -2 alpha/sqrt(pi) q_i and the charged-system energy correction.
+// ---------------------------------------------------------------------------
+int pdmk_ewald_nufft(const double* cell, int N, const double* pos, const double* q, double s, double* pot,
+                     double* energy) {
+    try {
+        if (!cell || !pos || !q || !pot) throw std::invalid_argument("null buffer");
+        if (N <= 0) throw std::invalid_argument("N must be positive");
+        const double* a[3] = {cell, cell + 3, cell + 6};
+        auto cross = [](const double* u, const double* v, double* w) {
+            w[0] = u[1] * v[2] - u[2] * v[1];
+            w[1] = u[2] * v[0] - u[0] * v[2];
+            w[2] = u[0] * v[1] - u[1] * v[0];
+        };
+        auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+        double c[3][3];
+        cross(a[1], a[2], c[0]);
+        cross(a[2], a[0], c[1]);
+        cross(a[0], a[1], c[2]);
+        const double V = std::fabs(dot(a[0], c[0]));
+        if (!(V > 0)) throw std::invalid_argument("degenerate cell");
+        const double alpha = std::pow(N * M_PI * M_PI * M_PI / (V * V), 1.0 / 6.0);
+        const double rcut = s / alpha, kmax = 2.0 * s * alpha;
+        int nmax[3], mmax[3];
+        for (int d = 0; d < 3; ++d) {
+            nmax[d] = (int)std::ceil(rcut / (V / std::sqrt(dot(c[d], c[d]))));
+            mmax[d] = (int)std::ceil(kmax * std::sqrt(dot(a[d], a[d])) / (2 * M_PI));
+        }
+        std::vector<double> phi(N, 0.0);
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j)
+                for (int n0 = -nmax[0]; n0 <= nmax[0]; ++n0)
+                    for (int n1 = -nmax[1]; n1 <= nmax[1]; ++n1)
+                        for (int n2 = -nmax[2]; n2 <= nmax[2]; ++n2) {
+                            if (i == j && !n0 && !n1 && !n2) continue;
+                            double dr[3];
+                            for (int d = 0; d < 3; ++d)
+                                dr[d] = pos[3 * i + d] - pos[3 * j + d] + n0 * a[0][d] + n1 * a[1][d] + n2 * a[2][d];
+                            const double r2 = dot(dr, dr);
+                            if (r2 > rcut * rcut) continue;
+                            const double r = std::sqrt(r2);
+                            phi[i] += q[j] * std::erfc(alpha * r) / r;
+                        }
+        double b[3][3];
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 3; ++e) b[d][e] = 2 * M_PI * c[d][e] / V;
+        for (int m3 = -mmax[2]; m3 <= mmax[2]; ++m3)
+            for (int m2 = -mmax[1]; m2 <= mmax[1]; ++m2)
+                for (int m1 = -mmax[0]; m1 <= mmax[0]; ++m1) {
+                    if (!m1 && !m2 && !m3) continue;
+                    double kv[3];
+                    for (int d = 0; d < 3; ++d) kv[d] = m1 * b[0][d] + m2 * b[1][d] + m3 * b[2][d];
+                    const double k2 = dot(kv, kv);
+                    if (k2 > kmax * kmax) continue;
+                    const double w = 4 * M_PI / V * std::exp(-k2 / (4 * alpha * alpha)) / k2;
+                    std::complex<double> S(0);
+                    for (int j = 0; j < N; ++j) S += q[j] * std::polar(1.0, -dot(kv, pos + 3 * j));
+                    for (int i = 0; i < N; ++i) phi[i] += w * (S * std::polar(1.0, dot(kv, pos + 3 * i))).real();
+                }
+        double E = 0, Q = 0;
+        for (int i = 0; i < N; ++i) {
+            phi[i] -= 2.0 * alpha / std::sqrt(M_PI) * q[i];
+            pot[i] = phi[i];
+            E += q[i] * phi[i];
+            Q += q[i];
+        }
+        if (energy) *energy = 0.5 * E - M_PI * Q * Q / (2 * V * alpha * alpha);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_ewald_nufft", e);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cubic cover: frame from the two longest lattice vectors, cube side from the
+// rotated bounding box's shortest width split into nz layers.
+// ---------------------------------------------------------------------------
+int pdmk_optimize_cubic_cover(const double* cell, int nz, int* m_out, int* n_out, int* p_out, double* e1_out,
+                              double* e2_out, double* e3_out, double* s_out, double* cost_out) {
+    try {
+        if (nz <= 0) return 1;
+        if (!cell || !m_out || !n_out || !p_out || !e1_out || !e2_out || !e3_out || !s_out || !cost_out)
+            throw std::invalid_argument("null buffer");
+        const double* a[3] = {cell, cell + 3, cell + 6};
+        auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+        double nrm[3];
+        for (int d = 0; d < 3; ++d) nrm[d] = std::sqrt(dot(a[d], a[d]));
+        int idx[3] = {0, 1, 2};
+        if (nrm[idx[0]] < nrm[idx[1]]) std::swap(idx[0], idx[1]);
+        if (nrm[idx[1]] < nrm[idx[2]]) std::swap(idx[1], idx[2]);
+        if (nrm[idx[0]] < nrm[idx[1]]) std::swap(idx[0], idx[1]);
+        const double* b1 = a[idx[0]];
+        const double* b2 = a[idx[1]];
+        if (!(nrm[idx[0]] > 0)) throw std::invalid_argument("degenerate lattice (zero-norm vector)");
+        double e1[3], e2[3], e3[3];
+        for (int d = 0; d < 3; ++d) e1[d] = b1[d] / nrm[idx[0]];
+        const double p12 = dot(b2, e1);
+        double v2[3];
+        for (int d = 0; d < 3; ++d) v2[d] = b2[d] - p12 * e1[d];
+        const double nv2 = std::sqrt(dot(v2, v2));
+        if (!(nv2 > 0)) throw std::invalid_argument("degenerate lattice (parallel vectors)");
+        for (int d = 0; d < 3; ++d) e2[d] = v2[d] / nv2;
+        e3[0] = e1[1] * e2[2] - e1[2] * e2[1];
+        e3[1] = e1[2] * e2[0] - e1[0] * e2[2];
+        e3[2] = e1[0] * e2[1] - e1[1] * e2[0];
+        double W[3] = {0, 0, 0};
+        for (int d = 0; d < 3; ++d) {
+            W[0] += std::fabs(dot(a[d], e1));
+            W[1] += std::fabs(dot(a[d], e2));
+            W[2] += std::fabs(dot(a[d], e3));
+        }
+        const double s = W[2] / nz;
+        const int m = std::max(1, (int)std::ceil(W[0] / s)), n = std::max(1, (int)std::ceil(W[1] / s));
+        double c[3] = {a[1][1] * a[2][2] - a[1][2] * a[2][1], a[1][2] * a[2][0] - a[1][0] * a[2][2],
+                       a[1][0] * a[2][1] - a[1][1] * a[2][0]};
+        const double V = std::fabs(dot(a[0], c));
+        *m_out = m;
+        *n_out = n;
+        *p_out = nz;
+        for (int d = 0; d < 3; ++d) {
+            e1_out[d] = e1[d];
+            e2_out[d] = e2[d];
+            e3_out[d] = e3[d];
+        }
+        *s_out = s;
+        *cost_out = (double)((m + 2) * (n + 2) * (nz + 2)) * s * s * s / V;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_optimize_cubic_cover", e);
+    }
+}
+
+}  // extern "C"

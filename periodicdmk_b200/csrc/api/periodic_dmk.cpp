@@ -1,0 +1,81 @@
+// PeriodicDMKTreeT<Real, 3>: host construction + GPU evaluate.
+//
+// Construction follows the reference's Impl constructor
+// (cpp/src/periodic_dmk.cpp:41-139): parameters from n_digits, lattice QR,
+// rc = min diag(umat) / nz, rotation of the positions into the umat frame,
+// lattice images, tree.  All of that is the host plan builder; the resulting
+// plan is uploaded once.  evaluate (cpp/src/periodic_dmk.cpp:141-186) runs
+// entirely on the GPU.
+#include "pdmk/periodic_dmk.hpp"
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "../device/device_tree.hpp"
+#include "../host/plan.hpp"
+#include "impl.hpp"
+
+namespace pdmk {
+
+template <typename Real, int DIM>
+PeriodicDMKTreeT<Real, DIM>::PeriodicDMKTreeT(const MatND<DIM>& cell, const std::vector<VecND<DIM>>& positions,
+                                              int n_digits, int n_per_leaf, int nz,
+                                              std::optional<std::array<double, DIM>> bloch) {
+    if (bloch.has_value())
+        throw std::logic_error("PeriodicDMKTreeT: quasi-periodic (bloch) evaluation is not provided by this build");
+    p_ = std::make_unique<Impl>();
+    double c[9];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) c[j * 3 + i] = cell[j][i];
+    std::vector<double> pos(3 * positions.size());
+    for (size_t i = 0; i < positions.size(); ++i)
+        for (int d = 0; d < 3; ++d) pos[3 * i + d] = positions[i][d];
+    p_->plan = std::make_unique<pdmkb::Plan>(
+        pdmkb::build_plan(c, (int)positions.size(), pos.data(), n_digits, n_per_leaf, nz));
+    p_->dev = std::make_unique<pdmkb::DeviceTree>(*p_->plan);
+    p_->single = std::is_same<Real, float>::value;
+    n_src_ = p_->plan->n_src;
+    rc_ = p_->plan->rc;
+}
+
+template <typename Real, int DIM>
+PeriodicDMKTreeT<Real, DIM>::~PeriodicDMKTreeT() = default;
+
+template <typename Real, int DIM>
+std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate(const std::vector<double>& charges) {
+    EvalTiming t;
+    return evaluate_timed(charges, t);
+}
+
+template <typename Real, int DIM>
+std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_timed(const std::vector<double>& charges, EvalTiming& timing) {
+    if ((int)charges.size() != n_src_) throw std::invalid_argument("charges size != n_src");
+    std::vector<double> pot(n_src_);
+    pdmkb::StageTimes st;
+    p_->dev->evaluate_host(charges.data(), pot.data(), &st);
+    timing.dmk_ms = st.dmk_ms;
+    timing.direct_ms = st.direct_ms;
+    timing.nufft_ms = st.nufft_ms;
+    timing.build_ms = 0.0;
+    return std::vector<Real>(pot.begin(), pot.end());
+}
+
+template <typename Real, int DIM>
+std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_multi(const std::vector<double>& charges, int k) {
+    if (k <= 0 || (int64_t)charges.size() != (int64_t)n_src_ * k)
+        throw std::invalid_argument("charges size != n_src * k");
+    std::vector<Real> out((size_t)n_src_ * k);
+    std::vector<double> pot(n_src_);
+    for (int c = 0; c < k; ++c) {
+        p_->dev->evaluate_host(charges.data() + (size_t)n_src_ * c, pot.data(), nullptr);
+        for (int i = 0; i < n_src_; ++i) out[(size_t)n_src_ * c + i] = (Real)pot[i];
+    }
+    return out;
+}
+
+template class PeriodicDMKTreeT<double, 3>;
+template class PeriodicDMKTreeT<float, 3>;
+
+}  // namespace pdmk

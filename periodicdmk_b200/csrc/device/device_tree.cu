@@ -1,0 +1,752 @@
+// DeviceTree: one-time upload of a host Plan and the evaluate pipeline.
+//
+// Device memory layout (all resident for the lifetime of the tree):
+//   src          double4[n_all]  sorted sources (x, y, z, q); q refreshed per evaluate
+//   trg          double4[N]      sorted targets (x, y, z, w0 of the target's leaf)
+//   proxy_up     double[n_up * p^3]   upward Chebyshev proxy charges, (p,p,p) x fastest
+//   proxy_down   double[n_down * p^3] downward proxy potentials
+//   pw_out       complex[n_pw * n*n*n2] outgoing plane-wave expansions
+//   tables       per level: poly2pw (n x p), poly2pw_half (n2 x p), pw2poly^T (p x n),
+//                weighted pw2poly^T (p x n2), 27 fused shift stencils; c2p / p2c (8 x 3 x p x p)
+//   far field    real fine grid n1*n2*n3, half spectrum n1*n2*(n3/2+1), multiplier
+// Every index list is built and bounds-checked here, on the host.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+
+#include "../host/pswf.hpp"
+#include "device_tree.hpp"
+
+namespace pdmkb {
+
+using dev::cd;
+
+namespace {
+
+void check(bool ok, const char* what) {
+    if (!ok) throw std::runtime_error(std::string("DeviceTree: inconsistent plan: ") + what);
+}
+
+int nice_fft_size(int n) {
+    for (int m = std::max(2, n);; ++m) {
+        if (m % 2) continue;
+        int r = m;
+        for (int f : {2, 3, 5, 7})
+            while (r % f == 0) r /= f;
+        if (r == 1) return m;
+    }
+}
+
+#define CUFFT_CHECK(expr)                                                                      \
+    do {                                                                                       \
+        cufftResult _r = (expr);                                                               \
+        if (_r != CUFFT_SUCCESS)                                                               \
+            throw std::runtime_error("cuFFT error " + std::to_string((int)_r) + " at " #expr); \
+    } while (0)
+
+}  // namespace
+
+template <typename T>
+T* DeviceTree::alloc(size_t n) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    PDMK_CUDA_CHECK(cudaMalloc(&p, bytes));
+    allocs_.push_back(p);
+    bytes_ += bytes;
+    return static_cast<T*>(p);
+}
+
+template <typename T>
+T* DeviceTree::upload(const std::vector<T>& v) {
+    T* p = alloc<T>(v.size());
+    if (!v.empty()) PDMK_CUDA_CHECK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return p;
+}
+
+DeviceTree::DeviceTree(const Plan& P, int device) {
+    try {
+        init(P, device);
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+void DeviceTree::init(const Plan& P, int device) {
+    if (device < 0) PDMK_CUDA_CHECK(cudaGetDevice(&device));
+    device_ = device;
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (auto& e : ev_) PDMK_CUDA_CHECK(cudaEventCreate(&e));
+
+    n_ = P.n_src;
+    n_all_ = P.n_all;
+    p_ = P.p;
+    npw_ = P.n_pw;
+    npw2_ = P.n_pw2;
+    M_ = P.n_modes;
+    const int p = p_, n = npw_, n2 = npw2_, M = M_;
+    const int64_t ncoef = (int64_t)p * p * p;
+
+    // ------------------------------------------------------------------ far-field bins
+    // NUFFT bins are contiguous ranges of sorted targets inside one leaf.  A leaf
+    // whose subgrid would be wider than kMaxEx cells is split by grid blocks,
+    // which permutes targets only inside that leaf (every stage is invariant
+    // to the order of points within a leaf).
+    const double eps = P.dp.eps;
+    int W = (int)std::ceil(-std::log10(eps / 4.0)) + 1;
+    W = std::min(14, std::max(4, W));
+    const int ng[3] = {nice_fft_size(std::max(2 * P.ms, 2 * W)), nice_fft_size(std::max(2 * P.mt, 2 * W)),
+                       nice_fft_size(std::max(2 * P.mu, 2 * W))};
+    constexpr int kMaxEx = 48;
+    std::vector<double> trg_sorted = P.trg_sorted;
+    std::vector<int> trg_perm = P.trg_perm;
+    std::vector<double> trg_selfw(n_, 0.0);
+    std::vector<double4> pt_t(n_);
+    std::vector<int4> pt_l0(n_);
+    struct Bin {
+        int start, count;
+        int4 org, ext;
+    };
+    std::vector<Bin> bins;
+    {
+        const double* v = P.umatinv;
+        auto frac_t = [&](const double* r, double* t) {
+            const double s[3] = {v[0] * r[0] + v[3] * r[1] + v[6] * r[2], v[4] * r[1] + v[7] * r[2], v[8] * r[2]};
+            for (int d = 0; d < 3; ++d) t[d] = (s[d] - std::floor(s[d])) * ng[d];
+        };
+        for (int b = 0; b < P.nboxes; ++b) {
+            if (!P.is_leaf[b] || P.trg_count[b] == 0) continue;
+            const int t0 = P.trg_start[b], nt = P.trg_count[b];
+            check(t0 >= 0 && t0 + nt <= n_, "target range");
+            const double w0 = P.w0[P.depth[b] + P.ifpwexp[b]];
+            std::vector<std::array<double, 3>> tt(nt);
+            for (int i = 0; i < nt; ++i) frac_t(&trg_sorted[3 * (size_t)(t0 + i)], tt[i].data());
+            // unwrap each axis so the leaf's points are contiguous in grid space
+            for (int d = 0; d < 3; ++d) {
+                double lo = 1e300, hi = -1e300;
+                for (auto& x : tt) lo = std::min(lo, x[d]), hi = std::max(hi, x[d]);
+                if (hi - lo > 0.5 * ng[d])
+                    for (auto& x : tt)
+                        if (x[d] > 0.5 * ng[d]) x[d] -= ng[d];
+            }
+            std::vector<std::array<int, 3>> l0(nt);
+            int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+            for (int i = 0; i < nt; ++i)
+                for (int d = 0; d < 3; ++d) {
+                    l0[i][d] = (int)std::ceil(tt[i][d] - 0.5 * W);
+                    lo[d] = std::min(lo[d], l0[i][d]);
+                    hi[d] = std::max(hi[d], l0[i][d]);
+                }
+            std::vector<int> order(nt);
+            std::iota(order.begin(), order.end(), 0);
+            std::vector<int64_t> key(nt, 0);
+            const bool split = (hi[0] - lo[0] + W > kMaxEx) || (hi[1] - lo[1] + W > kMaxEx) || (hi[2] - lo[2] + W > kMaxEx);
+            if (split) {
+                const int B = kMaxEx - W;
+                for (int i = 0; i < nt; ++i) {
+                    int64_t kx = (l0[i][0] - lo[0]) / B, ky = (l0[i][1] - lo[1]) / B, kz = (l0[i][2] - lo[2]) / B;
+                    key[i] = (kx * 4096 + ky) * 4096 + kz;
+                }
+                std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
+            }
+            // apply the within-leaf permutation
+            std::vector<double> pos_tmp(3 * (size_t)nt);
+            std::vector<int> perm_tmp(nt);
+            for (int i = 0; i < nt; ++i) {
+                const int o = order[i];
+                for (int d = 0; d < 3; ++d) pos_tmp[3 * i + d] = P.trg_sorted[3 * (size_t)(t0 + o) + d];
+                perm_tmp[i] = P.trg_perm[t0 + o];
+            }
+            for (int i = 0; i < nt; ++i) {
+                for (int d = 0; d < 3; ++d) trg_sorted[3 * (size_t)(t0 + i) + d] = pos_tmp[3 * i + d];
+                trg_perm[t0 + i] = perm_tmp[i];
+                trg_selfw[t0 + i] = w0;
+                const int o = order[i];
+                pt_t[t0 + i] = make_double4(tt[o][0], tt[o][1], tt[o][2], 0.0);
+                pt_l0[t0 + i] = make_int4(l0[o][0], l0[o][1], l0[o][2], 0);
+            }
+            for (int i = 0; i < nt;) {
+                int j = i;
+                while (j < nt && key[order[j]] == key[order[i]]) ++j;
+                Bin bn{t0 + i, j - i, make_int4(INT32_MAX, INT32_MAX, INT32_MAX, 0), make_int4(0, 0, 0, 0)};
+                int bhi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+                for (int k = i; k < j; ++k) {
+                    const int4 l = pt_l0[t0 + k];
+                    bn.org.x = std::min(bn.org.x, l.x);
+                    bn.org.y = std::min(bn.org.y, l.y);
+                    bn.org.z = std::min(bn.org.z, l.z);
+                    bhi[0] = std::max(bhi[0], l.x);
+                    bhi[1] = std::max(bhi[1], l.y);
+                    bhi[2] = std::max(bhi[2], l.z);
+                }
+                bn.ext = make_int4(bhi[0] - bn.org.x + W, bhi[1] - bn.org.y + W, bhi[2] - bn.org.z + W, 0);
+                check(bn.ext.x <= kMaxEx && bn.ext.y <= kMaxEx && bn.ext.z <= kMaxEx, "NUFFT bin extent");
+                bins.push_back(bn);
+                i = j;
+            }
+        }
+    }
+
+    // ------------------------------------------------------------------ points
+    {
+        std::vector<double4> src(n_all_);
+        for (int i = 0; i < n_all_; ++i)
+            src[i] = make_double4(P.src_sorted[3 * (size_t)i], P.src_sorted[3 * (size_t)i + 1],
+                                  P.src_sorted[3 * (size_t)i + 2], 0.0);
+        for (int i : P.src_charge_idx) check(i >= 0 && i < n_, "source charge index");
+        src_ = upload(src);
+        src_charge_idx_ = upload(P.src_charge_idx);
+        std::vector<double4> trg(n_);
+        for (int i = 0; i < n_; ++i)
+            trg[i] = make_double4(trg_sorted[3 * (size_t)i], trg_sorted[3 * (size_t)i + 1], trg_sorted[3 * (size_t)i + 2],
+                                  trg_selfw[i]);
+        for (int i : trg_perm) check(i >= 0 && i < n_, "target permutation");
+        trg_ = upload(trg);
+        trg_perm_ = upload(trg_perm);
+        pot_sorted_ = alloc<double>(n_);
+        far_sorted_ = alloc<double>(n_);
+        q_sorted_ = alloc<double>(n_);
+        q_dev_ = alloc<double>(n_);
+        pot_dev_ = alloc<double>(n_);
+    }
+
+    // ------------------------------------------------------------------ expansions
+    n_up_ = P.n_proxy_up;
+    n_down_ = P.n_proxy_down;
+    n_pw_ = P.n_pw_exp;
+    proxy_up_ = alloc<double>(n_up_ * ncoef);
+    proxy_down_ = alloc<double>(n_down_ * ncoef);
+    pw_out_ = alloc<cd>(n_pw_ * M);
+
+    // ------------------------------------------------------------------ tables
+    {
+        std::vector<double> c2p((size_t)8 * 3 * p * p);
+        for (int c = 0; c < 8; ++c)
+            for (int d = 0; d < 3; ++d)
+                for (int a = 0; a < p; ++a)
+                    for (int i = 0; i < p; ++i)
+                        c2p[((size_t)c * 3 + d) * p * p + a + (size_t)p * i] = P.p2c[((size_t)c * 3 + d) * p * p + i + (size_t)p * a];
+        c2p_ = upload(c2p);
+        p2c_ = upload(P.p2c);
+        lev_.resize(P.nlevels);
+        for (int l = 0; l < P.nlevels; ++l) {
+            const auto& T = P.lev[l];
+            std::vector<cd> a((size_t)n * p), h((size_t)n2 * p), bt((size_t)p * n), btw((size_t)p * n2);
+            for (int k = 0; k < n; ++k)
+                for (int m = 0; m < p; ++m) {
+                    const cplx v = T.poly2pw[k + (size_t)n * m];
+                    a[k + (size_t)n * m] = cd{v.real(), v.imag()};
+                    if (k < n2) h[k + (size_t)n2 * m] = cd{v.real(), v.imag()};
+                    const cplx u = T.pw2poly[k + (size_t)n * m];
+                    bt[m + (size_t)p * k] = cd{u.real(), u.imag()};
+                    if (k < n2) {
+                        const double w = k >= n / 2 ? 0.5 : 1.0;
+                        btw[m + (size_t)p * k] = cd{w * u.real(), w * u.imag()};
+                    }
+                }
+            lev_[l].poly2pw = upload(a);
+            lev_[l].poly2pw_half = upload(h);
+            lev_[l].pw2polyT = upload(bt);
+            lev_[l].pw2polyTw = upload(btw);
+            lev_[l].shift = upload(T.shift);
+        }
+    }
+
+    int64_t scratch_need = 0, pw_in_need = 0;
+
+    // ------------------------------------------------------------------ upward: proxy moments
+    {
+        std::vector<std::vector<int>> by_center(P.nboxes);
+        for (int w = 0; w < (int)P.c2proxy_work.size(); ++w) by_center[P.c2proxy_work[w].center_box].push_back(w);
+        std::vector<int> slot, rng{0}, s0, sc;
+        std::vector<double4> cs;
+        for (int b = 0; b < P.nboxes; ++b) {
+            if (by_center[b].empty()) continue;
+            check(P.proxy_up_off[b] >= 0, "proxy_up of work centre");
+            slot.push_back((int)(P.proxy_up_off[b] / ncoef));
+            const int lvl = P.c2proxy_work[by_center[b][0]].level;
+            cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / P.boxsize[lvl]));
+            for (int w : by_center[b]) {
+                const auto& W2 = P.c2proxy_work[w];
+                check(W2.level == lvl, "work level");
+                check(P.src_start[W2.src_box] >= 0 && P.src_start[W2.src_box] + P.src_count[W2.src_box] <= n_all_,
+                      "work source range");
+                s0.push_back(P.src_start[W2.src_box]);
+                sc.push_back(P.src_count[W2.src_box]);
+            }
+            rng.push_back((int)s0.size());
+        }
+        c2x_.src = src_;
+        c2x_.proxy_up = proxy_up_;
+        c2x_.n_centers = (int)slot.size();
+        c2x_.slot = upload(slot);
+        c2x_.center_scale = upload(cs);
+        c2x_.rng_start = upload(rng);
+        c2x_.src_start = upload(s0);
+        c2x_.src_count = upload(sc);
+        launches_ += 1;
+    }
+    // ------------------------------------------------------------------ upward: c2p groups
+    for (int l = P.nlevels - 1; l >= 0; --l) {
+        for (int c = 0; c < 8; ++c) {
+            std::vector<int64_t> in, out;
+            for (int b : P.level_boxes[l]) {
+                if (!P.has_proxy_from_children[b]) continue;
+                const int ch = P.children[b][c];
+                if (ch < 0 || !(P.src_count[ch] > 0 && P.ifpwexp[ch])) continue;
+                check(P.proxy_up_off[ch] >= 0 && P.proxy_up_off[b] >= 0, "c2p offsets");
+                in.push_back(P.proxy_up_off[ch]);
+                out.push_back(P.proxy_up_off[b]);
+            }
+            if (in.empty()) continue;
+            C2PGroup g;
+            g.n = (int)in.size();
+            g.in_off = upload(in);
+            g.out_off = upload(out);
+            g.child = c;
+            c2p_groups_.push_back(g);
+            scratch_need = std::max<int64_t>(scratch_need, (int64_t)g.n * ncoef);
+            launches_ += 3;
+        }
+    }
+    // ------------------------------------------------------------------ outgoing plane waves
+    for (int l = 0; l < P.nlevels; ++l) {
+        std::vector<int64_t> in, out;
+        for (int b : P.level_boxes[l]) {
+            if (P.pw_off[b] < 0) continue;
+            check(P.proxy_up_off[b] >= 0, "pw box without proxy");
+            in.push_back(P.proxy_up_off[b]);
+            out.push_back(P.pw_off[b]);
+        }
+        if (in.empty()) continue;
+        PwGroup g;
+        g.level = l;
+        g.n = (int)in.size();
+        g.in_off = upload(in);
+        g.out_off = upload(out);
+        pw_groups_.push_back(g);
+        scratch_need = std::max<int64_t>(scratch_need, (int64_t)g.n * std::max<int64_t>((int64_t)p * p * n, (int64_t)p * n * n));
+        launches_ += 3;
+    }
+    // ------------------------------------------------------------------ downward per level
+    for (int l = 0; l < P.nlevels; ++l) {
+        const double bs = P.boxsize[l];
+        std::vector<int> ts{0}, tslot, tst;
+        std::vector<int64_t> down, pin, pout, pmat;
+        for (int b : P.level_boxes[l]) {
+            if (!(P.ifpwexp[b] && P.src_count[b] + P.trg_count[b] > 0 && P.trg_count[b] > 0)) continue;
+            check(P.pw_off[b] >= 0 && P.proxy_down_off[b] >= 0, "form-eval box storage");
+            tslot.push_back((int)(P.pw_off[b] / M));
+            tst.push_back(13);
+            for (int ind = 0; ind < 27; ++ind) {
+                const int nb = P.colleagues[b][ind];
+                if (nb < 0 || nb == b) continue;
+                if (P.is_leaf[b] && P.is_leaf[nb]) continue;
+                if (P.pw_off[nb] < 0) continue;
+                int st = 0, stride = 1;
+                for (int d = 0; d < 3; ++d) {
+                    const int kd = (int)std::lround((P.centers[3 * b + d] - P.centers[3 * nb + d]) / bs) + 1;
+                    check(kd >= 0 && kd <= 2, "shift stencil");
+                    st += kd * stride;
+                    stride *= 3;
+                }
+                tslot.push_back((int)(P.pw_off[nb] / M));
+                tst.push_back(st);
+            }
+            ts.push_back((int)tslot.size());
+            down.push_back(P.proxy_down_off[b]);
+            if (!P.iftensprodeval[b]) {
+                for (int c = 0; c < 8; ++c) {
+                    const int ch = P.children[b][c];
+                    if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch])) continue;
+                    check(P.proxy_down_off[ch] >= 0, "p2c child storage");
+                    pin.push_back(P.proxy_down_off[b]);
+                    pout.push_back(P.proxy_down_off[ch]);
+                    pmat.push_back((int64_t)c * 3 * p * p);
+                }
+            }
+        }
+        if (down.empty()) continue;
+        EvalLevel E;
+        E.level = l;
+        E.n = (int)down.size();
+        E.term_start = upload(ts);
+        E.term_slot = upload(tslot);
+        E.term_stencil = upload(tst);
+        E.down_off = upload(down);
+        E.n_p2c = (int)pin.size();
+        if (E.n_p2c) {
+            E.p2c_in = upload(pin);
+            E.p2c_out = upload(pout);
+            E.p2c_mat = upload(pmat);
+        }
+        eval_levels_.push_back(E);
+        pw_in_need = std::max<int64_t>(pw_in_need, (int64_t)E.n * M);
+        scratch_need = std::max<int64_t>(scratch_need, (int64_t)E.n * std::max<int64_t>((int64_t)n * n2 * p, (int64_t)n2 * p * p));
+        scratch_need = std::max<int64_t>(scratch_need, (int64_t)E.n_p2c * ncoef);
+        launches_ += 4 + (E.n_p2c ? 3 : 0);
+    }
+    // ------------------------------------------------------------------ leaf evaluation
+    {
+        std::vector<int> slot, t0, tc;
+        std::vector<double4> cs;
+        for (int b = 0; b < P.nboxes; ++b) {
+            if (!P.iftensprodeval[b] || P.trg_count[b] == 0) continue;
+            check(P.proxy_down_off[b] >= 0, "leaf proxy_down");
+            slot.push_back((int)(P.proxy_down_off[b] / ncoef));
+            t0.push_back(P.trg_start[b]);
+            tc.push_back(P.trg_count[b]);
+            cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / P.boxsize[P.depth[b]]));
+        }
+        eval_.trg = trg_;
+        eval_.proxy_down = proxy_down_;
+        eval_.pot = pot_sorted_;
+        eval_.n_leaves = (int)slot.size();
+        eval_.slot = upload(slot);
+        eval_.trg_start = upload(t0);
+        eval_.trg_count = upload(tc);
+        eval_.center_scale = upload(cs);
+        launches_ += 1;
+    }
+    // ------------------------------------------------------------------ near field
+    {
+        // Contact-geometry cull of the reference (cpp/include/dmk/tree.hpp:111-220,
+        // applied at cpp/src/dmk/pbc_tree.cpp:1528-1563), used here only to count
+        // the pairs the reference evaluates: a point is kept if its squared
+        // distance to the shared face/edge/corner of the two boxes is < b^2.
+        int filter_min = 64;
+        if (const char* fs = std::getenv("DMK_FILTER_NTRG_MIN")) filter_min = std::atoi(fs);
+        auto count_in_range = [&](int sb, int tb, double d2max, bool sources) {
+            const double sa = P.boxsize[P.depth[sb]], sbb = P.boxsize[P.depth[tb]];
+            int tdim[3], nt = 0, odim[3], no = 0;
+            double tco[3], olo[3], ohi[3];
+            for (int d = 0; d < 3; ++d) {
+                const double a = P.centers[3 * sb + d] - sa / 2, b = P.centers[3 * tb + d] - sbb / 2;
+                if (a + sa == b) {
+                    tdim[nt] = d; tco[nt++] = b;
+                } else if (b + sbb == a) {
+                    tdim[nt] = d; tco[nt++] = a;
+                } else {
+                    odim[no] = d; olo[no] = std::max(a, b); ohi[no++] = std::min(a + sa, b + sbb);
+                }
+            }
+            const double* pts = sources ? P.src_sorted.data() : P.trg_sorted.data();
+            const int s0 = sources ? P.src_start[sb] : P.trg_start[tb];
+            const int cnt = sources ? P.src_count[sb] : P.trg_count[tb];
+            int64_t kept = 0;
+            for (int i = s0; i < s0 + cnt; ++i) {
+                const double* x = pts + 3 * (size_t)i;
+                double d2 = 0;
+                for (int k = 0; k < nt; ++k) d2 += (x[tdim[k]] - tco[k]) * (x[tdim[k]] - tco[k]);
+                for (int k = 0; k < no; ++k) {
+                    const double c = std::min(std::max(x[odim[k]], olo[k]), ohi[k]);
+                    d2 += (x[odim[k]] - c) * (x[odim[k]] - c);
+                }
+                if (d2 < d2max) kept++;
+            }
+            return kept;
+        };
+        std::vector<int> t0, tc, ps{0}, s0, sc;
+        std::vector<double> bsz;
+        for (int tb : P.direct_work) {
+            if (P.trg_count[tb] == 0) continue;
+            t0.push_back(P.trg_start[tb]);
+            tc.push_back(P.trg_count[tb]);
+            const int tl = P.depth[tb];
+            for (int li = P.list1_start[tb]; li < P.list1_start[tb + 1]; ++li) {
+                const int sb = P.list1[li];
+                const int sl = P.depth[sb];
+                double b = P.boxsize[sl];
+                if (P.ifpwexp[sb] && sb == tb)
+                    b /= 2.0;
+                else if (sl < tl)
+                    b = P.boxsize[tl];
+                check(P.src_start[sb] >= 0 && P.src_start[sb] + P.src_count[sb] <= n_all_, "near source range");
+                {
+                    const bool src_larger = sl < tl, trg_larger = sl > tl;
+                    const bool filter_same = !src_larger && !trg_larger && filter_min >= 0 && P.trg_count[tb] >= filter_min;
+                    const int64_t ns = (src_larger || filter_same) ? count_in_range(sb, tb, b * b, true) : P.src_count[sb];
+                    const int64_t ntg = trg_larger ? count_in_range(sb, tb, b * b, false) : P.trg_count[tb];
+                    near_pairs_culled_ += ns * ntg;
+                    near_pairs_nominal_ += (int64_t)P.src_count[sb] * P.trg_count[tb];
+                }
+                s0.push_back(P.src_start[sb]);
+                sc.push_back(P.src_count[sb]);
+                bsz.push_back(b);
+            }
+            ps.push_back((int)s0.size());
+        }
+        near_.trg = trg_;
+        near_.src = src_;
+        near_.pot = pot_sorted_;
+        near_.n_leaves = (int)t0.size();
+        near_.trg_start = upload(t0);
+        near_.trg_count = upload(tc);
+        near_.pair_start = upload(ps);
+        near_.pair_src_start = upload(s0);
+        near_.pair_src_count = upload(sc);
+        near_.pair_bsize = upload(bsz);
+        check(P.resid.size() <= 32, "residual polynomial length");
+        near_.nc = (int)P.resid.size();
+        for (int i = 0; i < near_.nc; ++i) near_.coef[i] = P.resid[i];
+        launches_ += 1;
+    }
+
+    // ------------------------------------------------------------------ scratch
+    scratch_elems_ = std::max<int64_t>(scratch_need, 1);
+    pw_in_elems_ = std::max<int64_t>(pw_in_need, 1);
+    scratch1_ = alloc<cd>(scratch_elems_);
+    scratch2_ = alloc<cd>(scratch_elems_);
+    pw_in_ = alloc<cd>(pw_in_elems_);
+
+    // ------------------------------------------------------------------ far field
+    {
+        n_grid_ = (int64_t)ng[0] * ng[1] * ng[2];
+        n_spec_ = (int64_t)ng[0] * ng[1] * (ng[2] / 2 + 1);
+        grid_ = alloc<double>(n_grid_);
+        spec_ = alloc<cd>(n_spec_);
+        // multiplier: 1/2 (in K(k) + in K(-k)) w(k) H^2 / Psi(k)^2
+        const double es_beta = 2.30 * W;
+        std::vector<double> gx(200), gw(200);
+        gauss_legendre(200, gx.data(), gw.data());
+        auto phihat = [&](int d, int k) {
+            const double h = 2.0 * M_PI / ng[d], alpha = 0.5 * W * h;
+            double s = 0;
+            for (int i = 0; i < 200; ++i) {
+                const double z = gx[i];
+                s += gw[i] * std::exp(es_beta * (std::sqrt(1.0 - z * z) - 1.0)) * std::cos(k * alpha * z);
+            }
+            return alpha * s;
+        };
+        std::vector<double> ph[3];
+        for (int d = 0; d < 3; ++d) {
+            ph[d].resize(ng[d]);
+            for (int i = 0; i < ng[d]; ++i) ph[d][i] = phihat(d, i <= ng[d] / 2 ? i : i - ng[d]);
+        }
+        const double H = std::pow(2.0 * M_PI, 3) / ((double)ng[0] * ng[1] * ng[2]);
+        const double* u = P.umat;
+        const double a11 = 1.0 / u[0], a21 = -u[3] / (u[0] * u[4]), a22 = 1.0 / u[4];
+        const double a31 = (u[3] * u[7] - u[6] * u[4]) / (u[0] * u[4] * u[8]);
+        const double a32 = -u[7] / (u[4] * u[8]), a33 = 1.0 / u[8];
+        Pswf0 pf(P.dp.beta);
+        const double psi0 = pf(0.0), twopi = 2.0 * M_PI;
+        const double dfac = 4.0 * M_PI / (psi0 * P.volume);
+        auto inK = [&](int k1, int k2, int k3) {
+            return k1 >= -P.ms / 2 && k1 <= (P.ms - 1) / 2 && k2 >= -P.mt / 2 && k2 <= (P.mt - 1) / 2 && k3 >= -P.mu / 2 &&
+                   k3 <= (P.mu - 1) / 2;
+        };
+        std::vector<double> mult(n_spec_, 0.0);
+        const int n3h = ng[2] / 2 + 1;
+        for (int i1 = 0; i1 < ng[0]; ++i1)
+            for (int i2 = 0; i2 < ng[1]; ++i2)
+                for (int i3 = 0; i3 < n3h; ++i3) {
+                    const int k1 = i1 <= ng[0] / 2 ? i1 : i1 - ng[0];
+                    const int k2 = i2 <= ng[1] / 2 ? i2 : i2 - ng[1];
+                    const int k3 = i3;
+                    const double frac = 0.5 * ((inK(k1, k2, k3) ? 1 : 0) + (inK(-k1, -k2, -k3) ? 1 : 0));
+                    if (frac == 0) continue;
+                    const double d1 = twopi * (a11 * k1);
+                    const double d2 = twopi * (a21 * k1 + a22 * k2);
+                    const double d3 = twopi * (a31 * k1 + a32 * k2 + a33 * k3);
+                    const double kk = d1 * d1 + d2 * d2 + d3 * d3;
+                    if (kk < 1e-30) continue;
+                    const double xval = std::sqrt(kk) * P.rc / P.dp.beta;
+                    if (xval > 1.0) continue;
+                    const double w = dfac * pf(xval) / kk;
+                    const double Ps = ph[0][i1] * ph[1][i2] * ph[2][i3];
+                    mult[((size_t)i1 * ng[1] + i2) * n3h + i3] = frac * w * H * H / (Ps * Ps);
+                }
+        mult_ = upload(mult);
+        CUFFT_CHECK(cufftPlan3d(&plan_fwd_, ng[0], ng[1], ng[2], CUFFT_D2Z));
+        CUFFT_CHECK(cufftPlan3d(&plan_inv_, ng[0], ng[1], ng[2], CUFFT_Z2D));
+        CUFFT_CHECK(cufftSetStream(plan_fwd_, stream_));
+        CUFFT_CHECK(cufftSetStream(plan_inv_, stream_));
+
+        std::vector<int> bs, bc;
+        std::vector<int4> bo, be;
+        for (auto& bn : bins) {
+            bs.push_back(bn.start);
+            bc.push_back(bn.count);
+            bo.push_back(bn.org);
+            be.push_back(bn.ext);
+            nufft_max_jk_ = std::max(nufft_max_jk_, bn.ext.y * bn.ext.z);
+            nufft_max_ex_ = std::max(nufft_max_ex_, bn.ext.x);
+        }
+        nufft_.n_leaves = (int)bins.size();
+        nufft_.trg_start = upload(bs);
+        nufft_.trg_count = upload(bc);
+        nufft_.sub_origin = upload(bo);
+        nufft_.sub_extent = upload(be);
+        nufft_.pt_t = upload(pt_t);
+        nufft_.pt_l0 = upload(pt_l0);
+        nufft_.q_sorted = q_sorted_;
+        nufft_.grid = grid_;
+        nufft_.far = far_sorted_;
+        nufft_.n1 = ng[0];
+        nufft_.n2 = ng[1];
+        nufft_.n3 = ng[2];
+        nufft_.w = W;
+        nufft_.es_beta = es_beta;
+        launches_ += 4;  // gather_q, spread, multiply, interp (the two cuFFT transforms are library kernels)
+    }
+    launches_ += 2;  // charge gather, final gather
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+DeviceTree::~DeviceTree() { release(); }
+
+void DeviceTree::release() {
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (plan_fwd_) cufftDestroy(plan_fwd_);
+    if (plan_inv_) cufftDestroy(plan_inv_);
+    for (void* p : allocs_) cudaFree(p);
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+    allocs_.clear();
+    plan_fwd_ = plan_inv_ = 0;
+    stream_ = nullptr;
+    for (auto& e : ev_) e = nullptr;
+}
+
+void DeviceTree::run(const double* q, double* pot) {
+    const int p = p_, n = npw_, n2 = npw2_, M = M_;
+    const int64_t ncoef = (int64_t)p * p * p;
+    cudaStream_t s = stream_;
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(pot_sorted_, 0, sizeof(double) * n_, s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(proxy_up_, 0, sizeof(double) * std::max<int64_t>(n_up_ * ncoef, 1), s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(proxy_down_, 0, sizeof(double) * std::max<int64_t>(n_down_ * ncoef, 1), s));
+    dev::launch_gather(src_, src_charge_idx_, q, n_all_, s);
+    // upward
+    dev::launch_c2proxy(c2x_, p, s);
+    for (const auto& g : c2p_groups_) {
+        const double* mx = c2p_ + (int64_t)g.child * 3 * p * p;
+        dev::ContractArgs a{};
+        a.n_entries = g.n;
+        // x: in (i,j,k) -> s1 (j,k,a)
+        a.in = proxy_up_; a.in_off = g.in_off; a.out = scratch1_; a.out_stride = ncoef;
+        a.mat = mx; a.ni = p; a.na = p; a.R = p * p; a.mode = dev::kStore;
+        dev::launch_contract(a, dev::kRRR, s);
+        // y: s1 -> s2 (k,a,b)
+        a.in = scratch1_; a.in_off = nullptr; a.in_stride = ncoef; a.out = scratch2_;
+        a.mat = mx + p * p;
+        dev::launch_contract(a, dev::kRRR, s);
+        // z: s2 -> parent (a,b,c), accumulated
+        a.in = scratch2_; a.out = proxy_up_; a.out_off = g.out_off; a.mat = mx + 2 * p * p; a.mode = dev::kAdd;
+        dev::launch_contract(a, dev::kRRR, s);
+    }
+    // outgoing plane waves
+    for (const auto& g : pw_groups_) {
+        const auto& L = lev_[g.level];
+        dev::ContractArgs a{};
+        a.n_entries = g.n;
+        a.in = proxy_up_; a.in_off = g.in_off; a.out = scratch1_; a.out_stride = (int64_t)p * p * n;
+        a.mat = L.poly2pw; a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore;
+        dev::launch_contract(a, dev::kRCC, s);
+        a.in = scratch1_; a.in_off = nullptr; a.in_stride = (int64_t)p * p * n; a.out = scratch2_;
+        a.out_stride = (int64_t)p * n * n; a.R = p * n;
+        dev::launch_contract(a, dev::kCCC, s);
+        a.in = scratch2_; a.in_stride = (int64_t)p * n * n; a.out = pw_out_; a.out_off = g.out_off;
+        a.mat = L.poly2pw_half; a.na = n2; a.R = n * n;
+        dev::launch_contract(a, dev::kCCC, s);
+    }
+    // downward: per level shift -> pw2proxy -> p2c
+    for (const auto& E : eval_levels_) {
+        const auto& L = lev_[E.level];
+        dev::ShiftArgs sa{pw_out_, L.shift, pw_in_, M, E.n, E.term_start, E.term_slot, E.term_stencil};
+        dev::launch_shift(sa, s);
+        dev::ContractArgs a{};
+        a.n_entries = E.n;
+        a.in = pw_in_; a.in_stride = M; a.out = scratch1_; a.out_stride = (int64_t)n * n2 * p;
+        a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
+        dev::launch_contract(a, dev::kCCC, s);
+        a.in = scratch1_; a.in_stride = (int64_t)n * n2 * p; a.out = scratch2_; a.out_stride = (int64_t)n2 * p * p;
+        a.R = n2 * p;
+        dev::launch_contract(a, dev::kCCC, s);
+        a.in = scratch2_; a.in_stride = (int64_t)n2 * p * p; a.out = proxy_down_; a.out_off = E.down_off;
+        a.mat = L.pw2polyTw; a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
+        dev::launch_contract(a, dev::kCCR, s);
+        if (E.n_p2c) {
+            dev::ContractArgs b{};
+            b.n_entries = E.n_p2c;
+            b.in = proxy_down_; b.in_off = E.p2c_in; b.out = scratch1_; b.out_stride = ncoef;
+            b.mat = p2c_; b.mat_off = E.p2c_mat; b.ni = p; b.na = p; b.R = p * p; b.mode = dev::kStore;
+            dev::launch_contract(b, dev::kRRR, s);
+            b.in = scratch1_; b.in_off = nullptr; b.in_stride = ncoef; b.out = scratch2_;
+            b.mat = p2c_ + p * p;
+            dev::launch_contract(b, dev::kRRR, s);
+            b.in = scratch2_; b.out = proxy_down_; b.out_off = E.p2c_out; b.mat = p2c_ + 2 * p * p; b.mode = dev::kAdd;
+            dev::launch_contract(b, dev::kRRR, s);
+        }
+    }
+    dev::launch_eval(eval_, p, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
+    dev::launch_near(near_, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[2], s));
+    // far field
+    dev::launch_nufft_gather_q(trg_perm_, q, q_sorted_, n_, s);
+    PDMK_CUDA_CHECK(cudaMemsetAsync(grid_, 0, sizeof(double) * n_grid_, s));
+    dev::launch_spread(nufft_, nufft_max_jk_, nufft_max_ex_, s);
+    CUFFT_CHECK(cufftExecD2Z(plan_fwd_, grid_, reinterpret_cast<cufftDoubleComplex*>(spec_)));
+    dev::launch_multiply(spec_, mult_, n_spec_, s);
+    CUFFT_CHECK(cufftExecZ2D(plan_inv_, reinterpret_cast<cufftDoubleComplex*>(spec_), grid_));
+    dev::launch_interp(nufft_, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
+    dev::launch_finalize(pot_sorted_, far_sorted_, trg_, trg_perm_, q, pot, n_, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[4], s));
+    PDMK_CUDA_CHECK(cudaGetLastError());
+}
+
+StageTimes DeviceTree::last_times() {
+    StageTimes t;
+    PDMK_CUDA_CHECK(cudaEventSynchronize(ev_[4]));
+    float t01, t12, t23, t34;
+    PDMK_CUDA_CHECK(cudaEventElapsedTime(&t01, ev_[0], ev_[1]));
+    PDMK_CUDA_CHECK(cudaEventElapsedTime(&t12, ev_[1], ev_[2]));
+    PDMK_CUDA_CHECK(cudaEventElapsedTime(&t23, ev_[2], ev_[3]));
+    PDMK_CUDA_CHECK(cudaEventElapsedTime(&t34, ev_[3], ev_[4]));
+    t.dmk_ms = t01;
+    t.direct_ms = t12 + t34;
+    t.nufft_ms = t23;
+    t.near_ms = t12;
+    t.finalize_ms = t34;
+    return t;
+}
+
+void DeviceTree::evaluate_device(const double* q_user_d, double* pot_user_d, StageTimes* times) {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    run(q_user_d, pot_user_d);
+    if (times) *times = last_times();
+}
+
+void DeviceTree::evaluate_parts_host(const double* q_user, double* tree_part, double* far_part) {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, q_user, sizeof(double) * n_, cudaMemcpyHostToDevice, stream_));
+    run(q_dev_, pot_dev_);
+    double* tp = nullptr;
+    double* fp = nullptr;
+    PDMK_CUDA_CHECK(cudaMallocAsync(&tp, sizeof(double) * n_, stream_));
+    PDMK_CUDA_CHECK(cudaMallocAsync(&fp, sizeof(double) * n_, stream_));
+    dev::launch_desort_parts(pot_sorted_, far_sorted_, trg_, trg_perm_, q_dev_, tp, fp, n_, stream_);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(tree_part, tp, sizeof(double) * n_, cudaMemcpyDeviceToHost, stream_));
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(far_part, fp, sizeof(double) * n_, cudaMemcpyDeviceToHost, stream_));
+    PDMK_CUDA_CHECK(cudaFreeAsync(tp, stream_));
+    PDMK_CUDA_CHECK(cudaFreeAsync(fp, stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+void DeviceTree::evaluate_host(const double* q_user, double* pot_user, StageTimes* times) {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, q_user, sizeof(double) * n_, cudaMemcpyHostToDevice, stream_));
+    evaluate_device(q_dev_, pot_dev_, times);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(pot_user, pot_dev_, sizeof(double) * n_, cudaMemcpyDeviceToHost, stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+}  // namespace pdmkb

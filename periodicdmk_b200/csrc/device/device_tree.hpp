@@ -1,0 +1,141 @@
+// Device-resident periodic DMK tree: uploads a host Plan once and runs the
+// evaluate path on one GPU.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "../host/plan.hpp"
+#include "kernels.cuh"
+
+namespace pdmkb {
+
+struct StageTimes {
+    double dmk_ms = 0;     // charge gather, upward pass, plane-wave downward pass, leaf evaluation
+    double direct_ms = 0;  // residual near field + self correction + desort
+    double nufft_ms = 0;   // periodic far field
+    double near_ms = 0;    // residual near-field kernel alone
+    double finalize_ms = 0;
+};
+
+class DeviceTree {
+  public:
+    DeviceTree(const Plan& P, int device = -1);
+    ~DeviceTree();
+    DeviceTree(const DeviceTree&) = delete;
+    DeviceTree& operator=(const DeviceTree&) = delete;
+
+    int n_points() const { return n_; }
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // Host buffers in, host buffers out (copies inside).  times may be null.
+    void evaluate_host(const double* q_user, double* pot_user, StageTimes* times = nullptr);
+    // Device buffers (N doubles each) on this tree's device; enqueued on stream_.
+    // With times != null the call synchronises to read the stage events.
+    void evaluate_device(const double* q_user_d, double* pot_user_d, StageTimes* times = nullptr);
+    // Tree part (near + plane-wave levels - self) and far field, user order, host buffers.
+    void evaluate_parts_host(const double* q_user, double* tree_part, double* far_part);
+    // Number of kernels one evaluate launches (for reporting).
+    int launches_per_evaluate() const { return launches_; }
+    // Stage times of the most recent evaluate (synchronises on its last event).
+    StageTimes last_times();
+    // Near-field pairs the reference evaluates after its contact-geometry cull
+    // (the algorithmic work of the residual sum) and before it (all list pairs).
+    int64_t near_pairs_culled() const { return near_pairs_culled_; }
+    int64_t near_pairs_nominal() const { return near_pairs_nominal_; }
+    int near_coeffs() const { return near_.nc; }
+    size_t device_bytes() const { return bytes_; }
+
+  private:
+    void init(const Plan& P, int device);
+    void release();
+    template <typename T>
+    T* alloc(size_t n);
+    template <typename T>
+    T* upload(const std::vector<T>& v);
+    void run(const double* q_user_d, double* pot_user_d);
+
+    int device_ = 0;
+    int n_ = 0, n_all_ = 0, p_ = 0, npw_ = 0, npw2_ = 0, M_ = 0;
+    size_t bytes_ = 0;
+    int launches_ = 0;
+    int64_t near_pairs_culled_ = 0, near_pairs_nominal_ = 0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_[5]{};
+    std::vector<void*> allocs_;
+
+    // points
+    double4* src_ = nullptr;
+    int* src_charge_idx_ = nullptr;
+    double4* trg_ = nullptr;  // .w = self-interaction weight of the target's leaf
+    int* trg_perm_ = nullptr;
+    double* pot_sorted_ = nullptr;
+    double* far_sorted_ = nullptr;
+    double* q_sorted_ = nullptr;
+    double* q_dev_ = nullptr;    // staging for host-buffer evaluate
+    double* pot_dev_ = nullptr;
+    // expansions
+    double* proxy_up_ = nullptr;
+    double* proxy_down_ = nullptr;
+    dev::cd* pw_out_ = nullptr;
+    int64_t n_up_ = 0, n_down_ = 0, n_pw_ = 0;
+    // tables
+    double* c2p_ = nullptr;
+    double* p2c_ = nullptr;
+    struct LevelDev {
+        dev::cd* poly2pw = nullptr;      // n x p
+        dev::cd* poly2pw_half = nullptr; // n2 x p
+        dev::cd* pw2polyT = nullptr;     // p x n
+        dev::cd* pw2polyTw = nullptr;    // p x n2, half-space weights folded in
+        double* shift = nullptr;         // 27 x 2M
+    };
+    std::vector<LevelDev> lev_;
+    // upward
+    dev::C2ProxyArgs c2x_{};
+    struct C2PGroup {  // one (level, child index) group of children -> parents
+        int n = 0;
+        int64_t* in_off = nullptr;
+        int64_t* out_off = nullptr;
+        int child = 0;
+    };
+    std::vector<C2PGroup> c2p_groups_;
+    struct PwGroup {  // boxes of one level whose outgoing expansion is formed
+        int level = 0, n = 0;
+        int64_t* in_off = nullptr;   // proxy_up element offset
+        int64_t* out_off = nullptr;  // pw_out element offset
+    };
+    std::vector<PwGroup> pw_groups_;
+    struct EvalLevel {  // boxes of one level that receive incoming expansions
+        int level = 0, n = 0;
+        int* term_start = nullptr;
+        int* term_slot = nullptr;
+        int* term_stencil = nullptr;
+        int64_t* down_off = nullptr;
+        int n_p2c = 0;
+        int64_t* p2c_in = nullptr;
+        int64_t* p2c_out = nullptr;
+        int64_t* p2c_mat = nullptr;  // element offset of the child's x matrix in p2c_
+    };
+    std::vector<EvalLevel> eval_levels_;
+    dev::EvalArgs eval_{};
+    dev::NearArgs near_{};
+    // scratch for the separable transforms
+    dev::cd* scratch1_ = nullptr;
+    dev::cd* scratch2_ = nullptr;
+    dev::cd* pw_in_ = nullptr;
+    int64_t scratch_elems_ = 0, pw_in_elems_ = 0;
+    // far field
+    dev::NufftArgs nufft_{};
+    int nufft_max_jk_ = 0, nufft_max_ex_ = 0;
+    double* grid_ = nullptr;
+    dev::cd* spec_ = nullptr;
+    double* mult_ = nullptr;
+    int64_t n_spec_ = 0, n_grid_ = 0;
+    cufftHandle plan_fwd_ = 0, plan_inv_ = 0;
+};
+
+}  // namespace pdmkb

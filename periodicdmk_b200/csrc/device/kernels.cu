@@ -1,0 +1,623 @@
+// CUDA kernels of the periodic DMK evaluate path, FP64 (plain) variant.
+//
+// Stage -> reference function it computes:
+//   k_gather      charge gather into tree order (periodic_dmk.cpp:165-169, pbc_tree.cpp:1807-1821)
+//   k_c2proxy     charge -> Chebyshev proxy moments (proxy.cpp:153-212)
+//   k_contract    separable tensor transforms: c2p/p2c (tensorprod.cpp:39-75),
+//                 proxy -> plane waves (proxy.cpp:42-90), plane waves -> proxy (planewave.cpp:49-105)
+//   k_shift       plane-wave translation with the kernel FT fused (pbc_tree.cpp:1294-1348, tree.hpp:287-316)
+//   k_eval        proxy -> potential at leaf targets (proxy.cpp:307-448)
+//   k_near        PSWF residual pair sum (pbc_tree.cpp:1442-1681, vector_kernels.hpp:354-421)
+//   k_spread / k_interp / k_multiply   periodic far field (pbc.cpp:359-541)
+//   k_finalize    self correction + desort + far field add (pbc_tree.cpp:1759-1805, periodic_dmk.cpp:177-183)
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace pdmkb {
+namespace dev {
+
+// ============================================================================
+// gather
+// ============================================================================
+__global__ void k_gather(double4* __restrict__ src, const int* __restrict__ idx, const double* __restrict__ q, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) src[i].w = q[idx[i]];
+}
+
+void launch_gather(double4* src, const int* src_charge_idx, const double* q_user, int n_all, cudaStream_t s) {
+    if (n_all <= 0) return;
+    k_gather<<<(n_all + 255) / 256, 256, 0, s>>>(src, src_charge_idx, q_user, n_all);
+}
+
+__global__ void k_gather_q(const int* __restrict__ perm, const double* __restrict__ q, double* __restrict__ out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = q[perm[i]];
+}
+
+void launch_nufft_gather_q(const int* trg_perm, const double* q_user, double* q_sorted, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_gather_q<<<(n + 255) / 256, 256, 0, s>>>(trg_perm, q_user, q_sorted, n);
+}
+
+// ============================================================================
+// charge -> proxy moments.  One CTA = one centre box x 128 (j,k) columns; each
+// thread accumulates the P coefficients along x of its column over all sources.
+// ============================================================================
+template <int P>
+__global__ void __launch_bounds__(128) k_c2proxy(C2ProxyArgs a) {
+    constexpr int TS = 32;
+    __shared__ double sx[TS][P], sy[TS][P], sz[TS][P];
+    const int e = blockIdx.x;
+    const int jk = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool active = jk < P * P;
+    const int j = jk % P, k = jk / P;
+    double acc[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) acc[i] = 0.0;
+    const double4 cs = a.center_scale[e];
+    for (int r = a.rng_start[e]; r < a.rng_start[e + 1]; ++r) {
+        const int s0 = a.src_start[r], ns = a.src_count[r];
+        for (int base = 0; base < ns; base += TS) {
+            const int nt = min(TS, ns - base);
+            __syncthreads();
+            for (int task = threadIdx.x; task < 3 * TS; task += blockDim.x) {
+                const int si = task % TS, d = task / TS;
+                double* dst = d == 0 ? sx[si] : (d == 1 ? sy[si] : sz[si]);
+                if (si < nt) {
+                    const double4 pt = a.src[s0 + base + si];
+                    const double x = (d == 0 ? pt.x - cs.x : (d == 1 ? pt.y - cs.y : pt.z - cs.z)) * cs.w;
+                    const double mult = d == 2 ? pt.w : 1.0;  // fold the charge into the z factor
+                    double t0 = 1.0, t1 = x;
+                    dst[0] = mult;
+                    if (P > 1) dst[1] = mult * x;
+                    for (int n = 2; n < P; ++n) {
+                        const double t2 = 2.0 * x * t1 - t0;
+                        dst[n] = mult * t2;
+                        t0 = t1;
+                        t1 = t2;
+                    }
+                } else {
+                    for (int n = 0; n < P; ++n) dst[n] = 0.0;
+                }
+            }
+            __syncthreads();
+            if (active) {
+                for (int s = 0; s < nt; ++s) {
+                    const double f = sy[s][j] * sz[s][k];
+#pragma unroll
+                    for (int i = 0; i < P; ++i) acc[i] = fma(f, sx[s][i], acc[i]);
+                }
+            }
+        }
+    }
+    if (active) {
+        double* out = a.proxy_up + (int64_t)a.slot[e] * (P * P * P) + (int64_t)P * jk;
+#pragma unroll
+        for (int i = 0; i < P; ++i) out[i] += acc[i];
+    }
+}
+
+void launch_c2proxy(const C2ProxyArgs& a, int p, cudaStream_t s) {
+    if (a.n_centers <= 0) return;
+    const dim3 grid(a.n_centers, (p * p + 127) / 128);
+    switch (p) {
+        case 9: k_c2proxy<9><<<grid, 128, 0, s>>>(a); break;
+        case 18: k_c2proxy<18><<<grid, 128, 0, s>>>(a); break;
+        case 28: k_c2proxy<28><<<grid, 128, 0, s>>>(a); break;
+        case 38: k_c2proxy<38><<<grid, 128, 0, s>>>(a); break;
+        default: throw std::runtime_error("unsupported expansion order");
+    }
+}
+
+// ============================================================================
+// batched separable contraction
+// ============================================================================
+template <typename TO>
+__device__ __forceinline__ void store_out(TO* p, double2 v, int mode, double scale);
+
+template <>
+__device__ __forceinline__ void store_out<double>(double* p, double2 v, int mode, double scale) {
+    if (mode == kStore)
+        *p = v.x;
+    else if (mode == kAdd)
+        *p += v.x;
+    else
+        *p += scale * v.x;
+}
+template <>
+__device__ __forceinline__ void store_out<cd>(cd* p, double2 v, int mode, double) {
+    if (mode == kStore) {
+        *p = cd{v.x, v.y};
+    } else {
+        cd o = *p;
+        *p = cd{o.x + v.x, o.y + v.y};
+    }
+}
+
+__device__ __forceinline__ double2 to2(double v) { return make_double2(v, 0.0); }
+__device__ __forceinline__ double2 to2(cd v) { return make_double2(v.x, v.y); }
+
+template <typename TI, typename TM, typename TO, int RT, int AB>
+__global__ void __launch_bounds__(256) k_contract(ContractArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using TA = decltype(mac(TM(), TI(), TM()));  // accumulator type: complex if either is
+    const int ni = a.ni, na = a.na, R = a.R;
+    const int e = blockIdx.x, r0 = blockIdx.y * RT;
+    TM* sM = reinterpret_cast<TM*>(smem_raw);
+    const size_t moff = ((size_t)na * ni * sizeof(TM) + 15) / 16 * 16;
+    TI* sIn = reinterpret_cast<TI*>(smem_raw + moff);
+    const TI* in = reinterpret_cast<const TI*>(a.in) + (a.in_off ? a.in_off[e] : (int64_t)e * a.in_stride);
+    TO* out = reinterpret_cast<TO*>(a.out) + (a.out_off ? a.out_off[e] : (int64_t)e * a.out_stride);
+    const TM* mat = reinterpret_cast<const TM*>(a.mat) + (a.mat_off ? a.mat_off[e] : 0);
+    for (int idx = threadIdx.x; idx < na * ni; idx += blockDim.x) sM[idx] = mat[idx];
+    const int nr = min(RT, R - r0);
+    const TI* inb = in + (int64_t)ni * r0;
+    for (int idx = threadIdx.x; idx < ni * nr; idx += blockDim.x) {
+        const int i = idx % ni, rr = idx / ni;
+        sIn[rr + RT * i] = inb[idx];
+    }
+    __syncthreads();
+    const int rr = threadIdx.x % RT, ag = threadIdx.x / RT, nag = blockDim.x / RT;
+    if (rr >= nr) return;
+    for (int a0 = ag * AB; a0 < na; a0 += nag * AB) {
+        TA acc[AB];
+#pragma unroll
+        for (int b = 0; b < AB; ++b) acc[b] = zero<TA>();
+        for (int i = 0; i < ni; ++i) {
+            const TI x = sIn[rr + RT * i];
+#pragma unroll
+            for (int b = 0; b < AB; ++b)
+                if (a0 + b < na) acc[b] = mac(sM[a0 + b + na * i], x, acc[b]);
+        }
+#pragma unroll
+        for (int b = 0; b < AB; ++b)
+            if (a0 + b < na) store_out<TO>(out + (r0 + rr) + (int64_t)R * (a0 + b), to2(acc[b]), a.mode, a.scale);
+    }
+}
+
+template <typename TI, typename TM, typename TO>
+static void launch_contract_t(const ContractArgs& a, cudaStream_t s) {
+    constexpr int RT = 32, AB = 4;
+    const size_t smem = ((size_t)a.na * a.ni * sizeof(TM) + 15) / 16 * 16 + (size_t)a.ni * RT * sizeof(TI);
+    static bool configured = false;
+    if (!configured) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_contract<TI, TM, TO, RT, AB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        configured = true;
+    }
+    if (smem > 200 * 1024) throw std::runtime_error("contraction tile exceeds shared memory");
+    const dim3 grid(a.n_entries, (a.R + RT - 1) / RT);
+    k_contract<TI, TM, TO, RT, AB><<<grid, 256, smem, s>>>(a);
+}
+
+void launch_contract(const ContractArgs& a, ContractType t, cudaStream_t s) {
+    if (a.n_entries <= 0) return;
+    switch (t) {
+        case kRRR: launch_contract_t<double, double, double>(a, s); break;
+        case kRCC: launch_contract_t<double, cd, cd>(a, s); break;
+        case kCCC: launch_contract_t<cd, cd, cd>(a, s); break;
+        case kCCR: launch_contract_t<cd, cd, double>(a, s); break;
+    }
+}
+
+// ============================================================================
+// plane-wave shift (translation x kernel FT)
+// ============================================================================
+__global__ void __launch_bounds__(256) k_shift(ShiftArgs a) {
+    const int e = blockIdx.x;
+    const int m = blockIdx.y * blockDim.x + threadIdx.x;
+    if (m >= a.M) return;
+    double ar = 0.0, ai = 0.0;
+    for (int t = a.term_start[e]; t < a.term_start[e + 1]; ++t) {
+        const cd v = a.pw_out[(int64_t)a.term_slot[t] * a.M + m];
+        const double* sh = a.shift + (int64_t)a.term_stencil[t] * 2 * a.M;
+        const double sr = sh[m], si = sh[a.M + m];
+        ar = fma(v.x, sr, fma(-v.y, si, ar));
+        ai = fma(v.x, si, fma(v.y, sr, ai));
+    }
+    a.pw_in[(int64_t)e * a.M + m] = cd{ar, ai};
+}
+
+void launch_shift(const ShiftArgs& a, cudaStream_t s) {
+    if (a.n_entries <= 0) return;
+    const dim3 grid(a.n_entries, (a.M + 255) / 256);
+    k_shift<<<grid, 256, 0, s>>>(a);
+}
+
+// ============================================================================
+// proxy -> leaf targets: pot_t += sum_ijk C(i,j,k) T_i(x) T_j(y) T_k(z)
+// ============================================================================
+template <int P>
+__global__ void __launch_bounds__(128) k_eval(EvalArgs a) {
+    __shared__ double slab[P * P];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const double4 cs = a.center_scale[e];
+    const double* C = a.proxy_down + (int64_t)a.slot[e] * (P * P * P);
+    for (int base = 0; base < nt; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const bool act = t < nt;
+        double tx[P];
+        double y = 0.0, z = 0.0;
+        {
+            double x = 0.0;
+            if (act) {
+                const double4 pt = a.trg[t0 + t];
+                x = (pt.x - cs.x) * cs.w;
+                y = (pt.y - cs.y) * cs.w;
+                z = (pt.z - cs.z) * cs.w;
+            }
+            tx[0] = 1.0;
+            if (P > 1) tx[1] = x;
+#pragma unroll
+            for (int n = 2; n < P; ++n) tx[n] = 2.0 * x * tx[n - 1] - tx[n - 2];
+        }
+        double acc = 0.0;
+        double za = 1.0, zb = z;
+        for (int k = 0; k < P; ++k) {
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < P * P; idx += blockDim.x) slab[idx] = C[(int64_t)k * P * P + idx];
+            __syncthreads();
+            double ya = 1.0, yb = y, sk = 0.0;
+            for (int j = 0; j < P; ++j) {
+                double r = 0.0;
+#pragma unroll
+                for (int i = 0; i < P; ++i) r = fma(slab[i + P * j], tx[i], r);
+                sk = fma(ya, r, sk);
+                const double yn = 2.0 * y * yb - ya;
+                ya = yb;
+                yb = yn;
+            }
+            acc = fma(za, sk, acc);
+            const double zn = 2.0 * z * zb - za;
+            za = zb;
+            zb = zn;
+        }
+        if (act) a.pot[t0 + t] += acc;
+    }
+}
+
+void launch_eval(const EvalArgs& a, int p, cudaStream_t s) {
+    if (a.n_leaves <= 0) return;
+    switch (p) {
+        case 9: k_eval<9><<<a.n_leaves, 128, 0, s>>>(a); break;
+        case 18: k_eval<18><<<a.n_leaves, 128, 0, s>>>(a); break;
+        case 28: k_eval<28><<<a.n_leaves, 128, 0, s>>>(a); break;
+        case 38: k_eval<38><<<a.n_leaves, 128, 0, s>>>(a); break;
+        default: throw std::runtime_error("unsupported expansion order");
+    }
+}
+
+// ============================================================================
+// residual near field
+// ============================================================================
+template <int NC>
+__global__ void __launch_bounds__(128) k_near(NearArgs a) {
+    constexpr int TPT = 4;
+    __shared__ double4 ss[128];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    double c[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) c[i] = a.coef[i];
+    for (int base = 0; base < nt; base += TPT * 128) {
+        double4 tp[TPT];
+        double acc[TPT];
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+            const int t = base + threadIdx.x + u * 128;
+            tp[u] = t < nt ? a.trg[t0 + t] : make_double4(1e300, 1e300, 1e300, 0.0);
+            acc[u] = 0.0;
+        }
+        for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
+            const int s0 = a.pair_src_start[pr], ns = a.pair_src_count[pr];
+            const double b = a.pair_bsize[pr];
+            const double d2max = b * b, rsc = 2.0 / b, cen = -0.5 * b;
+            for (int sb = 0; sb < ns; sb += 128) {
+                __syncthreads();
+                if (sb + (int)threadIdx.x < ns) ss[threadIdx.x] = a.src[s0 + sb + threadIdx.x];
+                __syncthreads();
+                const int m = min(128, ns - sb);
+                for (int j = 0; j < m; ++j) {
+                    const double4 y = ss[j];
+#pragma unroll
+                    for (int u = 0; u < TPT; ++u) {
+                        const double dx = tp[u].x - y.x, dy = tp[u].y - y.y, dz = tp[u].z - y.z;
+                        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                        if (r2 > 1e-30 && r2 < d2max) {
+                            const double rinv = rsqrt_nr(r2);
+                            const double x = fma(r2, rinv, cen) * rsc;
+                            double pv = c[NC - 1];
+#pragma unroll
+                            for (int i = NC - 2; i >= 0; --i) pv = fma(pv, x, c[i]);
+                            acc[u] = fma(y.w * pv, rinv, acc[u]);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+            const int t = base + threadIdx.x + u * 128;
+            if (t < nt) a.pot[t0 + t] += acc[u];
+        }
+    }
+}
+
+void launch_near(const NearArgs& a, cudaStream_t s) {
+    if (a.n_leaves <= 0) return;
+    switch (a.nc) {
+#define PDMK_NEAR_CASE(NC) \
+    case NC: k_near<NC><<<a.n_leaves, 128, 0, s>>>(a); break;
+        PDMK_NEAR_CASE(5)
+        PDMK_NEAR_CASE(6)
+        PDMK_NEAR_CASE(9)
+        PDMK_NEAR_CASE(11)
+        PDMK_NEAR_CASE(12)
+        PDMK_NEAR_CASE(15)
+        PDMK_NEAR_CASE(17)
+        PDMK_NEAR_CASE(18)
+        PDMK_NEAR_CASE(22)
+        PDMK_NEAR_CASE(23)
+        PDMK_NEAR_CASE(25)
+#undef PDMK_NEAR_CASE
+        default: throw std::runtime_error("unsupported residual polynomial length");
+    }
+}
+
+// ============================================================================
+// final gather
+// ============================================================================
+__global__ void k_finalize(const double* __restrict__ pot, const double* __restrict__ far, const double4* __restrict__ trg,
+                           const int* __restrict__ perm, const double* __restrict__ q, double* __restrict__ out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int u = perm[i];
+    out[u] = pot[i] + far[i] - trg[i].w * q[u];
+}
+
+void launch_finalize(const double* pot_sorted, const double* far_sorted, const double4* trg, const int* trg_perm,
+                     const double* q_user, double* pot_user, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_finalize<<<(n + 255) / 256, 256, 0, s>>>(pot_sorted, far_sorted, trg, trg_perm, q_user, pot_user, n);
+}
+
+// ============================================================================
+// FMA throughput probe (for roofline denominators): 8 independent FMA chains
+// per thread; the result is written only if it equals a sentinel that it
+// cannot reach, so the chains stay live.
+// ============================================================================
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_probe(T b, T c, int iters, T* sink) {
+    T a[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = (T)(threadIdx.x + i) * (T)1e-3;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = fma(a[i], b, c);
+        }
+    }
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += a[i];
+    if (s == (T)-12345.678) sink[threadIdx.x] = s;
+}
+
+double fma_probe_tflops(bool fp64) {
+    int dev = 0, sms = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
+    PDMK_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8, threads = 256, iters = fp64 ? 2000 : 8000;
+    void* sink = nullptr;
+    PDMK_CUDA_CHECK(cudaMalloc(&sink, 256 * sizeof(double)));
+    cudaEvent_t e0, e1;
+    PDMK_CUDA_CHECK(cudaEventCreate(&e0));
+    PDMK_CUDA_CHECK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        PDMK_CUDA_CHECK(cudaEventRecord(e0));
+        if (fp64)
+            k_fma_probe<double><<<blocks, threads>>>(0.999999, 1e-7, iters, (double*)sink);
+        else
+            k_fma_probe<float><<<blocks, threads>>>(0.9999f, 1e-7f, iters, (float*)sink);
+        PDMK_CUDA_CHECK(cudaEventRecord(e1));
+        PDMK_CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0;
+        PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0) best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    return flops / (best * 1e-3) / 1e12;
+}
+
+__global__ void k_desort_parts(const double* __restrict__ pot, const double* __restrict__ far,
+                               const double4* __restrict__ trg, const int* __restrict__ perm,
+                               const double* __restrict__ q, double* __restrict__ tree_part,
+                               double* __restrict__ far_part, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int u = perm[i];
+    tree_part[u] = pot[i] - trg[i].w * q[u];
+    far_part[u] = far[i];
+}
+
+void launch_desort_parts(const double* pot_sorted, const double* far_sorted, const double4* trg, const int* trg_perm,
+                         const double* q_user, double* tree_part, double* far_part, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_desort_parts<<<(n + 255) / 256, 256, 0, s>>>(pot_sorted, far_sorted, trg, trg_perm, q_user, tree_part,
+                                                   far_part, n);
+}
+
+// ============================================================================
+// NUFFT: exponential-of-semicircle spreading kernel phi(z) = exp(beta (sqrt(1-z^2) - 1))
+// (Barnett, Magland, af Klinteberg, SIAM J. Sci. Comput. 41 (2019)), width W grid cells.
+// ============================================================================
+__device__ __forceinline__ double es_kernel(double z, double beta) {
+    const double z2 = z * z;
+    return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
+}
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// Spread: each CTA builds one leaf's subgrid S(i,j,k) = sum_pts q Bx_i By_j Bz_k in
+// registers (thread = (j,k) column, x along the register array) and flushes it
+// once into the global periodic grid with atomics.
+template <int W, int NX>
+__global__ void __launch_bounds__(128) k_spread(NufftArgs a) {
+    constexpr int TS = 32;
+    __shared__ double sBx[TS][NX];
+    __shared__ double sKy[TS][W], sKz[TS][W];
+    __shared__ int sBy[TS], sBz[TS];
+    __shared__ double sQ[TS];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const int4 org = a.sub_origin[e], ext = a.sub_extent[e];
+    const int jk = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool active = jk < ext.y * ext.z;
+    const int kk = jk % max(ext.z, 1), jj = jk / max(ext.z, 1);
+    const double hw = 0.5 * W;
+    double acc[NX];
+#pragma unroll
+    for (int i = 0; i < NX; ++i) acc[i] = 0.0;
+    for (int base = 0; base < nt; base += TS) {
+        const int m = min(TS, nt - base);
+        __syncthreads();
+        if (threadIdx.x < TS) {
+            const int s = threadIdx.x;
+            if (s < m) {
+                const double4 t = a.pt_t[t0 + base + s];
+                const int4 l0 = a.pt_l0[t0 + base + s];
+                const int bx = l0.x - org.x;
+                for (int i = 0; i < NX; ++i) {
+                    const int o = i - bx;
+                    sBx[s][i] = (o >= 0 && o < W) ? es_kernel((t.x - (double)(l0.x + o)) / hw, a.es_beta) : 0.0;
+                }
+                for (int c = 0; c < W; ++c) {
+                    sKy[s][c] = es_kernel((t.y - (double)(l0.y + c)) / hw, a.es_beta);
+                    sKz[s][c] = es_kernel((t.z - (double)(l0.z + c)) / hw, a.es_beta);
+                }
+                sBy[s] = l0.y - org.y;
+                sBz[s] = l0.z - org.z;
+                sQ[s] = a.q_sorted[t0 + base + s];
+            }
+        }
+        __syncthreads();
+        if (active) {
+            for (int s = 0; s < m; ++s) {
+                const int dj = jj - sBy[s], dk = kk - sBz[s];
+                if (dj < 0 || dj >= W || dk < 0 || dk >= W) continue;
+                const double f = sQ[s] * sKy[s][dj] * sKz[s][dk];
+#pragma unroll
+                for (int i = 0; i < NX; ++i) acc[i] = fma(f, sBx[s][i], acc[i]);
+            }
+        }
+    }
+    if (!active) return;
+    const int gy = wrapi(org.y + jj, a.n2), gz = wrapi(org.z + kk, a.n3);
+#pragma unroll
+    for (int i = 0; i < NX; ++i) {
+        if (i < ext.x && acc[i] != 0.0) {
+            const int gx = wrapi(org.x + i, a.n1);
+            atomicAdd(a.grid + ((int64_t)gx * a.n2 + gy) * a.n3 + gz, acc[i]);
+        }
+    }
+}
+
+template <int W>
+__global__ void __launch_bounds__(128) k_interp(NufftArgs a) {
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const double hw = 0.5 * W;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        const double4 tt = a.pt_t[t0 + t];
+        const int4 l0 = a.pt_l0[t0 + t];
+        double kx[W], ky[W], kz[W];
+        int iy[W], iz[W];
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+            kx[c] = es_kernel((tt.x - (double)(l0.x + c)) / hw, a.es_beta);
+            ky[c] = es_kernel((tt.y - (double)(l0.y + c)) / hw, a.es_beta);
+            kz[c] = es_kernel((tt.z - (double)(l0.z + c)) / hw, a.es_beta);
+            iy[c] = wrapi(l0.y + c, a.n2);
+            iz[c] = wrapi(l0.z + c, a.n3);
+        }
+        double u = 0.0;
+#pragma unroll 1
+        for (int ia = 0; ia < W; ++ia) {
+            const double* gx = a.grid + (int64_t)wrapi(l0.x + ia, a.n1) * a.n2 * a.n3;
+            double sa = 0.0;
+#pragma unroll
+            for (int ib = 0; ib < W; ++ib) {
+                const double* gy = gx + (int64_t)iy[ib] * a.n3;
+                double sb = 0.0;
+#pragma unroll
+                for (int ic = 0; ic < W; ++ic) sb = fma(kz[ic], __ldg(gy + iz[ic]), sb);
+                sa = fma(ky[ib], sb, sa);
+            }
+            u = fma(kx[ia], sa, u);
+        }
+        a.far[t0 + t] = u;
+    }
+}
+
+__global__ void k_multiply(cd* spec, const double* mult, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double m = mult[i];
+    cd v = spec[i];
+    spec[i] = cd{v.x * m, v.y * m};
+}
+
+void launch_multiply(cd* spec, const double* mult, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_multiply<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, mult, n);
+}
+
+template <int W>
+static void launch_spread_w(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s) {
+    const dim3 grid(a.n_leaves, (max_jk + 127) / 128);
+    if (max_ex <= 16)
+        k_spread<W, 16><<<grid, 128, 0, s>>>(a);
+    else if (max_ex <= 32)
+        k_spread<W, 32><<<grid, 128, 0, s>>>(a);
+    else if (max_ex <= 48)
+        k_spread<W, 48><<<grid, 128, 0, s>>>(a);
+    else
+        throw std::runtime_error("NUFFT leaf subgrid too large");
+}
+
+void launch_spread(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s) {
+    if (a.n_leaves <= 0) return;
+    switch (a.w) {
+#define PDMK_W_CASE(W) \
+    case W: launch_spread_w<W>(a, max_jk, max_ex, s); break;
+        PDMK_W_CASE(4) PDMK_W_CASE(5) PDMK_W_CASE(6) PDMK_W_CASE(7) PDMK_W_CASE(8) PDMK_W_CASE(9)
+        PDMK_W_CASE(10) PDMK_W_CASE(11) PDMK_W_CASE(12) PDMK_W_CASE(13) PDMK_W_CASE(14)
+#undef PDMK_W_CASE
+        default: throw std::runtime_error("unsupported NUFFT kernel width");
+    }
+}
+
+void launch_interp(const NufftArgs& a, cudaStream_t s) {
+    if (a.n_leaves <= 0) return;
+    switch (a.w) {
+#define PDMK_W_CASE(W) \
+    case W: k_interp<W><<<a.n_leaves, 128, 0, s>>>(a); break;
+        PDMK_W_CASE(4) PDMK_W_CASE(5) PDMK_W_CASE(6) PDMK_W_CASE(7) PDMK_W_CASE(8) PDMK_W_CASE(9)
+        PDMK_W_CASE(10) PDMK_W_CASE(11) PDMK_W_CASE(12) PDMK_W_CASE(13) PDMK_W_CASE(14)
+#undef PDMK_W_CASE
+        default: throw std::runtime_error("unsupported NUFFT kernel width");
+    }
+}
+
+}  // namespace dev
+}  // namespace pdmkb
