@@ -91,6 +91,19 @@ int pdmk_stage_times_double(void* h, double* out8);
  * else FP32), 2 flops per FMA; the denominator of CUDA-core rooflines. */
 int pdmk_fma_peak(int fp64, double* tflops);
 
+/* Evaluate that allocates no device memory (no counterpart in the reference).
+ * For callers that cannot allocate device memory while they run -- e.g. an
+ * engine whose caching allocator owns the GPU memory pool, or a time-step
+ * loop that cannot take the device-wide synchronisation of cudaMalloc/cudaFree.
+ * The tree is created beforehand (pdmk_create_double allocates its buffers);
+ * charges_dev / pot_dev are N doubles on the tree's device, owned by the caller.
+ * Transform scratch lives in one static 32 MiB device array held by every GPU
+ * that loads the library until exit; trees needing more per box are rejected
+ * (-1).  The first call on a device looks up that array's address: make it
+ * before any stream capture.  Calls share the array, so calls that overlap on
+ * the GPU race and must be serialised by the caller.  Synchronous. */
+int pdmk_evaluate_device_noalloc_double(void* h, const double* charges_dev, double* pot_dev);
+
 /* Last error message of the calling thread ("" if none). */
 const char* pdmk_last_error(void);
 

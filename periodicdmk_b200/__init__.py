@@ -28,7 +28,7 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
     "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
-    "pdmk_stage_times_double", "pdmk_fma_peak", "pdmk_last_error",
+    "pdmk_stage_times_double", "pdmk_fma_peak", "pdmk_evaluate_device_noalloc_double", "pdmk_last_error",
 ]
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -80,6 +80,8 @@ def library():
     lib.pdmk_optimize_cubic_cover.restype = ctypes.c_int
     lib.pdmk_stage_times_double.argtypes = [v, _D]
     lib.pdmk_stage_times_double.restype = ctypes.c_int
+    lib.pdmk_evaluate_device_noalloc_double.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pdmk_evaluate_device_noalloc_double.restype = ctypes.c_int
     lib.pdmk_fma_peak.argtypes = [ctypes.c_int, _D]
     lib.pdmk_fma_peak.restype = ctypes.c_int
     lib.pdmk_last_error.argtypes = []
@@ -189,6 +191,18 @@ class PeriodicDMKTree:
         f = self._lib.pdmk_evaluate_device_double if self.precision == "double" else \
             self._lib.pdmk_evaluate_device_float
         self._check(f(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(pot_ptr)), "pdmk_evaluate_device")
+
+    def evaluate_device_noalloc(self, q_ptr, pot_ptr):
+        """Device-resident evaluate that allocates no device memory (double trees).
+
+        For callers that must not allocate device memory once running (their
+        own allocator owns the pool, or cudaMalloc's device-wide
+        synchronisation is unacceptable in their loop).  Uses the library's
+        static 32 MiB scratch array; overlapping calls on one GPU race."""
+        if self.precision != "double":
+            raise RuntimeError("evaluate_device_noalloc is provided for double trees")
+        rc = self._lib.pdmk_evaluate_device_noalloc_double(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(pot_ptr))
+        self._check(rc, "pdmk_evaluate_device_noalloc_double")
 
     def evaluate_parts(self, charges):
         """(tree part, far-field part), both user order; double trees only."""

@@ -37,6 +37,10 @@ class DeviceTree {
     // Device buffers (N doubles each) on this tree's device; enqueued on stream_.
     // With times != null the call synchronises to read the stage events.
     void evaluate_device(const double* q_user_d, double* pot_user_d, StageTimes* times = nullptr);
+    // Same as evaluate_device, but the transform scratch is the library's fixed
+    // static device array instead of the tree's buffers, and nothing is
+    // allocated; synchronous.  Defined in noalloc.cu.
+    void evaluate_device_noalloc(const double* q_user_d, double* pot_user_d);
     // Tree part (near + plane-wave levels - self) and far field, user order, host buffers.
     void evaluate_parts_host(const double* q_user, double* tree_part, double* far_part);
     // Number of kernels one evaluate launches (for reporting).
