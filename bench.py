@@ -1,11 +1,13 @@
 #!/usr/bin/env python
 """Throughput benchmark of the periodic DMK evaluate path on B200.
 
-Workload (one step = one evaluate of one charge vector on a resident tree):
-  uniform cube, L = 1, N = 10^6 positions uniform in [0,1)^3 (seed 1), charges
-  uniform in [-1,1] minus their mean, n_digits = 6, n_per_leaf = 300, nz = 4,
-  plain FP64 path, 1 RHS.  Synthetic data; the tree is built once (untimed),
-  as in the reference's build-once / evaluate-many contract.
+Workload (one step = one batched evaluate of 64 charge vectors on a resident tree):
+  uniform cube, L = 1, N = 10^6 positions uniform in [0,1)^3 (seed 1), 64
+  charge vectors uniform in [-1,1] minus their mean, n_digits = 6,
+  n_per_leaf = 300, nz = 4, mixed-precision path.  The plain FP64 evaluate of
+  one charge vector on the same tree is measured beside it.  Synthetic data;
+  the trees are built once (untimed), as in the reference's build-once /
+  evaluate-many contract.
 
 Metric: Mpts*RHS/s = N * RHS / t_evaluate / 1e6 (whole job: summed over ranks).
 
@@ -130,6 +132,8 @@ def run_reference(args):
 
 
 def run_ours(args):
+    import ctypes
+
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -142,109 +146,165 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import periodicdmk_b200 as pd
 
-    n = args.n
+    n, k = args.n, args.rhs
     cell, pos, q = make_system(n, seed=1)
+    rng = np.random.default_rng(7)
+    Q = rng.uniform(-1.0, 1.0, (n, k))
+    Q -= Q.mean(axis=0)
+    Q[:, 0] = q
     t_build = time.perf_counter()
-    tree = pd.PeriodicDMKTree(cell, pos, n_digits=6, n_per_leaf=300, nz=4, precision="double")
+    tree_d = pd.PeriodicDMKTree(cell, pos, n_digits=6, n_per_leaf=300, nz=4, precision="double")
     t_build = time.perf_counter() - t_build
-    info = tree.info()
+    tree_f = pd.PeriodicDMKTree(cell, pos, n_digits=6, n_per_leaf=300, nz=4, precision="float")
+    info = tree_d.info()
     dev = torch.device("cuda", local)
-    q_d = torch.from_numpy(q).to(dev)
-    pot_d = torch.empty(n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
-    for _ in range(args.warmup):
-        tree.evaluate_device(q_d.data_ptr(), pot_d.data_ptr())
-    torch.cuda.synchronize()
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # ---- device-resident throughput: per-step device time from the events the
-    # library records on its launching stream; L2 flushed between steps.
-    step_ms = []
-    stages = []
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        tt = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    # ---------------- plain FP64, one RHS (the reference's double evaluate)
+    q_d = torch.from_numpy(q).to(dev)
+    pot_d = torch.empty(n, dtype=torch.float64, device=dev)
+    for _ in range(args.warmup):
+        tree_d.evaluate_device(q_d.data_ptr(), pot_d.data_ptr())
+    torch.cuda.synchronize()
+    plain_st = []
     barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local) as clk1:
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            tree.evaluate_device(q_d.data_ptr(), pot_d.data_ptr())
-            st = tree.stage_times()
-            stages.append(st)
-            step_ms.append(st["total_ms"])
+            tree_d.evaluate_device(q_d.data_ptr(), pot_d.data_ptr())
+            plain_st.append(tree_d.stage_times())
     torch.cuda.synchronize()
     barrier()
-    t_dev = sum(step_ms) / 1e3
-    if dist is not None:
-        tt = torch.tensor([t_dev], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev = float(tt.item())
-    ms_per_step = t_dev / args.steps * 1e3
-    value = world * n / (t_dev / args.steps) / 1e6
+    t_plain = max_over_ranks(sum(s["total_ms"] for s in plain_st) / 1e3)
+    plain_value = world * n / (t_plain / args.steps) / 1e6
+    pot_plain = pot_d.cpu().numpy()
 
-    # ---- end to end through the public C ABI with host (pinned) buffers
-    q_h = torch.from_numpy(q).pin_memory()
-    pot_h = torch.empty(n, dtype=torch.float64).pin_memory()
-    import ctypes
-    D = ctypes.POINTER(ctypes.c_double)
-    qp = ctypes.cast(q_h.data_ptr(), D)
-    pp = ctypes.cast(pot_h.data_ptr(), D)
+    # ---------------- mixed precision, k RHS in one batched call (headline)
+    Qc_d = torch.from_numpy(np.ascontiguousarray(Q.T)).to(dev)       # column-major N x k
+    P_d = torch.empty_like(Qc_d)
+    for _ in range(args.warmup):
+        tree_f.evaluate_multi_device(k, Qc_d.data_ptr(), P_d.data_ptr())
+    torch.cuda.synchronize()
+    mixed_st = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk2:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            tree_f.evaluate_multi_device(k, Qc_d.data_ptr(), P_d.data_ptr())
+            mixed_st.append(tree_f.stage_times())
+    torch.cuda.synchronize()
+    barrier()
+    t_mixed = max_over_ranks(sum(s["total_ms"] for s in mixed_st) / 1e3)
+    value = world * n * k / (t_mixed / args.steps) / 1e6
+    finfo = tree_f.info()
+    P_mixed = P_d.cpu().numpy()  # (k, N): row c = RHS c
+
+    # accuracy of the mixed batched result vs the plain FP64 evaluate
+    errs = [float(np.linalg.norm(P_mixed[0] - pot_plain) / np.linalg.norm(pot_plain))]
+    for c in (1, k // 2, k - 1):
+        if c <= 0 or c >= k:
+            continue
+        qc = torch.from_numpy(np.ascontiguousarray(Q[:, c])).to(dev)
+        tree_d.evaluate_device(qc.data_ptr(), pot_d.data_ptr())
+        ref = pot_d.cpu().numpy()
+        errs.append(float(np.linalg.norm(P_mixed[c] - ref) / np.linalg.norm(ref)))
+
+    # ---------------- end to end through the public C ABI, pinned host buffers:
+    # pdmk_evaluate_multi_float (float tree = mixed path), charges N x k doubles in,
+    # potentials N x k floats out
+    Qh = torch.from_numpy(np.ascontiguousarray(Q.T)).pin_memory()
+    Ph = torch.empty((k, n), dtype=torch.float32).pin_memory()
     lib = pd.library()
+    D = ctypes.POINTER(ctypes.c_double)
+    F = ctypes.POINTER(ctypes.c_float)
+    qp = ctypes.cast(Qh.data_ptr(), D)
+    pp = ctypes.cast(Ph.data_ptr(), F)
     e2e = []
     barrier()
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rc = lib.pdmk_evaluate_double(tree._h, n, None, qp, pp)
+        rc = lib.pdmk_evaluate_multi_float(tree_f._h, n, k, qp, pp)
         e2e.append(time.perf_counter() - t0)
         if rc != 0:
-            raise RuntimeError("pdmk_evaluate_double failed: " + pd._last_error())
+            raise RuntimeError("pdmk_evaluate_multi_float failed: " + pd._last_error())
     barrier()
-    t_e2e = sum(e2e)
-    if dist is not None:
-        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e_value = world * n / (t_e2e / args.steps) / 1e6
-    assert np.allclose(pot_h.numpy(), pot_d.cpu().numpy(), rtol=1e-12, atol=1e-12)
+    t_e2e = max_over_ranks(sum(e2e))
+    e2e_value = world * n * k / (t_e2e / args.steps) / 1e6
+    assert np.allclose(Ph.numpy()[0], P_mixed[0], rtol=1e-5, atol=1e-5)
 
-    # ---- roofline of the dominant kernel (residual near field, FP64 CUDA cores)
-    near_ms = statistics.median(s["near_ms"] for s in stages)
-    flop_per_pair = 2 * int(stages[0]["near_ncoef"]) + 14
-    near_flop = stages[0]["near_pairs_culled"] * flop_per_pair
-    achieved = near_flop / (near_ms * 1e-3) / 1e12
-    peak = pd.fma_peak_tflops(fp64=True)
-    roofline = {"bound": "fp64", "kernel": "k_near (residual near field)", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                "peak_source": "measured FP64 FMA probe on this GPU (pdmk_fma_peak)",
-                "algorithmic_flop_per_launch": near_flop,
-                "stage_ms_median": {k: statistics.median(s[k] for s in stages)
-                                    for k in ("dmk_ms", "near_ms", "nufft_ms", "finalize_ms", "total_ms")}}
+    # ---------------- rooflines: dominant kernel of each path (CUDA-core FMA bound)
+    pk64 = pd.fma_peak_tflops(fp64=True)
+    pk32 = pd.fma_peak_tflops(fp64=False)
 
+    def med(sts, key):
+        return statistics.median(s[key] for s in sts)
+
+    ncoef = int(plain_st[0]["near_ncoef"])
+    pairs = plain_st[0]["near_pairs_culled"]
+    near_flop_plain = pairs * (2 * ncoef + 14)
+    near_flop_mixed = pairs * (2 * ncoef + 14 + 2 * k)
+    ach_plain = near_flop_plain / (med(plain_st, "near_ms") * 1e-3) / 1e12
+    ach_mixed = near_flop_mixed / (med(mixed_st, "near_ms") * 1e-3) / 1e12
+    stage_keys = ("dmk_ms", "near_ms", "nufft_ms", "finalize_ms", "total_ms")
+    roofline = {"bound": "fp32", "kernel": "k_near_m32 (residual near field, %d RHS per call)" % k,
+                "achieved": ach_mixed, "peak": pk32, "unit": "TFLOP/s", "frac": ach_mixed / pk32,
+                "traffic": None, "peak_source": "measured FP32 FMA probe on this GPU (pdmk_fma_peak)",
+                "algorithmic_flop_per_launch": near_flop_mixed,
+                "flop_convention": "culled pairs x (2*NC + 14 + 2*k)",
+                "stage_ms_median": {kk: med(mixed_st, kk) for kk in stage_keys}}
+    plain = {"value": plain_value, "unit": "Mpts*RHS/s", "ms_per_step": t_plain / args.steps * 1e3,
+             "gpu_launches": info["launches_per_evaluate"] * args.steps,
+             "roofline": {"bound": "fp64", "kernel": "k_near (residual near field)", "achieved": ach_plain,
+                          "peak": pk64, "unit": "TFLOP/s", "frac": ach_plain / pk64,
+                          "peak_source": "measured FP64 FMA probe on this GPU (pdmk_fma_peak)",
+                          "algorithmic_flop_per_launch": near_flop_plain,
+                          "stage_ms_median": {kk: med(plain_st, kk) for kk in stage_keys}},
+             "clocks": clk1.summary()}
     line = {"metric": METRIC, "value": value, "unit": "Mpts*RHS/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "uniform cube N=1e6 (seed 1), charges U[-1,1] minus mean, 6 digits, "
-                                   "n_per_leaf 300, nz 4, 1 RHS, plain FP64 path",
-                       "n_points": n, "rhs": 1, "n_digits": 6, "n_per_leaf": 300, "nz": 4,
+            "warmup": args.warmup, "ms_per_step": t_mixed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "uniform cube N=1e6 (seed 1), %d charge vectors U[-1,1] minus mean, "
+                                   "6 digits, n_per_leaf 300, nz 4, mixed-precision batched evaluate" % k,
+                       "n_points": n, "rhs": k, "n_digits": 6, "n_per_leaf": 300, "nz": 4,
                        "parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",
-                       "tree": {k: info[k] for k in ("n_all", "n_boxes", "n_levels", "n_target_leaves", "p",
-                                                     "n_pw", "device_bytes")},
-                       "tree_build_s": t_build},
-            "e2e": {"value": e2e_value, "unit": "Mpts*RHS/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
-                    "ms_per_step": t_e2e / args.steps * 1e3},
-            "gpu_launches": info["launches_per_evaluate"] * args.steps,
-            "roofline": roofline, "clocks": clk.summary()}
+                       "tree": {kk: info[kk] for kk in ("n_all", "n_boxes", "n_levels", "n_target_leaves",
+                                                         "p", "n_pw", "device_bytes")},
+                       "tree_build_s": t_build,
+                       "precision": "FP32 near field (double-float coordinate differences, FP64 merge), FP32 "
+                                    "transforms, FP64 far field and accumulation"},
+            "rel_l2_vs_fp64": max(errs),
+            "mixed_vs_plain_fp64": value / plain_value,
+            "plain_fp64_single_rhs": plain,
+            "e2e": {"value": e2e_value, "unit": "Mpts*RHS/s", "h2d_bytes_per_step": 8 * n * k,
+                    "d2h_bytes_per_step": 4 * n * k, "ms_per_step": t_e2e / args.steps * 1e3,
+                    "api": "pdmk_evaluate_multi_float (pinned host buffers)"},
+            "gpu_launches": finfo["launches_last_multi"] * args.steps,
+            "roofline": roofline, "clocks": clk2.summary()}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, desc, _ = cpu_baseline(n, 3, threads)
         line["cpu_baseline"] = {"value": v, "unit": "Mpts*RHS/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    tree.close()
+    tree_d.close()
+    tree_f.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -258,6 +318,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=1000000)
+    ap.add_argument("--rhs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -70,22 +70,32 @@ int pdmk_evaluate_multi_float(void* h, int N, int k, const double* charges_Nxk, 
 int pdmk_evaluate_device_double(void* h, const double* charges_dev, double* pot_dev);
 int pdmk_evaluate_device_float(void* h, const double* charges_dev, float* pot_dev);
 
+/* k charge vectors on device buffers (Q_dev and pot_dev: N x k doubles,
+ * column-major).  mixed != 0 selects the mixed-precision path (FP32 near field
+ * and transforms, FP64 far field and accumulation); 0 the plain FP64 path.
+ * The float-tree variant always uses the mixed path.  Synchronous. */
+int pdmk_evaluate_multi_device_double(void* h, int k, const double* Q_dev, double* pot_dev, int mixed);
+int pdmk_evaluate_multi_device_float(void* h, int k, const double* Q_dev, double* pot_dev);
+
 /* The two parts of the potential in user order: the tree part (near field +
  * plane-wave levels - self term) and the periodic far field. */
 int pdmk_evaluate_parts_double(void* h, const double* charges, double* tree_part, double* far_part);
 
-/* Tree facts: out[0..11] = N, n_all (originals + images), boxes, levels,
+/* Tree facts: out[0..15] = N, n_all (originals + images), boxes, levels,
  * target leaves, expansion order p, plane waves per axis, kernel launches per
- * evaluate, device bytes, far-field modes (ms, mt, mu product), near-field
- * box pairs, plane-wave boxes. */
-int pdmk_info_double(void* h, int64_t* out12);
-int pdmk_info_float(void* h, int64_t* out12);
+ * single-RHS evaluate, device bytes, far-field modes (ms, mt, mu product),
+ * near-field box pairs, plane-wave boxes, kernel launches of the last
+ * multi-RHS evaluate, tree digit count, mixed path available (1/0), 0. */
+int pdmk_info_double(void* h, int64_t* out16);
+int pdmk_info_float(void* h, int64_t* out16);
 
-/* Stage times of the most recent evaluate of a double tree: out8[0..7] =
+/* Stage times of the most recent evaluate (multi-RHS: summed over its RHS
+ * blocks): out8[0..7] =
  * dmk_ms, near_ms (residual near-field kernel), nufft_ms, finalize_ms,
  * total_ms, near-field pairs after the reference's contact-geometry cull,
  * near-field pairs before it, residual polynomial length. */
 int pdmk_stage_times_double(void* h, double* out8);
+int pdmk_stage_times_float(void* h, double* out8);
 
 /* Measured FMA throughput of the current device in TFLOP/s (fp64 != 0: FP64,
  * else FP32), 2 flops per FMA; the denominator of CUDA-core rooflines. */

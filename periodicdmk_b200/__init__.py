@@ -27,8 +27,9 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_timed_double", "pdmk_evaluate_timed_float",
     "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
     "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
+    "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float",
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
-    "pdmk_stage_times_double", "pdmk_fma_peak", "pdmk_evaluate_device_noalloc_double", "pdmk_last_error",
+    "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_evaluate_device_noalloc_double", "pdmk_last_error",
 ]
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -63,11 +64,16 @@ def library():
     lib.pdmk_evaluate_device_double.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_evaluate_device_float.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_evaluate_parts_double.argtypes = [v, _D, _D, _D]
+    lib.pdmk_evaluate_multi_device_double.argtypes = [v, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.pdmk_evaluate_multi_device_double.restype = ctypes.c_int
+    lib.pdmk_evaluate_multi_device_float.argtypes = [v, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pdmk_evaluate_multi_device_float.restype = ctypes.c_int
     lib.pdmk_info_double.argtypes = [v, _I64]
     lib.pdmk_info_float.argtypes = [v, _I64]
     for f in ("pdmk_evaluate_double", "pdmk_evaluate_float", "pdmk_evaluate_timed_double",
               "pdmk_evaluate_timed_float", "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
-              "pdmk_evaluate_device_double", "pdmk_evaluate_device_float", "pdmk_evaluate_parts_double",
+              "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
+    "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float", "pdmk_evaluate_parts_double",
               "pdmk_info_double", "pdmk_info_float"):
         getattr(lib, f).restype = ctypes.c_int
     lib.pdmk_destroy_double.argtypes = [v]
@@ -80,6 +86,8 @@ def library():
     lib.pdmk_optimize_cubic_cover.restype = ctypes.c_int
     lib.pdmk_stage_times_double.argtypes = [v, _D]
     lib.pdmk_stage_times_double.restype = ctypes.c_int
+    lib.pdmk_stage_times_float.argtypes = [v, _D]
+    lib.pdmk_stage_times_float.restype = ctypes.c_int
     lib.pdmk_evaluate_device_noalloc_double.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_evaluate_device_noalloc_double.restype = ctypes.c_int
     lib.pdmk_fma_peak.argtypes = [ctypes.c_int, _D]
@@ -115,7 +123,8 @@ class PeriodicDMKTree:
     """
 
     INFO_KEYS = ["n_points", "n_all", "n_boxes", "n_levels", "n_target_leaves", "p", "n_pw",
-                 "launches_per_evaluate", "device_bytes", "far_modes", "near_pairs", "pw_boxes"]
+                 "launches_per_evaluate", "device_bytes", "far_modes", "near_pairs", "pw_boxes",
+                 "launches_last_multi", "n_digits_tree", "mixed_available", "reserved"]
 
     def __init__(self, cell, positions, n_digits=6, n_per_leaf=300, nz=4, precision="double"):
         if precision not in ("double", "float"):
@@ -204,6 +213,19 @@ class PeriodicDMKTree:
         rc = self._lib.pdmk_evaluate_device_noalloc_double(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(pot_ptr))
         self._check(rc, "pdmk_evaluate_device_noalloc_double")
 
+    def evaluate_multi_device(self, k, q_ptr, pot_ptr, mixed=None):
+        """k charge vectors on device buffers (N x k column-major doubles in and out).
+
+        mixed: True for the mixed-precision path, False for plain FP64 (double
+        trees only; float trees always use the mixed path)."""
+        if self.precision == "double":
+            rc = self._lib.pdmk_evaluate_multi_device_double(self._h, int(k), ctypes.c_void_p(q_ptr),
+                                                             ctypes.c_void_p(pot_ptr), 1 if mixed else 0)
+        else:
+            rc = self._lib.pdmk_evaluate_multi_device_float(self._h, int(k), ctypes.c_void_p(q_ptr),
+                                                            ctypes.c_void_p(pot_ptr))
+        self._check(rc, "pdmk_evaluate_multi_device")
+
     def evaluate_parts(self, charges):
         """(tree part, far-field part), both user order; double trees only."""
         if self.precision != "double":
@@ -216,7 +238,7 @@ class PeriodicDMKTree:
         return a, b
 
     def info(self):
-        out = np.zeros(12, dtype=np.int64)
+        out = np.zeros(16, dtype=np.int64)
         f = self._lib.pdmk_info_double if self.precision == "double" else self._lib.pdmk_info_float
         self._check(f(self._h, _ptr(out, _I64)), "pdmk_info")
         return dict(zip(self.INFO_KEYS, [int(x) for x in out]))
@@ -225,9 +247,10 @@ class PeriodicDMKTree:
                   "near_pairs_nominal", "near_ncoef"]
 
     def stage_times(self):
-        """Stage times of the most recent evaluate (double trees)."""
+        """Stage times of the most recent evaluate (multi-RHS: summed over RHS blocks)."""
         out = np.zeros(8)
-        self._check(self._lib.pdmk_stage_times_double(self._h, _ptr(out)), "pdmk_stage_times")
+        f = self._lib.pdmk_stage_times_double if self.precision == "double" else self._lib.pdmk_stage_times_float
+        self._check(f(self._h, _ptr(out)), "pdmk_stage_times")
         return dict(zip(self.STAGE_KEYS, out.tolist()))
 
     def close(self):

@@ -11,6 +11,7 @@
 #include <exception>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "impl.hpp"
@@ -68,16 +69,18 @@ int evaluate_impl(void* h, const double* q, Out* pot, double* timing4) {
     try {
         if (!q || !pot) throw std::invalid_argument("null charges or output");
         auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
-        const int n = t->n_points();
-        std::vector<double> qv(q, q + n);
-        pdmk::EvalTiming tm;
-        auto r = t->evaluate_timed(qv, tm);
-        for (int i = 0; i < n; ++i) pot[i] = (Out)r[i];
+        auto* dv = t->impl()->dev.get();
+        pdmkb::StageTimes st;
+        // Straight from the caller's buffers: no intermediate host copies.
+        if (std::is_same<Real, double>::value)
+            dv->evaluate_host(q, reinterpret_cast<double*>(pot), &st);
+        else
+            dv->evaluate_multi_host(q, 1, pot, /*pot_float=*/std::is_same<Out, float>::value, /*fp32=*/true, &st);
         if (timing4) {
-            timing4[0] = tm.nufft_ms;
-            timing4[1] = tm.dmk_ms;
-            timing4[2] = tm.direct_ms;
-            timing4[3] = tm.build_ms;
+            timing4[0] = st.nufft_ms;
+            timing4[1] = st.dmk_ms;
+            timing4[2] = st.direct_ms;
+            timing4[3] = 0.0;
         }
         return 0;
     } catch (const std::exception& e) {
@@ -93,15 +96,36 @@ int evaluate_multi_impl(void* h, int k, const double* q, Out* pot) {
     }
     try {
         if (!q || !pot) throw std::invalid_argument("null charges or output");
-        auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
-        const size_t n = (size_t)t->n_points();
         if (k <= 0) throw std::invalid_argument("k must be positive");
-        std::vector<double> qv(q, q + n * k);
-        auto r = t->evaluate_multi(qv, k);
-        for (size_t i = 0; i < n * k; ++i) pot[i] = (Out)r[i];
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
+        t->impl()->dev->evaluate_multi_host(q, k, pot, std::is_same<Out, float>::value,
+                                            /*fp32=*/std::is_same<Real, float>::value, nullptr);
         return 0;
     } catch (const std::exception& e) {
         return fail("pdmk_evaluate_multi", e);
+    }
+}
+
+template <typename Real>
+int stage_times_impl(void* h, double* out8) {
+    if (!h || !out8) {
+        set_error("pdmk_stage_times", "null handle or output");
+        return -1;
+    }
+    try {
+        auto* dv = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h)->impl()->dev.get();
+        const pdmkb::StageTimes t = dv->last_was_multi_ ? dv->last_multi_times() : dv->last_times();
+        out8[0] = t.dmk_ms;
+        out8[1] = t.near_ms;
+        out8[2] = t.nufft_ms;
+        out8[3] = t.finalize_ms;
+        out8[4] = t.dmk_ms + t.direct_ms + t.nufft_ms;
+        out8[5] = (double)dv->near_pairs_culled();
+        out8[6] = (double)dv->near_pairs_nominal();
+        out8[7] = (double)dv->near_coeffs();
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_stage_times", e);
     }
 }
 
@@ -129,7 +153,29 @@ int info_impl(void* h, int64_t* out) {
     out[9] = (int64_t)P.ms * P.mt * P.mu;
     out[10] = (int64_t)P.list1.size();
     out[11] = P.n_pw_exp;
+    out[12] = im->dev->multi_launches_;
+    out[13] = P.dp.n_digits_tree;
+    out[14] = im->dev->mixed_allowed() ? 1 : 0;
+    out[15] = 0;
     return 0;
+}
+
+template <typename Real>
+int multi_device_impl(void* h, int k, const double* Q, double* pot, bool fp32) {
+    if (!h) {
+        set_error("pdmk_evaluate_multi_device", "null handle");
+        return -1;
+    }
+    try {
+        if (!Q || !pot) throw std::invalid_argument("null device pointer");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h);
+        auto* dv = t->impl()->dev.get();
+        dv->evaluate_multi_device(Q, k, pot, fp32, nullptr);
+        PDMK_CUDA_CHECK(cudaStreamSynchronize(dv->stream()));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_multi_device", e);
+    }
 }
 
 }  // namespace
@@ -189,8 +235,16 @@ int pdmk_evaluate_device_float(void* h, const double* q_dev, float* pot_dev) {
         set_error("pdmk_evaluate_device", "null handle");
         return -1;
     }
-    set_error("pdmk_evaluate_device_float", "not available for this tree type");
+    set_error("pdmk_evaluate_device_float", "not available for this tree type: use pdmk_evaluate_multi_device_float");
     return -1;
+}
+
+int pdmk_evaluate_multi_device_double(void* h, int k, const double* Q_dev, double* pot_dev, int mixed) {
+    return multi_device_impl<double>(h, k, Q_dev, pot_dev, mixed != 0);
+}
+
+int pdmk_evaluate_multi_device_float(void* h, int k, const double* Q_dev, double* pot_dev) {
+    return multi_device_impl<float>(h, k, Q_dev, pot_dev, true);
 }
 
 int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, double* far_part) {
@@ -210,27 +264,8 @@ int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, doub
 
 int pdmk_info_double(void* h, int64_t* out) { return info_impl<double>(h, out); }
 
-int pdmk_stage_times_double(void* h, double* out8) {
-    if (!h || !out8) {
-        set_error("pdmk_stage_times", "null handle or output");
-        return -1;
-    }
-    try {
-        auto* dv = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h)->impl()->dev.get();
-        const pdmkb::StageTimes t = dv->last_times();
-        out8[0] = t.dmk_ms;
-        out8[1] = t.near_ms;
-        out8[2] = t.nufft_ms;
-        out8[3] = t.finalize_ms;
-        out8[4] = t.dmk_ms + t.direct_ms + t.nufft_ms;
-        out8[5] = (double)dv->near_pairs_culled();
-        out8[6] = (double)dv->near_pairs_nominal();
-        out8[7] = (double)dv->near_coeffs();
-        return 0;
-    } catch (const std::exception& e) {
-        return fail("pdmk_stage_times", e);
-    }
-}
+int pdmk_stage_times_double(void* h, double* out8) { return stage_times_impl<double>(h, out8); }
+int pdmk_stage_times_float(void* h, double* out8) { return stage_times_impl<float>(h, out8); }
 
 int pdmk_fma_peak(int fp64, double* tflops) {
     try {

@@ -54,7 +54,10 @@ std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_timed(const std::vector<
     if ((int)charges.size() != n_src_) throw std::invalid_argument("charges size != n_src");
     std::vector<double> pot(n_src_);
     pdmkb::StageTimes st;
-    p_->dev->evaluate_host(charges.data(), pot.data(), &st);
+    if (p_->single)
+        p_->dev->evaluate_multi_host(charges.data(), 1, pot.data(), /*pot_float=*/false, /*fp32=*/true, &st);
+    else
+        p_->dev->evaluate_host(charges.data(), pot.data(), &st);
     timing.dmk_ms = st.dmk_ms;
     timing.direct_ms = st.direct_ms;
     timing.nufft_ms = st.nufft_ms;
@@ -66,13 +69,9 @@ template <typename Real, int DIM>
 std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_multi(const std::vector<double>& charges, int k) {
     if (k <= 0 || (int64_t)charges.size() != (int64_t)n_src_ * k)
         throw std::invalid_argument("charges size != n_src * k");
-    std::vector<Real> out((size_t)n_src_ * k);
-    std::vector<double> pot(n_src_);
-    for (int c = 0; c < k; ++c) {
-        p_->dev->evaluate_host(charges.data() + (size_t)n_src_ * c, pot.data(), nullptr);
-        for (int i = 0; i < n_src_; ++i) out[(size_t)n_src_ * c + i] = (Real)pot[i];
-    }
-    return out;
+    std::vector<double> pot((size_t)n_src_ * k);
+    p_->dev->evaluate_multi_host(charges.data(), k, pot.data(), /*pot_float=*/false, /*fp32=*/p_->single, nullptr);
+    return std::vector<Real>(pot.begin(), pot.end());
 }
 
 template class PeriodicDMKTreeT<double, 3>;

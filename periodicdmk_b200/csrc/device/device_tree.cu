@@ -83,6 +83,7 @@ void DeviceTree::init(const Plan& P, int device) {
     for (auto& e : ev_) PDMK_CUDA_CHECK(cudaEventCreate(&e));
 
     n_ = P.n_src;
+    n_digits_ = P.dp.n_digits_tree;
     n_all_ = P.n_all;
     p_ = P.p;
     npw_ = P.n_pw;
@@ -602,6 +603,9 @@ DeviceTree::~DeviceTree() { release(); }
 void DeviceTree::release() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
+    multi_[0].reset();
+    multi_[1].reset();
+    if (stream_) cudaStreamSynchronize(stream_);
     if (plan_fwd_) cufftDestroy(plan_fwd_);
     if (plan_inv_) cufftDestroy(plan_inv_);
     for (void* p : allocs_) cudaFree(p);
@@ -721,6 +725,7 @@ StageTimes DeviceTree::last_times() {
 
 void DeviceTree::evaluate_device(const double* q_user_d, double* pot_user_d, StageTimes* times) {
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    last_was_multi_ = false;
     run(q_user_d, pot_user_d);
     if (times) *times = last_times();
 }

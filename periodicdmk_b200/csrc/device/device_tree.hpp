@@ -37,6 +37,19 @@ class DeviceTree {
     // Device buffers (N doubles each) on this tree's device; enqueued on stream_.
     // With times != null the call synchronises to read the stage events.
     void evaluate_device(const double* q_user_d, double* pot_user_d, StageTimes* times = nullptr);
+    // k charge vectors (N x k column-major, device buffers): potentials N x k.
+    // fp32: mixed-precision path, else FP64.  RHS processed in blocks sized to
+    // the free device memory (at most 64).  times (optional) sums the blocks.
+    void evaluate_multi_device(const double* Q_dev, int k, double* pot_dev, bool fp32, StageTimes* times = nullptr);
+    // Host buffers (pinned or pageable).  pot is double* or, with pot_float,
+    // float* (converted on the device before the copy back).
+    void evaluate_multi_host(const double* Q, int k, void* pot, bool pot_float, bool fp32,
+                             StageTimes* times = nullptr);
+    // Whether the mixed-precision path is used for this tree's digit count
+    // (it is for n_digits <= 6; above that the FP64 path runs).
+    bool mixed_allowed() const { return n_digits_ <= 6; }
+    // Stage times of the last multi-RHS evaluate (summed over RHS blocks).
+    StageTimes last_multi_times() const { return last_multi_; }
     // Same as evaluate_device, but the transform scratch is the library's fixed
     // static device array instead of the tree's buffers, and nothing is
     // allocated; synchronous.  Defined in noalloc.cu.
@@ -55,6 +68,22 @@ class DeviceTree {
     size_t device_bytes() const { return bytes_; }
 
   private:
+    struct MultiState;
+    struct MultiStateDeleter {
+        void operator()(MultiState* m) const;
+    };
+    int multi_block(int k, bool fp32) const;
+    MultiState& multi_state(int kb, bool fp32);
+    template <typename T>
+    void run_multi_block(MultiState& m, const double* Q, int kvalid, double* pot_user);
+    std::unique_ptr<MultiState, MultiStateDeleter> multi_[2];
+    StageTimes last_multi_{};
+
+  public:
+    bool last_was_multi_ = false;
+    int multi_launches_ = 0;  // kernels launched by the last multi-RHS evaluate
+
+  private:
     void init(const Plan& P, int device);
     void release();
     template <typename T>
@@ -64,6 +93,7 @@ class DeviceTree {
     void run(const double* q_user_d, double* pot_user_d);
 
     int device_ = 0;
+    int n_digits_ = 6;
     int n_ = 0, n_all_ = 0, p_ = 0, npw_ = 0, npw2_ = 0, M_ = 0;
     size_t bytes_ = 0;
     int launches_ = 0;

@@ -481,6 +481,8 @@ __global__ void __launch_bounds__(128) k_spread(NufftArgs a) {
     const int e = blockIdx.x;
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
     const int4 org = a.sub_origin[e], ext = a.sub_extent[e];
+    const double* __restrict__ qs = a.q_sorted + blockIdx.z * a.rhs_q_stride;
+    double* __restrict__ grid = a.grid + blockIdx.z * a.rhs_grid_stride;
     const int jk = blockIdx.y * blockDim.x + threadIdx.x;
     const bool active = jk < ext.y * ext.z;
     const int kk = jk % max(ext.z, 1), jj = jk / max(ext.z, 1);
@@ -507,7 +509,7 @@ __global__ void __launch_bounds__(128) k_spread(NufftArgs a) {
                 }
                 sBy[s] = l0.y - org.y;
                 sBz[s] = l0.z - org.z;
-                sQ[s] = a.q_sorted[t0 + base + s];
+                sQ[s] = qs[t0 + base + s];
             }
         }
         __syncthreads();
@@ -527,7 +529,7 @@ __global__ void __launch_bounds__(128) k_spread(NufftArgs a) {
     for (int i = 0; i < NX; ++i) {
         if (i < ext.x && acc[i] != 0.0) {
             const int gx = wrapi(org.x + i, a.n1);
-            atomicAdd(a.grid + ((int64_t)gx * a.n2 + gy) * a.n3 + gz, acc[i]);
+            atomicAdd(grid + ((int64_t)gx * a.n2 + gy) * a.n3 + gz, acc[i]);
         }
     }
 }
@@ -537,6 +539,8 @@ __global__ void __launch_bounds__(128) k_interp(NufftArgs a) {
     const int e = blockIdx.x;
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
     const double hw = 0.5 * W;
+    const double* __restrict__ grid = a.grid + blockIdx.z * a.rhs_grid_stride;
+    double* __restrict__ far = a.far + blockIdx.z * a.rhs_far_stride;
     for (int t = threadIdx.x; t < nt; t += blockDim.x) {
         const double4 tt = a.pt_t[t0 + t];
         const int4 l0 = a.pt_l0[t0 + t];
@@ -553,7 +557,7 @@ __global__ void __launch_bounds__(128) k_interp(NufftArgs a) {
         double u = 0.0;
 #pragma unroll 1
         for (int ia = 0; ia < W; ++ia) {
-            const double* gx = a.grid + (int64_t)wrapi(l0.x + ia, a.n1) * a.n2 * a.n3;
+            const double* gx = grid + (int64_t)wrapi(l0.x + ia, a.n1) * a.n2 * a.n3;
             double sa = 0.0;
 #pragma unroll
             for (int ib = 0; ib < W; ++ib) {
@@ -565,26 +569,27 @@ __global__ void __launch_bounds__(128) k_interp(NufftArgs a) {
             }
             u = fma(kx[ia], sa, u);
         }
-        a.far[t0 + t] = u;
+        far[t0 + t] = u;
     }
 }
 
-__global__ void k_multiply(cd* spec, const double* mult, int64_t n) {
+__global__ void k_multiply(cd* spec, const double* mult, int64_t n, int64_t total) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double m = mult[i];
+    if (i >= total) return;
+    const double m = mult[i % n];
     cd v = spec[i];
     spec[i] = cd{v.x * m, v.y * m};
 }
 
-void launch_multiply(cd* spec, const double* mult, int64_t n, cudaStream_t s) {
-    if (n <= 0) return;
-    k_multiply<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, mult, n);
+void launch_multiply(cd* spec, const double* mult, int64_t n, cudaStream_t s, int nrhs) {
+    if (n <= 0 || nrhs <= 0) return;
+    const int64_t total = n * nrhs;
+    k_multiply<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(spec, mult, n, total);
 }
 
 template <int W>
-static void launch_spread_w(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s) {
-    const dim3 grid(a.n_leaves, (max_jk + 127) / 128);
+static void launch_spread_w(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s, int nrhs) {
+    const dim3 grid(a.n_leaves, (max_jk + 127) / 128, nrhs);
     if (max_ex <= 16)
         k_spread<W, 16><<<grid, 128, 0, s>>>(a);
     else if (max_ex <= 32)
@@ -595,11 +600,11 @@ static void launch_spread_w(const NufftArgs& a, int max_jk, int max_ex, cudaStre
         throw std::runtime_error("NUFFT leaf subgrid too large");
 }
 
-void launch_spread(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s) {
-    if (a.n_leaves <= 0) return;
+void launch_spread(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s, int nrhs) {
+    if (a.n_leaves <= 0 || nrhs <= 0) return;
     switch (a.w) {
 #define PDMK_W_CASE(W) \
-    case W: launch_spread_w<W>(a, max_jk, max_ex, s); break;
+    case W: launch_spread_w<W>(a, max_jk, max_ex, s, nrhs); break;
         PDMK_W_CASE(4) PDMK_W_CASE(5) PDMK_W_CASE(6) PDMK_W_CASE(7) PDMK_W_CASE(8) PDMK_W_CASE(9)
         PDMK_W_CASE(10) PDMK_W_CASE(11) PDMK_W_CASE(12) PDMK_W_CASE(13) PDMK_W_CASE(14)
 #undef PDMK_W_CASE
@@ -607,11 +612,12 @@ void launch_spread(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s) {
     }
 }
 
-void launch_interp(const NufftArgs& a, cudaStream_t s) {
-    if (a.n_leaves <= 0) return;
+void launch_interp(const NufftArgs& a, cudaStream_t s, int nrhs) {
+    if (a.n_leaves <= 0 || nrhs <= 0) return;
+    const dim3 grid(a.n_leaves, 1, nrhs);
     switch (a.w) {
 #define PDMK_W_CASE(W) \
-    case W: k_interp<W><<<a.n_leaves, 128, 0, s>>>(a); break;
+    case W: k_interp<W><<<grid, 128, 0, s>>>(a); break;
         PDMK_W_CASE(4) PDMK_W_CASE(5) PDMK_W_CASE(6) PDMK_W_CASE(7) PDMK_W_CASE(8) PDMK_W_CASE(9)
         PDMK_W_CASE(10) PDMK_W_CASE(11) PDMK_W_CASE(12) PDMK_W_CASE(13) PDMK_W_CASE(14)
 #undef PDMK_W_CASE

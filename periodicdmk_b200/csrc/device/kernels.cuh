@@ -116,11 +116,15 @@ struct NufftArgs {
     int n1, n2, n3;
     int w;
     double es_beta;
+    // RHS batching (blockIdx.z = RHS index): element strides between RHS of
+    // q_sorted, grid and far; 0 for a single RHS.
+    int64_t rhs_q_stride = 0, rhs_grid_stride = 0, rhs_far_stride = 0;
 };
 void launch_nufft_gather_q(const int* trg_perm, const double* q_user, double* q_sorted, int n, cudaStream_t s);
-void launch_spread(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s);
-void launch_interp(const NufftArgs& a, cudaStream_t s);
-void launch_multiply(cd* spec, const double* mult, int64_t n, cudaStream_t s);
+void launch_spread(const NufftArgs& a, int max_jk, int max_ex, cudaStream_t s, int nrhs = 1);
+void launch_interp(const NufftArgs& a, cudaStream_t s, int nrhs = 1);
+// spec[c * n + i] *= mult[i] for c < nrhs
+void launch_multiply(cd* spec, const double* mult, int64_t n, cudaStream_t s, int nrhs = 1);
 
 }  // namespace dev
 }  // namespace pdmkb

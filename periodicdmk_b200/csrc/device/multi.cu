@@ -1,0 +1,923 @@
+// Multi-RHS evaluate: k charge vectors on one tree, in RHS blocks of kb.
+//
+// Same stages as the single-RHS path (kernels.cu), with an RHS dimension:
+//   charges    T[n_all * kb]            source-major, RHS fastest (near field reads a source's kb charges)
+//   proxy      T[slots * kb * p^3]      (slot, rhs) tensors contiguous -> transforms batch over (box, rhs)
+//   plane wave complex<T>[slots * kb * M]
+//   potentials double[kb * N]           RHS-major (coalesced per RHS)
+// T = double: plain FP64.  T = float: mixed precision -- FP32 Chebyshev moments,
+// transforms, shifts and leaf evaluation; FP32 near field on double-float
+// coordinate differences with per-box FP32 partial sums merged in FP64; FP64
+// far field (NUFFT), self term and final accumulation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+#include "device_tree.hpp"
+
+namespace pdmkb {
+namespace dev {
+
+struct cf {  // complex float
+    float x, y;
+};
+
+template <>
+__device__ __forceinline__ float zero<float>() { return 0.0f; }
+template <>
+__device__ __forceinline__ cf zero<cf>() { return {0.0f, 0.0f}; }
+__device__ __forceinline__ float mac(float m, float x, float acc) { return fmaf(m, x, acc); }
+__device__ __forceinline__ cf mac(cf m, float x, cf acc) { return {fmaf(m.x, x, acc.x), fmaf(m.y, x, acc.y)}; }
+__device__ __forceinline__ cf mac(cf m, cf x, cf acc) {
+    return {fmaf(m.x, x.x, fmaf(-m.y, x.y, acc.x)), fmaf(m.x, x.y, fmaf(m.y, x.x, acc.y))};
+}
+
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<double> {
+    using type = cd;
+};
+template <>
+struct Cplx<float> {
+    using type = cf;
+};
+
+// ---------------------------------------------------------------------------
+// conversions and gathers
+// ---------------------------------------------------------------------------
+__global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+// double-float split of positions: hi = fl(x), lo = fl(x - hi); .w of hi keeps the
+// point's fourth field (self weight for targets) rounded to float.
+__global__ void k_split_positions(const double4* __restrict__ in, float4* __restrict__ hi, float4* __restrict__ lo,
+                                  int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = in[i];
+    const float hx = (float)p.x, hy = (float)p.y, hz = (float)p.z;
+    hi[i] = make_float4(hx, hy, hz, (float)p.w);
+    lo[i] = make_float4((float)(p.x - (double)hx), (float)(p.y - (double)hy), (float)(p.z - (double)hz), 0.0f);
+}
+
+template <typename T>
+__global__ void k_gather_src_m(T* __restrict__ src_q, const int* __restrict__ idx, const double* __restrict__ Q,
+                               int64_t n_all, int64_t N, int kb, int kvalid) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_all * kb) return;
+    const int64_t s = i / kb;
+    const int c = (int)(i % kb);
+    src_q[i] = c < kvalid ? (T)Q[(int64_t)c * N + idx[s]] : T(0);
+}
+
+__global__ void k_gather_trg_m(double* __restrict__ q_t, const int* __restrict__ perm, const double* __restrict__ Q,
+                               int64_t N, int kb, int kvalid) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * kb) return;
+    const int c = (int)(i / N);
+    const int64_t t = i % N;
+    q_t[i] = c < kvalid ? Q[(int64_t)c * N + perm[t]] : 0.0;
+}
+
+__global__ void k_finalize_m(const double* __restrict__ pot, const double* __restrict__ far,
+                             const double4* __restrict__ trg, const int* __restrict__ perm,
+                             const double* __restrict__ q_t, double* __restrict__ out, int64_t N, int kvalid) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * kvalid) return;
+    const int64_t c = i / N, t = i % N;
+    out[c * N + perm[t]] = pot[i] + far[i] - trg[t].w * q_t[i];
+}
+
+// ---------------------------------------------------------------------------
+// proxy moments: grid (centres, jk chunks, rhs)
+// ---------------------------------------------------------------------------
+template <typename T, int P>
+__global__ void __launch_bounds__(128)
+    k_c2proxy_m(C2ProxyArgs a, const T* __restrict__ src_q, T* __restrict__ proxy_up, int kb) {
+    constexpr int TS = 32;
+    __shared__ T sx[TS][P], sy[TS][P], sz[TS][P];
+    const int e = blockIdx.x, c = blockIdx.z;
+    const int jk = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool active = jk < P * P;
+    const int j = jk % P, k = jk / P;
+    T acc[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) acc[i] = T(0);
+    const double4 cs = a.center_scale[e];
+    for (int r = a.rng_start[e]; r < a.rng_start[e + 1]; ++r) {
+        const int s0 = a.src_start[r], ns = a.src_count[r];
+        for (int base = 0; base < ns; base += TS) {
+            const int nt = min(TS, ns - base);
+            __syncthreads();
+            for (int task = threadIdx.x; task < 3 * TS; task += blockDim.x) {
+                const int si = task % TS, d = task / TS;
+                T* dst = d == 0 ? sx[si] : (d == 1 ? sy[si] : sz[si]);
+                if (si < nt) {
+                    const double4 pt = a.src[s0 + base + si];
+                    const T x = (T)((d == 0 ? pt.x - cs.x : (d == 1 ? pt.y - cs.y : pt.z - cs.z)) * cs.w);
+                    const T mult = d == 2 ? src_q[(int64_t)(s0 + base + si) * kb + c] : T(1);
+                    T t0 = T(1), t1 = x;
+                    dst[0] = mult;
+                    if (P > 1) dst[1] = mult * x;
+                    for (int n = 2; n < P; ++n) {
+                        const T t2 = T(2) * x * t1 - t0;
+                        dst[n] = mult * t2;
+                        t0 = t1;
+                        t1 = t2;
+                    }
+                } else {
+                    for (int n = 0; n < P; ++n) dst[n] = T(0);
+                }
+            }
+            __syncthreads();
+            if (active) {
+                for (int s = 0; s < nt; ++s) {
+                    const T f = sy[s][j] * sz[s][k];
+#pragma unroll
+                    for (int i = 0; i < P; ++i) acc[i] = fma(f, sx[s][i], acc[i]);
+                }
+            }
+        }
+    }
+    if (active) {
+        T* out = proxy_up + ((int64_t)a.slot[e] * kb + c) * (P * P * P) + (int64_t)P * jk;
+#pragma unroll
+        for (int i = 0; i < P; ++i) out[i] += acc[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// batched contraction with an RHS dimension:
+// out[r + R*a] (op)= sum_i M[a + na*i] * in[i + ni*r] for entry ge = e0 + blockIdx.x,
+// box eb = ge / rhs, rhs ec = ge % rhs.
+// in = in_base + (in_off ? in_off[eb]*rhs + ec*in_unit : blockIdx.x*in_stride), same for out;
+// M = mat_base + (mat_off ? mat_off[eb] : 0).
+// ---------------------------------------------------------------------------
+struct ContractM {
+    const void* in;
+    const int64_t* in_off;
+    int64_t in_stride, in_unit;
+    void* out;
+    const int64_t* out_off;
+    int64_t out_stride, out_unit;
+    const void* mat;
+    const int64_t* mat_off;
+    int ni, na, R, n_entries, rhs;
+    int64_t e0;
+    int mode;
+    double scale;
+};
+
+template <typename TO, typename TA>
+__device__ __forceinline__ void store_m(TO* p, TA v, int mode, double scale);
+template <>
+__device__ __forceinline__ void store_m<double, double>(double* p, double v, int mode, double scale) {
+    if (mode == kStore) *p = v; else if (mode == kAdd) *p += v; else *p += scale * v;
+}
+template <>
+__device__ __forceinline__ void store_m<double, cd>(double* p, cd v, int mode, double scale) {
+    if (mode == kStore) *p = v.x; else if (mode == kAdd) *p += v.x; else *p += scale * v.x;
+}
+template <>
+__device__ __forceinline__ void store_m<cd, cd>(cd* p, cd v, int mode, double) {
+    if (mode == kStore) *p = v; else { cd o = *p; *p = cd{o.x + v.x, o.y + v.y}; }
+}
+template <>
+__device__ __forceinline__ void store_m<float, float>(float* p, float v, int mode, double scale) {
+    if (mode == kStore) *p = v; else if (mode == kAdd) *p += v; else *p += (float)scale * v;
+}
+template <>
+__device__ __forceinline__ void store_m<float, cf>(float* p, cf v, int mode, double scale) {
+    if (mode == kStore) *p = v.x; else if (mode == kAdd) *p += v.x; else *p += (float)scale * v.x;
+}
+template <>
+__device__ __forceinline__ void store_m<cf, cf>(cf* p, cf v, int mode, double) {
+    if (mode == kStore) *p = v; else { cf o = *p; *p = cf{o.x + v.x, o.y + v.y}; }
+}
+
+template <typename TI, typename TM, typename TO, int RT, int AB>
+__global__ void __launch_bounds__(256) k_contract_m(ContractM a) {
+    extern __shared__ __align__(16) unsigned char smem_m[];
+    using TA = decltype(mac(TM(), TI(), TM()));
+    const int ni = a.ni, na = a.na, R = a.R;
+    const int e = blockIdx.x, r0 = blockIdx.y * RT;
+    const int64_t ge = a.e0 + e;
+    const int rhs = a.rhs > 0 ? a.rhs : 1;
+    const int64_t eb = ge / rhs, ec = ge % rhs;
+    TM* sM = reinterpret_cast<TM*>(smem_m);
+    const size_t moff = ((size_t)na * ni * sizeof(TM) + 15) / 16 * 16;
+    TI* sIn = reinterpret_cast<TI*>(smem_m + moff);
+    const TI* in = reinterpret_cast<const TI*>(a.in) + (a.in_off ? a.in_off[eb] * rhs + ec * a.in_unit : (int64_t)e * a.in_stride);
+    TO* out = reinterpret_cast<TO*>(a.out) + (a.out_off ? a.out_off[eb] * rhs + ec * a.out_unit : (int64_t)e * a.out_stride);
+    const TM* mat = reinterpret_cast<const TM*>(a.mat) + (a.mat_off ? a.mat_off[eb] : 0);
+    for (int idx = threadIdx.x; idx < na * ni; idx += blockDim.x) sM[idx] = mat[idx];
+    const int nr = min(RT, R - r0);
+    const TI* inb = in + (int64_t)ni * r0;
+    for (int idx = threadIdx.x; idx < ni * nr; idx += blockDim.x) {
+        const int i = idx % ni, rr = idx / ni;
+        sIn[rr + RT * i] = inb[idx];
+    }
+    __syncthreads();
+    const int rr = threadIdx.x % RT, ag = threadIdx.x / RT, nag = blockDim.x / RT;
+    if (rr >= nr) return;
+    for (int a0 = ag * AB; a0 < na; a0 += nag * AB) {
+        TA acc[AB];
+#pragma unroll
+        for (int b = 0; b < AB; ++b) acc[b] = zero<TA>();
+        for (int i = 0; i < ni; ++i) {
+            const TI x = sIn[rr + RT * i];
+#pragma unroll
+            for (int b = 0; b < AB; ++b)
+                if (a0 + b < na) acc[b] = mac(sM[a0 + b + na * i], x, acc[b]);
+        }
+#pragma unroll
+        for (int b = 0; b < AB; ++b)
+            if (a0 + b < na) store_m<TO, TA>(out + (r0 + rr) + (int64_t)R * (a0 + b), acc[b], a.mode, a.scale);
+    }
+}
+
+template <typename TI, typename TM, typename TO>
+void launch_contract_m(const ContractM& a, cudaStream_t s) {
+    constexpr int RT = 32, AB = 4;
+    if (a.n_entries <= 0) return;
+    const size_t smem = ((size_t)a.na * a.ni * sizeof(TM) + 15) / 16 * 16 + (size_t)a.ni * RT * sizeof(TI);
+    static bool configured = false;
+    if (!configured) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_contract_m<TI, TM, TO, RT, AB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        configured = true;
+    }
+    if (smem > 200 * 1024) throw std::runtime_error("contraction tile exceeds shared memory");
+    const dim3 grid(a.n_entries, (a.R + RT - 1) / RT);
+    k_contract_m<TI, TM, TO, RT, AB><<<grid, 256, smem, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// plane-wave shift: grid (boxes in chunk, mode chunks, rhs)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_shift_m(const typename Cplx<T>::type* __restrict__ pw_out,
+                                                 const T* __restrict__ shift, typename Cplx<T>::type* __restrict__ pw_in,
+                                                 int M, const int* __restrict__ term_start,
+                                                 const int* __restrict__ term_slot, const int* __restrict__ term_stencil,
+                                                 int kb, int e0) {
+    using C = typename Cplx<T>::type;
+    const int e = blockIdx.x, c = blockIdx.z;
+    const int m = blockIdx.y * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    T ar = T(0), ai = T(0);
+    for (int t = term_start[e0 + e]; t < term_start[e0 + e + 1]; ++t) {
+        const C v = pw_out[((int64_t)term_slot[t] * kb + c) * M + m];
+        const T* sh = shift + (int64_t)term_stencil[t] * 2 * M;
+        const T sr = sh[m], si = sh[M + m];
+        ar = fma(v.x, sr, fma(-v.y, si, ar));
+        ai = fma(v.x, si, fma(v.y, sr, ai));
+    }
+    pw_in[((int64_t)e * kb + c) * M + m] = C{ar, ai};
+}
+
+// ---------------------------------------------------------------------------
+// proxy -> leaf targets: grid (leaves, 1, rhs)
+// ---------------------------------------------------------------------------
+template <typename T, int P>
+__global__ void __launch_bounds__(128)
+    k_eval_m(EvalArgs a, const T* __restrict__ proxy_down, double* __restrict__ pot, int64_t N, int kb) {
+    __shared__ T slab[P * P];
+    const int e = blockIdx.x, c = blockIdx.z;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const double4 cs = a.center_scale[e];
+    const T* C = proxy_down + ((int64_t)a.slot[e] * kb + c) * (P * P * P);
+    double* potc = pot + (int64_t)c * N;
+    for (int base = 0; base < nt; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const bool act = t < nt;
+        T tx[P];
+        T y = T(0), z = T(0);
+        {
+            T x = T(0);
+            if (act) {
+                const double4 pt = a.trg[t0 + t];
+                x = (T)((pt.x - cs.x) * cs.w);
+                y = (T)((pt.y - cs.y) * cs.w);
+                z = (T)((pt.z - cs.z) * cs.w);
+            }
+            tx[0] = T(1);
+            if (P > 1) tx[1] = x;
+#pragma unroll
+            for (int n = 2; n < P; ++n) tx[n] = T(2) * x * tx[n - 1] - tx[n - 2];
+        }
+        T acc = T(0);
+        T za = T(1), zb = z;
+        for (int k = 0; k < P; ++k) {
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < P * P; idx += blockDim.x) slab[idx] = C[(int64_t)k * P * P + idx];
+            __syncthreads();
+            T ya = T(1), yb = y, sk = T(0);
+            for (int j = 0; j < P; ++j) {
+                T r = T(0);
+#pragma unroll
+                for (int i = 0; i < P; ++i) r = fma(slab[i + P * j], tx[i], r);
+                sk = fma(ya, r, sk);
+                const T yn = T(2) * y * yb - ya;
+                ya = yb;
+                yb = yn;
+            }
+            acc = fma(za, sk, acc);
+            const T zn = T(2) * z * zb - za;
+            za = zb;
+            zb = zn;
+        }
+        if (act) potc[t0 + t] += (double)acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// residual near field with an RHS block of KB per pass
+// ---------------------------------------------------------------------------
+struct NearM {
+    const int* trg_start;
+    const int* trg_count;
+    const int* pair_start;
+    const int* pair_src_start;
+    const int* pair_src_count;
+    const double* pair_bsize;
+    double coef[32];
+    int n_leaves;
+    int64_t N;
+    int kb;
+};
+
+// FP64: positions double4, charges double[s * kb + c]
+template <int NC, int KB>
+__global__ void __launch_bounds__(128) k_near_m64(NearM a, const double4* __restrict__ trg,
+                                                  const double4* __restrict__ src, const double* __restrict__ src_q,
+                                                  double* __restrict__ pot) {
+    constexpr int TPT = 2;
+    __shared__ double4 ss[128];
+    __shared__ double sq[128][KB];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    double c[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) c[i] = a.coef[i];
+    for (int cb = 0; cb < a.kb; cb += KB) {
+        for (int base = 0; base < nt; base += TPT * 128) {
+            double4 tp[TPT];
+            double acc[TPT][KB];
+#pragma unroll
+            for (int u = 0; u < TPT; ++u) {
+                const int t = base + threadIdx.x + u * 128;
+                tp[u] = t < nt ? trg[t0 + t] : make_double4(1e300, 1e300, 1e300, 0.0);
+#pragma unroll
+                for (int q = 0; q < KB; ++q) acc[u][q] = 0.0;
+            }
+            for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
+                const int s0 = a.pair_src_start[pr], ns = a.pair_src_count[pr];
+                const double b = a.pair_bsize[pr];
+                const double d2max = b * b, rsc = 2.0 / b, cen = -0.5 * b;
+                for (int sb = 0; sb < ns; sb += 128) {
+                    __syncthreads();
+                    const int js = sb + threadIdx.x;
+                    if (js < ns) {
+                        ss[threadIdx.x] = src[s0 + js];
+#pragma unroll
+                        for (int q = 0; q < KB; ++q)
+                            sq[threadIdx.x][q] = (cb + q < a.kb) ? src_q[(int64_t)(s0 + js) * a.kb + cb + q] : 0.0;
+                    }
+                    __syncthreads();
+                    const int m = min(128, ns - sb);
+                    for (int j = 0; j < m; ++j) {
+                        const double4 y = ss[j];
+#pragma unroll
+                        for (int u = 0; u < TPT; ++u) {
+                            const double dx = tp[u].x - y.x, dy = tp[u].y - y.y, dz = tp[u].z - y.z;
+                            const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                            if (r2 > 1e-30 && r2 < d2max) {
+                                const double rinv = rsqrt_nr(r2);
+                                const double x = fma(r2, rinv, cen) * rsc;
+                                double pv = c[NC - 1];
+#pragma unroll
+                                for (int i = NC - 2; i >= 0; --i) pv = fma(pv, x, c[i]);
+                                const double w = pv * rinv;
+#pragma unroll
+                                for (int q = 0; q < KB; ++q) acc[u][q] = fma(w, sq[j][q], acc[u][q]);
+                            }
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < TPT; ++u) {
+                const int t = base + threadIdx.x + u * 128;
+                if (t < nt)
+#pragma unroll
+                    for (int q = 0; q < KB; ++q)
+                        if (cb + q < a.kb) pot[(int64_t)(cb + q) * a.N + t0 + t] += acc[u][q];
+            }
+        }
+    }
+}
+
+// FP32: double-float positions, FP32 pair arithmetic, per-box FP32 partial
+// sums merged into FP64 accumulators.
+template <int NC, int KB>
+__global__ void __launch_bounds__(128) k_near_m32(NearM a, const float4* __restrict__ trg_hi,
+                                                  const float4* __restrict__ trg_lo, const float4* __restrict__ src_hi,
+                                                  const float4* __restrict__ src_lo, const float* __restrict__ src_q,
+                                                  double* __restrict__ pot) {
+    constexpr int TPT = 2;
+    __shared__ float4 sh[128], sl[128];
+    __shared__ float sq[128][KB];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    float c[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) c[i] = (float)a.coef[i];
+    for (int cb = 0; cb < a.kb; cb += KB) {
+        for (int base = 0; base < nt; base += TPT * 128) {
+            float4 th[TPT], tl[TPT];
+            double acc[TPT][KB];
+#pragma unroll
+            for (int u = 0; u < TPT; ++u) {
+                const int t = base + threadIdx.x + u * 128;
+                th[u] = t < nt ? trg_hi[t0 + t] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                tl[u] = t < nt ? trg_lo[t0 + t] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < KB; ++q) acc[u][q] = 0.0;
+            }
+            for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
+                const int s0 = a.pair_src_start[pr], ns = a.pair_src_count[pr];
+                const double bd = a.pair_bsize[pr];
+                const float d2max = (float)(bd * bd), rsc = (float)(2.0 / bd), cen = (float)(-0.5 * bd);
+                float part[TPT][KB];
+#pragma unroll
+                for (int u = 0; u < TPT; ++u)
+#pragma unroll
+                    for (int q = 0; q < KB; ++q) part[u][q] = 0.f;
+                for (int sb = 0; sb < ns; sb += 128) {
+                    __syncthreads();
+                    const int js = sb + threadIdx.x;
+                    if (js < ns) {
+                        sh[threadIdx.x] = src_hi[s0 + js];
+                        sl[threadIdx.x] = src_lo[s0 + js];
+#pragma unroll
+                        for (int q = 0; q < KB; ++q)
+                            sq[threadIdx.x][q] = (cb + q < a.kb) ? src_q[(int64_t)(s0 + js) * a.kb + cb + q] : 0.f;
+                    }
+                    __syncthreads();
+                    const int m = min(128, ns - sb);
+                    for (int j = 0; j < m; ++j) {
+                        const float4 yh = sh[j], yl = sl[j];
+#pragma unroll
+                        for (int u = 0; u < TPT; ++u) {
+                            const float dx = (th[u].x - yh.x) + (tl[u].x - yl.x);
+                            const float dy = (th[u].y - yh.y) + (tl[u].y - yl.y);
+                            const float dz = (th[u].z - yh.z) + (tl[u].z - yl.z);
+                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            if (r2 > 1e-30f && r2 < d2max) {
+                                const float rinv = rsqrtf(r2);
+                                const float x = fmaf(r2, rinv, cen) * rsc;
+                                float pv = c[NC - 1];
+#pragma unroll
+                                for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, c[i]);
+                                const float w = pv * rinv;
+#pragma unroll
+                                for (int q = 0; q < KB; ++q) part[u][q] = fmaf(w, sq[j][q], part[u][q]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < TPT; ++u)
+#pragma unroll
+                    for (int q = 0; q < KB; ++q) acc[u][q] += (double)part[u][q];
+            }
+#pragma unroll
+            for (int u = 0; u < TPT; ++u) {
+                const int t = base + threadIdx.x + u * 128;
+                if (t < nt)
+#pragma unroll
+                    for (int q = 0; q < KB; ++q)
+                        if (cb + q < a.kb) pot[(int64_t)(cb + q) * a.N + t0 + t] += acc[u][q];
+            }
+        }
+    }
+}
+
+template <int KB>
+static void launch_near_m64_kb(const NearM& a, const double4* trg, const double4* src, const double* q, double* pot,
+                               int nc, cudaStream_t s) {
+    switch (nc) {
+#define C64(NC) case NC: k_near_m64<NC, KB><<<a.n_leaves, 128, 0, s>>>(a, trg, src, q, pot); break;
+        C64(5) C64(6) C64(9) C64(11) C64(12) C64(15) C64(17) C64(18) C64(22) C64(23) C64(25)
+#undef C64
+        default: throw std::runtime_error("unsupported residual polynomial length");
+    }
+}
+
+template <int KB>
+static void launch_near_m32_kb(const NearM& a, const float4* th, const float4* tl, const float4* sh,
+                               const float4* sl, const float* q, double* pot, int nc, cudaStream_t s) {
+    switch (nc) {
+#define C32(NC) case NC: k_near_m32<NC, KB><<<a.n_leaves, 128, 0, s>>>(a, th, tl, sh, sl, q, pot); break;
+        C32(5) C32(6) C32(9) C32(11) C32(12) C32(15) C32(17) C32(18) C32(22) C32(23) C32(25)
+#undef C32
+        default: throw std::runtime_error("unsupported residual polynomial length");
+    }
+}
+
+}  // namespace dev
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using dev::cd;
+using dev::cf;
+
+struct DeviceTree::MultiState {
+    bool fp32 = false;
+    int kb = 0;
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    void* src_q = nullptr;
+    void* proxy_up = nullptr;
+    void* proxy_down = nullptr;
+    void* pw_out = nullptr;
+    void* s1 = nullptr;
+    void* s2 = nullptr;
+    void* pw_in = nullptr;
+    int64_t scratch_bytes = 0;
+    double* pot = nullptr;
+    double* far = nullptr;
+    double* q_t = nullptr;
+    double* grid = nullptr;
+    cd* spec = nullptr;
+    cufftHandle fwd = 0, inv = 0;
+    // FP32 copies of tables and positions
+    float* c2p = nullptr;
+    float* p2c = nullptr;
+    struct Lev {
+        cf *poly2pw = nullptr, *poly2pw_half = nullptr, *pw2polyT = nullptr, *pw2polyTw = nullptr;
+        float* shift = nullptr;
+    };
+    std::vector<Lev> lev;
+    float4 *src_hi = nullptr, *src_lo = nullptr, *trg_hi = nullptr, *trg_lo = nullptr;
+
+    template <typename T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        const size_t b = std::max<size_t>(n, 1) * sizeof(T);
+        PDMK_CUDA_CHECK(cudaMalloc(&p, b));
+        allocs.push_back(p);
+        bytes += b;
+        return static_cast<T*>(p);
+    }
+    ~MultiState() {
+        if (fwd) cufftDestroy(fwd);
+        if (inv) cufftDestroy(inv);
+        for (void* p : allocs) cudaFree(p);
+    }
+};
+
+void DeviceTree::MultiStateDeleter::operator()(MultiState* m) const { delete m; }
+
+int DeviceTree::multi_block(int k, bool fp32) const {
+    // bytes per RHS of the per-RHS buffers
+    const int64_t ts = fp32 ? 4 : 8;
+    const int64_t ncoef = (int64_t)p_ * p_ * p_;
+    const int64_t per = ts * ((int64_t)n_all_ + (n_up_ + n_down_) * ncoef + 2 * n_pw_ * (int64_t)M_) +
+                        8 * 3 * (int64_t)n_ + 8 * n_grid_ + 16 * n_spec_;
+    size_t freeb = 0, totb = 0;
+    cudaMemGetInfo(&freeb, &totb);
+    const int64_t budget = (int64_t)(0.5 * (double)freeb) - ((int64_t)3 << 30);
+    int kb = (int)std::max<int64_t>(1, budget / std::max<int64_t>(per, 1));
+    kb = std::min(kb, 64);
+    kb = std::min(kb, std::max(1, k));
+    return kb;
+}
+
+DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
+    auto& slot = multi_[fp32 ? 1 : 0];
+    if (slot && slot->kb == kb) return *slot;
+    slot.reset();
+    std::unique_ptr<MultiState, MultiStateDeleter> m(new MultiState);
+    m->fp32 = fp32;
+    m->kb = kb;
+    const int64_t ts = fp32 ? 4 : 8;
+    const int64_t ncoef = (int64_t)p_ * p_ * p_;
+    m->src_q = m->alloc<unsigned char>((size_t)(ts * n_all_ * kb));
+    m->proxy_up = m->alloc<unsigned char>((size_t)(ts * n_up_ * ncoef * kb));
+    m->proxy_down = m->alloc<unsigned char>((size_t)(ts * n_down_ * ncoef * kb));
+    m->pw_out = m->alloc<unsigned char>((size_t)(2 * ts * n_pw_ * (int64_t)M_ * kb));
+    // Scratch: the largest per-entry tensor of any transform step, for at
+    // least one box with all kb RHS (the downward pass chunks by box).
+    const int64_t per_entry = 2 * ts * std::max<int64_t>({(int64_t)p_ * p_ * npw_, (int64_t)p_ * npw_ * npw_,
+                                                          (int64_t)npw_ * npw2_ * p_, (int64_t)npw2_ * p_ * p_,
+                                                          (int64_t)M_, ncoef});
+    m->scratch_bytes = std::max<int64_t>((int64_t)512 << 20, per_entry * kb);
+    m->s1 = m->alloc<unsigned char>((size_t)m->scratch_bytes);
+    m->s2 = m->alloc<unsigned char>((size_t)m->scratch_bytes);
+    m->pw_in = m->alloc<unsigned char>((size_t)m->scratch_bytes);
+    m->pot = m->alloc<double>((size_t)n_ * kb);
+    m->far = m->alloc<double>((size_t)n_ * kb);
+    m->q_t = m->alloc<double>((size_t)n_ * kb);
+    m->grid = m->alloc<double>((size_t)(n_grid_ * kb));
+    m->spec = m->alloc<cd>((size_t)(n_spec_ * kb));
+    {
+        int dims[3] = {nufft_.n1, nufft_.n2, nufft_.n3};
+        if (cufftPlanMany(&m->fwd, 3, dims, nullptr, 1, (int)n_grid_, nullptr, 1, (int)n_spec_, CUFFT_D2Z, kb) !=
+                CUFFT_SUCCESS ||
+            cufftPlanMany(&m->inv, 3, dims, nullptr, 1, (int)n_spec_, nullptr, 1, (int)n_grid_, CUFFT_Z2D, kb) !=
+                CUFFT_SUCCESS)
+            throw std::runtime_error("cuFFT error: batched plan creation failed");
+        cufftSetStream(m->fwd, stream_);
+        cufftSetStream(m->inv, stream_);
+    }
+    if (fp32) {
+        auto conv = [&](const void* src, int64_t n_doubles) {
+            float* d = m->alloc<float>((size_t)n_doubles);
+            dev::k_to_float<<<(unsigned)((n_doubles + 255) / 256), 256, 0, stream_>>>(static_cast<const double*>(src), d,
+                                                                                      n_doubles);
+            return d;
+        };
+        const int64_t pp = (int64_t)p_ * p_;
+        m->c2p = conv(c2p_, 8 * 3 * pp);
+        m->p2c = conv(p2c_, 8 * 3 * pp);
+        m->lev.resize(lev_.size());
+        for (size_t l = 0; l < lev_.size(); ++l) {
+            m->lev[l].poly2pw = reinterpret_cast<cf*>(conv(lev_[l].poly2pw, 2 * (int64_t)npw_ * p_));
+            m->lev[l].poly2pw_half = reinterpret_cast<cf*>(conv(lev_[l].poly2pw_half, 2 * (int64_t)npw2_ * p_));
+            m->lev[l].pw2polyT = reinterpret_cast<cf*>(conv(lev_[l].pw2polyT, 2 * (int64_t)npw_ * p_));
+            m->lev[l].pw2polyTw = reinterpret_cast<cf*>(conv(lev_[l].pw2polyTw, 2 * (int64_t)npw2_ * p_));
+            m->lev[l].shift = conv(lev_[l].shift, 27 * 2 * (int64_t)M_);
+        }
+        m->src_hi = m->alloc<float4>(n_all_);
+        m->src_lo = m->alloc<float4>(n_all_);
+        m->trg_hi = m->alloc<float4>(n_);
+        m->trg_lo = m->alloc<float4>(n_);
+        dev::k_split_positions<<<(n_all_ + 255) / 256, 256, 0, stream_>>>(src_, m->src_hi, m->src_lo, n_all_);
+        dev::k_split_positions<<<(n_ + 255) / 256, 256, 0, stream_>>>(trg_, m->trg_hi, m->trg_lo, n_);
+    }
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    slot = std::move(m);
+    return *slot;
+}
+
+template <typename T>
+void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, double* pot_user) {
+    using C = typename dev::Cplx<T>::type;
+    constexpr bool f32 = std::is_same<T, float>::value;
+    const int p = p_, n = npw_, n2 = npw2_, M = M_;
+    const int64_t ncoef = (int64_t)p * p * p;
+    const int kb = m.kb;
+    cudaStream_t s = stream_;
+    T* src_q = static_cast<T*>(m.src_q);
+    T* up = static_cast<T*>(m.proxy_up);
+    T* down = static_cast<T*>(m.proxy_down);
+    C* pw = static_cast<C*>(m.pw_out);
+    const T* c2pm = f32 ? reinterpret_cast<const T*>(m.c2p) : reinterpret_cast<const T*>(c2p_);
+    const T* p2cm = f32 ? reinterpret_cast<const T*>(m.p2c) : reinterpret_cast<const T*>(p2c_);
+    auto levtab = [&](int l, int which) -> const void* {
+        if (f32) {
+            const auto& L = m.lev[l];
+            return which == 0 ? (const void*)L.poly2pw : which == 1 ? (const void*)L.poly2pw_half
+                 : which == 2 ? (const void*)L.pw2polyT : which == 3 ? (const void*)L.pw2polyTw : (const void*)L.shift;
+        }
+        const auto& L = lev_[l];
+        return which == 0 ? (const void*)L.poly2pw : which == 1 ? (const void*)L.poly2pw_half
+             : which == 2 ? (const void*)L.pw2polyT : which == 3 ? (const void*)L.pw2polyTw : (const void*)L.shift;
+    };
+    const int64_t sbytes = m.scratch_bytes;
+
+    int nl = 0;
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(m.pot, 0, sizeof(double) * n_ * kb, s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(up, 0, sizeof(T) * std::max<int64_t>(n_up_ * ncoef * kb, 1), s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(down, 0, sizeof(T) * std::max<int64_t>(n_down_ * ncoef * kb, 1), s));
+    {
+        const int64_t tot = (int64_t)n_all_ * kb;
+        dev::k_gather_src_m<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src_q, src_charge_idx_, Q, n_all_, n_, kb,
+                                                                             kvalid); ++nl;
+        const int64_t tt = (int64_t)n_ * kb;
+        dev::k_gather_trg_m<<<(unsigned)((tt + 255) / 256), 256, 0, s>>>(m.q_t, trg_perm_, Q, n_, kb, kvalid); ++nl;
+    }
+    // proxy moments
+    if (c2x_.n_centers > 0) {
+        const dim3 grid(c2x_.n_centers, (p * p + 127) / 128, kb);
+        switch (p) {
+            case 9: dev::k_c2proxy_m<T, 9><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
+            case 18: dev::k_c2proxy_m<T, 18><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
+            case 28: dev::k_c2proxy_m<T, 28><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
+            case 38: dev::k_c2proxy_m<T, 38><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
+            default: throw std::runtime_error("unsupported expansion order");
+        }
+    }
+    // chunked batched contraction helper over (box, rhs) entries
+    auto chunked = [&](int n_boxes, int64_t per_entry_bytes, auto&& body) {
+        const int64_t total = (int64_t)n_boxes * kb;
+        const int64_t C = std::max<int64_t>(1, sbytes / std::max<int64_t>(per_entry_bytes, 1));
+        for (int64_t e0 = 0; e0 < total; e0 += C) body(e0, (int)std::min<int64_t>(C, total - e0));
+    };
+    // upward children -> parents
+    for (const auto& g : c2p_groups_) {
+        const T* mx = c2pm + (int64_t)g.child * 3 * p * p;
+        chunked(g.n, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {
+            dev::ContractM a{};
+            a.rhs = kb; a.e0 = e0; a.n_entries = ne;
+            a.in = up; a.in_off = g.in_off; a.in_unit = ncoef; a.out = m.s1; a.out_stride = ncoef;
+            a.mat = mx; a.ni = p; a.na = p; a.R = p * p; a.mode = dev::kStore;
+            dev::launch_contract_m<T, T, T>(a, s); ++nl;
+            a.in = m.s1; a.in_off = nullptr; a.in_stride = ncoef; a.out = m.s2; a.mat = mx + p * p;
+            dev::launch_contract_m<T, T, T>(a, s); ++nl;
+            a.in = m.s2; a.out = up; a.out_off = g.out_off; a.out_unit = ncoef; a.mat = mx + 2 * p * p; a.mode = dev::kAdd;
+            dev::launch_contract_m<T, T, T>(a, s); ++nl;
+        });
+    }
+    // outgoing plane waves
+    for (const auto& g : pw_groups_) {
+        const int64_t e1 = (int64_t)p * p * n, e2 = (int64_t)p * n * n;
+        chunked(g.n, (int64_t)sizeof(C) * std::max(e1, e2), [&](int64_t e0, int ne) {
+            dev::ContractM a{};
+            a.rhs = kb; a.e0 = e0; a.n_entries = ne;
+            a.in = up; a.in_off = g.in_off; a.in_unit = ncoef; a.out = m.s1; a.out_stride = e1;
+            a.mat = levtab(g.level, 0); a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore;
+            dev::launch_contract_m<T, C, C>(a, s); ++nl;
+            a.in = m.s1; a.in_off = nullptr; a.in_stride = e1; a.out = m.s2; a.out_stride = e2; a.R = p * n;
+            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            a.in = m.s2; a.in_stride = e2; a.out = pw; a.out_off = g.out_off; a.out_unit = M;
+            a.mat = levtab(g.level, 1); a.na = n2; a.R = n * n;
+            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+        });
+    }
+    // downward per level
+    for (const auto& E : eval_levels_) {
+        const int64_t e1 = (int64_t)n * n2 * p, e2 = (int64_t)n2 * p * p;
+        // chunk over boxes (all rhs of a box together): pw_in holds C boxes x kb x M
+        const int64_t per_box = (int64_t)sizeof(C) * std::max<int64_t>({(int64_t)M, e1, e2}) * kb;
+        const int Cb = (int)std::max<int64_t>(1, sbytes / per_box);
+        for (int b0 = 0; b0 < E.n; b0 += Cb) {
+            const int nb = std::min(Cb, E.n - b0);
+            {
+                const dim3 grid(nb, (M + 255) / 256, kb);
+                dev::k_shift_m<T><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
+                                                       static_cast<C*>(m.pw_in), M, E.term_start, E.term_slot,
+                                                       E.term_stencil, kb, b0); ++nl;
+            }
+            dev::ContractM a{};
+            a.rhs = kb; a.e0 = (int64_t)b0 * kb; a.n_entries = nb * kb;
+            a.in = m.pw_in; a.in_stride = M; a.out = m.s1; a.out_stride = e1;
+            a.mat = levtab(E.level, 2); a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
+            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            a.in = m.s1; a.in_stride = e1; a.out = m.s2; a.out_stride = e2; a.R = n2 * p;
+            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            a.in = m.s2; a.in_stride = e2; a.out = down; a.out_off = E.down_off; a.out_unit = ncoef;
+            a.mat = levtab(E.level, 3); a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
+            dev::launch_contract_m<C, C, T>(a, s); ++nl;
+        }
+        if (E.n_p2c) {
+            chunked(E.n_p2c, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {
+                dev::ContractM b{};
+                b.rhs = kb; b.e0 = e0; b.n_entries = ne;
+                b.in = down; b.in_off = E.p2c_in; b.in_unit = ncoef; b.out = m.s1; b.out_stride = ncoef;
+                b.mat = p2cm; b.mat_off = E.p2c_mat; b.ni = p; b.na = p; b.R = p * p; b.mode = dev::kStore;
+                dev::launch_contract_m<T, T, T>(b, s); ++nl;
+                b.in = m.s1; b.in_off = nullptr; b.in_stride = ncoef; b.out = m.s2; b.mat = p2cm + p * p;
+                dev::launch_contract_m<T, T, T>(b, s); ++nl;
+                b.in = m.s2; b.out = down; b.out_off = E.p2c_out; b.out_unit = ncoef; b.mat = p2cm + 2 * p * p;
+                b.mode = dev::kAdd;
+                dev::launch_contract_m<T, T, T>(b, s); ++nl;
+            });
+        }
+    }
+    // leaf evaluation
+    if (eval_.n_leaves > 0) {
+        const dim3 grid(eval_.n_leaves, 1, kb);
+        switch (p) {
+            case 9: dev::k_eval_m<T, 9><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 18: dev::k_eval_m<T, 18><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 28: dev::k_eval_m<T, 28><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 38: dev::k_eval_m<T, 38><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            default: throw std::runtime_error("unsupported expansion order");
+        }
+    }
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
+    // near field
+    if (near_.n_leaves > 0) {
+        dev::NearM a{};
+        a.trg_start = near_.trg_start; a.trg_count = near_.trg_count; a.pair_start = near_.pair_start;
+        a.pair_src_start = near_.pair_src_start; a.pair_src_count = near_.pair_src_count;
+        a.pair_bsize = near_.pair_bsize; a.n_leaves = near_.n_leaves; a.N = n_; a.kb = kb;
+        for (int i = 0; i < near_.nc; ++i) a.coef[i] = near_.coef[i];
+        if constexpr (f32) {
+            if (kb >= 16)
+                dev::launch_near_m32_kb<16>(a, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo, reinterpret_cast<const float*>(src_q),
+                                            m.pot, near_.nc, s);
+            else if (kb >= 4)
+                dev::launch_near_m32_kb<4>(a, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo, reinterpret_cast<const float*>(src_q),
+                                           m.pot, near_.nc, s);
+            else
+                dev::launch_near_m32_kb<1>(a, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo, reinterpret_cast<const float*>(src_q),
+                                           m.pot, near_.nc, s);
+        } else {
+            if (kb >= 8)
+                dev::launch_near_m64_kb<8>(a, trg_, src_, reinterpret_cast<const double*>(src_q), m.pot, near_.nc, s);
+            else
+                dev::launch_near_m64_kb<1>(a, trg_, src_, reinterpret_cast<const double*>(src_q), m.pot, near_.nc, s);
+        }
+        ++nl;
+    }
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[2], s));
+    // far field, FP64, all rhs of the block at once
+    {
+        dev::NufftArgs na = nufft_;
+        na.q_sorted = m.q_t;
+        na.grid = m.grid;
+        na.far = m.far;
+        na.rhs_q_stride = n_;
+        na.rhs_grid_stride = n_grid_;
+        na.rhs_far_stride = n_;
+        PDMK_CUDA_CHECK(cudaMemsetAsync(m.grid, 0, sizeof(double) * n_grid_ * kb, s));
+        dev::launch_spread(na, nufft_max_jk_, nufft_max_ex_, s, kb); ++nl;
+        if (cufftExecD2Z(m.fwd, m.grid, reinterpret_cast<cufftDoubleComplex*>(m.spec)) != CUFFT_SUCCESS)
+            throw std::runtime_error("cuFFT error in the batched forward transform");
+        dev::launch_multiply(m.spec, mult_, n_spec_, s, kb); ++nl;
+        if (cufftExecZ2D(m.inv, reinterpret_cast<cufftDoubleComplex*>(m.spec), m.grid) != CUFFT_SUCCESS)
+            throw std::runtime_error("cuFFT error in the batched inverse transform");
+        dev::launch_interp(na, s, kb); ++nl;
+    }
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
+    {
+        const int64_t tot = (int64_t)n_ * kvalid;
+        dev::k_finalize_m<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m.pot, m.far, trg_, trg_perm_, m.q_t, pot_user,
+                                                                        n_, kvalid); ++nl;
+    }
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[4], s));
+    PDMK_CUDA_CHECK(cudaGetLastError());
+    multi_launches_ += nl;
+}
+
+void DeviceTree::evaluate_multi_device(const double* Q, int k, double* pot, bool fp32, StageTimes* times) {
+    if (k <= 0) throw std::invalid_argument("k must be positive");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    fp32 = fp32 && mixed_allowed();
+    const int kb = multi_block(k, fp32);
+    MultiState& m = multi_state(kb, fp32);
+    StageTimes acc;
+    multi_launches_ = 0;
+    for (int c0 = 0; c0 < k; c0 += m.kb) {
+        const int kv = std::min(m.kb, k - c0);
+        if (fp32)
+            run_multi_block<float>(m, Q + (int64_t)c0 * n_, kv, pot + (int64_t)c0 * n_);
+        else
+            run_multi_block<double>(m, Q + (int64_t)c0 * n_, kv, pot + (int64_t)c0 * n_);
+        // per-block stage times (the events are reused by the next block)
+        const StageTimes t = last_times();
+        acc.dmk_ms += t.dmk_ms;
+        acc.direct_ms += t.direct_ms;
+        acc.nufft_ms += t.nufft_ms;
+        acc.near_ms += t.near_ms;
+        acc.finalize_ms += t.finalize_ms;
+    }
+    if (times) *times = acc;
+    last_multi_ = acc;
+    last_was_multi_ = true;
+}
+
+namespace dev {
+__global__ void k_to_float_out(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+}  // namespace dev
+
+void DeviceTree::evaluate_multi_host(const double* Q, int k, void* pot, bool pot_float, bool fp32,
+                                     StageTimes* times) {
+    if (k <= 0) throw std::invalid_argument("k must be positive");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    double* qd = nullptr;
+    double* pd = nullptr;
+    const int64_t n = (int64_t)n_ * k;
+    const size_t bytes = sizeof(double) * (size_t)n;
+    PDMK_CUDA_CHECK(cudaMallocAsync(&qd, bytes, stream_));
+    PDMK_CUDA_CHECK(cudaMallocAsync(&pd, bytes, stream_));
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(qd, Q, bytes, cudaMemcpyHostToDevice, stream_));
+    evaluate_multi_device(qd, k, pd, fp32, times);
+    if (pot_float) {
+        // reuse the charge buffer for the float copy of the potentials
+        float* pf = reinterpret_cast<float*>(qd);
+        dev::k_to_float_out<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(pd, pf, n);
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pf, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, stream_));
+    } else {
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pd, bytes, cudaMemcpyDeviceToHost, stream_));
+    }
+    PDMK_CUDA_CHECK(cudaFreeAsync(qd, stream_));
+    PDMK_CUDA_CHECK(cudaFreeAsync(pd, stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+}  // namespace pdmkb

@@ -1,0 +1,114 @@
+"""GPU tests of the multi-RHS evaluate (k charge vectors on one tree) and of the
+mixed-precision path, through the C ABI.
+
+Tolerances (relative L2, per charge vector):
+  * plain FP64 multi-RHS vs single-RHS FP64 evaluates: 1e-12 (same arithmetic);
+  * mixed precision vs the FP64 path: 1e-6 at 6 digits (the accuracy target of
+    the batched mode), 2e-4 at 3 digits; both also vs the CPU oracle;
+  * n_digits > 6 with mixed requested: the FP64 path runs (1e-12 vs FP64).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+import periodicdmk_b200 as pd
+from conftest import TRICLINIC, clustered_system, rel_l2, uniform_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _charges(n, k, seed):
+    rng = np.random.default_rng(seed)
+    Q = rng.uniform(-1.0, 1.0, (n, k))
+    Q -= Q.mean(axis=0)
+    return Q
+
+
+def _multi_device(tree, Q, mixed):
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    q_d = torch.from_numpy(np.ascontiguousarray(Q.T)).to(dev)  # column-major N x k
+    p_d = torch.empty_like(q_d)
+    torch.cuda.synchronize()
+    tree.evaluate_multi_device(Q.shape[1], q_d.data_ptr(), p_d.data_ptr(), mixed=mixed)
+    return p_d.cpu().numpy().T
+
+
+@pytest.mark.parametrize("system", ["cube", "triclinic"])
+def test_fp64_multi_equals_single(system):
+    if system == "cube":
+        cell, pos, _ = uniform_system(3000, 41)
+    else:
+        cell, pos, _ = clustered_system(3000, 42, TRICLINIC, n_clusters=4, sigma=0.02)
+    Q = _charges(len(pos), 5, 1)
+    t = pd.PeriodicDMKTree(cell, pos, 6, 30, 4)
+    P = _multi_device(t, Q, mixed=False)
+    for c in range(5):
+        assert rel_l2(P[:, c], t.evaluate(Q[:, c])) < 1e-12
+    # host-buffer path, same numbers
+    P2 = t.evaluate_multi(Q)
+    assert rel_l2(P2, P) < 1e-14
+    t.close()
+
+
+@pytest.mark.parametrize("nd,tol", [(6, 1e-6), (3, 2e-4)])
+@pytest.mark.parametrize("system", ["cube", "triclinic"])
+def test_mixed_multi_accuracy(system, nd, tol):
+    if system == "cube":
+        cell, pos, _ = uniform_system(4000, 43)
+        npl = 40
+    else:
+        cell, pos, _ = clustered_system(4000, 44, TRICLINIC, n_clusters=4, sigma=0.02)
+        npl = 30
+    Q = _charges(len(pos), 8, 2)
+    t = pd.PeriodicDMKTree(cell, pos, nd, npl, 4)
+    Pm = _multi_device(t, Q, mixed=True)
+    Pd = _multi_device(t, Q, mixed=False)
+    for c in range(8):
+        assert rel_l2(Pm[:, c], Pd[:, c]) < tol, c
+    ref = oracle.evaluate(cell, pos, Q[:, 0], nd, npl, 4)
+    assert rel_l2(Pm[:, 0], ref) < tol + 0.2 * 10.0 ** (-nd)
+    t.close()
+
+
+def test_mixed_request_above_six_digits_runs_fp64():
+    cell, pos, _ = uniform_system(2000, 45)
+    Q = _charges(len(pos), 3, 3)
+    t = pd.PeriodicDMKTree(cell, pos, 9, 30, 4)
+    Pm = _multi_device(t, Q, mixed=True)
+    Pd = _multi_device(t, Q, mixed=False)
+    assert rel_l2(Pm, Pd) < 1e-13
+    t.close()
+
+
+def test_rhs_blocks_tail():
+    # k = 70 > the 64-RHS block: two blocks (64 + 6)
+    cell, pos, _ = uniform_system(1500, 46)
+    Q = _charges(len(pos), 70, 4)
+    t = pd.PeriodicDMKTree(cell, pos, 6, 40, 4)
+    P = t.evaluate_multi(Q)
+    for c in (0, 63, 64, 69):
+        assert rel_l2(P[:, c], t.evaluate(Q[:, c])) < 1e-12
+    t.close()
+
+
+def test_float_tree_mixed_path():
+    cell, pos, q = uniform_system(4000, 47, charges="uniform")
+    td = pd.PeriodicDMKTree(cell, pos, 6, 40, 4)
+    tf = pd.PeriodicDMKTree(cell, pos, 6, 40, 4, precision="float")
+    a = td.evaluate(q)
+    b = tf.evaluate(q)
+    assert b.dtype == np.float32
+    assert rel_l2(b, a) < 1e-6
+    c, tm = tf.evaluate_timed(q)
+    assert rel_l2(c, b) < 1e-7 and tm["direct_ms"] > 0
+    Q = _charges(len(q), 4, 5)
+    F = tf.evaluate_multi(Q)
+    assert F.dtype == np.float32
+    for j in range(4):
+        assert rel_l2(F[:, j], td.evaluate(Q[:, j])) < 1e-6
+    td.close()
+    tf.close()
