@@ -16,6 +16,7 @@
 #include <stdexcept>
 
 #include "device_tree.hpp"
+#include "tc_kernels.cuh"
 
 namespace pdmkb {
 namespace dev {
@@ -531,6 +532,218 @@ static void launch_near_m32_kb(const NearM& a, const float4* th, const float4* t
     }
 }
 
+// ---------------------------------------------------------------------------
+// fused separable transform out(a,b,c) (+)= sum Ux(a,i) Uy(b,j) Uz(c,k) in(i,j,k)
+// for one (box, rhs) entry per CTA, the tensor held in shared memory.
+// Matrices U_d column-major P x P at mat + mat_off[eb] + d*P*P.
+// ---------------------------------------------------------------------------
+struct Sep3 {
+    const void* in;
+    const int64_t* in_off;
+    void* out;
+    const int64_t* out_off;
+    const void* mat;
+    const int64_t* mat_off;  // null: mat
+    int rhs;
+    int64_t e0;
+    int accumulate;
+};
+
+template <typename T, int P>
+__device__ __forceinline__ void sep3_step(const T* __restrict__ src, T* __restrict__ dst, const T* __restrict__ Ut,
+                                          int nthr) {
+    // dst[r + P*P*a] = sum_i Ut[i*P + a] * src[i + P*r], two columns r per thread
+    for (int r = threadIdx.x; r < P * P; r += 2 * nthr) {
+        const int r2 = r + nthr;
+        const bool two = r2 < P * P;
+        T acc0[P], acc1[P];
+#pragma unroll
+        for (int a = 0; a < P; ++a) acc0[a] = acc1[a] = T(0);
+        for (int i = 0; i < P; ++i) {
+            const T x0 = src[i + P * r];
+            const T x1 = two ? src[i + P * r2] : T(0);
+#pragma unroll
+            for (int a = 0; a < P; ++a) {
+                const T u = Ut[i * P + a];
+                acc0[a] = fma(u, x0, acc0[a]);
+                acc1[a] = fma(u, x1, acc1[a]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            dst[r + P * P * a] = acc0[a];
+            if (two) dst[r2 + P * P * a] = acc1[a];
+        }
+    }
+}
+
+template <typename T, int P>
+__global__ void k_sep3(Sep3 a) {
+    extern __shared__ __align__(16) unsigned char smem_s3[];
+    constexpr int P3 = P * P * P;
+    T* b0 = reinterpret_cast<T*>(smem_s3);
+    T* b1 = b0 + P3;
+    T* Ut = b1 + P3;  // 3 transposed matrices
+    const int64_t ge = a.e0 + blockIdx.x;
+    const int rhs = a.rhs > 0 ? a.rhs : 1;
+    const int64_t eb = ge / rhs, ec = ge % rhs;
+    const T* in = reinterpret_cast<const T*>(a.in) + a.in_off[eb] * rhs + ec * P3;
+    T* out = reinterpret_cast<T*>(a.out) + a.out_off[eb] * rhs + ec * P3;
+    const T* mat = reinterpret_cast<const T*>(a.mat) + (a.mat_off ? a.mat_off[eb] : 0);
+    const int nthr = blockDim.x;
+    for (int idx = threadIdx.x; idx < P3; idx += nthr) b0[idx] = in[idx];
+    for (int idx = threadIdx.x; idx < 3 * P * P; idx += nthr) {
+        const int d = idx / (P * P), w = idx % (P * P);
+        const int i = w / P, aa = w % P;
+        Ut[d * P * P + i * P + aa] = mat[d * P * P + aa + P * i];
+    }
+    __syncthreads();
+    sep3_step<T, P>(b0, b1, Ut, nthr);
+    __syncthreads();
+    sep3_step<T, P>(b1, b0, Ut + P * P, nthr);
+    __syncthreads();
+    // last step straight into the output (coalesced along r)
+    const T* Uz = Ut + 2 * P * P;
+    for (int r = threadIdx.x; r < P * P; r += nthr) {
+        T acc[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) acc[c] = T(0);
+        for (int k = 0; k < P; ++k) {
+            const T x = b0[k + P * r];
+#pragma unroll
+            for (int c = 0; c < P; ++c) acc[c] = fma(Uz[k * P + c], x, acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < P; ++c) {
+            if (a.accumulate)
+                out[r + P * P * c] += acc[c];
+            else
+                out[r + P * P * c] = acc[c];
+        }
+    }
+}
+
+template <typename T, int P>
+static size_t sep3_smem() { return sizeof(T) * (2 * (size_t)P * P * P + 3 * (size_t)P * P); }
+
+template <typename T, int P>
+static void launch_sep3_p(const Sep3& a, int n_entries, cudaStream_t s) {
+    static bool configured = false;
+    const size_t smem = sep3_smem<T, P>();
+    if (!configured) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_sep3<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    const int thr = std::max(32, ((P * P + 1) / 2 + 31) / 32 * 32);
+    k_sep3<T, P><<<n_entries, thr, smem, s>>>(a);
+}
+
+// true if the fused kernel handles (T, P) (tensor pair fits in shared memory)
+template <typename T>
+bool sep3_supported(int p) {
+    if (p == 9 || p == 18) return true;
+    if (p == 28) return sizeof(T) == 4;
+    return false;
+}
+
+template <typename T>
+void launch_sep3(const Sep3& a, int p, int n_entries, cudaStream_t s) {
+    if (n_entries <= 0) return;
+    switch (p) {
+        case 9: launch_sep3_p<T, 9>(a, n_entries, s); break;
+        case 18: launch_sep3_p<T, 18>(a, n_entries, s); break;
+        case 28:
+            if constexpr (sizeof(T) == 4) {
+                launch_sep3_p<T, 28>(a, n_entries, s);
+                break;
+            }
+            [[fallthrough]];
+        default: throw std::runtime_error("fused transform not available for this order");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// proxy -> leaf targets, TPT targets per thread: grid (leaves, 1, rhs)
+// ---------------------------------------------------------------------------
+template <typename T, int P, int TPT>
+__global__ void __launch_bounds__(128)
+    k_eval_g(EvalArgs a, const T* __restrict__ proxy_down, double* __restrict__ pot, int64_t N, int kb) {
+    __shared__ T slab[P * P];
+    const int e = blockIdx.x, c = blockIdx.z;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const double4 cs = a.center_scale[e];
+    const T* C = proxy_down + ((int64_t)a.slot[e] * kb + c) * (P * P * P);
+    double* potc = pot + (int64_t)c * N;
+    for (int base = 0; base < nt; base += TPT * blockDim.x) {
+        T tx[TPT][P], y[TPT], z[TPT];
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+            const int t = base + threadIdx.x + u * blockDim.x;
+            T x = T(0);
+            y[u] = z[u] = T(0);
+            if (t < nt) {
+                const double4 pt = a.trg[t0 + t];
+                x = (T)((pt.x - cs.x) * cs.w);
+                y[u] = (T)((pt.y - cs.y) * cs.w);
+                z[u] = (T)((pt.z - cs.z) * cs.w);
+            }
+            tx[u][0] = T(1);
+            if (P > 1) tx[u][1] = x;
+#pragma unroll
+            for (int n = 2; n < P; ++n) tx[u][n] = T(2) * x * tx[u][n - 1] - tx[u][n - 2];
+        }
+        T acc[TPT], za[TPT], zb[TPT];
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+            acc[u] = T(0);
+            za[u] = T(1);
+            zb[u] = z[u];
+        }
+        for (int k = 0; k < P; ++k) {
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < P * P; idx += blockDim.x) slab[idx] = C[(int64_t)k * P * P + idx];
+            __syncthreads();
+            T ya[TPT], yb[TPT], sk[TPT];
+#pragma unroll
+            for (int u = 0; u < TPT; ++u) {
+                ya[u] = T(1);
+                yb[u] = y[u];
+                sk[u] = T(0);
+            }
+            for (int j = 0; j < P; ++j) {
+                T rr[TPT];
+#pragma unroll
+                for (int u = 0; u < TPT; ++u) rr[u] = T(0);
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    const T cv = slab[i + P * j];
+#pragma unroll
+                    for (int u = 0; u < TPT; ++u) rr[u] = fma(cv, tx[u][i], rr[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < TPT; ++u) {
+                    sk[u] = fma(ya[u], rr[u], sk[u]);
+                    const T yn = T(2) * y[u] * yb[u] - ya[u];
+                    ya[u] = yb[u];
+                    yb[u] = yn;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < TPT; ++u) {
+                acc[u] = fma(za[u], sk[u], acc[u]);
+                const T zn = T(2) * z[u] * zb[u] - za[u];
+                za[u] = zb[u];
+                zb[u] = zn;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+            const int t = base + threadIdx.x + u * blockDim.x;
+            if (t < nt) potc[t0 + t] += (double)acc[u];
+        }
+    }
+}
+
 }  // namespace dev
 
 // ===========================================================================
@@ -567,6 +780,7 @@ struct DeviceTree::MultiState {
     };
     std::vector<Lev> lev;
     float4 *src_hi = nullptr, *src_lo = nullptr, *trg_hi = nullptr, *trg_lo = nullptr;
+    int* err = nullptr;  // set by tensor-core kernels whose pipeline wait timed out
 
     template <typename T>
     T* alloc(size_t n) {
@@ -627,6 +841,8 @@ DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
     m->far = m->alloc<double>((size_t)n_ * kb);
     m->q_t = m->alloc<double>((size_t)n_ * kb);
     m->grid = m->alloc<double>((size_t)(n_grid_ * kb));
+    m->err = m->alloc<int>(1);
+    PDMK_CUDA_CHECK(cudaMemsetAsync(m->err, 0, sizeof(int), stream_));
     m->spec = m->alloc<cd>((size_t)(n_spec_ * kb));
     {
         int dims[3] = {nufft_.n1, nufft_.n2, nufft_.n3};
@@ -706,15 +922,24 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         const int64_t tt = (int64_t)n_ * kb;
         dev::k_gather_trg_m<<<(unsigned)((tt + 255) / 256), 256, 0, s>>>(m.q_t, trg_perm_, Q, n_, kb, kvalid); ++nl;
     }
-    // proxy moments
+    // proxy moments: tensor-core GEMM (FP32 blocks of >= 16 RHS), else per-RHS CUDA-core kernel
     if (c2x_.n_centers > 0) {
-        const dim3 grid(c2x_.n_centers, (p * p + 127) / 128, kb);
-        switch (p) {
-            case 9: dev::k_c2proxy_m<T, 9><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
-            case 18: dev::k_c2proxy_m<T, 18><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
-            case 28: dev::k_c2proxy_m<T, 28><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
-            case 38: dev::k_c2proxy_m<T, 38><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); ++nl; break;
-            default: throw std::runtime_error("unsupported expansion order");
+        bool done = false;
+        if constexpr (f32) {
+            done = dev::launch_c2proxy_tc(c2x_, src_q, up, kb, p, m.err, s);
+        }
+        if (done) {
+            ++nl;
+        } else {
+            const dim3 grid(c2x_.n_centers, (p * p + 127) / 128, kb);
+            switch (p) {
+                case 9: dev::k_c2proxy_m<T, 9><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); break;
+                case 18: dev::k_c2proxy_m<T, 18><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); break;
+                case 28: dev::k_c2proxy_m<T, 28><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); break;
+                case 38: dev::k_c2proxy_m<T, 38><<<grid, 128, 0, s>>>(c2x_, src_q, up, kb); break;
+                default: throw std::runtime_error("unsupported expansion order");
+            }
+            ++nl;
         }
     }
     // chunked batched contraction helper over (box, rhs) entries
@@ -723,9 +948,17 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         const int64_t C = std::max<int64_t>(1, sbytes / std::max<int64_t>(per_entry_bytes, 1));
         for (int64_t e0 = 0; e0 < total; e0 += C) body(e0, (int)std::min<int64_t>(C, total - e0));
     };
+    const bool fused = dev::sep3_supported<T>(p);
     // upward children -> parents
     for (const auto& g : c2p_groups_) {
         const T* mx = c2pm + (int64_t)g.child * 3 * p * p;
+        if (fused) {
+            dev::Sep3 f{};
+            f.in = up; f.in_off = g.in_off; f.out = up; f.out_off = g.out_off; f.mat = mx; f.rhs = kb;
+            f.accumulate = 1;
+            dev::launch_sep3<T>(f, p, g.n * kb, s); ++nl;
+            continue;
+        }
         chunked(g.n, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {
             dev::ContractM a{};
             a.rhs = kb; a.e0 = e0; a.n_entries = ne;
@@ -779,7 +1012,12 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             a.mat = levtab(E.level, 3); a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
             dev::launch_contract_m<C, C, T>(a, s); ++nl;
         }
-        if (E.n_p2c) {
+        if (E.n_p2c && fused) {
+            dev::Sep3 f{};
+            f.in = down; f.in_off = E.p2c_in; f.out = down; f.out_off = E.p2c_out; f.mat = p2cm;
+            f.mat_off = E.p2c_mat; f.rhs = kb; f.accumulate = 1;
+            dev::launch_sep3<T>(f, p, E.n_p2c * kb, s); ++nl;
+        } else if (E.n_p2c) {
             chunked(E.n_p2c, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {
                 dev::ContractM b{};
                 b.rhs = kb; b.e0 = e0; b.n_entries = ne;
@@ -798,10 +1036,10 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     if (eval_.n_leaves > 0) {
         const dim3 grid(eval_.n_leaves, 1, kb);
         switch (p) {
-            case 9: dev::k_eval_m<T, 9><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
-            case 18: dev::k_eval_m<T, 18><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
-            case 28: dev::k_eval_m<T, 28><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
-            case 38: dev::k_eval_m<T, 38><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 9: dev::k_eval_g<T, 9, 4><<<grid, 64, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 18: dev::k_eval_g<T, 18, 4><<<grid, 64, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 28: dev::k_eval_g<T, 28, 2><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
+            case 38: dev::k_eval_g<T, 38, 2><<<grid, 128, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
             default: throw std::runtime_error("unsupported expansion order");
         }
     }
@@ -877,6 +1115,12 @@ void DeviceTree::evaluate_multi_device(const double* Q, int k, double* pot, bool
             run_multi_block<double>(m, Q + (int64_t)c0 * n_, kv, pot + (int64_t)c0 * n_);
         // per-block stage times (the events are reused by the next block)
         const StageTimes t = last_times();
+        int err = 0;
+        PDMK_CUDA_CHECK(cudaMemcpy(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) {
+            PDMK_CUDA_CHECK(cudaMemset(m.err, 0, sizeof(int)));
+            throw std::runtime_error("CUDA error: tensor-core pipeline wait timed out in the multi-RHS evaluate");
+        }
         acc.dmk_ms += t.dmk_ms;
         acc.direct_ms += t.direct_ms;
         acc.nufft_ms += t.nufft_ms;

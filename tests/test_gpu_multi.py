@@ -6,6 +6,9 @@ Tolerances (relative L2, per charge vector):
   * mixed precision vs the FP64 path: 1e-6 at 6 digits (the accuracy target of
     the batched mode), 2e-4 at 3 digits; both also vs the CPU oracle;
   * n_digits > 6 with mixed requested: the FP64 path runs (1e-12 vs FP64).
+Blocks of 16 or more RHS form the proxy moments on the tensor cores (TF32
+hi/lo split); blocks of fewer RHS use the CUDA-core kernel.  Both are held to
+the same tolerances.
 """
 import ctypes
 
@@ -112,3 +115,16 @@ def test_float_tree_mixed_path():
         assert rel_l2(F[:, j], td.evaluate(Q[:, j])) < 1e-6
     td.close()
     tf.close()
+
+
+@pytest.mark.parametrize("nd,tol", [(6, 1e-6), (3, 2e-4)])
+@pytest.mark.parametrize("k", [16, 37, 64, 70])
+def test_mixed_tensor_core_blocks(nd, tol, k):
+    cell, pos, _ = clustered_system(6000, 48, TRICLINIC, n_clusters=4, sigma=0.03)
+    Q = _charges(len(pos), k, 6)
+    t = pd.PeriodicDMKTree(cell, pos, nd, 40, 4)
+    Pm = _multi_device(t, Q, mixed=True)
+    Pd = _multi_device(t, Q, mixed=False)
+    errs = [rel_l2(Pm[:, c], Pd[:, c]) for c in range(k)]
+    assert max(errs) < tol, (int(np.argmax(errs)), max(errs))
+    t.close()
