@@ -481,6 +481,10 @@ void DeviceTree::init(const Plan& P, int device) {
             }
             ps.push_back((int)s0.size());
         }
+        for (size_t i = 0; i < tc.size(); ++i) {
+            near_max_trg_ = std::max(near_max_trg_, tc[i]);
+            near_max_pairs_ = std::max(near_max_pairs_, ps[i + 1] - ps[i]);
+        }
         near_.trg = trg_;
         near_.src = src_;
         near_.pot = pot_sorted_;

@@ -98,6 +98,7 @@ class DeviceTree {
     size_t bytes_ = 0;
     int launches_ = 0;
     int64_t near_pairs_culled_ = 0, near_pairs_nominal_ = 0;
+    int near_max_trg_ = 0, near_max_pairs_ = 0;  // largest target count / source-box count of a near-field leaf
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev_[5]{};
     std::vector<void*> allocs_;

@@ -16,6 +16,7 @@
 #include <stdexcept>
 
 #include "device_tree.hpp"
+#include "nufft_multi.cuh"
 #include "tc_kernels.cuh"
 
 namespace pdmkb {
@@ -781,6 +782,7 @@ struct DeviceTree::MultiState {
     std::vector<Lev> lev;
     float4 *src_hi = nullptr, *src_lo = nullptr, *trg_hi = nullptr, *trg_lo = nullptr;
     int* err = nullptr;  // set by tensor-core kernels whose pipeline wait timed out
+    double* esw = nullptr;  // NUFFT spreading weights per sorted target (3 x W)
 
     template <typename T>
     T* alloc(size_t n) {
@@ -843,6 +845,8 @@ DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
     m->grid = m->alloc<double>((size_t)(n_grid_ * kb));
     m->err = m->alloc<int>(1);
     PDMK_CUDA_CHECK(cudaMemsetAsync(m->err, 0, sizeof(int), stream_));
+    m->esw = m->alloc<double>((size_t)n_ * 3 * nufft_.w);
+    dev::launch_es_weights(nufft_, n_, m->esw, stream_);
     m->spec = m->alloc<cd>((size_t)(n_spec_ * kb));
     {
         int dims[3] = {nufft_.n1, nufft_.n2, nufft_.n3};
@@ -1051,7 +1055,21 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         a.pair_src_start = near_.pair_src_start; a.pair_src_count = near_.pair_src_count;
         a.pair_bsize = near_.pair_bsize; a.n_leaves = near_.n_leaves; a.N = n_; a.kb = kb;
         for (int i = 0; i < near_.nc; ++i) a.coef[i] = near_.coef[i];
+        bool tc_done = false;
         if constexpr (f32) {
+            if (near_max_pairs_ <= dev::kNearTcMaxPairs) {
+                dev::NearTc t{};
+                t.trg_start = near_.trg_start; t.trg_count = near_.trg_count; t.pair_start = near_.pair_start;
+                t.pair_src_start = near_.pair_src_start; t.pair_src_count = near_.pair_src_count;
+                t.pair_bsize = near_.pair_bsize; t.n_leaves = near_.n_leaves; t.max_trg = near_max_trg_;
+                t.N = n_; t.kb = kb;
+                for (int i = 0; i < near_.nc; ++i) t.coef[i] = near_.coef[i];
+                tc_done = dev::launch_near_tc(t, near_.nc, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo,
+                                              reinterpret_cast<const float*>(src_q), m.pot, m.err, s);
+            }
+        }
+        if (tc_done) {
+        } else if constexpr (f32) {
             if (kb >= 16)
                 dev::launch_near_m32_kb<16>(a, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo, reinterpret_cast<const float*>(src_q),
                                             m.pot, near_.nc, s);
@@ -1080,13 +1098,13 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         na.rhs_grid_stride = n_grid_;
         na.rhs_far_stride = n_;
         PDMK_CUDA_CHECK(cudaMemsetAsync(m.grid, 0, sizeof(double) * n_grid_ * kb, s));
-        dev::launch_spread(na, nufft_max_jk_, nufft_max_ex_, s, kb); ++nl;
+        dev::launch_spread_multi(na, m.esw, nufft_max_jk_, nufft_max_ex_, kb, s); ++nl;
         if (cufftExecD2Z(m.fwd, m.grid, reinterpret_cast<cufftDoubleComplex*>(m.spec)) != CUFFT_SUCCESS)
             throw std::runtime_error("cuFFT error in the batched forward transform");
         dev::launch_multiply(m.spec, mult_, n_spec_, s, kb); ++nl;
         if (cufftExecZ2D(m.inv, reinterpret_cast<cufftDoubleComplex*>(m.spec), m.grid) != CUFFT_SUCCESS)
             throw std::runtime_error("cuFFT error in the batched inverse transform");
-        dev::launch_interp(na, s, kb); ++nl;
+        dev::launch_interp_multi(na, m.esw, n_, kb, s); ++nl;
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
     {

@@ -1,0 +1,248 @@
+// Far-field NUFFT spreading / interpolation for blocks of RHS (FP64).
+//
+// The spreading-kernel weights of a target depend only on its position, so
+// they are evaluated once per tree (k_es_weights) and shared by every RHS of
+// every block and by both the spread and the interpolation.  Spread keeps the
+// per-bin subgrid layout of the single-RHS kernel (thread = (y,z) column, x in
+// registers) with an inner block of CB RHS per thread; interpolation runs one
+// thread per target with CB RHS accumulated in registers.
+// Grid layout (cuFFT batched real input): grid[c * rhs_grid_stride + (x*n2 + y)*n3 + z].
+#include <stdexcept>
+
+#include "kernels.cuh"
+#include "nufft_multi.cuh"
+
+namespace pdmkb {
+namespace dev {
+
+namespace {
+
+// exponential-of-semicircle kernel phi(z) = exp(beta (sqrt(1 - z^2) - 1)), |z| < 1
+__device__ __forceinline__ double es_phi(double z, double beta) {
+    const double z2 = z * z;
+    return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
+}
+
+__device__ __forceinline__ int wrap_index(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+template <int W>
+__global__ void k_es_weights(NufftArgs a, int64_t n, double* __restrict__ w) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double4 tt = a.pt_t[t];
+    const int4 l0 = a.pt_l0[t];
+    const double hw = 0.5 * W;
+    double* o = w + t * 3 * W;
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+        o[c] = es_phi((tt.x - (double)(l0.x + c)) / hw, a.es_beta);
+        o[W + c] = es_phi((tt.y - (double)(l0.y + c)) / hw, a.es_beta);
+        o[2 * W + c] = es_phi((tt.z - (double)(l0.z + c)) / hw, a.es_beta);
+    }
+}
+
+template <int W, int NX, int CB>
+__global__ void __launch_bounds__(128) k_spread_m(NufftArgs a, const double* __restrict__ esw) {
+    constexpr int TS = 32;
+    __shared__ double sBx[TS][NX];
+    __shared__ double sKy[TS][W], sKz[TS][W];
+    __shared__ int sOy[TS], sOz[TS];
+    __shared__ double sQ[CB][TS];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const int4 org = a.sub_origin[e], ext = a.sub_extent[e];
+    const int c0 = blockIdx.z * CB;
+    const int jk = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool active = jk < ext.y * ext.z;
+    const int ez = max(ext.z, 1);
+    const int kk = jk % ez, jj = jk / ez;
+    double acc[NX][CB];
+#pragma unroll
+    for (int i = 0; i < NX; ++i)
+#pragma unroll
+        for (int c = 0; c < CB; ++c) acc[i][c] = 0.0;
+    for (int base = 0; base < nt; base += TS) {
+        const int m = min(TS, nt - base);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < TS * NX; idx += blockDim.x) {
+            const int s = idx / NX, i = idx - s * NX;
+            double v = 0.0;
+            if (s < m) {
+                const int o = i - (a.pt_l0[t0 + base + s].x - org.x);
+                if (o >= 0 && o < W) v = esw[(int64_t)(t0 + base + s) * 3 * W + o];
+            }
+            sBx[s][i] = v;
+        }
+        for (int idx = threadIdx.x; idx < TS * 2 * W; idx += blockDim.x) {
+            const int s = idx / (2 * W), r = idx - s * 2 * W;
+            const double v = s < m ? esw[(int64_t)(t0 + base + s) * 3 * W + W + r] : 0.0;
+            if (r < W)
+                sKy[s][r] = v;
+            else
+                sKz[s][r - W] = v;
+        }
+        for (int idx = threadIdx.x; idx < CB * TS; idx += blockDim.x) {
+            const int c = idx / TS, s = idx - c * TS;
+            sQ[c][s] = s < m ? a.q_sorted[(int64_t)(c0 + c) * a.rhs_q_stride + t0 + base + s] : 0.0;
+        }
+        if (threadIdx.x < TS) {
+            const int s = threadIdx.x;
+            if (s < m) {
+                const int4 l0 = a.pt_l0[t0 + base + s];
+                sOy[s] = l0.y - org.y;
+                sOz[s] = l0.z - org.z;
+            } else {
+                sOy[s] = sOz[s] = -(1 << 20);
+            }
+        }
+        __syncthreads();
+        if (active) {
+            for (int s = 0; s < m; ++s) {
+                const int dj = jj - sOy[s], dk = kk - sOz[s];
+                if (dj < 0 || dj >= W || dk < 0 || dk >= W) continue;
+                const double kyz = sKy[s][dj] * sKz[s][dk];
+                double f[CB];
+#pragma unroll
+                for (int c = 0; c < CB; ++c) f[c] = kyz * sQ[c][s];
+#pragma unroll
+                for (int i = 0; i < NX; ++i) {
+                    const double bx = sBx[s][i];
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) acc[i][c] = fma(f[c], bx, acc[i][c]);
+                }
+            }
+        }
+    }
+    if (!active) return;
+    const int gy = wrap_index(org.y + jj, a.n2), gz = wrap_index(org.z + kk, a.n3);
+#pragma unroll
+    for (int i = 0; i < NX; ++i) {
+        if (i >= ext.x) continue;
+        const int gx = wrap_index(org.x + i, a.n1);
+        const int64_t cell = ((int64_t)gx * a.n2 + gy) * a.n3 + gz;
+#pragma unroll
+        for (int c = 0; c < CB; ++c)
+            if (acc[i][c] != 0.0) atomicAdd(a.grid + (int64_t)(c0 + c) * a.rhs_grid_stride + cell, acc[i][c]);
+    }
+}
+
+template <int W, int CB>
+__global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __restrict__ esw, int64_t n) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int c0 = blockIdx.y * CB;
+    const int4 l0 = a.pt_l0[t];
+    const double* wt = esw + t * 3 * W;
+    double wy[W], wz[W];
+    int iy[W], iz[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+        wy[c] = wt[W + c];
+        wz[c] = wt[2 * W + c];
+        iy[c] = wrap_index(l0.y + c, a.n2);
+        iz[c] = wrap_index(l0.z + c, a.n3);
+    }
+    const double* g0 = a.grid + (int64_t)c0 * a.rhs_grid_stride;
+    double u[CB];
+#pragma unroll
+    for (int c = 0; c < CB; ++c) u[c] = 0.0;
+    // x taps stay rolled (weights re-read from L1) so that the y/z tap arrays stay in registers
+#pragma unroll 1
+    for (int ia = 0; ia < W; ++ia) {
+        const double wxa = wt[ia];
+        const int64_t gx = (int64_t)wrap_index(l0.x + ia, a.n1) * a.n2;
+#pragma unroll
+        for (int ib = 0; ib < W; ++ib) {
+            const double wxy = wxa * wy[ib];
+            const double* row = g0 + (gx + iy[ib]) * a.n3;
+#pragma unroll
+            for (int ic = 0; ic < W; ++ic) {
+                const double w = wxy * wz[ic];
+                const double* p = row + iz[ic];
+#pragma unroll
+                for (int c = 0; c < CB; ++c) u[c] = fma(w, __ldg(p + (int64_t)c * a.rhs_grid_stride), u[c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + t] = u[c];
+}
+
+template <int W>
+void spread_w(const NufftArgs& a, const double* esw, int max_jk, int max_ex, int nrhs, cudaStream_t s) {
+    const int yb = (max_jk + 127) / 128;
+    if (max_ex <= 16) {
+        if (nrhs % 4 == 0) {
+            k_spread_m<W, 16, 4><<<dim3(a.n_leaves, yb, nrhs / 4), 128, 0, s>>>(a, esw);
+            return;
+        }
+        k_spread_m<W, 16, 1><<<dim3(a.n_leaves, yb, nrhs), 128, 0, s>>>(a, esw);
+    } else if (max_ex <= 32) {
+        if (nrhs % 2 == 0) {
+            k_spread_m<W, 32, 2><<<dim3(a.n_leaves, yb, nrhs / 2), 128, 0, s>>>(a, esw);
+            return;
+        }
+        k_spread_m<W, 32, 1><<<dim3(a.n_leaves, yb, nrhs), 128, 0, s>>>(a, esw);
+    } else if (max_ex <= 48) {
+        k_spread_m<W, 48, 1><<<dim3(a.n_leaves, yb, nrhs), 128, 0, s>>>(a, esw);
+    } else {
+        throw std::runtime_error("NUFFT leaf subgrid too large");
+    }
+}
+
+template <int W>
+void interp_w(const NufftArgs& a, const double* esw, int64_t n, int nrhs, cudaStream_t s) {
+    const unsigned bx = (unsigned)((n + 127) / 128);
+    if (nrhs % 8 == 0)
+        k_interp_m<W, 8><<<dim3(bx, nrhs / 8), 128, 0, s>>>(a, esw, n);
+    else
+        k_interp_m<W, 1><<<dim3(bx, nrhs), 128, 0, s>>>(a, esw, n);
+}
+
+}  // namespace
+
+#define PDMK_NUFFT_W_SWITCH(W_, CALL)                                                                   \
+    switch (W_) {                                                                                       \
+        case 4: CALL(4); break;                                                                         \
+        case 5: CALL(5); break;                                                                         \
+        case 6: CALL(6); break;                                                                         \
+        case 7: CALL(7); break;                                                                         \
+        case 8: CALL(8); break;                                                                         \
+        case 9: CALL(9); break;                                                                         \
+        case 10: CALL(10); break;                                                                       \
+        case 11: CALL(11); break;                                                                       \
+        case 12: CALL(12); break;                                                                       \
+        case 13: CALL(13); break;                                                                       \
+        case 14: CALL(14); break;                                                                       \
+        default: throw std::runtime_error("unsupported NUFFT kernel width");                            \
+    }
+
+void launch_es_weights(const NufftArgs& a, int64_t n, double* w, cudaStream_t s) {
+    if (n <= 0) return;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+#define PDMK_ESW(W) k_es_weights<W><<<blocks, 256, 0, s>>>(a, n, w)
+    PDMK_NUFFT_W_SWITCH(a.w, PDMK_ESW)
+#undef PDMK_ESW
+}
+
+void launch_spread_multi(const NufftArgs& a, const double* esw, int max_jk, int max_ex, int nrhs, cudaStream_t s) {
+    if (a.n_leaves <= 0 || nrhs <= 0) return;
+#define PDMK_SPW(W) spread_w<W>(a, esw, max_jk, max_ex, nrhs, s)
+    PDMK_NUFFT_W_SWITCH(a.w, PDMK_SPW)
+#undef PDMK_SPW
+}
+
+void launch_interp_multi(const NufftArgs& a, const double* esw, int64_t n, int nrhs, cudaStream_t s) {
+    if (n <= 0 || nrhs <= 0) return;
+#define PDMK_INW(W) interp_w<W>(a, esw, n, nrhs, s)
+    PDMK_NUFFT_W_SWITCH(a.w, PDMK_INW)
+#undef PDMK_INW
+}
+
+#undef PDMK_NUFFT_W_SWITCH
+
+}  // namespace dev
+}  // namespace pdmkb

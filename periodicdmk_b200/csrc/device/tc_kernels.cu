@@ -330,5 +330,336 @@ bool launch_c2proxy_tc(const C2ProxyArgs& a, const float* src_q, float* proxy_up
     }
 }
 
+// ===========================================================================
+// Residual near field on the tensor cores.
+//   D[t, c] = sum_s K(t, s) Q[c, s]  per source box, A = K (targets x sources),
+//   B = Q (RHS x sources), both K-major in shared memory, 32 sources per chunk.
+// Per chunk: warps generate A (kernel values) and B (charges) into one of two
+// stages; one thread issues 4 k-steps x 3 TF32 MMAs into the accumulator of
+// the current source box (two TMEM buffers of 64 columns alternate by box).
+// When a box ends, warps 0-3 (TMEM lanes = targets) add its accumulator to
+// FP64 sums in shared memory while the next box proceeds.
+// ===========================================================================
+namespace {
+
+constexpr int kNKC = 32;            // sources per chunk
+constexpr int kNKCH = kNKC / 4;     // 16-byte K chunks per operand row
+constexpr int kNThreads = 512;
+constexpr int kNSBO = kNKCH * 128;  // bytes between 8-row groups
+constexpr int kNA = 128 * kNKC * 4; // bytes of one A part
+constexpr int kNB = 64 * kNKC * 4;  // bytes of one B part (64 RHS rows)
+constexpr int kN_OFF_AH = 0, kN_OFF_AL = kNA, kN_OFF_BH = 2 * kNA, kN_OFF_BL = 2 * kNA + kNB;
+constexpr int kNStage = 2 * kNA + 2 * kNB;
+constexpr int kN_OFF_SRC = 2 * kNStage;          // [2][hi 32 float4 | lo 32 float4]
+constexpr int kNSrc = kNKC * 32;
+constexpr int kN_OFF_ACC = kN_OFF_SRC + 2 * kNSrc;  // double [64][128]
+constexpr int kN_OFF_PAIR = kN_OFF_ACC + 64 * 128 * 8;
+constexpr int kNPairBytes = kNearTcMaxPairs * 24;   // int start, count, nch; float d2max, rsc, cen
+constexpr int kN_OFF_BAR = kN_OFF_PAIR + kNPairBytes;
+constexpr int kNSmem = kN_OFF_BAR + 64;
+static_assert(kNSmem <= 227 * 1024, "near smem");
+
+struct NearPair {
+    int start, count, nch;
+    float d2max, rsc, cen;
+};
+
+struct ChunkCur {
+    int p, j;
+};
+
+template <int NC>
+__global__ void __launch_bounds__(kNThreads, 1)
+    k_near_tc(NearTc a, const float4* __restrict__ trg_hi, const float4* __restrict__ trg_lo,
+              const float4* __restrict__ src_hi, const float4* __restrict__ src_lo, const float* __restrict__ src_q,
+              double* __restrict__ pot, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const int m0 = blockIdx.y * 128;
+    if (m0 >= nt) return;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kN_OFF_BAR);  // [0,1] stage free, [2,3] box accumulated
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kN_OFF_BAR + 32);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kN_OFF_BAR + 36);  // [3]
+    int* s_np = reinterpret_cast<int*>(sm + kN_OFF_BAR + 48);
+    int* s_nch = reinterpret_cast<int*>(sm + kN_OFF_BAR + 52);
+    NearPair* pairs = reinterpret_cast<NearPair*>(sm + kN_OFF_PAIR);
+    double* acc64 = reinterpret_cast<double*>(sm + kN_OFF_ACC);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int kb = a.kb;
+    const int NBp = (kb + 15) & ~15;
+
+    if (warp == 0) {
+        tc::tmem_alloc(s_tmem, 128);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::mbar_init(&bar[2], 1);
+        tc::mbar_init(&bar[3], 1);
+        s_abort[0] = s_abort[1] = s_abort[2] = 0;
+        int np = 0, nch = 0;
+        for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
+            const int cnt = a.pair_src_count[pr];
+            if (cnt <= 0 || np >= kNearTcMaxPairs) continue;
+            const double b = a.pair_bsize[pr];
+            NearPair q;
+            q.start = a.pair_src_start[pr];
+            q.count = cnt;
+            q.nch = (cnt + kNKC - 1) / kNKC;
+            q.d2max = (float)(b * b);
+            q.rsc = (float)(2.0 / b);
+            q.cen = (float)(-0.5 * b);
+            pairs[np++] = q;
+            nch += q.nch;
+        }
+        *s_np = np;
+        *s_nch = nch;
+        tc::fence_mbar_init();
+    }
+    for (int i = tid; i < 64 * 128; i += kNThreads) acc64[i] = 0.0;
+
+    // A role: target row am, source groups ag0 and ag0 + 4
+    const int am = tid & 127, ag0 = tid >> 7;
+    const bool tval = m0 + am < nt;
+    const float4 th = tval ? trg_hi[t0 + m0 + am] : make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+    const float4 tl = tval ? trg_lo[t0 + m0 + am] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float cf[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) cf[i] = (float)a.coef[i];
+    // B role (warps 4-7): RHS group bcg (4 RHS), source group bsg (4 sources)
+    const bool brole = tid >= 128 && tid < 256;
+    const int bcg = (tid - 128) & 15, bsg = ((tid - 128) >> 4) & 7;
+    // position prefetch role (warps 8-9): source tid-256 (hi) or tid-288 (lo)
+    const bool prole = tid >= 256 && tid < 256 + 2 * kNKC;
+    const int ps_ = (tid - 256) & (kNKC - 1);
+    const bool plo = tid >= 256 + kNKC;
+
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *s_tmem;
+    const int np = *s_np, nchunks = *s_nch;
+
+    auto advance = [&](ChunkCur c) {
+        if (++c.j >= pairs[c.p].nch) {
+            c.j = 0;
+            ++c.p;
+        }
+        return c;
+    };
+    auto chunk_src = [&](ChunkCur c, int& g0, int& n) {
+        const NearPair& q = pairs[c.p];
+        g0 = q.start + c.j * kNKC;
+        n = min(kNKC, q.count - c.j * kNKC);
+    };
+    auto load_q = [&](ChunkCur c, float (&qv)[4][4]) {
+        int g0, n;
+        chunk_src(c, g0, n);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int s = bsg * 4 + u;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int cc = bcg * 4 + i;
+                qv[u][i] = (s < n && cc < kb) ? __ldg(src_q + (int64_t)(g0 + s) * kb + cc) : 0.0f;
+            }
+        }
+    };
+    auto load_pos = [&](ChunkCur c) -> float4 {
+        int g0, n;
+        chunk_src(c, g0, n);
+        if (ps_ >= n) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return plo ? __ldg(src_lo + g0 + ps_) : __ldg(src_hi + g0 + ps_);
+    };
+    auto store_pos = [&](int buf, float4 v) {
+        float4* dst = reinterpret_cast<float4*>(sm + kN_OFF_SRC + buf * kNSrc);
+        dst[(plo ? kNKC : 0) + ps_] = v;
+    };
+    auto drain = [&](int bb) -> bool {
+        // warps 0-3: add box bb's accumulator (TMEM buffer bb & 1) to the FP64 sums
+        const bool waited = tc::mbar_wait(&bar[2 + (bb & 1)], (bb >> 1) & 1);
+        if (!__all_sync(0xffffffffu, waited)) return false;  // keep the warp-collective loads uniform
+        tc::fence_after_sync();
+        const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((bb & 1) * 64);
+        for (int c0 = 0; c0 < NBp; c0 += 16) {
+            float v[16];
+            tc::tmem_ld_x8(base + c0, v);
+            tc::tmem_ld_x8(base + c0 + 8, v + 8);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc64[(c0 + i) * 128 + am] += (double)v[i];
+        }
+        tc::fence_before_sync();
+        return true;
+    };
+
+    float qcur[4][4], qnext[4][4];
+    float4 pnext = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    ChunkCur c0 = {0, 0}, c1 = c0, c2 = c0;
+    if (nchunks > 0) {
+        if (brole) load_q(c0, qcur);
+        if (prole) store_pos(0, load_pos(c0));
+        if (nchunks > 1) {
+            c1 = advance(c0);
+            if (prole) pnext = load_pos(c1);
+        }
+        if (nchunks > 2) c2 = advance(c1);
+    }
+    __syncthreads();
+
+    int issued = 0;
+    for (int q = 0; q < nchunks; ++q) {
+        const int st = q & 1;
+        const int b = c0.p;
+        const NearPair pr = pairs[b];
+        const bool first = c0.j == 0, last = c0.j == pr.nch - 1;
+        const int nv = min(kNKC, pr.count - c0.j * kNKC);
+        if (q + 1 < nchunks) {
+            if (brole) load_q(c1, qnext);
+            if (prole) {
+                store_pos(st ^ 1, pnext);
+                if (q + 2 < nchunks) pnext = load_pos(c2);
+            }
+        }
+        if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1)) s_abort[st] = 1;
+        unsigned char* stage = sm + st * kNStage;
+        const float4* sh = reinterpret_cast<const float4*>(sm + kN_OFF_SRC + st * kNSrc);
+        const float4* sl = sh + kNKC;
+        // A: kernel values for target am, sources 4g..4g+3
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int g = ag0 + 4 * u;
+            float r2v[4];
+            bool anyin = false;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int s = 4 * g + k;
+                const float4 yh = sh[s], yl = sl[s];
+                const float dx = (th.x - yh.x) + (tl.x - yl.x);
+                const float dy = (th.y - yh.y) + (tl.y - yl.y);
+                const float dz = (th.z - yh.z) + (tl.z - yl.z);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool in = s < nv && r2 > 1e-30f && r2 < pr.d2max;
+                r2v[k] = in ? r2 : -1.0f;
+                anyin |= in;
+            }
+            float w[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (__any_sync(0xffffffffu, anyin)) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float r2 = r2v[k] > 0.0f ? r2v[k] : 1.0f;
+                    const float rinv = rsqrtf(r2);
+                    const float x = fmaf(r2, rinv, pr.cen) * pr.rsc;
+                    float pv = cf[NC - 1];
+#pragma unroll
+                    for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, cf[i]);
+                    w[k] = r2v[k] > 0.0f ? pv * rinv : 0.0f;
+                }
+            }
+            const uint32_t off = tc::kmajor_offset(am, 4 * g, kNKCH);
+            split_store(make_float4(w[0], w[1], w[2], w[3]), stage + kN_OFF_AH + off, stage + kN_OFF_AL + off);
+        }
+        // B: charges, rows = RHS, K = sources
+        if (brole) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int cc = bcg * 4 + i;
+                const uint32_t off = tc::kmajor_offset(cc, 4 * bsg, kNKCH);
+                split_store(make_float4(qcur[0][i], qcur[1][i], qcur[2][i], qcur[3][i]), stage + kN_OFF_BH + off,
+                            stage + kN_OFF_BL + off);
+            }
+        }
+        // the previous box is complete: fold its accumulator into the FP64 sums
+        if (first && b > 0 && warp < 4) {
+            if (!drain(b - 1)) s_abort[st] = 1;
+        }
+        tc::fence_proxy_async();
+        __syncthreads();
+        if (s_abort[st]) break;
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t base = tc::smem_u32(stage);
+            const uint32_t idesc = tc::idesc_tf32(128, NBp);
+            const uint32_t d = tmem + (uint32_t)((b & 1) * 64);
+#pragma unroll
+            for (int ks = 0; ks < kNKC / 8; ++ks) {
+                const uint32_t kofs = ks * 256;
+                const uint64_t ah = tc::smem_desc_k_noswizzle(base + kN_OFF_AH + kofs, 128, kNSBO);
+                const uint64_t alo = tc::smem_desc_k_noswizzle(base + kN_OFF_AL + kofs, 128, kNSBO);
+                const uint64_t bh = tc::smem_desc_k_noswizzle(base + kN_OFF_BH + kofs, 128, kNSBO);
+                const uint64_t blo = tc::smem_desc_k_noswizzle(base + kN_OFF_BL + kofs, 128, kNSBO);
+                tc::mma_tf32(d, ah, bh, idesc, (first && ks == 0) ? 0u : 1u);
+                tc::mma_tf32(d, ah, blo, idesc, 1u);
+                tc::mma_tf32(d, alo, bh, idesc, 1u);
+            }
+            tc::commit(&bar[st]);
+            if (last) tc::commit(&bar[2 + (b & 1)]);
+        }
+        issued = q + 1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) qcur[u][i] = qnext[u][i];
+        c0 = c1;
+        c1 = c2;
+        if (q + 3 < nchunks) c2 = advance(c2);
+    }
+    bool ok = s_abort[0] == 0 && s_abort[1] == 0;
+    if (ok && issued > 0 && warp < 4) {
+        if (!drain(np - 1)) s_abort[2] = 1;
+    } else if (!ok && issued > 0) {
+        const int ql = issued - 1;
+        tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1);
+    }
+    __syncthreads();
+    ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;
+    if (ok) {
+        for (int i = tid; i < kb * 128; i += kNThreads) {
+            const int c = i >> 7, mm = i & 127;
+            if (m0 + mm < nt) pot[(int64_t)c * a.N + t0 + m0 + mm] += acc64[c * 128 + mm];
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 128);
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+}
+
+template <int NC>
+void launch_near_tc_nc(const NearTc& a, const float4* th, const float4* tl, const float4* sh, const float4* sl,
+                       const float* q, double* pot, int* err, cudaStream_t s) {
+    static bool configured[64] = {};
+    int dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+    if (!configured[dev]) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_near_tc<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNSmem));
+        configured[dev] = true;
+    }
+    const dim3 grid(a.n_leaves, (a.max_trg + 127) / 128);
+    k_near_tc<NC><<<grid, kNThreads, kNSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
+}
+
+}  // namespace
+
+bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4* trg_lo, const float4* src_hi,
+                    const float4* src_lo, const float* src_q, double* pot, int* err, cudaStream_t s) {
+    if (a.kb < 1 || a.kb > 64 || a.n_leaves <= 0 || a.max_trg <= 0) return false;
+    switch (nc) {
+#define PDMK_NTC(NC)                                                                  \
+    case NC: launch_near_tc_nc<NC>(a, trg_hi, trg_lo, src_hi, src_lo, src_q, pot, err, s); \
+        return true;
+        PDMK_NTC(5) PDMK_NTC(6) PDMK_NTC(9) PDMK_NTC(11) PDMK_NTC(12)
+#undef PDMK_NTC
+        default: return false;
+    }
+}
+
 }  // namespace dev
 }  // namespace pdmkb

@@ -17,5 +17,30 @@ namespace dev {
 bool launch_c2proxy_tc(const C2ProxyArgs& a, const float* src_q, float* proxy_up, int kb, int p, int* err,
                        cudaStream_t s);
 
+// Residual near field of kb charge vectors as a GEMM per (target leaf, 128-target tile):
+//   pot[c*N + t] += sum_s K(t,s) q[s*kb + c],   K(t,s) = P((r - b/2) 2/b) / r for 1e-30 < r^2 < b^2
+// over the leaf's list-1 source boxes (b per box).  The kernel values are
+// generated from double-float coordinates in FP32 on the CUDA cores, the
+// products run on the tensor cores (TF32 hi/lo split) into a tensor-memory
+// accumulator per source box, and each box's sum is added to FP64
+// accumulators.  Covers nc in {5, 6, 9, 11, 12}, 1 <= kb <= 64 and leaves with
+// at most 128 source boxes.
+struct NearTc {
+    const int* trg_start;
+    const int* trg_count;
+    const int* pair_start;  // CSR over target leaves
+    const int* pair_src_start;
+    const int* pair_src_count;
+    const double* pair_bsize;
+    double coef[32];
+    int n_leaves;
+    int max_trg;  // largest trg_count (grid extent over 128-target tiles)
+    int64_t N;
+    int kb;
+};
+constexpr int kNearTcMaxPairs = 128;
+bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4* trg_lo, const float4* src_hi,
+                    const float4* src_lo, const float* src_q, double* pot, int* err, cudaStream_t s);
+
 }  // namespace dev
 }  // namespace pdmkb
