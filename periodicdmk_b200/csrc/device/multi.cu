@@ -17,6 +17,7 @@
 
 #include "device_tree.hpp"
 #include "nufft_multi.cuh"
+#include "pw_fused.cuh"
 #include "tc_kernels.cuh"
 
 namespace pdmkb {
@@ -976,7 +977,15 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         });
     }
     // outgoing plane waves
+    const bool pw_fused = dev::pw_fused_supported<T>(p, n, n2);
     for (const auto& g : pw_groups_) {
+        if (pw_fused) {
+            dev::PwFused f{};
+            f.in = up; f.in_off = g.in_off; f.out = pw; f.out_off = g.out_off;
+            f.mat_a = levtab(g.level, 0); f.mat_b = levtab(g.level, 1); f.rhs = kb; f.e0 = 0;
+            dev::launch_pw_out_fused<T>(f, p, n, n2, g.n * kb, s); ++nl;
+            continue;
+        }
         const int64_t e1 = (int64_t)p * p * n, e2 = (int64_t)p * n * n;
         chunked(g.n, (int64_t)sizeof(C) * std::max(e1, e2), [&](int64_t e0, int ne) {
             dev::ContractM a{};
@@ -1004,6 +1013,13 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                 dev::k_shift_m<T><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
                                                        static_cast<C*>(m.pw_in), M, E.term_start, E.term_slot,
                                                        E.term_stencil, kb, b0); ++nl;
+            }
+            if (pw_fused) {
+                dev::PwFused f{};
+                f.in = m.pw_in; f.in_stride = M; f.out = down; f.out_off = E.down_off;
+                f.mat_a = levtab(E.level, 2); f.mat_b = levtab(E.level, 3); f.rhs = kb; f.e0 = (int64_t)b0 * kb;
+                dev::launch_pw_in_fused<T>(f, p, n, n2, nb * kb, s); ++nl;
+                continue;
             }
             dev::ContractM a{};
             a.rhs = kb; a.e0 = (int64_t)b0 * kb; a.n_entries = nb * kb;
