@@ -82,6 +82,7 @@ void DeviceTree::init(const Plan& P, int device) {
     PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto& e : ev_) PDMK_CUDA_CHECK(cudaEventCreate(&e));
 
+    if (const char* tm = std::getenv("PDMK_TC_MASK")) tc_mask_ = std::atoi(tm) & 7;
     n_ = P.n_src;
     n_digits_ = P.dp.n_digits_tree;
     n_all_ = P.n_all;
@@ -407,6 +408,7 @@ void DeviceTree::init(const Plan& P, int device) {
         eval_.proxy_down = proxy_down_;
         eval_.pot = pot_sorted_;
         eval_.n_leaves = (int)slot.size();
+        for (int c : tc) eval_max_trg_ = std::max(eval_max_trg_, c);
         eval_.slot = upload(slot);
         eval_.trg_start = upload(t0);
         eval_.trg_count = upload(tc);

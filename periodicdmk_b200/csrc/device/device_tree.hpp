@@ -82,6 +82,10 @@ class DeviceTree {
   public:
     bool last_was_multi_ = false;
     int multi_launches_ = 0;  // kernels launched by the last multi-RHS evaluate
+    // Tensor-core kernels the mixed-precision path may use (bit 0 proxy
+    // moments, bit 1 near field, bit 2 leaf evaluation); the CUDA-core
+    // kernels cover the rest.  Initialised from PDMK_TC_MASK (default 7).
+    int tc_mask_ = 7;
 
   private:
     void init(const Plan& P, int device);
@@ -98,7 +102,8 @@ class DeviceTree {
     size_t bytes_ = 0;
     int launches_ = 0;
     int64_t near_pairs_culled_ = 0, near_pairs_nominal_ = 0;
-    int near_max_trg_ = 0, near_max_pairs_ = 0;  // largest target count / source-box count of a near-field leaf
+    int near_max_trg_ = 0, near_max_pairs_ = 0;
+    int eval_max_trg_ = 0;  // largest target count of an evaluated leaf  // largest target count / source-box count of a near-field leaf
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev_[5]{};
     std::vector<void*> allocs_;

@@ -931,7 +931,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     if (c2x_.n_centers > 0) {
         bool done = false;
         if constexpr (f32) {
-            done = dev::launch_c2proxy_tc(c2x_, src_q, up, kb, p, m.err, s);
+            if (tc_mask_ & 1) done = dev::launch_c2proxy_tc(c2x_, src_q, up, kb, p, m.err, s);
         }
         if (done) {
             ++nl;
@@ -1052,8 +1052,20 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             });
         }
     }
-    // leaf evaluation
-    if (eval_.n_leaves > 0) {
+    // leaf evaluation: tensor-core GEMM for FP32 blocks of 16/32/64 RHS, else CUDA cores
+    bool eval_done = false;
+    if constexpr (f32) {
+        if ((tc_mask_ & 4) && eval_.n_leaves > 0) {
+            dev::EvalTc t{};
+            t.trg = trg_; t.proxy_down = reinterpret_cast<const float*>(down); t.pot = m.pot;
+            t.n_leaves = eval_.n_leaves; t.max_trg = eval_max_trg_; t.slot = eval_.slot;
+            t.trg_start = eval_.trg_start; t.trg_count = eval_.trg_count; t.center_scale = eval_.center_scale;
+            t.N = n_;
+            eval_done = dev::launch_eval_tc(t, p, kb, m.err, s);
+            if (eval_done) ++nl;
+        }
+    }
+    if (eval_.n_leaves > 0 && !eval_done) {
         const dim3 grid(eval_.n_leaves, 1, kb);
         switch (p) {
             case 9: dev::k_eval_g<T, 9, 4><<<grid, 64, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
@@ -1073,7 +1085,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         for (int i = 0; i < near_.nc; ++i) a.coef[i] = near_.coef[i];
         bool tc_done = false;
         if constexpr (f32) {
-            if (near_max_pairs_ <= dev::kNearTcMaxPairs) {
+            if ((tc_mask_ & 2) && near_max_pairs_ <= dev::kNearTcMaxPairs) {
                 dev::NearTc t{};
                 t.trg_start = near_.trg_start; t.trg_count = near_.trg_count; t.pair_start = near_.pair_start;
                 t.pair_src_start = near_.pair_src_start; t.pair_src_count = near_.pair_src_count;

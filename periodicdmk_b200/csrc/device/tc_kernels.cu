@@ -25,30 +25,39 @@ namespace dev {
 
 namespace {
 
-constexpr int kKC = 16;       // sources per pipeline stage (two MMA k-steps of 8)
-constexpr int kKCH = kKC / 4; // 16-byte K chunks per operand row
+constexpr int kKC = 32;        // sources per pipeline stage (four MMA k-steps of 8)
+constexpr int kKCH = kKC / 4;  // 16-byte K chunks per operand row
+constexpr int kSeg = 2;        // chunks accumulated in tensor memory before a drain
 constexpr int kThreads = 256;
 constexpr int kMaxKb = 64;
 constexpr int kMinKb = 16;
 
+// Columns (i, j) < P^2 are split into NSPLIT ranges so that two accumulators
+// (one being filled, one being drained) fit in the 512 tensor-memory columns.
 template <int P>
 struct C2PShape {
     static constexpr int P2 = P * P;
-    static constexpr int NB = (P2 + 15) / 16 * 16;  // B rows (i,j), padded to the MMA N granule
-    static constexpr int TMEM_COLS = NB <= 32 ? 32 : NB <= 64 ? 64 : NB <= 128 ? 128 : NB <= 256 ? 256 : 512;
-    static constexpr int SBO = kKCH * 128;  // bytes between 8-row groups
+    static constexpr int NSPLIT = 2 * ((P2 + 15) / 16 * 16) <= 512 ? 1 : 2;
+    static constexpr int CW = (P2 + NSPLIT - 1) / NSPLIT;  // columns of one CTA
+    static constexpr int NB = (CW + 15) / 16 * 16;         // B rows, padded to the MMA N granule
+    static constexpr int BUF = NB <= 128 ? 128 : 256;      // column offset of the second accumulator
+    static constexpr int TMEM_COLS = 2 * BUF <= 256 ? 256 : 512;
+    static constexpr int HALF = NB / 2;                    // drain columns per thread (two warps per lane quarter)
+    static constexpr int SBO = kKCH * 128;
     static constexpr int A_BYTES = 128 * kKC * 4;
     static constexpr int B_BYTES = NB * kKC * 4;
     static constexpr int OFF_AH = 0, OFF_AL = A_BYTES, OFF_BH = 2 * A_BYTES, OFF_BL = 2 * A_BYTES + B_BYTES;
     static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
-    // Chebyshev values of one chunk: [dim][k group][degree][4 sources], two buffers
-    static constexpr int T_FLOATS = 3 * kKCH * P * 4;
+    static constexpr int T_FLOATS = 3 * kKCH * P * 4;  // [dim][k group][degree][4 sources]
     static constexpr int OFF_T = 2 * STAGE;
     static constexpr int OFF_BAR = OFF_T + 2 * T_FLOATS * 4;
-    static constexpr int SMEM = OFF_BAR + 64;
-    static constexpr int A_ITEMS = 128 * kKCH / kThreads;  // (row, k group) items of A per thread
+    // at least 120 KB so that two CTAs never share an SM's tensor memory when TMEM_COLS is 512
+    static constexpr int SMEM_USED = OFF_BAR + 64;
+    static constexpr int SMEM = TMEM_COLS == 512 && SMEM_USED < 120 * 1024 ? 120 * 1024 : SMEM_USED;
+    static constexpr int A_ITEMS = 128 * kKCH / kThreads;
     static constexpr int B_ITEMS = (NB * kKCH + kThreads - 1) / kThreads;
-    static_assert(NB <= 512, "accumulator exceeds tensor memory");
+    static_assert(2 * BUF <= TMEM_COLS && NB <= BUF, "accumulators exceed tensor memory");
+    static_assert(HALF % 8 == 0, "drain column split");
     static_assert((128 * kKCH) % kThreads == 0, "A items per thread");
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
@@ -85,15 +94,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                  int* __restrict__ err) {
     using S = C2PShape<P>;
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);  // MMA completion, one per stage
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + S::OFF_BAR + 16);
-    volatile int* s_abort = reinterpret_cast<volatile int*>(sm + S::OFF_BAR + 20);  // [3], sticky
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);  // [0,1] stage free, [2,3] segment done
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + S::OFF_BAR + 32);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(sm + S::OFF_BAR + 36);  // [3], sticky
     float* sT = reinterpret_cast<float*>(sm + S::OFF_T);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int e = blockIdx.x;
     const int rows = P * kb;
     const int row0 = blockIdx.y * 128;
+    const int col0 = blockIdx.z * S::CW;                 // first (i, j) column of this CTA
+    const int ncol = min(S::CW, S::P2 - col0);
     const int r0 = a.rng_start[e], r1 = a.rng_start[e + 1];
     int nchunks = 0;
     for (int r = r0; r < r1; ++r) nchunks += (a.src_count[r] + kKC - 1) / kKC;
@@ -104,13 +115,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+        for (int i = 0; i < 4; ++i) tc::mbar_init(&bar[i], 1);
         s_abort[0] = s_abort[1] = s_abort[2] = 0;
         tc::fence_mbar_init();
     }
 
-    // A rows of this thread: row m = tid % 128, k groups kg0 + 2u (u < A_ITEMS)
+    // A rows of this thread: row m = tid % 128, k groups akg0 + 2u
     const int am = tid & 127, akg0 = tid >> 7;
     const int aR = row0 + am;
     const bool arow = aR < rows;
@@ -155,6 +165,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     };
 
+    // FP32 sums of the drained segments: lane quarter warp % 4 (rows), column half warp / 4
+    const int dq = warp & 3, dh = warp >> 2;
+    float accd[S::HALF];
+#pragma unroll
+    for (int i = 0; i < S::HALF; ++i) accd[i] = 0.0f;
     float qcur[S::A_ITEMS][4], qnext[S::A_ITEMS][4];
     double xnext = 0.0;
     if (nchunks > 0) {
@@ -171,10 +186,30 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *s_tmem;
+    auto drain = [&](int gg) -> bool {
+        const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1);
+        if (!__all_sync(0xffffffffu, waited)) return false;
+        tc::fence_after_sync();
+        const uint32_t base =
+            tmem + ((uint32_t)(dq * 32) << 16) + (uint32_t)((gg & 1) * S::BUF + dh * S::HALF);
+#pragma unroll
+        for (int c0 = 0; c0 < S::HALF; c0 += 8) {
+            float v[8];
+            tc::tmem_ld_x8(base + (uint32_t)c0, v);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int u = 0; u < 8; ++u) accd[c0 + u] += v[u];
+        }
+        tc::fence_before_sync();
+        return true;
+    };
+
 
     int issued = 0;  // chunks whose MMAs were issued and committed
     for (int q = 0; q < nchunks; ++q) {
         const int st = q & 1;
+        const int seg = q / kSeg;
+        const bool first = q % kSeg == 0, last = q % kSeg == kSeg - 1 || q == nchunks - 1;
         int g1 = 0, nt1 = 0, g2 = 0, nt2 = 0;
         if (q + 1 < nchunks) {
             chunk_at(a, r0, r1, q + 1, g1, nt1);
@@ -194,20 +229,21 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t off = tc::kmajor_offset(am, kg * 4, kKCH);
             split_store(v, stage + S::OFF_AH + off, stage + S::OFF_AL + off);
         }
-        // B = T_i(x_s) T_j(y_s), rows n = i + P j
+        // B = T_i(x_s) T_j(y_s), rows n - col0 for the columns n = i + P j of this CTA
 #pragma unroll
         for (int u = 0; u < S::B_ITEMS; ++u) {
             const int it = tid + u * kThreads;
             if (it < S::NB * kKCH) {
-                const int n = it % S::NB, kg = it / S::NB;
+                const int nl = it % S::NB, kg = it / S::NB;
                 float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (n < S::P2) {
+                if (nl < ncol) {
+                    const int n = col0 + nl;
                     const int i = n % P, j = n / P;
                     const float4 tx = *reinterpret_cast<const float4*>(T + ((0 * kKCH + kg) * P + i) * 4);
                     const float4 ty = *reinterpret_cast<const float4*>(T + ((1 * kKCH + kg) * P + j) * 4);
                     v = make_float4(tx.x * ty.x, tx.y * ty.y, tx.z * ty.z, tx.w * ty.w);
                 }
-                const uint32_t off = tc::kmajor_offset(n, kg * 4, kKCH);
+                const uint32_t off = tc::kmajor_offset(nl, kg * 4, kKCH);
                 split_store(v, stage + S::OFF_BH + off, stage + S::OFF_BL + off);
             }
         }
@@ -216,12 +252,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             cheb_store(st ^ 1, xnext, nt1);
             if (q + 2 < nchunks) xnext = load_x(g2, nt2);
         }
+        // the previous segment is complete: fold it into the FP32 sums
+        if (first && seg > 0) {
+            if (!drain(seg - 1)) s_abort[st] = 1;
+        }
         tc::fence_proxy_async();
         __syncthreads();
         if (s_abort[st]) break;
         if (tid == 0) {
             tc::fence_after_sync();
             const uint32_t base = tc::smem_u32(stage);
+            const uint32_t d = tmem + (uint32_t)((seg & 1) * S::BUF);
 #pragma unroll
             for (int ks = 0; ks < kKC / 8; ++ks) {
                 const uint32_t kofs = ks * 256;  // 8 K elements = two 16-byte chunks of 128 B each
@@ -234,13 +275,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t boff = (uint32_t)(n0 / 8) * S::SBO + kofs;
                     const uint64_t bh = tc::smem_desc_k_noswizzle(base + S::OFF_BH + boff, 128, S::SBO);
                     const uint64_t blo = tc::smem_desc_k_noswizzle(base + S::OFF_BL + boff, 128, S::SBO);
-                    const uint32_t d = tmem + (uint32_t)n0;
-                    tc::mma_tf32(d, ah, bh, idesc, (q > 0 || ks > 0) ? 1u : 0u);
-                    tc::mma_tf32(d, ah, blo, idesc, 1u);
-                    tc::mma_tf32(d, alo, bh, idesc, 1u);
+                    tc::mma_tf32(d + (uint32_t)n0, ah, bh, idesc, (first && ks == 0) ? 0u : 1u);
+                    tc::mma_tf32(d + (uint32_t)n0, ah, blo, idesc, 1u);
+                    tc::mma_tf32(d + (uint32_t)n0, alo, bh, idesc, 1u);
                 }
             }
             tc::commit(&bar[st]);
+            if (last) tc::commit(&bar[2 + (seg & 1)]);
         }
         issued = q + 1;
 #pragma unroll
@@ -248,49 +289,25 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int w = 0; w < 4; ++w) qcur[u][w] = qnext[u][w];
     }
-    if (issued > 0) {
+    bool ok = s_abort[0] == 0 && s_abort[1] == 0;
+    if (ok && issued > 0) {
+        if (!drain((issued - 1) / kSeg)) s_abort[2] = 1;
+    } else if (!ok && issued > 0) {
         const int ql = issued - 1;
-        if (!tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1)) s_abort[2] = 1;
+        tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1);
     }
     __syncthreads();
-    const bool ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;
+    ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;
     if (ok && issued > 0) {
-        tc::fence_after_sync();
-        const int quarter = warp & 3, half = warp >> 2;
-        const int m = quarter * 32 + lane;
+        const int m = dq * 32 + lane;
         const int R = row0 + m;
-        const bool valid = R < rows;
-        float* out = nullptr;
-        if (valid) {
+        if (R < rows) {
             const int l = R / kb, c = R - l * kb;
-            out = proxy_up + ((int64_t)a.slot[e] * kb + c) * (P * P * P) + (int64_t)S::P2 * l;
-        }
-        constexpr int HALF = S::NB / 2;
-        static_assert(HALF % 8 == 0, "epilogue column split");
-        const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
-        for (int c0 = half * HALF; c0 < half * HALF + HALF; c0 += 8) {
-            float v[8];
-            tc::tmem_ld_x8(lane_addr + (uint32_t)c0, v);
-            tc::tmem_wait_ld();
-            if (!valid) continue;
-            if constexpr (S::P2 % 4 == 0) {
+            float* out = proxy_up + ((int64_t)a.slot[e] * kb + c) * (P * P * P) + (int64_t)S::P2 * l + col0;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int n = c0 + 4 * h;
-                    if (n < S::P2) {
-                        float4* o = reinterpret_cast<float4*>(out + n);
-                        float4 w = *o;
-                        w.x += v[4 * h];
-                        w.y += v[4 * h + 1];
-                        w.z += v[4 * h + 2];
-                        w.w += v[4 * h + 3];
-                        *o = w;
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (c0 + u < S::P2) out[c0 + u] += v[u];
+            for (int i = 0; i < S::HALF; ++i) {
+                const int nl = dh * S::HALF + i;
+                if (nl < ncol) out[nl] += accd[i];
             }
         }
     }
@@ -314,7 +331,7 @@ void launch_c2proxy_tc_p(const C2ProxyArgs& a, const float* src_q, float* up, in
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_c2proxy_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
         configured[dev] = true;
     }
-    const dim3 grid(a.n_centers, (P * kb + 127) / 128);
+    const dim3 grid(a.n_centers, (P * kb + 127) / 128, S::NSPLIT);
     k_c2proxy_tc<P><<<grid, kThreads, S::SMEM, s>>>(a, src_q, up, kb, err);
 }
 
@@ -343,6 +360,7 @@ bool launch_c2proxy_tc(const C2ProxyArgs& a, const float* src_q, float* proxy_up
 namespace {
 
 constexpr int kNKC = 32;            // sources per chunk
+constexpr int kNSeg = 2;            // chunks accumulated in tensor memory before a drain
 constexpr int kNKCH = kNKC / 4;     // 16-byte K chunks per operand row
 constexpr int kNThreads = 512;
 constexpr int kNSBO = kNKCH * 128;  // bytes between 8-row groups
@@ -429,9 +447,8 @@ __global__ void __launch_bounds__(kNThreads, 1)
     float cf[NC];
 #pragma unroll
     for (int i = 0; i < NC; ++i) cf[i] = (float)a.coef[i];
-    // B role (warps 4-7): RHS group bcg (4 RHS), source group bsg (4 sources)
-    const bool brole = tid >= 128 && tid < 256;
-    const int bcg = (tid - 128) & 15, bsg = ((tid - 128) >> 4) & 7;
+    // B role (all threads): RHS row bc, source group bsg (4 sources)
+    const int bc = tid & 63, bsg = tid >> 6;
     // position prefetch role (warps 8-9): source tid-256 (hi) or tid-288 (lo)
     const bool prole = tid >= 256 && tid < 256 + 2 * kNKC;
     const int ps_ = (tid - 256) & (kNKC - 1);
@@ -441,7 +458,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *s_tmem;
-    const int np = *s_np, nchunks = *s_nch;
+    const int nchunks = *s_nch;
 
     auto advance = [&](ChunkCur c) {
         if (++c.j >= pairs[c.p].nch) {
@@ -455,17 +472,13 @@ __global__ void __launch_bounds__(kNThreads, 1)
         g0 = q.start + c.j * kNKC;
         n = min(kNKC, q.count - c.j * kNKC);
     };
-    auto load_q = [&](ChunkCur c, float (&qv)[4][4]) {
+    auto load_q = [&](ChunkCur c, float (&qv)[4]) {
         int g0, n;
         chunk_src(c, g0, n);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int s = bsg * 4 + u;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int cc = bcg * 4 + i;
-                qv[u][i] = (s < n && cc < kb) ? __ldg(src_q + (int64_t)(g0 + s) * kb + cc) : 0.0f;
-            }
+            qv[u] = (s < n && bc < kb) ? __ldg(src_q + (int64_t)(g0 + s) * kb + bc) : 0.0f;
         }
     };
     auto load_pos = [&](ChunkCur c) -> float4 {
@@ -478,29 +491,32 @@ __global__ void __launch_bounds__(kNThreads, 1)
         float4* dst = reinterpret_cast<float4*>(sm + kN_OFF_SRC + buf * kNSrc);
         dst[(plo ? kNKC : 0) + ps_] = v;
     };
-    auto drain = [&](int bb) -> bool {
-        // warps 0-3: add box bb's accumulator (TMEM buffer bb & 1) to the FP64 sums
-        const bool waited = tc::mbar_wait(&bar[2 + (bb & 1)], (bb >> 1) & 1);
+    // Add segment gg's accumulator (TMEM buffer gg & 1) to the FP64 sums.  Warp w
+    // reads TMEM lanes 32 (w % 4) .. +31 (targets) and columns 16 (w / 4) .. +15 (RHS).
+    auto drain = [&](int gg) -> bool {
+        const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1);
         if (!__all_sync(0xffffffffu, waited)) return false;  // keep the warp-collective loads uniform
         tc::fence_after_sync();
-        const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((bb & 1) * 64);
-        for (int c0 = 0; c0 < NBp; c0 += 16) {
+        const int lq = warp & 3, cg = warp >> 2;
+        if (16 * cg < NBp) {
+            const uint32_t base = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((gg & 1) * 64 + 16 * cg);
             float v[16];
-            tc::tmem_ld_x8(base + c0, v);
-            tc::tmem_ld_x8(base + c0 + 8, v + 8);
+            tc::tmem_ld_x8(base, v);
+            tc::tmem_ld_x8(base + 8, v + 8);
             tc::tmem_wait_ld();
+            const int m = lq * 32 + lane;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc64[(c0 + i) * 128 + am] += (double)v[i];
+            for (int i = 0; i < 16; ++i) acc64[(16 * cg + i) * 128 + m] += (double)v[i];
         }
         tc::fence_before_sync();
         return true;
     };
 
-    float qcur[4][4], qnext[4][4];
+    float qcur[4], qnext[4];
     float4 pnext = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     ChunkCur c0 = {0, 0}, c1 = c0, c2 = c0;
     if (nchunks > 0) {
-        if (brole) load_q(c0, qcur);
+        load_q(c0, qcur);
         if (prole) store_pos(0, load_pos(c0));
         if (nchunks > 1) {
             c1 = advance(c0);
@@ -510,15 +526,19 @@ __global__ void __launch_bounds__(kNThreads, 1)
     }
     __syncthreads();
 
-    int issued = 0;
+    // The accumulator is drained every kNSeg chunks (and at each box end): the
+    // tensor-core FP32 accumulation loses low bits on every MMA step, so each
+    // segment stays short and the sums continue in FP64 on the CUDA cores.
+    int issued = 0, seg = -1;
     for (int q = 0; q < nchunks; ++q) {
         const int st = q & 1;
         const int b = c0.p;
         const NearPair pr = pairs[b];
-        const bool first = c0.j == 0, last = c0.j == pr.nch - 1;
+        const bool first = c0.j % kNSeg == 0, last = c0.j % kNSeg == kNSeg - 1 || c0.j == pr.nch - 1;
+        if (first) ++seg;
         const int nv = min(kNKC, pr.count - c0.j * kNKC);
         if (q + 1 < nchunks) {
-            if (brole) load_q(c1, qnext);
+            load_q(c1, qnext);
             if (prole) {
                 store_pos(st ^ 1, pnext);
                 if (q + 2 < nchunks) pnext = load_pos(c2);
@@ -563,18 +583,14 @@ __global__ void __launch_bounds__(kNThreads, 1)
             split_store(make_float4(w[0], w[1], w[2], w[3]), stage + kN_OFF_AH + off, stage + kN_OFF_AL + off);
         }
         // B: charges, rows = RHS, K = sources
-        if (brole) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int cc = bcg * 4 + i;
-                const uint32_t off = tc::kmajor_offset(cc, 4 * bsg, kNKCH);
-                split_store(make_float4(qcur[0][i], qcur[1][i], qcur[2][i], qcur[3][i]), stage + kN_OFF_BH + off,
-                            stage + kN_OFF_BL + off);
-            }
+        {
+            const uint32_t off = tc::kmajor_offset(bc, 4 * bsg, kNKCH);
+            split_store(make_float4(qcur[0], qcur[1], qcur[2], qcur[3]), stage + kN_OFF_BH + off,
+                        stage + kN_OFF_BL + off);
         }
         // the previous box is complete: fold its accumulator into the FP64 sums
-        if (first && b > 0 && warp < 4) {
-            if (!drain(b - 1)) s_abort[st] = 1;
+        if (first && seg > 0) {
+            if (!drain(seg - 1)) s_abort[st] = 1;
         }
         tc::fence_proxy_async();
         __syncthreads();
@@ -583,7 +599,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
             tc::fence_after_sync();
             const uint32_t base = tc::smem_u32(stage);
             const uint32_t idesc = tc::idesc_tf32(128, NBp);
-            const uint32_t d = tmem + (uint32_t)((b & 1) * 64);
+            const uint32_t d = tmem + (uint32_t)((seg & 1) * 64);
 #pragma unroll
             for (int ks = 0; ks < kNKC / 8; ++ks) {
                 const uint32_t kofs = ks * 256;
@@ -596,20 +612,18 @@ __global__ void __launch_bounds__(kNThreads, 1)
                 tc::mma_tf32(d, alo, bh, idesc, 1u);
             }
             tc::commit(&bar[st]);
-            if (last) tc::commit(&bar[2 + (b & 1)]);
+            if (last) tc::commit(&bar[2 + (seg & 1)]);
         }
         issued = q + 1;
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int i = 0; i < 4; ++i) qcur[u][i] = qnext[u][i];
+        for (int u = 0; u < 4; ++u) qcur[u] = qnext[u];
         c0 = c1;
         c1 = c2;
         if (q + 3 < nchunks) c2 = advance(c2);
     }
     bool ok = s_abort[0] == 0 && s_abort[1] == 0;
-    if (ok && issued > 0 && warp < 4) {
-        if (!drain(np - 1)) s_abort[2] = 1;
+    if (ok && issued > 0) {
+        if (!drain(seg)) s_abort[2] = 1;
     } else if (!ok && issued > 0) {
         const int ql = issued - 1;
         tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1);
@@ -659,6 +673,297 @@ bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4*
 #undef PDMK_NTC
         default: return false;
     }
+}
+
+// ===========================================================================
+// Leaf evaluation on the tensor cores.  Rows (l, c) of the proxy coefficients
+// are processed in passes of up to 256 (whole l values); K = (i, j) in chunks
+// of 16.  The A operand (T_i(x) T_j(y) of the tile's targets) is regenerated
+// per pass from tables in shared memory; B is loaded from the coefficients and
+// split.  Every kESeg chunks the accumulator (two alternating 256-column
+// buffers) is folded with T_l(z) into per-target FP32 sums of the kb RHS by all
+// eight warps (lane quarter = targets, half = l range), so no tensor-memory
+// accumulation runs over more than a few MMA steps.
+// ===========================================================================
+namespace {
+
+constexpr int kEKC = 16;
+constexpr int kEKCH = kEKC / 4;
+constexpr int kESeg = 4;
+constexpr int kEThreads = 256;
+constexpr int kESBO = kEKCH * 128;
+constexpr int kEA = 128 * kEKC * 4;
+constexpr int kEB = 256 * kEKC * 4;
+constexpr int kE_OFF_AH = 0, kE_OFF_AL = kEA, kE_OFF_BH = 2 * kEA, kE_OFF_BL = 2 * kEA + kEB;
+constexpr int kEStage = 2 * kEA + 2 * kEB;
+
+template <int P, int KB>
+struct EvShape {
+    static constexpr int P2 = P * P;
+    static constexpr int P3 = P * P * P;
+    static constexpr int NKC = (P2 + kEKC - 1) / kEKC;
+    static constexpr int LP = (256 / KB) < P ? (256 / KB) : P;  // l values per pass
+    static constexpr int NPASS = (P + LP - 1) / LP;
+    static constexpr int NSEGP = (NKC + kESeg - 1) / kESeg;     // segments per pass
+    static constexpr int TSTR = P | 1;  // odd row stride of the T tables (bank spread)
+    static constexpr int OFF_T = 2 * kEStage;
+    static constexpr int T_BYTES = 3 * 128 * TSTR * 4;
+    static constexpr int OFF_BAR = (OFF_T + T_BYTES + 15) / 16 * 16;
+    static constexpr int SMEM_USED = OFF_BAR + 64;
+    static constexpr int SMEM = SMEM_USED < 120 * 1024 ? 120 * 1024 : SMEM_USED;  // one CTA per SM (512 TMEM cols)
+    static constexpr int B_ITEMS = 256 * kEKCH / kEThreads;
+    static_assert(SMEM <= 227 * 1024, "eval smem");
+    static_assert(KB % 16 == 0 && KB <= 64, "RHS block");
+    static_assert(128 * KB * 4 <= kEStage, "half-sum exchange buffer");
+};
+
+template <int P, int KB>
+__global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restrict__ err) {
+    using S = EvShape<P, KB>;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const int m0 = blockIdx.y * 128;
+    if (m0 >= nt) return;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);  // [0,1] stage free, [2,3] segment done
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + S::OFF_BAR + 32);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(sm + S::OFF_BAR + 36);  // [3]
+    float* sT = reinterpret_cast<float*>(sm + S::OFF_T);  // [3][128][TSTR]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0) {
+        tc::tmem_alloc(s_tmem, 512);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int i = 0; i < 4; ++i) tc::mbar_init(&bar[i], 1);
+        s_abort[0] = s_abort[1] = s_abort[2] = 0;
+        tc::fence_mbar_init();
+    }
+    const double4 cs = a.center_scale[e];
+    if (tid < 128) {
+        const bool valid = m0 + tid < nt;
+        double4 pt = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (valid) pt = a.trg[t0 + m0 + tid];
+        const float xs[3] = {(float)((pt.x - cs.x) * cs.w), (float)((pt.y - cs.y) * cs.w),
+                             (float)((pt.z - cs.z) * cs.w)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            float* dst = sT + (d * 128 + tid) * S::TSTR;
+            const float x = xs[d];
+            float t0v = 1.0f, t1v = x;
+            dst[0] = valid ? 1.0f : 0.0f;
+            dst[1] = valid ? x : 0.0f;
+#pragma unroll
+            for (int n = 2; n < P; ++n) {
+                const float t2 = 2.0f * x * t1v - t0v;
+                dst[n] = valid ? t2 : 0.0f;
+                t0v = t1v;
+                t1v = t2;
+            }
+        }
+    }
+    const float* C0 = a.proxy_down + (int64_t)a.slot[e] * KB * S::P3;
+
+    // B items of this thread: (row group, k group, row in group) -> coalesced loads, conflict-free stores
+    auto load_b = [&](int q, float4 (&bv)[S::B_ITEMS]) {
+        const int pass = q / S::NKC, kc = q - pass * S::NKC;
+        const int l0 = pass * S::LP;
+        const int nrows = min(S::LP, P - l0) * KB;
+        const int k0 = kc * kEKC;
+#pragma unroll
+        for (int u = 0; u < S::B_ITEMS; ++u) {
+            const int idx = tid + u * kEThreads;
+            const int r = (idx >> 5) * 8 + (idx & 7), g = (idx >> 3) & 3;
+            const int k = k0 + 4 * g;
+            float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (r < nrows) {
+                const int l = l0 + r / KB, c = r % KB;
+                const float* src = C0 + (int64_t)c * S::P3 + S::P2 * l + k;
+                if constexpr (P % 2 == 0) {
+                    if (k + 3 < S::P2) {
+                        v = __ldg(reinterpret_cast<const float4*>(src));
+                    } else {
+                        if (k < S::P2) v.x = __ldg(src);
+                        if (k + 1 < S::P2) v.y = __ldg(src + 1);
+                        if (k + 2 < S::P2) v.z = __ldg(src + 2);
+                    }
+                } else {
+                    if (k < S::P2) v.x = __ldg(src);
+                    if (k + 1 < S::P2) v.y = __ldg(src + 1);
+                    if (k + 2 < S::P2) v.z = __ldg(src + 2);
+                    if (k + 3 < S::P2) v.w = __ldg(src + 3);
+                }
+            }
+            bv[u] = v;
+        }
+    };
+
+    float acc[KB];
+#pragma unroll
+    for (int c = 0; c < KB; ++c) acc[c] = 0.0f;
+    const int nchunks = S::NPASS * S::NKC;
+    float4 bcur[S::B_ITEMS], bnext[S::B_ITEMS];
+    load_b(0, bcur);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *s_tmem;
+
+    // fold segment gg (TMEM buffer gg & 1) into acc: lane quarter warp % 4, l half warp / 4
+    const int dq = warp & 3, dh = warp >> 2;
+    auto drain = [&](int gg) -> bool {
+        const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1);
+        if (!__all_sync(0xffffffffu, waited)) return false;
+        tc::fence_after_sync();
+        const int pass = gg / S::NSEGP;
+        const int l0 = pass * S::LP;
+        const int nl = min(S::LP, P - l0);
+        const int hl = (nl + 1) / 2;
+        const int lb = dh * hl, le = min(nl, lb + hl);
+        const float* Tz = sT + (2 * 128 + dq * 32 + lane) * S::TSTR;
+        const uint32_t lane_base = tmem + ((uint32_t)(dq * 32) << 16) + (uint32_t)((gg & 1) * 256);
+        for (int li = lb; li < le; ++li) {
+            const float tz = Tz[l0 + li];
+#pragma unroll
+            for (int c8 = 0; c8 < KB / 8; ++c8) {
+                float v[8];
+                tc::tmem_ld_x8(lane_base + (uint32_t)(li * KB + c8 * 8), v);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc[c8 * 8 + u] = fmaf(tz, v[u], acc[c8 * 8 + u]);
+            }
+        }
+        tc::fence_before_sync();
+        return true;
+    };
+
+    int issued = 0;
+    for (int q = 0; q < nchunks; ++q) {
+        const int st = q & 1;
+        const int pass = q / S::NKC, kc = q - pass * S::NKC;
+        const int seg = pass * S::NSEGP + kc / kESeg;
+        const bool first = kc % kESeg == 0, last = kc % kESeg == kESeg - 1 || kc == S::NKC - 1;
+        if (q + 1 < nchunks) load_b(q + 1, bnext);
+        if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1)) s_abort[st] = 1;
+        unsigned char* stage = sm + st * kEStage;
+        const int k0 = kc * kEKC;
+        // A = T_i(x_t) T_j(y_t), K index k = i + P j
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int idx = tid + u * kEThreads;
+            const int m = idx & 127, g = idx >> 7;
+            const float* Tx = sT + (0 * 128 + m) * S::TSTR;
+            const float* Ty = sT + (1 * 128 + m) * S::TSTR;
+            float v[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int k = k0 + 4 * g + w;
+                const int i = k % P, j = k / P;
+                v[w] = k < S::P2 ? Tx[i] * Ty[j] : 0.0f;
+            }
+            const uint32_t off = tc::kmajor_offset(m, 4 * g, kEKCH);
+            split_store(make_float4(v[0], v[1], v[2], v[3]), stage + kE_OFF_AH + off, stage + kE_OFF_AL + off);
+        }
+#pragma unroll
+        for (int u = 0; u < S::B_ITEMS; ++u) {
+            const int idx = tid + u * kEThreads;
+            const int r = (idx >> 5) * 8 + (idx & 7), g = (idx >> 3) & 3;
+            const uint32_t off = tc::kmajor_offset(r, 4 * g, kEKCH);
+            split_store(bcur[u], stage + kE_OFF_BH + off, stage + kE_OFF_BL + off);
+        }
+        if (first && seg > 0) {
+            if (!drain(seg - 1)) s_abort[st] = 1;
+        }
+        tc::fence_proxy_async();
+        __syncthreads();
+        if (s_abort[st]) break;
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const int nrows = min(S::LP, P - pass * S::LP) * KB;
+            const uint32_t base = tc::smem_u32(stage);
+            const uint32_t idesc = tc::idesc_tf32(128, nrows);
+            const uint32_t d = tmem + (uint32_t)((seg & 1) * 256);
+#pragma unroll
+            for (int ks = 0; ks < kEKC / 8; ++ks) {
+                const uint32_t kofs = ks * 256;
+                const uint64_t ah = tc::smem_desc_k_noswizzle(base + kE_OFF_AH + kofs, 128, kESBO);
+                const uint64_t alo = tc::smem_desc_k_noswizzle(base + kE_OFF_AL + kofs, 128, kESBO);
+                const uint64_t bh = tc::smem_desc_k_noswizzle(base + kE_OFF_BH + kofs, 128, kESBO);
+                const uint64_t blo = tc::smem_desc_k_noswizzle(base + kE_OFF_BL + kofs, 128, kESBO);
+                tc::mma_tf32(d, ah, bh, idesc, (first && ks == 0) ? 0u : 1u);
+                tc::mma_tf32(d, ah, blo, idesc, 1u);
+                tc::mma_tf32(d, alo, bh, idesc, 1u);
+            }
+            tc::commit(&bar[st]);
+            if (last) tc::commit(&bar[2 + (seg & 1)]);
+        }
+        issued = q + 1;
+#pragma unroll
+        for (int u = 0; u < S::B_ITEMS; ++u) bcur[u] = bnext[u];
+    }
+    bool ok = s_abort[0] == 0 && s_abort[1] == 0;
+    if (ok && issued == nchunks) {
+        if (!drain(S::NPASS * S::NSEGP - 1)) s_abort[2] = 1;
+    } else if (issued > 0) {
+        const int ql = issued - 1;
+        tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1);
+    }
+    __syncthreads();
+    ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;
+    // combine the two l halves: half 1 publishes its sums, half 0 adds and writes
+    float* xch = reinterpret_cast<float*>(sm);  // stage 0, idle now
+    const int m = dq * 32 + lane;
+    if (dh == 1) {
+#pragma unroll
+        for (int c = 0; c < KB; ++c) xch[c * 128 + m] = acc[c];
+    }
+    __syncthreads();
+    if (ok && dh == 0 && m0 + m < nt) {
+        double* pt = a.pot + t0 + m0 + m;
+#pragma unroll
+        for (int c = 0; c < KB; ++c) pt[(int64_t)c * a.N] += (double)(acc[c] + xch[c * 128 + m]);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 512);
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+}
+
+template <int P, int KB>
+void launch_eval_tc_pk(const EvalTc& a, int* err, cudaStream_t s) {
+    using S = EvShape<P, KB>;
+    static bool configured[64] = {};
+    int dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+    if (!configured[dev]) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_eval_tc<P, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+        configured[dev] = true;
+    }
+    const dim3 grid(a.n_leaves, (a.max_trg + 127) / 128);
+    k_eval_tc<P, KB><<<grid, kEThreads, S::SMEM, s>>>(a, err);
+}
+
+}  // namespace
+
+bool launch_eval_tc(const EvalTc& a, int p, int kb, int* err, cudaStream_t s) {
+    if (a.n_leaves <= 0 || a.max_trg <= 0) return false;
+    if (p != 9 && p != 18) return false;
+    if (kb != 16 && kb != 32 && kb != 64) return false;
+    if (p == 9) {
+        if (kb == 16) launch_eval_tc_pk<9, 16>(a, err, s);
+        else if (kb == 32) launch_eval_tc_pk<9, 32>(a, err, s);
+        else launch_eval_tc_pk<9, 64>(a, err, s);
+    } else {
+        if (kb == 16) launch_eval_tc_pk<18, 16>(a, err, s);
+        else if (kb == 32) launch_eval_tc_pk<18, 32>(a, err, s);
+        else launch_eval_tc_pk<18, 64>(a, err, s);
+    }
+    return true;
 }
 
 }  // namespace dev

@@ -42,5 +42,24 @@ constexpr int kNearTcMaxPairs = 128;
 bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4* trg_lo, const float4* src_hi,
                     const float4* src_lo, const float* src_q, double* pot, int* err, cudaStream_t s);
 
+// Leaf evaluation of kb RHS as a GEMM per (leaf, 128-target tile):
+//   pot[c*N + t] += sum_l T_l(z_t) sum_{(i,j)} T_i(x_t) T_j(y_t) C[(slot*kb + c)*p^3 + i + p j + p^2 l]
+// with D[t, (l,c)] = A[t, (i,j)] B[(l,c), (i,j)] on the tensor cores (TF32
+// hi/lo split) and the z sum in the epilogue.  Covers p in {9, 18}, kb in
+// {16, 32, 64}.
+struct EvalTc {
+    const double4* trg;
+    const float* proxy_down;
+    double* pot;
+    int n_leaves;
+    int max_trg;
+    const int* slot;
+    const int* trg_start;
+    const int* trg_count;
+    const double4* center_scale;
+    int64_t N;
+};
+bool launch_eval_tc(const EvalTc& a, int p, int kb, int* err, cudaStream_t s);
+
 }  // namespace dev
 }  // namespace pdmkb

@@ -128,3 +128,19 @@ def test_mixed_tensor_core_blocks(nd, tol, k):
     errs = [rel_l2(Pm[:, c], Pd[:, c]) for c in range(k)]
     assert max(errs) < tol, (int(np.argmax(errs)), max(errs))
     t.close()
+
+
+def test_mixed_accuracy_many_sources_per_box():
+    # npl 300 at N = 2e5: ~2000 sources per proxy centre and ~250 targets per
+    # leaf, the sizes at which long tensor-core accumulations lose accuracy
+    cell, pos, _ = uniform_system(200000, 49)
+    k = 64
+    Q = _charges(len(pos), k, 7)
+    tf = pd.PeriodicDMKTree(cell, pos, 6, 300, 4, precision="float")
+    td = pd.PeriodicDMKTree(cell, pos, 6, 300, 4)
+    Pm = _multi_device(tf, Q, mixed=True)
+    for c in (0, 31, 63):
+        ref = td.evaluate(Q[:, c])
+        assert rel_l2(Pm[:, c], ref) < 1e-6, (c, rel_l2(Pm[:, c], ref))
+    tf.close()
+    td.close()
