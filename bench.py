@@ -263,7 +263,8 @@ def run_ours(args):
     ach_plain = near_flop_plain / (med(plain_st, "near_ms") * 1e-3) / 1e12
     ach_mixed = near_flop_mixed / (med(mixed_st, "near_ms") * 1e-3) / 1e12
     stage_keys = ("dmk_ms", "near_ms", "nufft_ms", "finalize_ms", "total_ms")
-    roofline = {"bound": "fp32", "kernel": "k_near_m32 (residual near field, %d RHS per call)" % k,
+    roofline = {"bound": "fp32", "kernel": "k_near_tc (residual near field, %d RHS per call: FP32 kernel values on "
+                                           "the CUDA cores, TF32 hi/lo products on the tensor cores)" % k,
                 "achieved": ach_mixed, "peak": pk32, "unit": "TFLOP/s", "frac": ach_mixed / pk32,
                 "traffic": None, "peak_source": "measured FP32 FMA probe on this GPU (pdmk_fma_peak)",
                 "algorithmic_flop_per_launch": near_flop_mixed,
@@ -288,7 +289,8 @@ def run_ours(args):
                                                          "p", "n_pw", "device_bytes")},
                        "tree_build_s": t_build,
                        "precision": "FP32 near field (double-float coordinate differences, FP64 merge), FP32 "
-                                    "transforms, FP64 far field and accumulation"},
+                                    "moments / transforms / leaf evaluation (tensor-core products on TF32 hi/lo "
+                                    "splits, short accumulation segments), FP64 far field and accumulation"},
             "rel_l2_vs_fp64": max(errs),
             "mixed_vs_plain_fp64": value / plain_value,
             "plain_fp64_single_rhs": plain,

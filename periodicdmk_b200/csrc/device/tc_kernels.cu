@@ -28,7 +28,7 @@ namespace {
 constexpr int kKC = 32;        // sources per pipeline stage (four MMA k-steps of 8)
 constexpr int kKCH = kKC / 4;  // 16-byte K chunks per operand row
 constexpr int kSeg = 2;        // chunks accumulated in tensor memory before a drain
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kMaxKb = 64;
 constexpr int kMinKb = 16;
 
@@ -42,7 +42,7 @@ struct C2PShape {
     static constexpr int NB = (CW + 15) / 16 * 16;         // B rows, padded to the MMA N granule
     static constexpr int BUF = NB <= 128 ? 128 : 256;      // column offset of the second accumulator
     static constexpr int TMEM_COLS = 2 * BUF <= 256 ? 256 : 512;
-    static constexpr int HALF = NB / 2;                    // drain columns per thread (two warps per lane quarter)
+    static constexpr int QCOL = NB / 4;                    // drain columns per thread (four warps per lane quarter)
     static constexpr int SBO = kKCH * 128;
     static constexpr int A_BYTES = 128 * kKC * 4;
     static constexpr int B_BYTES = NB * kKC * 4;
@@ -55,9 +55,14 @@ struct C2PShape {
     static constexpr int SMEM_USED = OFF_BAR + 64;
     static constexpr int SMEM = TMEM_COLS == 512 && SMEM_USED < 120 * 1024 ? 120 * 1024 : SMEM_USED;
     static constexpr int A_ITEMS = 128 * kKCH / kThreads;
-    static constexpr int B_ITEMS = (NB * kKCH + kThreads - 1) / kThreads;
+    // B items: two rounds over all threads, further rounds over the threads
+    // that do not evaluate Chebyshev values (tid >= 3 * kKC)
+    static constexpr int B_TOTAL = NB * kKCH;
+    static constexpr int B_LATE = kThreads - 3 * kKC;
+    static constexpr int B_ITEMS =
+        B_TOTAL <= 2 * kThreads ? (B_TOTAL + kThreads - 1) / kThreads : 2 + (B_TOTAL - 2 * kThreads + B_LATE - 1) / B_LATE;
     static_assert(2 * BUF <= TMEM_COLS && NB <= BUF, "accumulators exceed tensor memory");
-    static_assert(HALF % 8 == 0, "drain column split");
+    static_assert(QCOL % 4 == 0, "drain column split");
     static_assert((128 * kKCH) % kThreads == 0, "A items per thread");
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
@@ -84,6 +89,22 @@ __device__ __forceinline__ void split_store(const float4 v, unsigned char* hi_p,
     tc::split_tf32(v.y, hi.y, lo.y);
     tc::split_tf32(v.z, hi.z, lo.z);
     tc::split_tf32(v.w, hi.w, lo.w);
+    *reinterpret_cast<uint4*>(hi_p) = hi;
+    *reinterpret_cast<uint4*>(lo_p) = lo;
+}
+
+// hi = TF32 rounding of x, lo = x - hi left unrounded (the tensor core reads
+// its leading TF32 bits, i.e. truncates it): relative error <= 2^-21 per operand.
+__device__ __forceinline__ void split_store_lo_trunc(const float4 v, unsigned char* hi_p, unsigned char* lo_p) {
+    uint4 hi, lo;
+    hi.x = tc::round_tf32_bits(__float_as_uint(v.x));
+    hi.y = tc::round_tf32_bits(__float_as_uint(v.y));
+    hi.z = tc::round_tf32_bits(__float_as_uint(v.z));
+    hi.w = tc::round_tf32_bits(__float_as_uint(v.w));
+    lo.x = __float_as_uint(v.x - __uint_as_float(hi.x));
+    lo.y = __float_as_uint(v.y - __uint_as_float(hi.y));
+    lo.z = __float_as_uint(v.z - __uint_as_float(hi.z));
+    lo.w = __float_as_uint(v.w - __uint_as_float(hi.w));
     *reinterpret_cast<uint4*>(hi_p) = hi;
     *reinterpret_cast<uint4*>(lo_p) = lo;
 }
@@ -120,11 +141,31 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::fence_mbar_init();
     }
 
-    // A rows of this thread: row m = tid % 128, k groups akg0 + 2u
+    // A items (row am, k group akg0 + 4u): Chebyshev-table offset of T_l and operand offset, fixed per thread
     const int am = tid & 127, akg0 = tid >> 7;
     const int aR = row0 + am;
     const bool arow = aR < rows;
     const int al = arow ? aR / kb : 0, ac = arow ? aR - al * kb : 0;
+    int a_t[S::A_ITEMS], a_o[S::A_ITEMS];
+#pragma unroll
+    for (int u = 0; u < S::A_ITEMS; ++u) {
+        const int kg = akg0 + 4 * u;
+        a_t[u] = ((2 * kKCH + kg) * P + al) * 16;  // byte offset of a 4-source float4
+        a_o[u] = (int)tc::kmajor_offset(am, kg * 4, kKCH);
+    }
+    // B items (row nl, k group): offsets of T_i and T_j (-1: zero row) and operand offset
+    int b_x[S::B_ITEMS], b_y[S::B_ITEMS], b_o[S::B_ITEMS];
+#pragma unroll
+    for (int u = 0; u < S::B_ITEMS; ++u) {
+        const int it = u < 2 ? tid + u * kThreads
+                             : (tid >= 3 * kKC ? 2 * kThreads + (u - 2) * S::B_LATE + tid - 3 * kKC : S::B_TOTAL);
+        const int nl = it % S::NB, kg = it / S::NB;
+        const int n = col0 + nl;
+        const bool valid = it < S::B_TOTAL && nl < ncol;
+        b_x[u] = valid ? ((0 * kKCH + kg) * P + n % P) * 16 : -1;  // byte offsets
+        b_y[u] = valid ? ((1 * kKCH + kg) * P + n / P) * 16 : -1;
+        b_o[u] = it < S::B_TOTAL ? (int)tc::kmajor_offset(nl, kg * 4, kKCH) : -1;
+    }
     // Chebyshev role: threads < 3*kKC evaluate one (source, dim) of the next chunk
     const bool cheb = tid < 3 * kKC;
     const int cs_s = tid % kKC, cs_d = tid / kKC;
@@ -135,7 +176,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int u = 0; u < S::A_ITEMS; ++u)
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
-                const int s = (akg0 + 2 * u) * 4 + w;
+                const int s = (akg0 + 4 * u) * 4 + w;
                 qv[u][w] = (arow && s < nt) ? __ldg(src_q + (int64_t)(g0 + s) * kb + ac) : 0.0f;
             }
     };
@@ -165,86 +206,80 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     };
 
-    // FP32 sums of the drained segments: lane quarter warp % 4 (rows), column half warp / 4
-    const int dq = warp & 3, dh = warp >> 2;
-    float accd[S::HALF];
-#pragma unroll
-    for (int i = 0; i < S::HALF; ++i) accd[i] = 0.0f;
     float qcur[S::A_ITEMS][4], qnext[S::A_ITEMS][4];
     double xnext = 0.0;
+    int g1 = 0, nt1 = 0;  // chunk q + 1
     if (nchunks > 0) {
         int g0, nt;
         chunk_at(a, r0, r1, 0, g0, nt);
         load_q(g0, nt, qcur);
         cheb_store(0, load_x(g0, nt), nt);
         if (nchunks > 1) {
-            chunk_at(a, r0, r1, 1, g0, nt);
-            xnext = load_x(g0, nt);
+            chunk_at(a, r0, r1, 1, g1, nt1);
+            xnext = load_x(g1, nt1);
         }
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *s_tmem;
+
+    // FP32 sums of the drained segments: lane quarter warp % 4 (rows), column quarter warp / 4
+    const int dq = warp & 3, dc = warp >> 2;
+    float accd[S::QCOL];
+#pragma unroll
+    for (int i = 0; i < S::QCOL; ++i) accd[i] = 0.0f;
     auto drain = [&](int gg) -> bool {
         const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1);
         if (!__all_sync(0xffffffffu, waited)) return false;
         tc::fence_after_sync();
         const uint32_t base =
-            tmem + ((uint32_t)(dq * 32) << 16) + (uint32_t)((gg & 1) * S::BUF + dh * S::HALF);
+            tmem + ((uint32_t)(dq * 32) << 16) + (uint32_t)((gg & 1) * S::BUF + dc * S::QCOL);
 #pragma unroll
-        for (int c0 = 0; c0 < S::HALF; c0 += 8) {
-            float v[8];
-            tc::tmem_ld_x8(base + (uint32_t)c0, v);
+        for (int c0 = 0; c0 < S::QCOL; c0 += 16) {
+            float v[16];
+#pragma unroll
+            for (int b4 = 0; b4 < 4; ++b4)
+                if (c0 + 4 * b4 < S::QCOL) tc::tmem_ld_x4(base + (uint32_t)(c0 + 4 * b4), v + 4 * b4);
             tc::tmem_wait_ld();
 #pragma unroll
-            for (int u = 0; u < 8; ++u) accd[c0 + u] += v[u];
+            for (int u = 0; u < 16; ++u)
+                if (c0 + u < S::QCOL) accd[c0 + u] += v[u];
         }
         tc::fence_before_sync();
         return true;
     };
-
 
     int issued = 0;  // chunks whose MMAs were issued and committed
     for (int q = 0; q < nchunks; ++q) {
         const int st = q & 1;
         const int seg = q / kSeg;
         const bool first = q % kSeg == 0, last = q % kSeg == kSeg - 1 || q == nchunks - 1;
-        int g1 = 0, nt1 = 0, g2 = 0, nt2 = 0;
-        if (q + 1 < nchunks) {
-            chunk_at(a, r0, r1, q + 1, g1, nt1);
-            load_q(g1, nt1, qnext);
-        }
+        int g2 = 0, nt2 = 0;
+        if (q + 1 < nchunks) load_q(g1, nt1, qnext);
         if (q + 2 < nchunks) chunk_at(a, r0, r1, q + 2, g2, nt2);
         // stage st was last read by the MMAs of chunk q-2
         if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1)) s_abort[st] = 1;
         unsigned char* stage = sm + st * S::STAGE;
-        const float* T = sT + st * S::T_FLOATS;
+        const unsigned char* T = reinterpret_cast<const unsigned char*>(sT + st * S::T_FLOATS);
         // A = T_l(z_s) q_sc
 #pragma unroll
         for (int u = 0; u < S::A_ITEMS; ++u) {
-            const int kg = akg0 + 2 * u;
-            const float4 tz = *reinterpret_cast<const float4*>(T + ((2 * kKCH + kg) * P + al) * 4);
+            const float4 tz = *reinterpret_cast<const float4*>(T + a_t[u]);
             const float4 v = make_float4(tz.x * qcur[u][0], tz.y * qcur[u][1], tz.z * qcur[u][2], tz.w * qcur[u][3]);
-            const uint32_t off = tc::kmajor_offset(am, kg * 4, kKCH);
-            split_store(v, stage + S::OFF_AH + off, stage + S::OFF_AL + off);
+            split_store_lo_trunc(v, stage + S::OFF_AH + a_o[u], stage + S::OFF_AL + a_o[u]);
         }
-        // B = T_i(x_s) T_j(y_s), rows n - col0 for the columns n = i + P j of this CTA
+        // B = T_i(x_s) T_j(y_s) for the columns n = i + P j of this CTA
 #pragma unroll
         for (int u = 0; u < S::B_ITEMS; ++u) {
-            const int it = tid + u * kThreads;
-            if (it < S::NB * kKCH) {
-                const int nl = it % S::NB, kg = it / S::NB;
+            if (b_o[u] >= 0) {
                 float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (nl < ncol) {
-                    const int n = col0 + nl;
-                    const int i = n % P, j = n / P;
-                    const float4 tx = *reinterpret_cast<const float4*>(T + ((0 * kKCH + kg) * P + i) * 4);
-                    const float4 ty = *reinterpret_cast<const float4*>(T + ((1 * kKCH + kg) * P + j) * 4);
+                if (b_x[u] >= 0) {
+                    const float4 tx = *reinterpret_cast<const float4*>(T + b_x[u]);
+                    const float4 ty = *reinterpret_cast<const float4*>(T + b_y[u]);
                     v = make_float4(tx.x * ty.x, tx.y * ty.y, tx.z * ty.z, tx.w * ty.w);
                 }
-                const uint32_t off = tc::kmajor_offset(nl, kg * 4, kKCH);
-                split_store(v, stage + S::OFF_BH + off, stage + S::OFF_BL + off);
+                split_store_lo_trunc(v, stage + S::OFF_BH + b_o[u], stage + S::OFF_BL + b_o[u]);
             }
         }
         // Chebyshev values of chunk q+1 (other buffer), prefetch of chunk q+2's coordinate
@@ -252,42 +287,43 @@ __global__ void __launch_bounds__(kThreads, 1)
             cheb_store(st ^ 1, xnext, nt1);
             if (q + 2 < nchunks) xnext = load_x(g2, nt2);
         }
-        // the previous segment is complete: fold it into the FP32 sums
-        if (first && seg > 0) {
-            if (!drain(seg - 1)) s_abort[st] = 1;
-        }
         tc::fence_proxy_async();
         __syncthreads();
         if (s_abort[st]) break;
         if (tid == 0) {
             tc::fence_after_sync();
+            static_assert(S::NB <= 256, "one MMA per k-step");
             const uint32_t base = tc::smem_u32(stage);
             const uint32_t d = tmem + (uint32_t)((seg & 1) * S::BUF);
+            constexpr uint32_t idesc = tc::idesc_tf32(128, S::NB);
+            // descriptors of k-step 0; each k-step advances the start address by 256 B (16 units)
+            const uint64_t ah = tc::smem_desc_k_noswizzle(base + S::OFF_AH, 128, S::SBO);
+            const uint64_t alo = tc::smem_desc_k_noswizzle(base + S::OFF_AL, 128, S::SBO);
+            const uint64_t bh = tc::smem_desc_k_noswizzle(base + S::OFF_BH, 128, S::SBO);
+            const uint64_t blo = tc::smem_desc_k_noswizzle(base + S::OFF_BL, 128, S::SBO);
 #pragma unroll
             for (int ks = 0; ks < kKC / 8; ++ks) {
-                const uint32_t kofs = ks * 256;  // 8 K elements = two 16-byte chunks of 128 B each
-                const uint64_t ah = tc::smem_desc_k_noswizzle(base + S::OFF_AH + kofs, 128, S::SBO);
-                const uint64_t alo = tc::smem_desc_k_noswizzle(base + S::OFF_AL + kofs, 128, S::SBO);
-#pragma unroll
-                for (int n0 = 0; n0 < S::NB; n0 += 256) {
-                    const int N = S::NB - n0 < 256 ? S::NB - n0 : 256;
-                    const uint32_t idesc = tc::idesc_tf32(128, N);
-                    const uint32_t boff = (uint32_t)(n0 / 8) * S::SBO + kofs;
-                    const uint64_t bh = tc::smem_desc_k_noswizzle(base + S::OFF_BH + boff, 128, S::SBO);
-                    const uint64_t blo = tc::smem_desc_k_noswizzle(base + S::OFF_BL + boff, 128, S::SBO);
-                    tc::mma_tf32(d + (uint32_t)n0, ah, bh, idesc, (first && ks == 0) ? 0u : 1u);
-                    tc::mma_tf32(d + (uint32_t)n0, ah, blo, idesc, 1u);
-                    tc::mma_tf32(d + (uint32_t)n0, alo, bh, idesc, 1u);
-                }
+                const uint64_t dk = (uint64_t)(16 * ks);
+                tc::mma_tf32(d, ah + dk, bh + dk, idesc, (first && ks == 0) ? 0u : 1u);
+                tc::mma_tf32(d, ah + dk, blo + dk, idesc, 1u);
+                tc::mma_tf32(d, alo + dk, bh + dk, idesc, 1u);
             }
             tc::commit(&bar[st]);
             if (last) tc::commit(&bar[2 + (seg & 1)]);
         }
         issued = q + 1;
+        // the previous segment is complete: fold it into the FP32 sums while the
+        // tensor core works on this segment (the other accumulator buffer).  A
+        // failure is flagged for the next iteration's check.
+        if (first && seg > 0) {
+            if (!drain(seg - 1)) s_abort[st ^ 1] = 1;
+        }
 #pragma unroll
         for (int u = 0; u < S::A_ITEMS; ++u)
 #pragma unroll
             for (int w = 0; w < 4; ++w) qcur[u][w] = qnext[u][w];
+        g1 = g2;
+        nt1 = nt2;
     }
     bool ok = s_abort[0] == 0 && s_abort[1] == 0;
     if (ok && issued > 0) {
@@ -305,8 +341,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int l = R / kb, c = R - l * kb;
             float* out = proxy_up + ((int64_t)a.slot[e] * kb + c) * (P * P * P) + (int64_t)S::P2 * l + col0;
 #pragma unroll
-            for (int i = 0; i < S::HALF; ++i) {
-                const int nl = dh * S::HALF + i;
+            for (int i = 0; i < S::QCOL; ++i) {
+                const int nl = dc * S::QCOL + i;
                 if (nl < ncol) out[nl] += accd[i];
             }
         }
@@ -589,9 +625,6 @@ __global__ void __launch_bounds__(kNThreads, 1)
                         stage + kN_OFF_BL + off);
         }
         // the previous box is complete: fold its accumulator into the FP64 sums
-        if (first && seg > 0) {
-            if (!drain(seg - 1)) s_abort[st] = 1;
-        }
         tc::fence_proxy_async();
         __syncthreads();
         if (s_abort[st]) break;
@@ -615,6 +648,10 @@ __global__ void __launch_bounds__(kNThreads, 1)
             if (last) tc::commit(&bar[2 + (seg & 1)]);
         }
         issued = q + 1;
+        // fold the previous segment while this one runs on the tensor core
+        if (first && seg > 0) {
+            if (!drain(seg - 1)) s_abort[st ^ 1] = 1;
+        }
 #pragma unroll
         for (int u = 0; u < 4; ++u) qcur[u] = qnext[u];
         c0 = c1;
@@ -826,12 +863,15 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
         for (int li = lb; li < le; ++li) {
             const float tz = Tz[l0 + li];
 #pragma unroll
-            for (int c8 = 0; c8 < KB / 8; ++c8) {
-                float v[8];
-                tc::tmem_ld_x8(lane_base + (uint32_t)(li * KB + c8 * 8), v);
+            for (int c0 = 0; c0 < KB; c0 += 32) {
+                float v[32];
+#pragma unroll
+                for (int b8 = 0; b8 < 4; ++b8)
+                    if (c0 + 8 * b8 < KB) tc::tmem_ld_x8(lane_base + (uint32_t)(li * KB + c0 + 8 * b8), v + 8 * b8);
                 tc::tmem_wait_ld();
 #pragma unroll
-                for (int u = 0; u < 8; ++u) acc[c8 * 8 + u] = fmaf(tz, v[u], acc[c8 * 8 + u]);
+                for (int u = 0; u < 32; ++u)
+                    if (c0 + u < KB) acc[c0 + u] = fmaf(tz, v[u], acc[c0 + u]);
             }
         }
         tc::fence_before_sync();
@@ -872,9 +912,6 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
             const uint32_t off = tc::kmajor_offset(r, 4 * g, kEKCH);
             split_store(bcur[u], stage + kE_OFF_BH + off, stage + kE_OFF_BL + off);
         }
-        if (first && seg > 0) {
-            if (!drain(seg - 1)) s_abort[st] = 1;
-        }
         tc::fence_proxy_async();
         __syncthreads();
         if (s_abort[st]) break;
@@ -899,6 +936,10 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
             if (last) tc::commit(&bar[2 + (seg & 1)]);
         }
         issued = q + 1;
+        // fold the previous segment while this one runs on the tensor core
+        if (first && seg > 0) {
+            if (!drain(seg - 1)) s_abort[st ^ 1] = 1;
+        }
 #pragma unroll
         for (int u = 0; u < S::B_ITEMS; ++u) bcur[u] = bnext[u];
     }
