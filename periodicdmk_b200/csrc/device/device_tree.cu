@@ -582,6 +582,7 @@ void DeviceTree::init(const Plan& P, int device) {
             be.push_back(bn.ext);
             nufft_max_jk_ = std::max(nufft_max_jk_, bn.ext.y * bn.ext.z);
             nufft_max_ex_ = std::max(nufft_max_ex_, bn.ext.x);
+            nufft_max_cells_ = std::max(nufft_max_cells_, bn.ext.x * bn.ext.y * bn.ext.z);
         }
         nufft_.n_leaves = (int)bins.size();
         nufft_.trg_start = upload(bs);
@@ -612,6 +613,10 @@ void DeviceTree::release() {
     multi_[0].reset();
     multi_[1].reset();
     if (stream_) cudaStreamSynchronize(stream_);
+    if (stage_q_) cudaFree(stage_q_);
+    if (stage_p_) cudaFree(stage_p_);
+    stage_q_ = stage_p_ = nullptr;
+    stage_elems_ = 0;
     if (plan_fwd_) cufftDestroy(plan_fwd_);
     if (plan_inv_) cufftDestroy(plan_inv_);
     for (void* p : allocs_) cudaFree(p);

@@ -78,6 +78,10 @@ class DeviceTree {
     void run_multi_block(MultiState& m, const double* Q, int kvalid, double* pot_user);
     std::unique_ptr<MultiState, MultiStateDeleter> multi_[2];
     StageTimes last_multi_{};
+    // device staging of the host-buffer multi-RHS calls (grow-only, freed with the tree)
+    double* stage_q_ = nullptr;
+    double* stage_p_ = nullptr;
+    size_t stage_elems_ = 0;
 
   public:
     bool last_was_multi_ = false;
@@ -170,7 +174,7 @@ class DeviceTree {
     int64_t scratch_elems_ = 0, pw_in_elems_ = 0;
     // far field
     dev::NufftArgs nufft_{};
-    int nufft_max_jk_ = 0, nufft_max_ex_ = 0;
+    int nufft_max_jk_ = 0, nufft_max_ex_ = 0, nufft_max_cells_ = 0;
     double* grid_ = nullptr;
     dev::cd* spec_ = nullptr;
     double* mult_ = nullptr;

@@ -851,10 +851,11 @@ DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
     m->spec = m->alloc<cd>((size_t)(n_spec_ * kb));
     {
         int dims[3] = {nufft_.n1, nufft_.n2, nufft_.n3};
-        if (cufftPlanMany(&m->fwd, 3, dims, nullptr, 1, (int)n_grid_, nullptr, 1, (int)n_spec_, CUFFT_D2Z, kb) !=
-                CUFFT_SUCCESS ||
-            cufftPlanMany(&m->inv, 3, dims, nullptr, 1, (int)n_spec_, nullptr, 1, (int)n_grid_, CUFFT_Z2D, kb) !=
-                CUFFT_SUCCESS)
+        const cufftResult r1 =
+            cufftPlanMany(&m->fwd, 3, dims, nullptr, 1, (int)n_grid_, nullptr, 1, (int)n_spec_, CUFFT_D2Z, kb);
+        const cufftResult r2 =
+            cufftPlanMany(&m->inv, 3, dims, nullptr, 1, (int)n_spec_, nullptr, 1, (int)n_grid_, CUFFT_Z2D, kb);
+        if (r1 != CUFFT_SUCCESS || r2 != CUFFT_SUCCESS)
             throw std::runtime_error("cuFFT error: batched plan creation failed");
         cufftSetStream(m->fwd, stream_);
         cufftSetStream(m->inv, stream_);
@@ -1189,12 +1190,20 @@ void DeviceTree::evaluate_multi_host(const double* Q, int k, void* pot, bool pot
                                      StageTimes* times) {
     if (k <= 0) throw std::invalid_argument("k must be positive");
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
-    double* qd = nullptr;
-    double* pd = nullptr;
     const int64_t n = (int64_t)n_ * k;
     const size_t bytes = sizeof(double) * (size_t)n;
-    PDMK_CUDA_CHECK(cudaMallocAsync(&qd, bytes, stream_));
-    PDMK_CUDA_CHECK(cudaMallocAsync(&pd, bytes, stream_));
+    if ((size_t)n > stage_elems_) {
+        PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+        if (stage_q_) cudaFree(stage_q_);
+        if (stage_p_) cudaFree(stage_p_);
+        stage_q_ = stage_p_ = nullptr;
+        stage_elems_ = 0;
+        PDMK_CUDA_CHECK(cudaMalloc(&stage_q_, bytes));
+        PDMK_CUDA_CHECK(cudaMalloc(&stage_p_, bytes));
+        stage_elems_ = (size_t)n;
+    }
+    double* qd = stage_q_;
+    double* pd = stage_p_;
     PDMK_CUDA_CHECK(cudaMemcpyAsync(qd, Q, bytes, cudaMemcpyHostToDevice, stream_));
     evaluate_multi_device(qd, k, pd, fp32, times);
     if (pot_float) {
@@ -1205,8 +1214,6 @@ void DeviceTree::evaluate_multi_host(const double* Q, int k, void* pot, bool pot
     } else {
         PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pd, bytes, cudaMemcpyDeviceToHost, stream_));
     }
-    PDMK_CUDA_CHECK(cudaFreeAsync(qd, stream_));
-    PDMK_CUDA_CHECK(cudaFreeAsync(pd, stream_));
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 
