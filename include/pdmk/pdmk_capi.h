@@ -114,6 +114,31 @@ int pdmk_fma_peak(int fp64, double* tflops);
  * the GPU race and must be serialised by the caller.  Synchronous. */
 int pdmk_evaluate_device_noalloc_double(void* h, const double* charges_dev, double* pot_dev);
 
+/* ---- batches of independent systems ------------------------------------ */
+
+/* Many independent periodic systems built and evaluated together (no
+ * reference counterpart; each system is what pdmk_create_* / pdmk_evaluate_*
+ * of cpp/include/pdmk/pdmk_capi.h:39-49 build and evaluate one at a time).
+ *   cells:     nsys column-major 3x3 cells, concatenated (9 doubles each)
+ *   Ns:        points per system
+ *   positions: column-major 3 x Ns[i] blocks, concatenated in system order
+ * pdmk_batch_create picks the precision as the reference's
+ * AutoPeriodicDMKTree (cpp/src/periodic_dmk.cpp:326-336): the float
+ * (mixed-precision) trees for n_digits <= 6, double above;
+ * pdmk_batch_create_double always uses double trees.  Host tree construction
+ * runs on all host threads.  Returns NULL on error. */
+void* pdmk_batch_create(int nsys, const double* cells, const int* Ns, const double* positions, int n_digits,
+                        int n_per_leaf, int nz);
+void* pdmk_batch_create_double(int nsys, const double* cells, const int* Ns, const double* positions, int n_digits,
+                               int n_per_leaf, int nz);
+/* Potentials of all systems; charges and pot_out are concatenated in system
+ * order (sum of Ns entries).  The systems run concurrently on the device. */
+int pdmk_batch_evaluate(void* h, const double* charges, double* pot_out);
+int pdmk_batch_evaluate_float(void* h, const double* charges, float* pot_out);
+/* out4 = {number of systems, total points, device bytes, 1 if float trees} */
+int pdmk_batch_info(void* h, int64_t* out4);
+void pdmk_batch_destroy(void* h);
+
 /* Last error message of the calling thread ("" if none). */
 const char* pdmk_last_error(void);
 

@@ -12,7 +12,8 @@ import os
 
 import numpy as np
 
-__all__ = ["PeriodicDMKTree", "library", "library_path", "ewald", "optimize_cubic_cover", "EXPORTED_SYMBOLS"]
+__all__ = ["PeriodicDMKTree", "PeriodicDMKBatch", "library", "library_path", "ewald", "optimize_cubic_cover",
+           "EXPORTED_SYMBOLS"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "lib", "libpdmk_b200.so")
@@ -29,7 +30,10 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
     "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float",
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
-    "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_evaluate_device_noalloc_double", "pdmk_last_error",
+    "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_evaluate_device_noalloc_double",
+    "pdmk_batch_create", "pdmk_batch_create_double", "pdmk_batch_evaluate", "pdmk_batch_evaluate_float",
+    "pdmk_batch_info", "pdmk_batch_destroy",
+    "pdmk_last_error",
 ]
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -92,6 +96,18 @@ def library():
     lib.pdmk_evaluate_device_noalloc_double.restype = ctypes.c_int
     lib.pdmk_fma_peak.argtypes = [ctypes.c_int, _D]
     lib.pdmk_fma_peak.restype = ctypes.c_int
+    lib.pdmk_batch_create.argtypes = [ctypes.c_int, _D, _I, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.pdmk_batch_create.restype = v
+    lib.pdmk_batch_create_double.argtypes = lib.pdmk_batch_create.argtypes
+    lib.pdmk_batch_create_double.restype = v
+    lib.pdmk_batch_evaluate.argtypes = [v, _D, _D]
+    lib.pdmk_batch_evaluate.restype = ctypes.c_int
+    lib.pdmk_batch_evaluate_float.argtypes = [v, _D, _F]
+    lib.pdmk_batch_evaluate_float.restype = ctypes.c_int
+    lib.pdmk_batch_info.argtypes = [v, _I64]
+    lib.pdmk_batch_info.restype = ctypes.c_int
+    lib.pdmk_batch_destroy.argtypes = [v]
+    lib.pdmk_batch_destroy.restype = None
     lib.pdmk_last_error.argtypes = []
     lib.pdmk_last_error.restype = ctypes.c_char_p
     _lib = lib
@@ -269,6 +285,68 @@ class PeriodicDMKTree:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class PeriodicDMKBatch:
+    """Many independent periodic systems built and evaluated together.
+
+    cells: sequence of 3x3 (columns = lattice vectors); positions: sequence of
+    (N_i, 3) arrays.  precision "auto" follows the reference's
+    AutoPeriodicDMKTree (float / mixed precision for n_digits <= 6, double
+    above); "double" forces double trees.  evaluate takes a sequence of charge
+    vectors and returns a list of potential arrays (float64).
+    """
+
+    def __init__(self, cells, positions, n_digits=6, n_per_leaf=300, nz=4, precision="auto"):
+        if precision not in ("auto", "double"):
+            raise ValueError("precision must be 'auto' or 'double'")
+        if len(cells) != len(positions) or len(cells) == 0:
+            raise ValueError("need one cell per system and at least one system")
+        self._lib = library()
+        pos = [np.ascontiguousarray(p, dtype=np.float64) for p in positions]
+        for p in pos:
+            if p.ndim != 2 or p.shape[1] != 3 or p.shape[0] == 0:
+                raise ValueError("positions must be non-empty (N_i, 3) arrays")
+        self.Ns = np.array([p.shape[0] for p in pos], dtype=np.int32)
+        self.offsets = np.concatenate([[0], np.cumsum(self.Ns, dtype=np.int64)])
+        c = np.concatenate([_cell_colmajor(cc) for cc in cells])
+        allpos = np.ascontiguousarray(np.concatenate(pos, axis=0))
+        create = self._lib.pdmk_batch_create if precision == "auto" else self._lib.pdmk_batch_create_double
+        self._h = create(len(pos), _ptr(c), _ptr(self.Ns, _I), _ptr(allpos), int(n_digits), int(n_per_leaf), int(nz))
+        if not self._h:
+            raise RuntimeError("pdmk_batch_create failed: " + _last_error())
+
+    def info(self):
+        out = np.zeros(4, dtype=np.int64)
+        if self._lib.pdmk_batch_info(self._h, _ptr(out, _I64)) != 0:
+            raise RuntimeError("pdmk_batch_info failed: " + _last_error())
+        return {"n_systems": int(out[0]), "n_points": int(out[1]), "device_bytes": int(out[2]),
+                "float_trees": bool(out[3])}
+
+    def evaluate(self, charges, out_dtype=np.float64):
+        q = np.ascontiguousarray(np.concatenate([np.asarray(c, dtype=np.float64) for c in charges]))
+        if q.shape != (int(self.offsets[-1]),):
+            raise ValueError("charges must match the systems' point counts")
+        if out_dtype == np.float32:
+            out = np.empty(q.shape[0], dtype=np.float32)
+            rc = self._lib.pdmk_batch_evaluate_float(self._h, _ptr(q), _ptr(out, _F))
+        else:
+            out = np.empty(q.shape[0], dtype=np.float64)
+            rc = self._lib.pdmk_batch_evaluate(self._h, _ptr(q), _ptr(out))
+        if rc != 0:
+            raise RuntimeError("pdmk_batch_evaluate failed (code %d): %s" % (rc, _last_error()))
+        return [out[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.Ns))]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pdmk_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def ewald(cell, positions, charges, s=4.8):

@@ -1,0 +1,182 @@
+// Batch of independent periodic systems (the many-systems form of the
+// reference's build-once / evaluate-many API, cpp/src/periodic_dmk.cpp:41-186,
+// one PeriodicDMKTreeT per system).
+//
+// Construction: the host plans (tree, lists, tables) of all systems are built
+// on all host threads, then uploaded one by one.  Evaluate: one host->device
+// copy of all charges, every system's evaluate enqueued on its own stream
+// after that copy, one device->host copy of all potentials after every
+// system's stream has finished.
+#include "batch.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <exception>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
+
+#include "../host/plan.hpp"
+
+namespace pdmkb {
+
+TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double* positions, int n_digits,
+                     int n_per_leaf, int nz, bool single)
+    : single_(single) {
+    if (nsys <= 0) throw std::invalid_argument("nsys must be positive");
+    if (!cells || !Ns || !positions) throw std::invalid_argument("null cells, Ns or positions");
+    off_.assign(nsys + 1, 0);
+    for (int i = 0; i < nsys; ++i) {
+        if (Ns[i] <= 0) throw std::invalid_argument("every system needs at least one point");
+        off_[i + 1] = off_[i] + Ns[i];
+    }
+    // host plans in parallel
+    std::vector<std::unique_ptr<Plan>> plans(nsys);
+    std::atomic<int> next{0};
+    std::exception_ptr first_error;
+    std::mutex err_mu;
+    auto work = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= nsys) return;
+            try {
+                plans[i] = std::make_unique<Plan>(
+                    build_plan(cells + 9 * (size_t)i, Ns[i], positions + 3 * off_[i], n_digits, n_per_leaf, nz));
+            } catch (...) {
+                std::lock_guard<std::mutex> g(err_mu);
+                if (!first_error) first_error = std::current_exception();
+            }
+        }
+    };
+    const int nthr = std::max(1, std::min<int>(nsys, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+    if (first_error) std::rethrow_exception(first_error);
+    try {
+        PDMK_CUDA_CHECK(cudaGetDevice(&device_));
+        trees_.reserve(nsys);
+        for (int i = 0; i < nsys; ++i) {
+            trees_.push_back(std::make_unique<DeviceTree>(*plans[i], device_, /*fp64_working_set=*/!single_));
+            plans[i].reset();  // the device tree keeps what it needs
+        }
+        PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
+        done_.assign(nsys, nullptr);
+        for (auto& e : done_) PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        const size_t n = (size_t)total_points();
+        PDMK_CUDA_CHECK(cudaMalloc(&q_dev_, sizeof(double) * n));
+        PDMK_CUDA_CHECK(cudaMalloc(&pot_dev_, sizeof(double) * n));
+        PDMK_CUDA_CHECK(cudaMalloc(&potf_dev_, sizeof(float) * n));
+        PDMK_CUDA_CHECK(cudaMallocHost(&err_host_, sizeof(int) * nsys));
+        graphs_.assign(nsys, nullptr);
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+void TreeBatch::release() {
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& g : graphs_)
+        if (g) cudaGraphExecDestroy(g);
+    graphs_.clear();
+    if (err_host_) cudaFreeHost(err_host_);
+    err_host_ = nullptr;
+    trees_.clear();
+    for (auto& e : done_)
+        if (e) cudaEventDestroy(e);
+    done_.clear();
+    if (ready_) cudaEventDestroy(ready_);
+    if (stream_) cudaStreamDestroy(stream_);
+    if (q_dev_) cudaFree(q_dev_);
+    if (pot_dev_) cudaFree(pot_dev_);
+    if (potf_dev_) cudaFree(potf_dev_);
+    ready_ = nullptr;
+    stream_ = nullptr;
+    q_dev_ = pot_dev_ = nullptr;
+    potf_dev_ = nullptr;
+}
+
+TreeBatch::~TreeBatch() { release(); }
+
+size_t TreeBatch::device_bytes() const {
+    size_t b = (sizeof(double) * 2 + sizeof(float)) * (size_t)total_points();
+    for (const auto& t : trees_) b += t->device_bytes();
+    return b;
+}
+
+void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
+    if (!charges || !pot) throw std::invalid_argument("null charges or output");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    const int64_t n = total_points();
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, charges, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    PDMK_CUDA_CHECK(cudaEventRecord(ready_, stream_));
+    // The first evaluate runs the systems directly (it creates their multi-RHS
+    // state); the second captures each system's launch sequence into a CUDA
+    // graph (device buffers and tables are fixed per system), later ones
+    // replay the graphs.
+    const bool capture = evaluates_ == 1;
+    for (size_t i = 0; i < trees_.size(); ++i) {
+        DeviceTree& t = *trees_[i];
+        cudaStream_t ts = t.stream();
+        PDMK_CUDA_CHECK(cudaStreamWaitEvent(ts, ready_, 0));
+        auto enqueue = [&]() {
+            if (single_)
+                t.enqueue_multi_device(q_dev_ + off_[i], 1, pot_dev_ + off_[i], /*fp32=*/true);
+            else
+                t.evaluate_device(q_dev_ + off_[i], pot_dev_ + off_[i], nullptr);
+        };
+        if (graphs_[i]) {
+            PDMK_CUDA_CHECK(cudaGraphLaunch(graphs_[i], ts));
+        } else if (capture) {
+            cudaGraph_t g = nullptr;
+            PDMK_CUDA_CHECK(cudaStreamBeginCapture(ts, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue();
+            } catch (...) {
+                cudaStreamEndCapture(ts, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            PDMK_CUDA_CHECK(cudaStreamEndCapture(ts, &g));
+            cudaGraphExec_t ge = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            PDMK_CUDA_CHECK(ie);
+            graphs_[i] = ge;
+            PDMK_CUDA_CHECK(cudaGraphLaunch(ge, ts));
+        } else {
+            enqueue();
+        }
+        PDMK_CUDA_CHECK(cudaEventRecord(done_[i], ts));
+        PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
+    }
+    if (pot_float) {
+        dev::launch_to_float(pot_dev_, potf_dev_, n, stream_);
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, potf_dev_, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_));
+    } else {
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pot_dev_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+    }
+    // error words of the tensor-core kernels: one asynchronous copy each, one wait
+    int n_err = 0;
+    if (single_) {
+        for (size_t i = 0; i < trees_.size(); ++i) {
+            const int* w = trees_[i]->multi_error_word(true);
+            err_host_[i] = 0;
+            if (w) {
+                PDMK_CUDA_CHECK(cudaMemcpyAsync(err_host_ + i, w, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+                ++n_err;
+            }
+        }
+    }
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    PDMK_CUDA_CHECK(cudaGetLastError());
+    ++evaluates_;
+    if (n_err)
+        for (size_t i = 0; i < trees_.size(); ++i)
+            if (err_host_[i]) trees_[i]->check_device_error();  // clears the word and throws
+}
+
+}  // namespace pdmkb

@@ -1,0 +1,49 @@
+// Batch of independent periodic systems: host trees built in parallel, device
+// evaluates enqueued concurrently (one stream per system).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "../device/device_tree.hpp"
+
+namespace pdmkb {
+
+class TreeBatch {
+  public:
+    // cells: nsys x 9 (column-major 3x3 each); positions: 3 x Ns[i] blocks in order.
+    // single: float (mixed-precision) trees, else double.
+    TreeBatch(int nsys, const double* cells, const int* Ns, const double* positions, int n_digits, int n_per_leaf,
+              int nz, bool single);
+    ~TreeBatch();
+    TreeBatch(const TreeBatch&) = delete;
+    TreeBatch& operator=(const TreeBatch&) = delete;
+
+    // charges / pot: concatenated host arrays of total_points() entries.
+    void evaluate(const double* charges, void* pot, bool pot_float);
+    int n_systems() const { return (int)trees_.size(); }
+    int64_t total_points() const { return off_.empty() ? 0 : off_.back(); }
+    size_t device_bytes() const;
+    bool single() const { return single_; }
+
+  private:
+    void release();
+    std::vector<std::unique_ptr<DeviceTree>> trees_;
+    std::vector<int64_t> off_;  // prefix sums of N (size nsys + 1)
+    bool single_ = false;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ready_ = nullptr;
+    std::vector<cudaEvent_t> done_;
+    double* q_dev_ = nullptr;
+    double* pot_dev_ = nullptr;
+    float* potf_dev_ = nullptr;
+    // after the first evaluate, each system's evaluate is replayed from a CUDA graph
+    std::vector<cudaGraphExec_t> graphs_;
+    int* err_host_ = nullptr;  // pinned, one word per system
+    int evaluates_ = 0;
+};
+
+}  // namespace pdmkb

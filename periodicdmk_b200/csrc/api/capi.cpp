@@ -14,6 +14,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "batch.hpp"
 #include "impl.hpp"
 #include "pdmk/periodic_dmk.hpp"
 
@@ -208,6 +209,62 @@ int pdmk_evaluate_multi_double(void* h, int, int k, const double* q, double* pot
 int pdmk_evaluate_multi_float(void* h, int, int k, const double* q, float* pot) {
     return evaluate_multi_impl<float, float>(h, k, q, pot);
 }
+void* pdmk_batch_create(int nsys, const double* cells, const int* Ns, const double* pos, int nd, int npl, int nz) {
+    try {
+        g_last_error.clear();
+        return new pdmkb::TreeBatch(nsys, cells, Ns, pos, nd, npl, nz, /*single=*/nd <= 6);
+    } catch (const std::exception& e) {
+        set_error("pdmk_batch_create", e.what());
+        return nullptr;
+    }
+}
+void* pdmk_batch_create_double(int nsys, const double* cells, const int* Ns, const double* pos, int nd, int npl,
+                               int nz) {
+    try {
+        g_last_error.clear();
+        return new pdmkb::TreeBatch(nsys, cells, Ns, pos, nd, npl, nz, /*single=*/false);
+    } catch (const std::exception& e) {
+        set_error("pdmk_batch_create_double", e.what());
+        return nullptr;
+    }
+}
+int pdmk_batch_evaluate(void* h, const double* q, double* pot) {
+    if (!h) {
+        set_error("pdmk_batch_evaluate", "null handle");
+        return -1;
+    }
+    try {
+        static_cast<pdmkb::TreeBatch*>(h)->evaluate(q, pot, /*pot_float=*/false);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_batch_evaluate", e);
+    }
+}
+int pdmk_batch_evaluate_float(void* h, const double* q, float* pot) {
+    if (!h) {
+        set_error("pdmk_batch_evaluate_float", "null handle");
+        return -1;
+    }
+    try {
+        static_cast<pdmkb::TreeBatch*>(h)->evaluate(q, pot, /*pot_float=*/true);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_batch_evaluate_float", e);
+    }
+}
+int pdmk_batch_info(void* h, int64_t* out4) {
+    if (!h || !out4) {
+        set_error("pdmk_batch_info", "null handle or output");
+        return -1;
+    }
+    const auto* b = static_cast<pdmkb::TreeBatch*>(h);
+    out4[0] = b->n_systems();
+    out4[1] = b->total_points();
+    out4[2] = (int64_t)b->device_bytes();
+    out4[3] = b->single() ? 1 : 0;
+    return 0;
+}
+void pdmk_batch_destroy(void* h) { delete static_cast<pdmkb::TreeBatch*>(h); }
 void pdmk_destroy_double(void* h) { delete static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h); }
 void pdmk_destroy_float(void* h) { delete static_cast<pdmk::PeriodicDMKTreeT<float, 3>*>(h); }
 

@@ -34,8 +34,8 @@ PeriodicDMKTreeT<Real, DIM>::PeriodicDMKTreeT(const MatND<DIM>& cell, const std:
         for (int d = 0; d < 3; ++d) pos[3 * i + d] = positions[i][d];
     p_->plan = std::make_unique<pdmkb::Plan>(
         pdmkb::build_plan(c, (int)positions.size(), pos.data(), n_digits, n_per_leaf, nz));
-    p_->dev = std::make_unique<pdmkb::DeviceTree>(*p_->plan);
     p_->single = std::is_same<Real, float>::value;
+    p_->dev = std::make_unique<pdmkb::DeviceTree>(*p_->plan, -1, /*fp64_working_set=*/!p_->single);
     n_src_ = p_->plan->n_src;
     rc_ = p_->plan->rc;
 }

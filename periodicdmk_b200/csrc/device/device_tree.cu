@@ -66,16 +66,16 @@ T* DeviceTree::upload(const std::vector<T>& v) {
     return p;
 }
 
-DeviceTree::DeviceTree(const Plan& P, int device) {
+DeviceTree::DeviceTree(const Plan& P, int device, bool fp64_working_set) {
     try {
-        init(P, device);
+        init(P, device, fp64_working_set);
     } catch (...) {
         release();
         throw;
     }
 }
 
-void DeviceTree::init(const Plan& P, int device) {
+void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     if (device < 0) PDMK_CUDA_CHECK(cudaGetDevice(&device));
     device_ = device;
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
@@ -220,9 +220,6 @@ void DeviceTree::init(const Plan& P, int device) {
     n_up_ = P.n_proxy_up;
     n_down_ = P.n_proxy_down;
     n_pw_ = P.n_pw_exp;
-    proxy_up_ = alloc<double>(n_up_ * ncoef);
-    proxy_down_ = alloc<double>(n_down_ * ncoef);
-    pw_out_ = alloc<cd>(n_pw_ * M);
 
     // ------------------------------------------------------------------ tables
     {
@@ -506,9 +503,7 @@ void DeviceTree::init(const Plan& P, int device) {
     // ------------------------------------------------------------------ scratch
     scratch_elems_ = std::max<int64_t>(scratch_need, 1);
     pw_in_elems_ = std::max<int64_t>(pw_in_need, 1);
-    scratch1_ = alloc<cd>(scratch_elems_);
-    scratch2_ = alloc<cd>(scratch_elems_);
-    pw_in_ = alloc<cd>(pw_in_elems_);
+    if (fp64_working_set) ensure_fp64_working_set();
 
     // ------------------------------------------------------------------ far field
     {
@@ -607,6 +602,19 @@ void DeviceTree::init(const Plan& P, int device) {
 
 DeviceTree::~DeviceTree() { release(); }
 
+void DeviceTree::ensure_fp64_working_set() {
+    if (proxy_up_) return;
+    const int64_t ncoef = (int64_t)p_ * p_ * p_;
+    proxy_up_ = alloc<double>(n_up_ * ncoef);
+    proxy_down_ = alloc<double>(n_down_ * ncoef);
+    pw_out_ = alloc<cd>(n_pw_ * (int64_t)M_);
+    scratch1_ = alloc<cd>(scratch_elems_);
+    scratch2_ = alloc<cd>(scratch_elems_);
+    pw_in_ = alloc<cd>(pw_in_elems_);
+    c2x_.proxy_up = proxy_up_;
+    eval_.proxy_down = proxy_down_;
+}
+
 void DeviceTree::release() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
@@ -630,6 +638,7 @@ void DeviceTree::release() {
 }
 
 void DeviceTree::run(const double* q, double* pot) {
+    ensure_fp64_working_set();
     const int p = p_, n = npw_, n2 = npw2_, M = M_;
     const int64_t ncoef = (int64_t)p * p * p;
     cudaStream_t s = stream_;

@@ -23,7 +23,10 @@ struct StageTimes {
 
 class DeviceTree {
   public:
-    DeviceTree(const Plan& P, int device = -1);
+    // fp64_working_set: allocate the single-RHS FP64 expansion and transform
+    // buffers now (double trees); float trees leave them to the first FP64
+    // evaluate, if any, since their evaluates use the multi-RHS state.
+    DeviceTree(const Plan& P, int device = -1, bool fp64_working_set = true);
     ~DeviceTree();
     DeviceTree(const DeviceTree&) = delete;
     DeviceTree& operator=(const DeviceTree&) = delete;
@@ -41,6 +44,14 @@ class DeviceTree {
     // fp32: mixed-precision path, else FP64.  RHS processed in blocks sized to
     // the free device memory (at most 64).  times (optional) sums the blocks.
     void evaluate_multi_device(const double* Q_dev, int k, double* pot_dev, bool fp32, StageTimes* times = nullptr);
+    // Same computation, enqueued on stream() without any host synchronisation
+    // (no stage times); check_device_error() after the stream has finished
+    // reports a tensor-core pipeline timeout of the enqueued work.
+    void enqueue_multi_device(const double* Q_dev, int k, double* pot_dev, bool fp32);
+    void check_device_error();
+    // Device word a tensor-core kernel of the multi-RHS state sets on a pipeline
+    // timeout (null before the first multi-RHS call of that precision).
+    int* multi_error_word(bool fp32) const;
     // Host buffers (pinned or pageable).  pot is double* or, with pot_float,
     // float* (converted on the device before the copy back).
     void evaluate_multi_host(const double* Q, int k, void* pot, bool pot_float, bool fp32,
@@ -72,7 +83,9 @@ class DeviceTree {
     struct MultiStateDeleter {
         void operator()(MultiState* m) const;
     };
-    int multi_block(int k, bool fp32) const;
+    int multi_block(int k, bool fp32);
+    int multi_block_size(int k, bool fp32) const;
+    int kb_cache_k_[2] = {0, 0}, kb_cache_[2] = {0, 0};  // last (k -> kb) per precision
     MultiState& multi_state(int kb, bool fp32);
     template <typename T>
     void run_multi_block(MultiState& m, const double* Q, int kvalid, double* pot_user);
@@ -92,7 +105,8 @@ class DeviceTree {
     int tc_mask_ = 7;
 
   private:
-    void init(const Plan& P, int device);
+    void init(const Plan& P, int device, bool fp64_working_set);
+    void ensure_fp64_working_set();
     void release();
     template <typename T>
     T* alloc(size_t n);

@@ -94,6 +94,9 @@ void launch_near(const NearArgs& a, cudaStream_t s);
 void launch_finalize(const double* pot_sorted, const double* far_sorted, const double4* trg, const int* trg_perm,
                      const double* q_user, double* pot_user, int n, cudaStream_t s);
 
+// ---- out[i] = (float)in[i]
+void launch_to_float(const double* in, float* out, int64_t n, cudaStream_t s);
+
 // ---- FMA throughput probe of the current device, TFLOP/s (2 flops per FMA)
 double fma_probe_tflops(bool fp64);
 

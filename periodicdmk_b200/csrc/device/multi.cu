@@ -803,7 +803,16 @@ struct DeviceTree::MultiState {
 
 void DeviceTree::MultiStateDeleter::operator()(MultiState* m) const { delete m; }
 
-int DeviceTree::multi_block(int k, bool fp32) const {
+int DeviceTree::multi_block(int k, bool fp32) {
+    // an existing state of this precision serves every k up to its block size
+    const int pi = fp32 ? 1 : 0;
+    if (kb_cache_k_[pi] == k && multi_[pi]) return kb_cache_[pi];
+    kb_cache_k_[pi] = k;
+    kb_cache_[pi] = multi_block_size(k, fp32);
+    return kb_cache_[pi];
+}
+
+int DeviceTree::multi_block_size(int k, bool fp32) const {
     // bytes per RHS of the per-RHS buffers
     const int64_t ts = fp32 ? 4 : 8;
     const int64_t ncoef = (int64_t)p_ * p_ * p_;
@@ -836,9 +845,19 @@ DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
     const int64_t per_entry = 2 * ts * std::max<int64_t>({(int64_t)p_ * p_ * npw_, (int64_t)p_ * npw_ * npw_,
                                                           (int64_t)npw_ * npw2_ * p_, (int64_t)npw2_ * p_ * p_,
                                                           (int64_t)M_, ncoef});
-    m->scratch_bytes = std::max<int64_t>((int64_t)512 << 20, per_entry * kb);
-    m->s1 = m->alloc<unsigned char>((size_t)m->scratch_bytes);
-    m->s2 = m->alloc<unsigned char>((size_t)m->scratch_bytes);
+    // enough for the largest batched step (all boxes of a group, all kb RHS),
+    // capped at 512 MB (larger steps are chunked), never below one box
+    int64_t max_boxes = 1;
+    for (const auto& g : c2p_groups_) max_boxes = std::max<int64_t>(max_boxes, g.n);
+    for (const auto& g : pw_groups_) max_boxes = std::max<int64_t>(max_boxes, g.n);
+    for (const auto& E : eval_levels_) max_boxes = std::max<int64_t>({max_boxes, (int64_t)E.n, (int64_t)E.n_p2c});
+    m->scratch_bytes = std::max<int64_t>(per_entry * kb, std::min<int64_t>((int64_t)512 << 20, per_entry * kb * max_boxes));
+    // s1 / s2 hold step-by-step transform intermediates; the fused transforms need none
+    const bool fused_all = fp32 ? (dev::sep3_supported<float>(p_) && dev::pw_fused_supported<float>(p_, npw_, npw2_))
+                                : (dev::sep3_supported<double>(p_) && dev::pw_fused_supported<double>(p_, npw_, npw2_));
+    const size_t s12 = fused_all ? 256 : (size_t)m->scratch_bytes;
+    m->s1 = m->alloc<unsigned char>(s12);
+    m->s2 = m->alloc<unsigned char>(s12);
     m->pw_in = m->alloc<unsigned char>((size_t)m->scratch_bytes);
     m->pot = m->alloc<double>((size_t)n_ * kb);
     m->far = m->alloc<double>((size_t)n_ * kb);
@@ -1086,7 +1105,9 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         for (int i = 0; i < near_.nc; ++i) a.coef[i] = near_.coef[i];
         bool tc_done = false;
         if constexpr (f32) {
-            if ((tc_mask_ & 2) && near_max_pairs_ <= dev::kNearTcMaxPairs) {
+            // tensor cores for blocks of 16+ RHS; a single RHS keeps 15/16 of every MMA idle
+            // and the CUDA-core kernel's occupancy wins
+            if ((tc_mask_ & 2) && kb >= 16 && near_max_pairs_ <= dev::kNearTcMaxPairs) {
                 dev::NearTc t{};
                 t.trg_start = near_.trg_start; t.trg_count = near_.trg_count; t.pair_start = near_.pair_start;
                 t.pair_src_start = near_.pair_src_start; t.pair_src_count = near_.pair_src_count;
@@ -1179,10 +1200,49 @@ void DeviceTree::evaluate_multi_device(const double* Q, int k, double* pot, bool
     last_was_multi_ = true;
 }
 
+void DeviceTree::enqueue_multi_device(const double* Q, int k, double* pot, bool fp32) {
+    if (k <= 0) throw std::invalid_argument("k must be positive");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    fp32 = fp32 && mixed_allowed();
+    const int kb = multi_block(k, fp32);
+    MultiState& m = multi_state(kb, fp32);
+    multi_launches_ = 0;
+    for (int c0 = 0; c0 < k; c0 += m.kb) {
+        const int kv = std::min(m.kb, k - c0);
+        if (fp32)
+            run_multi_block<float>(m, Q + (int64_t)c0 * n_, kv, pot + (int64_t)c0 * n_);
+        else
+            run_multi_block<double>(m, Q + (int64_t)c0 * n_, kv, pot + (int64_t)c0 * n_);
+    }
+    last_was_multi_ = true;
+}
+
+int* DeviceTree::multi_error_word(bool fp32) const {
+    const auto& slot = multi_[fp32 ? 1 : 0];
+    return slot ? slot->err : nullptr;
+}
+
+void DeviceTree::check_device_error() {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    for (auto& slot : multi_) {
+        if (!slot) continue;
+        int err = 0;
+        PDMK_CUDA_CHECK(cudaMemcpy(&err, slot->err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) {
+            PDMK_CUDA_CHECK(cudaMemset(slot->err, 0, sizeof(int)));
+            throw std::runtime_error("CUDA error: tensor-core pipeline wait timed out in the multi-RHS evaluate");
+        }
+    }
+}
+
 namespace dev {
 __global__ void k_to_float_out(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (float)in[i];
+}
+void launch_to_float(const double* in, float* out, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_to_float_out<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, out, n);
 }
 }  // namespace dev
 

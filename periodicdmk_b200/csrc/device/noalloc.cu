@@ -72,6 +72,8 @@ dev::cd* scratch_address(int device) {
 
 void DeviceTree::evaluate_device_noalloc(const double* q, double* pot) {
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    if (!proxy_up_)
+        throw std::invalid_argument("the no-allocation evaluate needs a tree built with its FP64 buffers (double tree)");
     dev::cd* scratch = scratch_address(device_);
     const int64_t cap = kNoAllocScratchElems;
     const int p = p_, n = npw_, n2 = npw2_, M = M_;

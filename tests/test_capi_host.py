@@ -112,3 +112,19 @@ def test_cubic_cover():
     assert r["p"] == 4 and r["m"] >= 4 and r["n"] >= 4
     with pytest.raises(RuntimeError):
         pd.optimize_cubic_cover(np.eye(3), nz=0)
+
+
+def test_batch_create_rejects_bad_input_without_compute():
+    import ctypes
+    lib = pd.library()
+    cells = np.tile(np.eye(3).reshape(-1), 2)
+    Ns = np.array([10, 0], dtype=np.int32)
+    pos = np.zeros(30)
+    h = lib.pdmk_batch_create(2, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              Ns.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                              pos.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 6, 300, 4)
+    assert not h
+    assert "at least one point" in pd._last_error()
+    h = lib.pdmk_batch_create(0, None, None, None, 6, 300, 4)
+    assert not h
+    assert lib.pdmk_batch_evaluate(None, None, None) == -1
