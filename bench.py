@@ -46,6 +46,75 @@ def make_system(n, seed=1, scale=1.0):
     return np.eye(3) * scale, pos, q
 
 
+def batch_systems(nsys, seed):
+    """Many-systems workload: triclinic cells (lengths U[0.8, 1.2], angles
+    U[75, 105] degrees, a1 along x, a2 in the xy plane), N log-uniform in
+    [1e3, 1e5], fractional-uniform points, +-1 neutral charges."""
+    rng = np.random.default_rng(seed)
+    cells, pos, qs = [], [], []
+    for _ in range(nsys):
+        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e5)))))
+        n += n % 2
+        L = rng.uniform(0.8, 1.2, 3)
+        al, be, ga = np.radians(rng.uniform(75.0, 105.0, 3))
+        cx = np.cos(be)
+        cy = (np.cos(al) - np.cos(be) * np.cos(ga)) / np.sin(ga)
+        cell = np.column_stack([[L[0], 0.0, 0.0], L[1] * np.array([np.cos(ga), np.sin(ga), 0.0]),
+                                L[2] * np.array([cx, cy, np.sqrt(max(1.0 - cx * cx - cy * cy, 1e-12))])])
+        q = np.ones(n)
+        q[: n // 2] = -1.0
+        rng.shuffle(q)
+        cells.append(cell)
+        pos.append(rng.uniform(0.0, 1.0, (n, 3)) @ cell.T)
+        qs.append(q)
+    return cells, pos, qs
+
+
+def lpt_partition(costs, parts):
+    """Greedy longest-processing-time assignment of items to parts."""
+    loads = [0.0] * parts
+    owner = [0] * len(costs)
+    for i in sorted(range(len(costs)), key=lambda j: -costs[j]):
+        r = min(range(parts), key=lambda p: loads[p])
+        owner[i] = r
+        loads[r] += costs[i]
+    return owner
+
+
+def run_batch(pd, args, world, rank, barrier, max_over_ranks):
+    """512 independent systems (cfg5 form) through pdmk_batch_evaluate, host
+    buffers in and out; systems split across ranks by LPT on their point
+    counts.  Returns the JSON fragment for the bench line."""
+    cells, pos, qs = batch_systems(args.batch_systems, seed=11)
+    owner = lpt_partition([len(q) for q in qs], world)
+    mine = [i for i in range(len(qs)) if owner[i] == rank]
+    t0 = time.perf_counter()
+    b = pd.PeriodicDMKBatch([cells[i] for i in mine], [pos[i] for i in mine], n_digits=6, n_per_leaf=300, nz=4)
+    t_build = time.perf_counter() - t0
+    q_mine = [qs[i] for i in mine]
+    for _ in range(max(3, args.warmup)):   # 1st creates the device state, 2nd records the graphs
+        b.evaluate(q_mine)
+    barrier()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        b.evaluate(q_mine)
+        ts.append(time.perf_counter() - t0)
+    barrier()
+    t = max_over_ranks(statistics.median(ts))
+    total = sum(len(q) for q in qs)
+    info = b.info()
+    b.close()
+    return {"workload": "%d independent periodic systems: triclinic cells (lengths U[0.8,1.2], angles "
+                        "U[75,105] deg), N log-uniform in [1e3,1e5] (total %d points), +-1 charges, 6 digits, "
+                        "npl 300, nz 4, float trees (mixed precision), one RHS" % (len(qs), total),
+            "value": total / t / 1e6, "unit": "Mpts/s", "ms_per_step": t * 1e3,
+            "timing": "host wall clock of the synchronous pdmk_batch_evaluate call (charges H2D and potentials "
+                      "D2H included), median of steps, max over ranks",
+            "partition": "LPT on point counts over %d rank(s)" % world,
+            "host_build_s": t_build, "device_bytes_rank0": info["device_bytes"]}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -299,14 +368,16 @@ def run_ours(args):
                     "api": "pdmk_evaluate_multi_float (pinned host buffers)"},
             "gpu_launches": finfo["launches_last_multi"] * args.steps,
             "roofline": roofline, "clocks": clk2.summary()}
+    tree_d.close()
+    tree_f.close()
+    if args.batch_systems > 0:
+        line["batch"] = run_batch(pd, args, world, rank, barrier, max_over_ranks)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, desc, _ = cpu_baseline(n, 3, threads)
         line["cpu_baseline"] = {"value": v, "unit": "Mpts*RHS/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    tree_d.close()
-    tree_f.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -322,6 +393,8 @@ def main():
     ap.add_argument("--n", type=int, default=1000000)
     ap.add_argument("--rhs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-systems", type=int, default=512,
+                    help="systems of the many-systems measurement (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
