@@ -19,6 +19,8 @@
 
 #include "../host/pswf.hpp"
 #include "device_tree.hpp"
+#include "pw_fused.cuh"
+#include "sep3.cuh"
 
 namespace pdmkb {
 
@@ -309,7 +311,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             g.child = c;
             c2p_groups_.push_back(g);
             scratch_need = std::max<int64_t>(scratch_need, (int64_t)g.n * ncoef);
-            launches_ += 3;
+            launches_ += dev::sep3_supported<double>(p) ? 1 : 3;
         }
     }
     // ------------------------------------------------------------------ outgoing plane waves
@@ -329,7 +331,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         g.out_off = upload(out);
         pw_groups_.push_back(g);
         scratch_need = std::max<int64_t>(scratch_need, (int64_t)g.n * std::max<int64_t>((int64_t)p * p * n, (int64_t)p * n * n));
-        launches_ += 3;
+        launches_ += dev::pw_fused_supported<double>(p, n, n2) ? 1 : 3;
     }
     // ------------------------------------------------------------------ downward per level
     for (int l = 0; l < P.nlevels; ++l) {
@@ -387,7 +389,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         pw_in_need = std::max<int64_t>(pw_in_need, (int64_t)E.n * M);
         scratch_need = std::max<int64_t>(scratch_need, (int64_t)E.n * std::max<int64_t>((int64_t)n * n2 * p, (int64_t)n2 * p * p));
         scratch_need = std::max<int64_t>(scratch_need, (int64_t)E.n_p2c * ncoef);
-        launches_ += 4 + (E.n_p2c ? 3 : 0);
+        launches_ += 1 + (dev::pw_fused_supported<double>(p, n, n2) ? 1 : 3) +
+                     (E.n_p2c ? (dev::sep3_supported<double>(p) ? 1 : 3) : 0);
     }
     // ------------------------------------------------------------------ leaf evaluation
     {
@@ -649,8 +652,18 @@ void DeviceTree::run(const double* q, double* pot) {
     dev::launch_gather(src_, src_charge_idx_, q, n_all_, s);
     // upward
     dev::launch_c2proxy(c2x_, p, s);
+    // fused transforms (intermediates in shared memory) where the order allows
+    const bool fused_c2p = dev::sep3_supported<double>(p);
+    const bool fused_pw = dev::pw_fused_supported<double>(p, n, n2);
     for (const auto& g : c2p_groups_) {
         const double* mx = c2p_ + (int64_t)g.child * 3 * p * p;
+        if (fused_c2p) {
+            dev::Sep3 f{};
+            f.in = proxy_up_; f.in_off = g.in_off; f.out = proxy_up_; f.out_off = g.out_off; f.mat = mx;
+            f.rhs = 1; f.accumulate = 1;
+            dev::launch_sep3<double>(f, p, g.n, s);
+            continue;
+        }
         dev::ContractArgs a{};
         a.n_entries = g.n;
         // x: in (i,j,k) -> s1 (j,k,a)
@@ -668,6 +681,13 @@ void DeviceTree::run(const double* q, double* pot) {
     // outgoing plane waves
     for (const auto& g : pw_groups_) {
         const auto& L = lev_[g.level];
+        if (fused_pw) {
+            dev::PwFused f{};
+            f.in = proxy_up_; f.in_off = g.in_off; f.out = pw_out_; f.out_off = g.out_off;
+            f.mat_a = L.poly2pw; f.mat_b = L.poly2pw_half; f.rhs = 1; f.e0 = 0;
+            dev::launch_pw_out_fused<double>(f, p, n, n2, g.n, s);
+            continue;
+        }
         dev::ContractArgs a{};
         a.n_entries = g.n;
         a.in = proxy_up_; a.in_off = g.in_off; a.out = scratch1_; a.out_stride = (int64_t)p * p * n;
@@ -685,18 +705,30 @@ void DeviceTree::run(const double* q, double* pot) {
         const auto& L = lev_[E.level];
         dev::ShiftArgs sa{pw_out_, L.shift, pw_in_, M, E.n, E.term_start, E.term_slot, E.term_stencil};
         dev::launch_shift(sa, s);
-        dev::ContractArgs a{};
-        a.n_entries = E.n;
-        a.in = pw_in_; a.in_stride = M; a.out = scratch1_; a.out_stride = (int64_t)n * n2 * p;
-        a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
-        dev::launch_contract(a, dev::kCCC, s);
-        a.in = scratch1_; a.in_stride = (int64_t)n * n2 * p; a.out = scratch2_; a.out_stride = (int64_t)n2 * p * p;
-        a.R = n2 * p;
-        dev::launch_contract(a, dev::kCCC, s);
-        a.in = scratch2_; a.in_stride = (int64_t)n2 * p * p; a.out = proxy_down_; a.out_off = E.down_off;
-        a.mat = L.pw2polyTw; a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
-        dev::launch_contract(a, dev::kCCR, s);
-        if (E.n_p2c) {
+        if (fused_pw) {
+            dev::PwFused f{};
+            f.in = pw_in_; f.in_stride = M; f.out = proxy_down_; f.out_off = E.down_off;
+            f.mat_a = L.pw2polyT; f.mat_b = L.pw2polyTw; f.rhs = 1; f.e0 = 0;
+            dev::launch_pw_in_fused<double>(f, p, n, n2, E.n, s);
+        } else {
+            dev::ContractArgs a{};
+            a.n_entries = E.n;
+            a.in = pw_in_; a.in_stride = M; a.out = scratch1_; a.out_stride = (int64_t)n * n2 * p;
+            a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
+            dev::launch_contract(a, dev::kCCC, s);
+            a.in = scratch1_; a.in_stride = (int64_t)n * n2 * p; a.out = scratch2_; a.out_stride = (int64_t)n2 * p * p;
+            a.R = n2 * p;
+            dev::launch_contract(a, dev::kCCC, s);
+            a.in = scratch2_; a.in_stride = (int64_t)n2 * p * p; a.out = proxy_down_; a.out_off = E.down_off;
+            a.mat = L.pw2polyTw; a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
+            dev::launch_contract(a, dev::kCCR, s);
+        }
+        if (E.n_p2c && fused_c2p) {
+            dev::Sep3 f{};
+            f.in = proxy_down_; f.in_off = E.p2c_in; f.out = proxy_down_; f.out_off = E.p2c_out; f.mat = p2c_;
+            f.mat_off = E.p2c_mat; f.rhs = 1; f.accumulate = 1;
+            dev::launch_sep3<double>(f, p, E.n_p2c, s);
+        } else if (E.n_p2c) {
             dev::ContractArgs b{};
             b.n_entries = E.n_p2c;
             b.in = proxy_down_; b.in_off = E.p2c_in; b.out = scratch1_; b.out_stride = ncoef;

@@ -18,6 +18,7 @@
 #include "device_tree.hpp"
 #include "nufft_multi.cuh"
 #include "pw_fused.cuh"
+#include "sep3.cuh"
 #include "tc_kernels.cuh"
 
 namespace pdmkb {
@@ -539,17 +540,7 @@ static void launch_near_m32_kb(const NearM& a, const float4* th, const float4* t
 // for one (box, rhs) entry per CTA, the tensor held in shared memory.
 // Matrices U_d column-major P x P at mat + mat_off[eb] + d*P*P.
 // ---------------------------------------------------------------------------
-struct Sep3 {
-    const void* in;
-    const int64_t* in_off;
-    void* out;
-    const int64_t* out_off;
-    const void* mat;
-    const int64_t* mat_off;  // null: mat
-    int rhs;
-    int64_t e0;
-    int accumulate;
-};
+
 
 template <typename T, int P>
 __device__ __forceinline__ void sep3_step(const T* __restrict__ src, T* __restrict__ dst, const T* __restrict__ Ut,
@@ -663,6 +654,11 @@ void launch_sep3(const Sep3& a, int p, int n_entries, cudaStream_t s) {
         default: throw std::runtime_error("fused transform not available for this order");
     }
 }
+
+template bool sep3_supported<float>(int);
+template bool sep3_supported<double>(int);
+template void launch_sep3<float>(const Sep3&, int, int, cudaStream_t);
+template void launch_sep3<double>(const Sep3&, int, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // proxy -> leaf targets, TPT targets per thread: grid (leaves, 1, rhs)
