@@ -10,6 +10,7 @@
 //   flags, lists, work lists       cpp/src/dmk/pbc_tree.cpp:776-1011
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <sstream>
@@ -488,6 +489,48 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
             for (int d = 0; d < 3; ++d)
                 if (std::abs(B.spos[3 * (size_t)i + d] - P.centers[3 * b + d]) > hb)
                     throw std::invalid_argument("point outside the cell's covering grid (positions must lie in the cell)");
+    }
+    // Inside each leaf, order the points along a Morton curve of the leaf box:
+    // consecutive points (one GPU warp's targets, one chunk of sources) then
+    // cover a compact sub-box, so the cutoff tests of the near field agree
+    // across a warp.  Sums over a leaf do not depend on the order.
+    {
+        auto spread3 = [](uint32_t v) {  // 10 bits -> every third bit of 30
+            uint64_t x = v & 0x3FF;
+            x = (x | (x << 16)) & 0x030000FF;
+            x = (x | (x << 8)) & 0x0300F00F;
+            x = (x | (x << 4)) & 0x030C30C3;
+            x = (x | (x << 2)) & 0x09249249;
+            return x;
+        };
+        auto morton_sort = [&](int b, int start, int count, std::vector<double>& pos, std::vector<int>& perm) {
+            if (count < 2) return;
+            const double h = P.boxsize[P.depth[b]] / 2.0;
+            std::vector<uint64_t> key(count);
+            std::vector<int> order(count);
+            for (int i = 0; i < count; ++i) {
+                uint64_t k = 0;
+                for (int d = 0; d < 3; ++d) {
+                    const double f = (pos[3 * (size_t)(start + i) + d] - (P.centers[3 * b + d] - h)) / (2.0 * h);
+                    const int qd = std::min(1023, std::max(0, (int)(f * 1024.0)));
+                    k |= spread3((uint32_t)qd) << d;
+                }
+                key[i] = k;
+                order[i] = i;
+            }
+            std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
+            std::vector<double> tp(pos.begin() + 3 * (size_t)start, pos.begin() + 3 * (size_t)(start + count));
+            std::vector<int> tq(perm.begin() + start, perm.begin() + start + count);
+            for (int i = 0; i < count; ++i) {
+                for (int d = 0; d < 3; ++d) pos[3 * (size_t)(start + i) + d] = tp[3 * (size_t)order[i] + d];
+                perm[start + i] = tq[order[i]];
+            }
+        };
+        for (int b = 0; b < nb; ++b) {
+            if (!P.is_leaf[b]) continue;
+            if (P.src_count[b] > 1) morton_sort(b, P.src_start[b], P.src_count[b], B.spos, B.sperm);
+            if (P.trg_count[b] > 1) morton_sort(b, P.trg_start[b], P.trg_count[b], B.tpos, B.tperm);
+        }
     }
     P.src_sorted = std::move(B.spos);
     P.trg_sorted = std::move(B.tpos);
