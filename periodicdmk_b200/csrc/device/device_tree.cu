@@ -21,6 +21,7 @@
 #include "device_tree.hpp"
 #include "pw_fused.cuh"
 #include "sep3.cuh"
+#include "tc_kernels.cuh"
 
 namespace pdmkb {
 
@@ -453,8 +454,33 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             }
             return kept;
         };
-        std::vector<int> t0, tc, ps{0}, s0, sc;
+        std::vector<int> t0, tc, ps{0}, s0, sc, pcb;
         std::vector<double> bsz;
+        // float bounding boxes (rounded outwards) of every 32-source chunk of the
+        // source boxes that appear in near pairs, one entry set per box
+        std::vector<int> box_cb(P.nboxes, -1);
+        std::vector<float4> clo, chi;
+        auto chunk_base = [&](int sb) {
+            if (box_cb[sb] >= 0) return box_cb[sb];
+            box_cb[sb] = (int)clo.size();
+            const int st = P.src_start[sb], cnt = P.src_count[sb];
+            for (int j0 = 0; j0 < cnt; j0 += dev::kNearTcChunk) {
+                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                for (int i = st + j0; i < st + std::min(cnt, j0 + dev::kNearTcChunk); ++i)
+                    for (int d = 0; d < 3; ++d) {
+                        lo[d] = std::min(lo[d], P.src_sorted[3 * (size_t)i + d]);
+                        hi[d] = std::max(hi[d], P.src_sorted[3 * (size_t)i + d]);
+                    }
+                float l[3], h[3];
+                for (int d = 0; d < 3; ++d) {
+                    l[d] = std::nextafter((float)lo[d], -INFINITY);
+                    h[d] = std::nextafter((float)hi[d], INFINITY);
+                }
+                clo.push_back(make_float4(l[0], l[1], l[2], 0.0f));
+                chi.push_back(make_float4(h[0], h[1], h[2], 0.0f));
+            }
+            return box_cb[sb];
+        };
         for (int tb : P.direct_work) {
             if (P.trg_count[tb] == 0) continue;
             t0.push_back(P.trg_start[tb]);
@@ -480,13 +506,20 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                 s0.push_back(P.src_start[sb]);
                 sc.push_back(P.src_count[sb]);
                 bsz.push_back(b);
+                pcb.push_back(P.src_count[sb] > 0 ? chunk_base(sb) : 0);
             }
             ps.push_back((int)s0.size());
         }
         for (size_t i = 0; i < tc.size(); ++i) {
             near_max_trg_ = std::max(near_max_trg_, tc[i]);
             near_max_pairs_ = std::max(near_max_pairs_, ps[i + 1] - ps[i]);
+            int ch = 0;
+            for (int k = ps[i]; k < ps[i + 1]; ++k) ch += (sc[k] + dev::kNearTcChunk - 1) / dev::kNearTcChunk;
+            near_max_chunks_ = std::max(near_max_chunks_, ch);
         }
+        near_pair_chunk_base_ = upload(pcb);
+        near_chunk_lo_ = upload(clo);
+        near_chunk_hi_ = upload(chi);
         near_.trg = trg_;
         near_.src = src_;
         near_.pot = pot_sorted_;

@@ -120,8 +120,12 @@ class DeviceTree {
     size_t bytes_ = 0;
     int launches_ = 0;
     int64_t near_pairs_culled_ = 0, near_pairs_nominal_ = 0;
-    int near_max_trg_ = 0, near_max_pairs_ = 0;
-    int eval_max_trg_ = 0;  // largest target count of an evaluated leaf  // largest target count / source-box count of a near-field leaf
+    int near_max_trg_ = 0, near_max_pairs_ = 0;  // largest target count / source-box count of a near-field leaf
+    int near_max_chunks_ = 0;                     // largest number of 32-source chunks of a near-field leaf
+    int* near_pair_chunk_base_ = nullptr;         // per near pair: first chunk bounding box of its source box
+    float4* near_chunk_lo_ = nullptr;
+    float4* near_chunk_hi_ = nullptr;
+    int eval_max_trg_ = 0;  // largest target count of an evaluated leaf
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev_[5]{};
     std::vector<void*> allocs_;

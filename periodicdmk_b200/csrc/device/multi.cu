@@ -1103,11 +1103,13 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         if constexpr (f32) {
             // tensor cores for blocks of 16+ RHS; a single RHS keeps 15/16 of every MMA idle
             // and the CUDA-core kernel's occupancy wins
-            if ((tc_mask_ & 2) && kb >= 16 && near_max_pairs_ <= dev::kNearTcMaxPairs) {
+            if ((tc_mask_ & 2) && kb >= 16 && near_max_pairs_ <= dev::kNearTcMaxPairs &&
+                near_max_chunks_ <= dev::kNearTcMaxChunks) {
                 dev::NearTc t{};
                 t.trg_start = near_.trg_start; t.trg_count = near_.trg_count; t.pair_start = near_.pair_start;
                 t.pair_src_start = near_.pair_src_start; t.pair_src_count = near_.pair_src_count;
                 t.pair_bsize = near_.pair_bsize; t.n_leaves = near_.n_leaves; t.max_trg = near_max_trg_;
+                t.pair_chunk_base = near_pair_chunk_base_; t.chunk_lo = near_chunk_lo_; t.chunk_hi = near_chunk_hi_;
                 t.N = n_; t.kb = kb;
                 for (int i = 0; i < near_.nc; ++i) t.coef[i] = near_.coef[i];
                 tc_done = dev::launch_near_tc(t, near_.nc, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo,

@@ -408,18 +408,17 @@ constexpr int kN_OFF_SRC = 2 * kNStage;          // [2][hi 32 float4 | lo 32 flo
 constexpr int kNSrc = kNKC * 32;
 constexpr int kN_OFF_ACC = kN_OFF_SRC + 2 * kNSrc;  // double [64][128]
 constexpr int kN_OFF_PAIR = kN_OFF_ACC + 64 * 128 * 8;
-constexpr int kNPairBytes = kNearTcMaxPairs * 24;   // int start, count, nch; float d2max, rsc, cen
-constexpr int kN_OFF_BAR = kN_OFF_PAIR + kNPairBytes;
-constexpr int kNSmem = kN_OFF_BAR + 64;
+constexpr int kNPairBytes = kNearTcMaxPairs * 28;   // int start, count, nch, cb; float d2max, rsc, cen
+constexpr int kN_OFF_PREF = kN_OFF_PAIR + kNPairBytes;  // int [kNearTcMaxPairs + 1] chunk prefix
+constexpr int kN_OFF_LIST = kN_OFF_PREF + (kNearTcMaxPairs + 1) * 4 + 60;  // int [kNearTcMaxChunks] kept chunks
+constexpr int kN_OFF_BAR = kN_OFF_LIST + kNearTcMaxChunks * 4;
+constexpr int kNSmem = kN_OFF_BAR + 256;
 static_assert(kNSmem <= 227 * 1024, "near smem");
+static_assert(kNKC == kNearTcChunk, "chunk size");
 
 struct NearPair {
-    int start, count, nch;
+    int start, count, nch, cb;
     float d2max, rsc, cen;
-};
-
-struct ChunkCur {
-    int p, j;
 };
 
 template <int NC>
@@ -432,12 +431,17 @@ __global__ void __launch_bounds__(kNThreads, 1)
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
     const int m0 = blockIdx.y * 128;
     if (m0 >= nt) return;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kN_OFF_BAR);  // [0,1] stage free, [2,3] box accumulated
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kN_OFF_BAR);  // [0,1] stage free, [2,3] segment accumulated
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kN_OFF_BAR + 32);
     volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kN_OFF_BAR + 36);  // [3]
     int* s_np = reinterpret_cast<int*>(sm + kN_OFF_BAR + 48);
-    int* s_nch = reinterpret_cast<int*>(sm + kN_OFF_BAR + 52);
+    int* s_nch = reinterpret_cast<int*>(sm + kN_OFF_BAR + 52);   // candidate chunks
+    int* s_kept = reinterpret_cast<int*>(sm + kN_OFF_BAR + 56);  // chunks kept after the cull
+    float* s_tbox = reinterpret_cast<float*>(sm + kN_OFF_BAR + 64);   // [4 warps][6], then tile box [6]
+    int* s_wcnt = reinterpret_cast<int*>(sm + kN_OFF_BAR + 192);      // [16] kept per warp
     NearPair* pairs = reinterpret_cast<NearPair*>(sm + kN_OFF_PAIR);
+    int* pref = reinterpret_cast<int*>(sm + kN_OFF_PREF);
+    int* list = reinterpret_cast<int*>(sm + kN_OFF_LIST);
     double* acc64 = reinterpret_cast<double*>(sm + kN_OFF_ACC);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -455,6 +459,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
         tc::mbar_init(&bar[3], 1);
         s_abort[0] = s_abort[1] = s_abort[2] = 0;
         int np = 0, nch = 0;
+        pref[0] = 0;
         for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
             const int cnt = a.pair_src_count[pr];
             if (cnt <= 0 || np >= kNearTcMaxPairs) continue;
@@ -463,14 +468,16 @@ __global__ void __launch_bounds__(kNThreads, 1)
             q.start = a.pair_src_start[pr];
             q.count = cnt;
             q.nch = (cnt + kNKC - 1) / kNKC;
+            q.cb = a.pair_chunk_base[pr];
             q.d2max = (float)(b * b);
             q.rsc = (float)(2.0 / b);
             q.cen = (float)(-0.5 * b);
             pairs[np++] = q;
             nch += q.nch;
+            pref[np] = nch;
         }
         *s_np = np;
-        *s_nch = nch;
+        *s_nch = min(nch, kNearTcMaxChunks);
         tc::fence_mbar_init();
     }
     for (int i = tid; i < 64 * 128; i += kNThreads) acc64[i] = 0.0;
@@ -480,6 +487,23 @@ __global__ void __launch_bounds__(kNThreads, 1)
     const bool tval = m0 + am < nt;
     const float4 th = tval ? trg_hi[t0 + m0 + am] : make_float4(1e30f, 1e30f, 1e30f, 0.0f);
     const float4 tl = tval ? trg_lo[t0 + m0 + am] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // bounding box of the tile's targets (warps 0-3 hold all 128 rows)
+    if (warp < 4) {
+        float lo[3] = {tval ? th.x : 3e38f, tval ? th.y : 3e38f, tval ? th.z : 3e38f};
+        float hi[3] = {tval ? th.x : -3e38f, tval ? th.y : -3e38f, tval ? th.z : -3e38f};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+            }
+        if (lane == 0)
+            for (int d = 0; d < 3; ++d) {
+                s_tbox[warp * 6 + d] = lo[d];
+                s_tbox[warp * 6 + 3 + d] = hi[d];
+            }
+    }
     float cf[NC];
 #pragma unroll
     for (int i = 0; i < NC; ++i) cf[i] = (float)a.coef[i];
@@ -494,32 +518,81 @@ __global__ void __launch_bounds__(kNThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *s_tmem;
-    const int nchunks = *s_nch;
-
-    auto advance = [&](ChunkCur c) {
-        if (++c.j >= pairs[c.p].nch) {
-            c.j = 0;
-            ++c.p;
+    const int np = *s_np, ncand = *s_nch;
+    if (tid == 0) {
+        for (int d = 0; d < 3; ++d) {
+            float lo = s_tbox[d], hi = s_tbox[3 + d];
+            for (int w = 1; w < 4; ++w) {
+                lo = fminf(lo, s_tbox[w * 6 + d]);
+                hi = fmaxf(hi, s_tbox[w * 6 + 3 + d]);
+            }
+            // widen by the FP32 rounding of hi-part coordinates (relative 2^-23)
+            const float pad = 2.5e-7f * fmaxf(fabsf(lo), fabsf(hi)) + 1e-30f;
+            s_tbox[24 + d] = lo - pad;
+            s_tbox[27 + d] = hi + pad;
         }
-        return c;
+        *s_kept = 0;
+    }
+    __syncthreads();
+    // keep the chunks whose bounding box comes within b of the tile (order preserved)
+    {
+        const float tlo[3] = {s_tbox[24], s_tbox[25], s_tbox[26]};
+        const float thi[3] = {s_tbox[27], s_tbox[28], s_tbox[29]};
+        for (int base = 0; base < ncand; base += kNThreads) {
+            const int c = base + tid;
+            bool keep = false;
+            int code = 0;
+            if (c < ncand) {
+                int lo = 0, hi = np - 1;  // pair p with pref[p] <= c < pref[p + 1]
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (pref[mid] <= c) lo = mid; else hi = mid - 1;
+                }
+                const int j = c - pref[lo];
+                const NearPair& q = pairs[lo];
+                const float4 clo = __ldg(a.chunk_lo + q.cb + j), chi = __ldg(a.chunk_hi + q.cb + j);
+                const float gx = fmaxf(0.0f, fmaxf(clo.x - thi[0], tlo[0] - chi.x));
+                const float gy = fmaxf(0.0f, fmaxf(clo.y - thi[1], tlo[1] - chi.y));
+                const float gz = fmaxf(0.0f, fmaxf(clo.z - thi[2], tlo[2] - chi.z));
+                keep = fmaf(gx, gx, fmaf(gy, gy, gz * gz)) <= q.d2max * 1.00001f;
+                code = (lo << 16) | j;
+            }
+            const unsigned ball = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) s_wcnt[warp] = __popc(ball);
+            __syncthreads();
+            int off = *s_kept;
+            for (int w = 0; w < warp; ++w) off += s_wcnt[w];
+            if (keep) list[off + __popc(ball & ((1u << lane) - 1u))] = code;
+            __syncthreads();
+            if (tid == 0) {
+                int tot = 0;
+                for (int w = 0; w < kNThreads / 32; ++w) tot += s_wcnt[w];
+                *s_kept += tot;
+            }
+            __syncthreads();
+        }
+    }
+    const int nchunks = *s_kept;
+
+    auto chunk_src = [&](int q, int& p, int& g0, int& n) {
+        const int v = list[q];
+        p = v >> 16;
+        const int j = v & 0xFFFF;
+        g0 = pairs[p].start + j * kNKC;
+        n = min(kNKC, pairs[p].count - j * kNKC);
     };
-    auto chunk_src = [&](ChunkCur c, int& g0, int& n) {
-        const NearPair& q = pairs[c.p];
-        g0 = q.start + c.j * kNKC;
-        n = min(kNKC, q.count - c.j * kNKC);
-    };
-    auto load_q = [&](ChunkCur c, float (&qv)[4]) {
-        int g0, n;
-        chunk_src(c, g0, n);
+    auto load_q = [&](int q, float (&qv)[4]) {
+        int p, g0, n;
+        chunk_src(q, p, g0, n);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int s = bsg * 4 + u;
             qv[u] = (s < n && bc < kb) ? __ldg(src_q + (int64_t)(g0 + s) * kb + bc) : 0.0f;
         }
     };
-    auto load_pos = [&](ChunkCur c) -> float4 {
-        int g0, n;
-        chunk_src(c, g0, n);
+    auto load_pos = [&](int q) -> float4 {
+        int p, g0, n;
+        chunk_src(q, p, g0, n);
         if (ps_ >= n) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return plo ? __ldg(src_lo + g0 + ps_) : __ldg(src_hi + g0 + ps_);
     };
@@ -550,34 +623,29 @@ __global__ void __launch_bounds__(kNThreads, 1)
 
     float qcur[4], qnext[4];
     float4 pnext = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    ChunkCur c0 = {0, 0}, c1 = c0, c2 = c0;
     if (nchunks > 0) {
-        load_q(c0, qcur);
-        if (prole) store_pos(0, load_pos(c0));
-        if (nchunks > 1) {
-            c1 = advance(c0);
-            if (prole) pnext = load_pos(c1);
-        }
-        if (nchunks > 2) c2 = advance(c1);
+        load_q(0, qcur);
+        if (prole) store_pos(0, load_pos(0));
+        if (nchunks > 1 && prole) pnext = load_pos(1);
     }
     __syncthreads();
 
-    // The accumulator is drained every kNSeg chunks (and at each box end): the
-    // tensor-core FP32 accumulation loses low bits on every MMA step, so each
-    // segment stays short and the sums continue in FP64 on the CUDA cores.
-    int issued = 0, seg = -1;
+    // The accumulator is drained every kNSeg chunks: the tensor-core FP32
+    // accumulation loses low bits on every MMA step, so each segment stays
+    // short and the sums continue in FP64 on the CUDA cores.
+    int issued = 0;
     for (int q = 0; q < nchunks; ++q) {
         const int st = q & 1;
-        const int b = c0.p;
-        const NearPair pr = pairs[b];
-        const bool first = c0.j % kNSeg == 0, last = c0.j % kNSeg == kNSeg - 1 || c0.j == pr.nch - 1;
-        if (first) ++seg;
-        const int nv = min(kNKC, pr.count - c0.j * kNKC);
+        const int seg = q / kNSeg;
+        const bool first = q % kNSeg == 0, last = q % kNSeg == kNSeg - 1 || q == nchunks - 1;
+        int pidx, g0c, nv;
+        chunk_src(q, pidx, g0c, nv);
+        const NearPair pr = pairs[pidx];
         if (q + 1 < nchunks) {
-            load_q(c1, qnext);
+            load_q(q + 1, qnext);
             if (prole) {
                 store_pos(st ^ 1, pnext);
-                if (q + 2 < nchunks) pnext = load_pos(c2);
+                if (q + 2 < nchunks) pnext = load_pos(q + 2);
             }
         }
         if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1)) s_abort[st] = 1;
@@ -654,13 +722,10 @@ __global__ void __launch_bounds__(kNThreads, 1)
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) qcur[u] = qnext[u];
-        c0 = c1;
-        c1 = c2;
-        if (q + 3 < nchunks) c2 = advance(c2);
     }
     bool ok = s_abort[0] == 0 && s_abort[1] == 0;
     if (ok && issued > 0) {
-        if (!drain(seg)) s_abort[2] = 1;
+        if (!drain((issued - 1) / kNSeg)) s_abort[2] = 1;
     } else if (!ok && issued > 0) {
         const int ql = issued - 1;
         tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1);

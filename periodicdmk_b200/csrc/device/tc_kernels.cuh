@@ -23,8 +23,9 @@ bool launch_c2proxy_tc(const C2ProxyArgs& a, const float* src_q, float* proxy_up
 // generated from double-float coordinates in FP32 on the CUDA cores, the
 // products run on the tensor cores (TF32 hi/lo split) into a tensor-memory
 // accumulator per source box, and each box's sum is added to FP64
-// accumulators.  Covers nc in {5, 6, 9, 11, 12}, 1 <= kb <= 64 and leaves with
-// at most 128 source boxes.
+// accumulators.  Chunks whose bounding box lies farther than b from the
+// tile's targets are skipped.  Covers nc in {5, 6, 9, 11, 12}, 1 <= kb <= 64 and
+// leaves with at most 128 source boxes and 4096 chunks.
 struct NearTc {
     const int* trg_start;
     const int* trg_count;
@@ -32,6 +33,11 @@ struct NearTc {
     const int* pair_src_start;
     const int* pair_src_count;
     const double* pair_bsize;
+    // bounding boxes of the 32-source chunks of each pair's source range:
+    // chunk j of pair pr is entry pair_chunk_base[pr] + j (float, rounded outwards)
+    const int* pair_chunk_base;
+    const float4* chunk_lo;
+    const float4* chunk_hi;
     double coef[32];
     int n_leaves;
     int max_trg;  // largest trg_count (grid extent over 128-target tiles)
@@ -39,6 +45,8 @@ struct NearTc {
     int kb;
 };
 constexpr int kNearTcMaxPairs = 128;
+constexpr int kNearTcChunk = 32;        // sources per chunk
+constexpr int kNearTcMaxChunks = 4096;  // chunks of one leaf's pairs (before the bounding-box cull)
 bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4* trg_lo, const float4* src_hi,
                     const float4* src_lo, const float* src_q, double* pot, int* err, cudaStream_t s);
 
