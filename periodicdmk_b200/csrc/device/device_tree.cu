@@ -520,6 +520,9 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         near_pair_chunk_base_ = upload(pcb);
         near_chunk_lo_ = upload(clo);
         near_chunk_hi_ = upload(chi);
+        near_.pair_chunk_base = near_pair_chunk_base_;
+        near_.chunk_lo = near_chunk_lo_;
+        near_.chunk_hi = near_chunk_hi_;
         near_.trg = trg_;
         near_.src = src_;
         near_.pot = pot_sorted_;

@@ -294,31 +294,67 @@ void launch_eval(const EvalArgs& a, int p, cudaStream_t s) {
 // ============================================================================
 template <int NC>
 __global__ void __launch_bounds__(128) k_near(NearArgs a) {
-    constexpr int TPT = 4;
-    __shared__ double4 ss[128];
+    // 2 targets per thread (256 per pass); sources in chunks of 32, each chunk
+    // skipped when its bounding box lies farther than b from every target of
+    // the pass (the points inside a leaf follow a Morton curve, so chunks are
+    // compact)
+    constexpr int TPT = 2, CH = 32;
+    __shared__ double4 ss[CH];
+    __shared__ double sbox[4][6];
     const int e = blockIdx.x;
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double c[NC];
 #pragma unroll
     for (int i = 0; i < NC; ++i) c[i] = a.coef[i];
     for (int base = 0; base < nt; base += TPT * 128) {
         double4 tp[TPT];
         double acc[TPT];
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
 #pragma unroll
         for (int u = 0; u < TPT; ++u) {
             const int t = base + threadIdx.x + u * 128;
             tp[u] = t < nt ? a.trg[t0 + t] : make_double4(1e300, 1e300, 1e300, 0.0);
             acc[u] = 0.0;
+            if (t < nt) {
+                lo[0] = fmin(lo[0], tp[u].x); hi[0] = fmax(hi[0], tp[u].x);
+                lo[1] = fmin(lo[1], tp[u].y); hi[1] = fmax(hi[1], tp[u].y);
+                lo[2] = fmin(lo[2], tp[u].z); hi[2] = fmax(hi[2], tp[u].z);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+            }
+        __syncthreads();
+        if (lane == 0)
+            for (int d = 0; d < 3; ++d) {
+                sbox[warp][d] = lo[d];
+                sbox[warp][3 + d] = hi[d];
+            }
+        __syncthreads();
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = fmin(fmin(sbox[0][d], sbox[1][d]), fmin(sbox[2][d], sbox[3][d]));
+            hi[d] = fmax(fmax(sbox[0][3 + d], sbox[1][3 + d]), fmax(sbox[2][3 + d], sbox[3][3 + d]));
         }
         for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
             const int s0 = a.pair_src_start[pr], ns = a.pair_src_count[pr];
             const double b = a.pair_bsize[pr];
             const double d2max = b * b, rsc = 2.0 / b, cen = -0.5 * b;
-            for (int sb = 0; sb < ns; sb += 128) {
+            const int cb = a.pair_chunk_base[pr];
+            for (int sb = 0; sb < ns; sb += CH) {
+                const float4 clo = __ldg(a.chunk_lo + cb + sb / CH), chi = __ldg(a.chunk_hi + cb + sb / CH);
+                const double gx = fmax(0.0, fmax((double)clo.x - hi[0], lo[0] - (double)chi.x));
+                const double gy = fmax(0.0, fmax((double)clo.y - hi[1], lo[1] - (double)chi.y));
+                const double gz = fmax(0.0, fmax((double)clo.z - hi[2], lo[2] - (double)chi.z));
+                if (fma(gx, gx, fma(gy, gy, gz * gz)) > d2max * (1.0 + 1e-12)) continue;  // uniform over the CTA
                 __syncthreads();
-                if (sb + (int)threadIdx.x < ns) ss[threadIdx.x] = a.src[s0 + sb + threadIdx.x];
+                if ((int)threadIdx.x < CH && sb + (int)threadIdx.x < ns) ss[threadIdx.x] = a.src[s0 + sb + threadIdx.x];
                 __syncthreads();
-                const int m = min(128, ns - sb);
+                const int m = min(CH, ns - sb);
                 for (int j = 0; j < m; ++j) {
                     const double4 y = ss[j];
 #pragma unroll

@@ -85,6 +85,11 @@ struct NearArgs {
     const int* pair_src_start;
     const int* pair_src_count;
     const double* pair_bsize;
+    // bounding boxes (float, rounded outwards) of the 32-source chunks of each
+    // pair's source range: chunk j of pair pr is entry pair_chunk_base[pr] + j
+    const int* pair_chunk_base;
+    const float4* chunk_lo;
+    const float4* chunk_hi;
     double coef[32];
     int nc;
 };
