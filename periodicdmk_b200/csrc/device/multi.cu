@@ -264,25 +264,47 @@ void launch_contract_m(const ContractM& a, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // plane-wave shift: grid (boxes in chunk, mode chunks, rhs)
 // ---------------------------------------------------------------------------
-template <typename T>
+// Each thread forms mode m of RB consecutive RHS: the box's (slot, stencil)
+// terms sit in shared memory, every term's multiplier is read once for the RB
+// RHS, and the RB plane-wave loads of a term are independent.
+template <typename T, int RB>
 __global__ void __launch_bounds__(256) k_shift_m(const typename Cplx<T>::type* __restrict__ pw_out,
                                                  const T* __restrict__ shift, typename Cplx<T>::type* __restrict__ pw_in,
                                                  int M, const int* __restrict__ term_start,
                                                  const int* __restrict__ term_slot, const int* __restrict__ term_stencil,
                                                  int kb, int e0) {
     using C = typename Cplx<T>::type;
-    const int e = blockIdx.x, c = blockIdx.z;
+    constexpr int kMaxTerms = 32;  // self + 26 colleagues
+    __shared__ int s_slot[kMaxTerms], s_st[kMaxTerms];
+    const int e = blockIdx.x, c0 = blockIdx.z * RB;
+    const int tb = term_start[e0 + e];
+    const int nterm = min(kMaxTerms, term_start[e0 + e + 1] - tb);
+    if ((int)threadIdx.x < nterm) {
+        s_slot[threadIdx.x] = term_slot[tb + threadIdx.x];
+        s_st[threadIdx.x] = term_stencil[tb + threadIdx.x];
+    }
+    __syncthreads();
     const int m = blockIdx.y * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    T ar = T(0), ai = T(0);
-    for (int t = term_start[e0 + e]; t < term_start[e0 + e + 1]; ++t) {
-        const C v = pw_out[((int64_t)term_slot[t] * kb + c) * M + m];
-        const T* sh = shift + (int64_t)term_stencil[t] * 2 * M;
+    T ar[RB], ai[RB];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) ar[r] = ai[r] = T(0);
+    for (int t = 0; t < nterm; ++t) {
+        const T* sh = shift + (int64_t)s_st[t] * 2 * M;
         const T sr = sh[m], si = sh[M + m];
-        ar = fma(v.x, sr, fma(-v.y, si, ar));
-        ai = fma(v.x, si, fma(v.y, sr, ai));
+        const C* src = pw_out + ((int64_t)s_slot[t] * kb + c0) * M + m;
+        C v[RB];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) v[r] = (c0 + r < kb) ? src[(int64_t)r * M] : C{T(0), T(0)};
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            ar[r] = fma(v[r].x, sr, fma(-v[r].y, si, ar[r]));
+            ai[r] = fma(v[r].x, si, fma(v[r].y, sr, ai[r]));
+        }
     }
-    pw_in[((int64_t)e * kb + c) * M + m] = C{ar, ai};
+#pragma unroll
+    for (int r = 0; r < RB; ++r)
+        if (c0 + r < kb) pw_in[((int64_t)e * kb + c0 + r) * M + m] = C{ar[r], ai[r]};
 }
 
 // ---------------------------------------------------------------------------
@@ -1025,8 +1047,8 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         for (int b0 = 0; b0 < E.n; b0 += Cb) {
             const int nb = std::min(Cb, E.n - b0);
             {
-                const dim3 grid(nb, (M + 255) / 256, kb);
-                dev::k_shift_m<T><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
+                const dim3 grid(nb, (M + 255) / 256, (kb + 3) / 4);
+                dev::k_shift_m<T, 4><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
                                                        static_cast<C*>(m.pw_in), M, E.term_start, E.term_slot,
                                                        E.term_stencil, kb, b0); ++nl;
             }

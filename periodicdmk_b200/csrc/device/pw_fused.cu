@@ -112,6 +112,11 @@ struct PwShape {
     static constexpr size_t IN_A = sizeof(C) * P * N * N2;
     static constexpr size_t IN_B = sizeof(C) * P * P * N2;
     static constexpr size_t IN_SMEM = IN_A + IN_B;
+    // staged incoming: R1 holds the input (n, n, n2), then (p, p, n2); R2 holds
+    // (p, n, n2), then the real (p, p, p) result
+    static constexpr size_t IN_R1 = sizeof(C) * N * N * N2;
+    static constexpr size_t IN_STAGED_SMEM = IN_R1 + IN_A;
+    static constexpr bool IN_STAGED = IN_STAGED_SMEM <= 227 * 1024;
 };
 
 template <typename T, int P, int N, int N2>
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(256) k_pw_out_fused(PwFused a) {
 }
 
 template <typename T, int P, int N, int N2>
-__global__ void __launch_bounds__(256) k_pw_in_fused(PwFused a) {
+__global__ void __launch_bounds__(512) k_pw_in_fused(PwFused a) {
     using C = typename CplxOf<T>::type;
     using S = PwShape<T, P, N, N2>;
     extern __shared__ __align__(16) unsigned char smem_pw[];
@@ -155,6 +160,23 @@ __global__ void __launch_bounds__(256) k_pw_in_fused(PwFused a) {
     T* out = reinterpret_cast<T*>(a.out) + a.out_off[eb] * rhs + ec * (int64_t)(P * P * P);
     const C* Uxy = reinterpret_cast<const C*>(a.mat_a);
     const C* Uz = reinterpret_cast<const C*>(a.mat_b);
+    if constexpr (S::IN_STAGED) {
+        // stage the input: every element of it is read by all the tasks of one output row
+        unsigned char* r1 = smem_pw;
+        unsigned char* r2 = smem_pw + S::IN_R1;
+        C* s1 = reinterpret_cast<C*>(r1);  // element copies: entries need not be 16-byte aligned
+        for (int i = threadIdx.x; i < N * N * N2; i += blockDim.x) s1[i] = in[i];
+        __syncthreads();
+        sep_step<N, N, N2, 0, P, 0, false, C, T>(reinterpret_cast<const C*>(r1), reinterpret_cast<C*>(r2), Uxy, T(1));
+        __syncthreads();
+        sep_step<P, N, N2, 1, P, 0, false, C, T>(reinterpret_cast<const C*>(r2), reinterpret_cast<C*>(r1), Uxy, T(1));
+        __syncthreads();
+        T* res = reinterpret_cast<T*>(r2);
+        sep_step<P, P, N2, 2, P, 1, false, C, T>(reinterpret_cast<const C*>(r1), res, Uz, T(2));
+        __syncthreads();
+        for (int i = threadIdx.x; i < P * P * P; i += blockDim.x) out[i] += res[i];
+        return;
+    }
     // (n,n,n2) from global -> (p,n,n2): contract x
     sep_step<N, N, N2, 0, P, 0, false, C, T>(in, reinterpret_cast<C*>(bufA), Uxy, T(1));
     __syncthreads();
@@ -190,12 +212,13 @@ void launch_in_pnn(const PwFused& a, int n_entries, cudaStream_t s) {
     int dev = 0;
     PDMK_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+    constexpr size_t smem = S::IN_STAGED ? S::IN_STAGED_SMEM : S::IN_SMEM;
     if (!configured[dev]) {
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_pw_in_fused<T, P, N, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)S::IN_SMEM));
+                                             (int)smem));
         configured[dev] = true;
     }
-    k_pw_in_fused<T, P, N, N2><<<n_entries, 256, S::IN_SMEM, s>>>(a);
+    k_pw_in_fused<T, P, N, N2><<<n_entries, S::IN_STAGED ? 512 : 256, smem, s>>>(a);
 }
 
 constexpr size_t kMaxSmem = 227 * 1024;
