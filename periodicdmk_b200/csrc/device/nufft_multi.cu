@@ -174,7 +174,13 @@ __global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __r
 template <int W>
 void spread_w(const NufftArgs& a, const double* esw, int max_jk, int max_ex, int nrhs, cudaStream_t s) {
     const int yb = (max_jk + 127) / 128;
-    if (max_ex <= 16) {
+    if (max_ex <= 12) {
+        if (nrhs % 4 == 0) {
+            k_spread_m<W, 12, 4><<<dim3(a.n_leaves, yb, nrhs / 4), 128, 0, s>>>(a, esw);
+            return;
+        }
+        k_spread_m<W, 12, 1><<<dim3(a.n_leaves, yb, nrhs), 128, 0, s>>>(a, esw);
+    } else if (max_ex <= 16) {
         if (nrhs % 4 == 0) {
             k_spread_m<W, 16, 4><<<dim3(a.n_leaves, yb, nrhs / 4), 128, 0, s>>>(a, esw);
             return;
