@@ -258,8 +258,6 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         }
     }
 
-    int64_t scratch_need = 0, pw_in_need = 0;
-
     // ------------------------------------------------------------------ upward: proxy moments
     {
         std::vector<std::vector<int>> by_center(P.nboxes);
@@ -311,8 +309,6 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             g.out_off = upload(out);
             g.child = c;
             c2p_groups_.push_back(g);
-            scratch_need = std::max<int64_t>(scratch_need, (int64_t)g.n * ncoef);
-            launches_ += dev::sep3_supported<double>(p) ? 1 : 3;
         }
     }
     // ------------------------------------------------------------------ outgoing plane waves
@@ -331,8 +327,6 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         g.in_off = upload(in);
         g.out_off = upload(out);
         pw_groups_.push_back(g);
-        scratch_need = std::max<int64_t>(scratch_need, (int64_t)g.n * std::max<int64_t>((int64_t)p * p * n, (int64_t)p * n * n));
-        launches_ += dev::pw_fused_supported<double>(p, n, n2) ? 1 : 3;
     }
     // ------------------------------------------------------------------ downward per level
     for (int l = 0; l < P.nlevels; ++l) {
@@ -387,11 +381,6 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             E.p2c_mat = upload(pmat);
         }
         eval_levels_.push_back(E);
-        pw_in_need = std::max<int64_t>(pw_in_need, (int64_t)E.n * M);
-        scratch_need = std::max<int64_t>(scratch_need, (int64_t)E.n * std::max<int64_t>((int64_t)n * n2 * p, (int64_t)n2 * p * p));
-        scratch_need = std::max<int64_t>(scratch_need, (int64_t)E.n_p2c * ncoef);
-        launches_ += 1 + (dev::pw_fused_supported<double>(p, n, n2) ? 1 : 3) +
-                     (E.n_p2c ? (dev::sep3_supported<double>(p) ? 1 : 3) : 0);
     }
     // ------------------------------------------------------------------ leaf evaluation
     {
@@ -406,7 +395,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / P.boxsize[P.depth[b]]));
         }
         eval_.trg = trg_;
-        eval_.proxy_down = proxy_down_;
+        eval_.proxy_down = nullptr;  // the multi-RHS path passes its own coefficients
         eval_.pot = pot_sorted_;
         eval_.n_leaves = (int)slot.size();
         for (int c : tc) eval_max_trg_ = std::max(eval_max_trg_, c);
@@ -414,7 +403,115 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         eval_.trg_start = upload(t0);
         eval_.trg_count = upload(tc);
         eval_.center_scale = upload(cs);
-        launches_ += 1;
+    }
+    // ------------------------------------------------------------------ FP64 single-RHS pass by level
+    // Same boxes and translations as the lists above, renumbered so that each
+    // level's plane waves and downward coefficients live in level-sized
+    // buffers.  The reference runs the downward pass in the same level order
+    // (form_eval_expansions per level, cpp/src/dmk/pbc_tree.cpp:1705-1709; its
+    // body, :1253-1430, shifts, converts to proxy coefficients, translates to
+    // the children and evaluates the leaves of one level).
+    {
+        std::vector<int64_t> loc_down(P.nboxes, -1), loc_pw(P.nboxes, -1);
+        f64_levels_.resize(P.nlevels);
+        for (int l = 0; l < P.nlevels; ++l) {
+            int64_t nd = 0, np = 0;
+            for (int b : P.level_boxes[l]) {
+                check(P.depth[b] == l, "level box depth");
+                if (P.proxy_down_off[b] >= 0) loc_down[b] = nd++;
+                if (P.pw_off[b] >= 0) loc_pw[b] = np++;
+            }
+            f64_levels_[l].level = l;
+            f64_levels_[l].n_down = nd;
+            down_level_boxes_[l & 1] = std::max(down_level_boxes_[l & 1], nd);
+            pw_level_boxes_ = std::max(pw_level_boxes_, np);
+        }
+        for (int l = 0; l < P.nlevels; ++l) {
+            Fp64Level& F = f64_levels_[l];
+            const double bs = P.boxsize[l];
+            std::vector<int64_t> pin, pout;
+            for (int b : P.level_boxes[l]) {
+                if (P.pw_off[b] < 0) continue;
+                check(P.proxy_up_off[b] >= 0, "pw box without proxy");
+                pin.push_back(P.proxy_up_off[b]);
+                pout.push_back(loc_pw[b] * M);
+            }
+            F.n_pw = (int)pin.size();
+            if (F.n_pw) {
+                F.pw_in_off = upload(pin);
+                F.pw_out_off = upload(pout);
+            }
+            std::vector<int> ts{0}, tslot, tst;
+            std::vector<int64_t> down, cin, cout, cmat;
+            std::vector<int> slot, t0, tc;
+            std::vector<double4> cs;
+            for (int b : P.level_boxes[l]) {
+                if (P.iftensprodeval[b] && P.trg_count[b] > 0) {
+                    check(loc_down[b] >= 0, "leaf proxy_down");
+                    slot.push_back((int)loc_down[b]);
+                    t0.push_back(P.trg_start[b]);
+                    tc.push_back(P.trg_count[b]);
+                    cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / bs));
+                }
+                if (!(P.ifpwexp[b] && P.src_count[b] + P.trg_count[b] > 0 && P.trg_count[b] > 0)) continue;
+                check(loc_pw[b] >= 0 && loc_down[b] >= 0, "form-eval box storage");
+                tslot.push_back((int)loc_pw[b]);
+                tst.push_back(13);
+                for (int ind = 0; ind < 27; ++ind) {
+                    const int nb = P.colleagues[b][ind];
+                    if (nb < 0 || nb == b) continue;
+                    if (P.is_leaf[b] && P.is_leaf[nb]) continue;
+                    if (P.pw_off[nb] < 0) continue;
+                    check(P.depth[nb] == l, "colleague level");
+                    int st = 0, stride = 1;
+                    for (int d = 0; d < 3; ++d) {
+                        const int kd = (int)std::lround((P.centers[3 * b + d] - P.centers[3 * nb + d]) / bs) + 1;
+                        check(kd >= 0 && kd <= 2, "shift stencil");
+                        st += kd * stride;
+                        stride *= 3;
+                    }
+                    tslot.push_back((int)loc_pw[nb]);
+                    tst.push_back(st);
+                }
+                ts.push_back((int)tslot.size());
+                down.push_back(loc_down[b] * ncoef);
+                if (!P.iftensprodeval[b]) {
+                    for (int c = 0; c < 8; ++c) {
+                        const int ch = P.children[b][c];
+                        if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch])) continue;
+                        check(loc_down[ch] >= 0 && P.depth[ch] == l + 1 && l + 1 < P.nlevels, "p2c child storage");
+                        cin.push_back(loc_down[b] * ncoef);
+                        cout.push_back(loc_down[ch] * ncoef);
+                        cmat.push_back((int64_t)c * 3 * p * p);
+                    }
+                }
+            }
+            F.n_in = (int)down.size();
+            if (F.n_in) {
+                F.term_start = upload(ts);
+                F.term_slot = upload(tslot);
+                F.term_stencil = upload(tst);
+                F.down_off = upload(down);
+            }
+            F.n_p2c = (int)cin.size();
+            if (F.n_p2c) {
+                F.p2c_in = upload(cin);
+                F.p2c_out = upload(cout);
+                F.p2c_mat = upload(cmat);
+            }
+            F.eval.trg = trg_;
+            F.eval.pot = pot_sorted_;
+            F.eval.n_leaves = (int)slot.size();
+            if (F.eval.n_leaves) {
+                F.eval.slot = upload(slot);
+                F.eval.trg_start = upload(t0);
+                F.eval.trg_count = upload(tc);
+                F.eval.center_scale = upload(cs);
+            }
+        }
+        int64_t leaves = 0;
+        for (const auto& F : f64_levels_) leaves += F.eval.n_leaves;
+        check(leaves == eval_.n_leaves, "leaf evaluation lists by level");
     }
     // ------------------------------------------------------------------ near field
     {
@@ -539,9 +636,32 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         launches_ += 1;
     }
 
-    // ------------------------------------------------------------------ scratch
-    scratch_elems_ = std::max<int64_t>(scratch_need, 1);
-    pw_in_elems_ = std::max<int64_t>(pw_in_need, 1);
+    // ------------------------------------------------------------------ FP64 transform scratch
+    // Enough for the largest level in one chunk, capped at PDMK_FP64_SCRATCH_MB
+    // (default 1024 MiB); larger levels run in chunks of boxes.
+    {
+        int64_t budget_mb = 1024;
+        if (const char* e = std::getenv("PDMK_FP64_SCRATCH_MB")) budget_mb = std::max<int64_t>(16, std::atoll(e));
+        const int64_t budget = (budget_mb << 20) / (int64_t)sizeof(cd);
+        int64_t want = 1;
+        for (const auto& F : f64_levels_) {
+            want = std::max(want, fp64_need_pw_out() * F.n_pw);
+            want = std::max(want, fp64_need_pw_in() * F.n_in);
+            want = std::max(want, fp64_need_c2p() * F.n_p2c);
+        }
+        for (const auto& g : c2p_groups_) want = std::max(want, fp64_need_c2p() * g.n);
+        f64_scratch_elems_ = std::min(want, std::max(budget, fp64_need_max()));
+        const Fp64Chunks C = fp64_chunks(f64_scratch_elems_);
+        const bool fc = dev::sep3_supported<double>(p), fpw = dev::pw_fused_supported<double>(p, n, n2);
+        auto nchunks = [](int64_t nb, int c) { return (int)((nb + c - 1) / c); };
+        for (const auto& g : c2p_groups_) launches_ += fc ? 1 : 3 * nchunks(g.n, C.c2p);
+        for (const auto& F : f64_levels_) {
+            if (F.n_pw) launches_ += fpw ? 1 : 3 * nchunks(F.n_pw, C.pw_out);
+            if (F.n_in) launches_ += (fpw ? 2 : 4) * nchunks(F.n_in, C.pw_in);
+            if (F.n_p2c) launches_ += fc ? 1 : 3 * nchunks(F.n_p2c, C.c2p);
+            if (F.eval.n_leaves) launches_ += 1;
+        }
+    }
     if (fp64_working_set) ensure_fp64_working_set();
 
     // ------------------------------------------------------------------ far field
@@ -645,13 +765,166 @@ void DeviceTree::ensure_fp64_working_set() {
     if (proxy_up_) return;
     const int64_t ncoef = (int64_t)p_ * p_ * p_;
     proxy_up_ = alloc<double>(n_up_ * ncoef);
-    proxy_down_ = alloc<double>(n_down_ * ncoef);
-    pw_out_ = alloc<cd>(n_pw_ * (int64_t)M_);
-    scratch1_ = alloc<cd>(scratch_elems_);
-    scratch2_ = alloc<cd>(scratch_elems_);
-    pw_in_ = alloc<cd>(pw_in_elems_);
+    down_level_[0] = alloc<double>(std::max<int64_t>(down_level_boxes_[0], 1) * ncoef);
+    down_level_[1] = alloc<double>(std::max<int64_t>(down_level_boxes_[1], 1) * ncoef);
+    pw_level_ = alloc<cd>(std::max<int64_t>(pw_level_boxes_, 1) * (int64_t)M_);
+    f64_scratch_ = alloc<cd>(f64_scratch_elems_);
     c2x_.proxy_up = proxy_up_;
-    eval_.proxy_down = proxy_down_;
+}
+
+int64_t DeviceTree::fp64_need_c2p() const {
+    const int64_t ncoef = (int64_t)p_ * p_ * p_;
+    return dev::sep3_supported<double>(p_) ? 0 : 2 * ((ncoef + 1) / 2);
+}
+int64_t DeviceTree::fp64_need_pw_out() const {
+    const int64_t p = p_, n = npw_;
+    return dev::pw_fused_supported<double>(p_, npw_, npw2_) ? 0 : p * p * n + p * n * n;
+}
+int64_t DeviceTree::fp64_need_pw_in() const {
+    const int64_t p = p_, n = npw_, n2 = npw2_;
+    return (int64_t)M_ + (dev::pw_fused_supported<double>(p_, npw_, npw2_) ? 0 : n * n2 * p + n2 * p * p);
+}
+int64_t DeviceTree::fp64_need_max() const {
+    return std::max({fp64_need_c2p(), fp64_need_pw_out(), fp64_need_pw_in()});
+}
+
+DeviceTree::Fp64Chunks DeviceTree::fp64_chunks(int64_t cap) const {
+    auto c = [cap](int64_t need) {
+        if (need <= 0) return (int)INT32_MAX;
+        return (int)std::min<int64_t>(INT32_MAX, std::max<int64_t>(1, cap / need));
+    };
+    Fp64Chunks r;
+    r.c2p = c(fp64_need_c2p());
+    r.pw_out = c(fp64_need_pw_out());
+    r.pw_in = c(fp64_need_pw_in());
+    return r;
+}
+
+int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStream_t s) {
+    const int p = p_, n = npw_, n2 = npw2_, M = M_;
+    const int64_t ncoef = (int64_t)p * p * p;
+    const int64_t ncoef_c = (ncoef + 1) / 2;  // a real (p,p,p) tensor in complex-sized slots
+    const bool fused_c2p = dev::sep3_supported<double>(p);
+    const bool fused_pw = dev::pw_fused_supported<double>(p, n, n2);
+    const Fp64Chunks C = fp64_chunks(cap);
+    int nl = 0;
+    PDMK_CUDA_CHECK(cudaMemsetAsync(proxy_up_, 0, sizeof(double) * std::max<int64_t>(n_up_ * ncoef, 1), s));
+    dev::launch_gather(src_, src_charge_idx_, q, n_all_, s);
+    dev::launch_c2proxy(c2x_, p, s);
+    nl += 2;
+    // child -> parent translation of real (p,p,p) tensors: one fused kernel, or
+    // three contractions through scratch in chunks of C.c2p translations
+    auto translate = [&](const double* in, const int64_t* in_off, double* out, const int64_t* out_off,
+                         const double* mat, const int64_t* mat_off, int count) {
+        if (fused_c2p) {
+            dev::Sep3 f{};
+            f.in = in; f.in_off = in_off; f.out = out; f.out_off = out_off; f.mat = mat; f.mat_off = mat_off;
+            f.rhs = 1; f.accumulate = 1;
+            dev::launch_sep3<double>(f, p, count, s);
+            ++nl;
+            return;
+        }
+        double* s1 = reinterpret_cast<double*>(scratch);
+        double* s2 = reinterpret_cast<double*>(scratch + (int64_t)std::min(C.c2p, count) * ncoef_c);
+        for (int c0 = 0; c0 < count; c0 += C.c2p) {
+            dev::ContractArgs a{};
+            a.n_entries = std::min(C.c2p, count - c0);
+            // x: in (i,j,k) -> s1 (j,k,a); y: s1 -> s2 (k,a,b); z: s2 -> out (a,b,c), accumulated
+            a.in = in; a.in_off = in_off + c0; a.out = s1; a.out_stride = ncoef;
+            a.mat = mat; a.mat_off = mat_off ? mat_off + c0 : nullptr; a.ni = p; a.na = p; a.R = p * p;
+            a.mode = dev::kStore;
+            dev::launch_contract(a, dev::kRRR, s);
+            a.in = s1; a.in_off = nullptr; a.in_stride = ncoef; a.out = s2; a.mat = mat + p * p;
+            dev::launch_contract(a, dev::kRRR, s);
+            a.in = s2; a.out = out; a.out_off = out_off + c0; a.mat = mat + 2 * p * p; a.mode = dev::kAdd;
+            dev::launch_contract(a, dev::kRRR, s);
+            nl += 3;
+        }
+    };
+    // upward
+    for (const auto& g : c2p_groups_)
+        translate(proxy_up_, g.in_off, proxy_up_, g.out_off, c2p_ + (int64_t)g.child * 3 * p * p, nullptr, g.n);
+    // downward, one level at a time
+    if (!f64_levels_.empty())
+        PDMK_CUDA_CHECK(cudaMemsetAsync(down_level_[0], 0, sizeof(double) * std::max<int64_t>(f64_levels_[0].n_down * ncoef, 1), s));
+    for (const auto& F : f64_levels_) {
+        const auto& L = lev_[F.level];
+        double* down = down_level_[F.level & 1];
+        // outgoing plane waves of this level
+        if (F.n_pw && fused_pw) {
+            dev::PwFused f{};
+            f.in = proxy_up_; f.in_off = F.pw_in_off; f.out = pw_level_; f.out_off = F.pw_out_off;
+            f.mat_a = L.poly2pw; f.mat_b = L.poly2pw_half; f.rhs = 1; f.e0 = 0;
+            dev::launch_pw_out_fused<double>(f, p, n, n2, F.n_pw, s);
+            ++nl;
+        } else if (F.n_pw) {
+            cd* s1 = scratch;
+            cd* s2 = scratch + (int64_t)std::min(C.pw_out, F.n_pw) * p * p * n;
+            for (int c0 = 0; c0 < F.n_pw; c0 += C.pw_out) {
+                dev::ContractArgs a{};
+                a.n_entries = std::min(C.pw_out, F.n_pw - c0);
+                a.in = proxy_up_; a.in_off = F.pw_in_off + c0; a.out = s1; a.out_stride = (int64_t)p * p * n;
+                a.mat = L.poly2pw; a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore;
+                dev::launch_contract(a, dev::kRCC, s);
+                a.in = s1; a.in_off = nullptr; a.in_stride = (int64_t)p * p * n; a.out = s2;
+                a.out_stride = (int64_t)p * n * n; a.R = p * n;
+                dev::launch_contract(a, dev::kCCC, s);
+                a.in = s2; a.in_stride = (int64_t)p * n * n; a.out = pw_level_; a.out_off = F.pw_out_off + c0;
+                a.mat = L.poly2pw_half; a.na = n2; a.R = n * n;
+                dev::launch_contract(a, dev::kCCC, s);
+                nl += 3;
+            }
+        }
+        // incoming: shift -> plane waves to proxy coefficients, in chunks of boxes
+        if (F.n_in) {
+            const int CI = C.pw_in;
+            const int cmax = std::min(CI, F.n_in);
+            cd* pin = scratch;
+            cd* s1 = pin + (int64_t)cmax * M;
+            cd* s2 = s1 + (int64_t)cmax * n * n2 * p;
+            for (int c0 = 0; c0 < F.n_in; c0 += CI) {
+                const int ne = std::min(CI, F.n_in - c0);
+                dev::ShiftArgs sa{pw_level_, L.shift, pin, M, ne, F.term_start + c0, F.term_slot, F.term_stencil};
+                dev::launch_shift(sa, s);
+                ++nl;
+                if (fused_pw) {
+                    dev::PwFused f{};
+                    f.in = pin; f.in_stride = M; f.out = down; f.out_off = F.down_off + c0;
+                    f.mat_a = L.pw2polyT; f.mat_b = L.pw2polyTw; f.rhs = 1; f.e0 = 0;
+                    dev::launch_pw_in_fused<double>(f, p, n, n2, ne, s);
+                    ++nl;
+                    continue;
+                }
+                dev::ContractArgs a{};
+                a.n_entries = ne;
+                a.in = pin; a.in_stride = M; a.out = s1; a.out_stride = (int64_t)n * n2 * p;
+                a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
+                dev::launch_contract(a, dev::kCCC, s);
+                a.in = s1; a.in_stride = (int64_t)n * n2 * p; a.out = s2; a.out_stride = (int64_t)n2 * p * p;
+                a.R = n2 * p;
+                dev::launch_contract(a, dev::kCCC, s);
+                a.in = s2; a.in_stride = (int64_t)n2 * p * p; a.out = down; a.out_off = F.down_off + c0;
+                a.mat = L.pw2polyTw; a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
+                dev::launch_contract(a, dev::kCCR, s);
+                nl += 3;
+            }
+        }
+        // leaves of this level
+        if (F.eval.n_leaves) {
+            dev::EvalArgs e = F.eval;
+            e.proxy_down = down;
+            dev::launch_eval(e, p, s);
+            ++nl;
+        }
+        // parent -> child into the next level's buffer
+        if (F.level + 1 < (int)f64_levels_.size()) {
+            double* next = down_level_[(F.level + 1) & 1];
+            const int64_t nd = f64_levels_[F.level + 1].n_down;
+            PDMK_CUDA_CHECK(cudaMemsetAsync(next, 0, sizeof(double) * std::max<int64_t>(nd * ncoef, 1), s));
+            if (F.n_p2c) translate(down, F.p2c_in, next, F.p2c_out, p2c_, F.p2c_mat, F.n_p2c);
+        }
+    }
+    return nl;
 }
 
 void DeviceTree::release() {
@@ -678,106 +951,10 @@ void DeviceTree::release() {
 
 void DeviceTree::run(const double* q, double* pot) {
     ensure_fp64_working_set();
-    const int p = p_, n = npw_, n2 = npw2_, M = M_;
-    const int64_t ncoef = (int64_t)p * p * p;
     cudaStream_t s = stream_;
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(pot_sorted_, 0, sizeof(double) * n_, s));
-    PDMK_CUDA_CHECK(cudaMemsetAsync(proxy_up_, 0, sizeof(double) * std::max<int64_t>(n_up_ * ncoef, 1), s));
-    PDMK_CUDA_CHECK(cudaMemsetAsync(proxy_down_, 0, sizeof(double) * std::max<int64_t>(n_down_ * ncoef, 1), s));
-    dev::launch_gather(src_, src_charge_idx_, q, n_all_, s);
-    // upward
-    dev::launch_c2proxy(c2x_, p, s);
-    // fused transforms (intermediates in shared memory) where the order allows
-    const bool fused_c2p = dev::sep3_supported<double>(p);
-    const bool fused_pw = dev::pw_fused_supported<double>(p, n, n2);
-    for (const auto& g : c2p_groups_) {
-        const double* mx = c2p_ + (int64_t)g.child * 3 * p * p;
-        if (fused_c2p) {
-            dev::Sep3 f{};
-            f.in = proxy_up_; f.in_off = g.in_off; f.out = proxy_up_; f.out_off = g.out_off; f.mat = mx;
-            f.rhs = 1; f.accumulate = 1;
-            dev::launch_sep3<double>(f, p, g.n, s);
-            continue;
-        }
-        dev::ContractArgs a{};
-        a.n_entries = g.n;
-        // x: in (i,j,k) -> s1 (j,k,a)
-        a.in = proxy_up_; a.in_off = g.in_off; a.out = scratch1_; a.out_stride = ncoef;
-        a.mat = mx; a.ni = p; a.na = p; a.R = p * p; a.mode = dev::kStore;
-        dev::launch_contract(a, dev::kRRR, s);
-        // y: s1 -> s2 (k,a,b)
-        a.in = scratch1_; a.in_off = nullptr; a.in_stride = ncoef; a.out = scratch2_;
-        a.mat = mx + p * p;
-        dev::launch_contract(a, dev::kRRR, s);
-        // z: s2 -> parent (a,b,c), accumulated
-        a.in = scratch2_; a.out = proxy_up_; a.out_off = g.out_off; a.mat = mx + 2 * p * p; a.mode = dev::kAdd;
-        dev::launch_contract(a, dev::kRRR, s);
-    }
-    // outgoing plane waves
-    for (const auto& g : pw_groups_) {
-        const auto& L = lev_[g.level];
-        if (fused_pw) {
-            dev::PwFused f{};
-            f.in = proxy_up_; f.in_off = g.in_off; f.out = pw_out_; f.out_off = g.out_off;
-            f.mat_a = L.poly2pw; f.mat_b = L.poly2pw_half; f.rhs = 1; f.e0 = 0;
-            dev::launch_pw_out_fused<double>(f, p, n, n2, g.n, s);
-            continue;
-        }
-        dev::ContractArgs a{};
-        a.n_entries = g.n;
-        a.in = proxy_up_; a.in_off = g.in_off; a.out = scratch1_; a.out_stride = (int64_t)p * p * n;
-        a.mat = L.poly2pw; a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore;
-        dev::launch_contract(a, dev::kRCC, s);
-        a.in = scratch1_; a.in_off = nullptr; a.in_stride = (int64_t)p * p * n; a.out = scratch2_;
-        a.out_stride = (int64_t)p * n * n; a.R = p * n;
-        dev::launch_contract(a, dev::kCCC, s);
-        a.in = scratch2_; a.in_stride = (int64_t)p * n * n; a.out = pw_out_; a.out_off = g.out_off;
-        a.mat = L.poly2pw_half; a.na = n2; a.R = n * n;
-        dev::launch_contract(a, dev::kCCC, s);
-    }
-    // downward: per level shift -> pw2proxy -> p2c
-    for (const auto& E : eval_levels_) {
-        const auto& L = lev_[E.level];
-        dev::ShiftArgs sa{pw_out_, L.shift, pw_in_, M, E.n, E.term_start, E.term_slot, E.term_stencil};
-        dev::launch_shift(sa, s);
-        if (fused_pw) {
-            dev::PwFused f{};
-            f.in = pw_in_; f.in_stride = M; f.out = proxy_down_; f.out_off = E.down_off;
-            f.mat_a = L.pw2polyT; f.mat_b = L.pw2polyTw; f.rhs = 1; f.e0 = 0;
-            dev::launch_pw_in_fused<double>(f, p, n, n2, E.n, s);
-        } else {
-            dev::ContractArgs a{};
-            a.n_entries = E.n;
-            a.in = pw_in_; a.in_stride = M; a.out = scratch1_; a.out_stride = (int64_t)n * n2 * p;
-            a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
-            dev::launch_contract(a, dev::kCCC, s);
-            a.in = scratch1_; a.in_stride = (int64_t)n * n2 * p; a.out = scratch2_; a.out_stride = (int64_t)n2 * p * p;
-            a.R = n2 * p;
-            dev::launch_contract(a, dev::kCCC, s);
-            a.in = scratch2_; a.in_stride = (int64_t)n2 * p * p; a.out = proxy_down_; a.out_off = E.down_off;
-            a.mat = L.pw2polyTw; a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
-            dev::launch_contract(a, dev::kCCR, s);
-        }
-        if (E.n_p2c && fused_c2p) {
-            dev::Sep3 f{};
-            f.in = proxy_down_; f.in_off = E.p2c_in; f.out = proxy_down_; f.out_off = E.p2c_out; f.mat = p2c_;
-            f.mat_off = E.p2c_mat; f.rhs = 1; f.accumulate = 1;
-            dev::launch_sep3<double>(f, p, E.n_p2c, s);
-        } else if (E.n_p2c) {
-            dev::ContractArgs b{};
-            b.n_entries = E.n_p2c;
-            b.in = proxy_down_; b.in_off = E.p2c_in; b.out = scratch1_; b.out_stride = ncoef;
-            b.mat = p2c_; b.mat_off = E.p2c_mat; b.ni = p; b.na = p; b.R = p * p; b.mode = dev::kStore;
-            dev::launch_contract(b, dev::kRRR, s);
-            b.in = scratch1_; b.in_off = nullptr; b.in_stride = ncoef; b.out = scratch2_;
-            b.mat = p2c_ + p * p;
-            dev::launch_contract(b, dev::kRRR, s);
-            b.in = scratch2_; b.out = proxy_down_; b.out_off = E.p2c_out; b.mat = p2c_ + 2 * p * p; b.mode = dev::kAdd;
-            dev::launch_contract(b, dev::kRRR, s);
-        }
-    }
-    dev::launch_eval(eval_, p, s);
+    run_fp64_tree(q, f64_scratch_, f64_scratch_elems_, s);
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
     dev::launch_near(near_, s);
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[2], s));

@@ -113,6 +113,21 @@ class DeviceTree {
     template <typename T>
     T* upload(const std::vector<T>& v);
     void run(const double* q_user_d, double* pot_user_d);
+    // Chunk sizes (boxes per launch) of the FP64 transforms for a scratch of cap complex elements.
+    struct Fp64Chunks {
+        int c2p = 1, pw_out = 1, pw_in = 1;
+    };
+    Fp64Chunks fp64_chunks(int64_t cap) const;
+    // Transform scratch per box (complex elements) of the child/parent
+    // translations, the outgoing and the incoming plane-wave transforms.
+    int64_t fp64_need_c2p() const;
+    int64_t fp64_need_pw_out() const;
+    int64_t fp64_need_pw_in() const;
+    int64_t fp64_need_max() const;
+    // Gather, proxy moments, upward pass and the level-by-level downward pass
+    // with leaf evaluation of the single-RHS FP64 path; transform scratch of
+    // cap complex elements.  Returns the number of kernels launched.
+    int run_fp64_tree(const double* q_user_d, dev::cd* scratch, int64_t cap, cudaStream_t s);
 
     int device_ = 0;
     int n_digits_ = 6;
@@ -142,8 +157,6 @@ class DeviceTree {
     double* pot_dev_ = nullptr;
     // expansions
     double* proxy_up_ = nullptr;
-    double* proxy_down_ = nullptr;
-    dev::cd* pw_out_ = nullptr;
     int64_t n_up_ = 0, n_down_ = 0, n_pw_ = 0;
     // tables
     double* c2p_ = nullptr;
@@ -185,11 +198,34 @@ class DeviceTree {
     std::vector<EvalLevel> eval_levels_;
     dev::EvalArgs eval_{};
     dev::NearArgs near_{};
-    // scratch for the separable transforms
-    dev::cd* scratch1_ = nullptr;
-    dev::cd* scratch2_ = nullptr;
-    dev::cd* pw_in_ = nullptr;
-    int64_t scratch_elems_ = 0, pw_in_elems_ = 0;
+    // Single-RHS FP64 path, one level at a time.  Besides proxy_up it holds the
+    // outgoing plane waves of one level, the downward proxy coefficients of two
+    // consecutive levels (ping-pong by level parity) and one transform scratch
+    // of bounded size; every offset below is local to its level's buffer.
+    struct Fp64Level {
+        int level = 0;
+        int64_t n_down = 0;             // boxes of this level with downward storage
+        int n_pw = 0;                   // outgoing expansions formed at this level
+        int64_t* pw_in_off = nullptr;   // proxy_up element offset
+        int64_t* pw_out_off = nullptr;  // element offset in the level's plane-wave buffer
+        int n_in = 0;                   // boxes that receive incoming expansions
+        int* term_start = nullptr;      // CSR over those boxes
+        int* term_slot = nullptr;       // plane-wave slot (units of M) in the level buffer
+        int* term_stencil = nullptr;
+        int64_t* down_off = nullptr;    // element offset in the level's proxy_down buffer
+        dev::EvalArgs eval{};           // leaves of this level (slot: level-local proxy_down slot)
+        int n_p2c = 0;                  // parent (this level) -> child (next level) translations
+        int64_t* p2c_in = nullptr;
+        int64_t* p2c_out = nullptr;
+        int64_t* p2c_mat = nullptr;
+    };
+    std::vector<Fp64Level> f64_levels_;
+    double* down_level_[2] = {nullptr, nullptr};  // proxy_down of even / odd levels
+    int64_t down_level_boxes_[2] = {0, 0};
+    dev::cd* pw_level_ = nullptr;                  // outgoing plane waves of the current level
+    int64_t pw_level_boxes_ = 0;
+    dev::cd* f64_scratch_ = nullptr;
+    int64_t f64_scratch_elems_ = 0;
     // far field
     dev::NufftArgs nufft_{};
     int nufft_max_jk_ = 0, nufft_max_ex_ = 0, nufft_max_cells_ = 0;

@@ -90,6 +90,25 @@ def test_repeatable_and_timed():
     t.close()
 
 
+@pytest.mark.parametrize("nd", [6, 12])
+def test_fp64_level_chunks_agree_with_one_chunk(nd, monkeypatch):
+    # The FP64 pass runs level by level with a bounded transform scratch
+    # (PDMK_FP64_SCRATCH_MB, read when the tree is built).  The smallest cap
+    # splits every level into chunks of a few boxes; chunking only changes
+    # which boxes share a launch, so the results agree to rounding (the far
+    # field's atomic spreading alone makes two runs differ in the last bits).
+    cell, pos, q = clustered_system(20000, 41, TRICLINIC, n_clusters=8, sigma=0.03)
+    ref_tree = _tree(cell, pos, nd, 40)
+    ref = ref_tree.evaluate(q)
+    ref_tree.close()
+    monkeypatch.setenv("PDMK_FP64_SCRATCH_MB", "16")
+    t = _tree(cell, pos, nd, 40)
+    assert rel_l2(t.evaluate(q), ref) < 1e-14
+    t.close()
+    if nd == 6:  # (the oracle takes about a minute at 12 digits on this size)
+        assert rel_l2(ref, oracle.evaluate(cell, pos, q, nd, 40, 4)) < 0.2 * 10.0 ** -nd
+
+
 def test_multi_rhs_equals_single_calls():
     (cell, pos, q), npl = SYSTEMS["cube_deep"]()
     rng = np.random.default_rng(5)
