@@ -220,9 +220,54 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     }
 
     // ------------------------------------------------------------------ expansions
-    n_up_ = P.n_proxy_up;
-    n_down_ = P.n_proxy_down;
-    n_pw_ = P.n_pw_exp;
+    // Storage only for expansions that some evaluation reads.  The plan (like
+    // the reference, cpp/src/dmk/pbc_tree.cpp:983-994 and its outgoing pass)
+    // gives every box with points an outgoing plane-wave expansion and
+    // downward coefficients; most of those boxes hold only lattice images and
+    // no target, and their expansions are never read.  Read are:
+    //   * plane waves of the boxes that receive incoming expansions (boxes
+    //     with targets) and of their colleagues in the shift lists;
+    //   * proxy_up of those boxes and of every box whose child-to-parent
+    //     translation feeds one of them;
+    //   * proxy_down of the boxes that receive incoming expansions or
+    //     evaluate at their targets.
+    // Skipping the rest changes no arithmetic on the expansions that are read.
+    std::vector<int64_t> up_slot(P.nboxes, -1), down_slot(P.nboxes, -1), pw_slot(P.nboxes, -1);
+    std::vector<char> incoming(P.nboxes, 0), leaf_eval(P.nboxes, 0);
+    {
+        std::vector<char> need_pw(P.nboxes, 0), need_up(P.nboxes, 0);
+        for (int b = 0; b < P.nboxes; ++b) {
+            incoming[b] = P.ifpwexp[b] && P.src_count[b] + P.trg_count[b] > 0 && P.trg_count[b] > 0;
+            leaf_eval[b] = P.iftensprodeval[b] && P.trg_count[b] > 0;
+            if (incoming[b]) check(P.pw_off[b] >= 0 && P.proxy_down_off[b] >= 0, "form-eval box storage");
+            if (leaf_eval[b]) check(P.proxy_down_off[b] >= 0, "leaf proxy_down");
+        }
+        for (int b = 0; b < P.nboxes; ++b) {
+            if (!incoming[b]) continue;
+            need_pw[b] = 1;
+            for (int ind = 0; ind < 27; ++ind) {
+                const int nb = P.colleagues[b][ind];
+                if (nb < 0 || nb == b || (P.is_leaf[b] && P.is_leaf[nb]) || P.pw_off[nb] < 0) continue;
+                need_pw[nb] = 1;
+            }
+        }
+        // top-down: a box's proxy_up is read by its own outgoing transform or
+        // through the translation into a parent whose proxy_up is read
+        for (int l = 0; l < P.nlevels; ++l)
+            for (int b : P.level_boxes[l]) {
+                const int par = P.parent[b];
+                const bool via = par >= 0 && need_up[par] && P.has_proxy_from_children[par] && P.src_count[b] > 0 &&
+                                 P.ifpwexp[b];
+                need_up[b] = need_pw[b] || via;
+                if (need_up[b]) check(P.proxy_up_off[b] >= 0, "proxy_up storage");
+            }
+        for (int l = 0; l < P.nlevels; ++l)
+            for (int b : P.level_boxes[l]) {
+                if (need_up[b]) up_slot[b] = n_up_++;
+                if (need_pw[b]) pw_slot[b] = n_pw_++;
+                if (incoming[b] || leaf_eval[b]) down_slot[b] = n_down_++;
+            }
+    }
 
     // ------------------------------------------------------------------ tables
     {
@@ -265,9 +310,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         std::vector<int> slot, rng{0}, s0, sc;
         std::vector<double4> cs;
         for (int b = 0; b < P.nboxes; ++b) {
-            if (by_center[b].empty()) continue;
-            check(P.proxy_up_off[b] >= 0, "proxy_up of work centre");
-            slot.push_back((int)(P.proxy_up_off[b] / ncoef));
+            if (by_center[b].empty() || up_slot[b] < 0) continue;
+            slot.push_back((int)up_slot[b]);
             const int lvl = P.c2proxy_work[by_center[b][0]].level;
             cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / P.boxsize[lvl]));
             for (int w : by_center[b]) {
@@ -295,12 +339,12 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         for (int c = 0; c < 8; ++c) {
             std::vector<int64_t> in, out;
             for (int b : P.level_boxes[l]) {
-                if (!P.has_proxy_from_children[b]) continue;
+                if (!P.has_proxy_from_children[b] || up_slot[b] < 0) continue;
                 const int ch = P.children[b][c];
                 if (ch < 0 || !(P.src_count[ch] > 0 && P.ifpwexp[ch])) continue;
-                check(P.proxy_up_off[ch] >= 0 && P.proxy_up_off[b] >= 0, "c2p offsets");
-                in.push_back(P.proxy_up_off[ch]);
-                out.push_back(P.proxy_up_off[b]);
+                check(up_slot[ch] >= 0, "c2p offsets");
+                in.push_back(up_slot[ch] * ncoef);
+                out.push_back(up_slot[b] * ncoef);
             }
             if (in.empty()) continue;
             C2PGroup g;
@@ -315,10 +359,10 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     for (int l = 0; l < P.nlevels; ++l) {
         std::vector<int64_t> in, out;
         for (int b : P.level_boxes[l]) {
-            if (P.pw_off[b] < 0) continue;
-            check(P.proxy_up_off[b] >= 0, "pw box without proxy");
-            in.push_back(P.proxy_up_off[b]);
-            out.push_back(P.pw_off[b]);
+            if (pw_slot[b] < 0) continue;
+            check(up_slot[b] >= 0, "pw box without proxy");
+            in.push_back(up_slot[b] * ncoef);
+            out.push_back(pw_slot[b] * M);
         }
         if (in.empty()) continue;
         PwGroup g;
@@ -334,9 +378,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         std::vector<int> ts{0}, tslot, tst;
         std::vector<int64_t> down, pin, pout, pmat;
         for (int b : P.level_boxes[l]) {
-            if (!(P.ifpwexp[b] && P.src_count[b] + P.trg_count[b] > 0 && P.trg_count[b] > 0)) continue;
-            check(P.pw_off[b] >= 0 && P.proxy_down_off[b] >= 0, "form-eval box storage");
-            tslot.push_back((int)(P.pw_off[b] / M));
+            if (!incoming[b]) continue;
+            tslot.push_back((int)pw_slot[b]);
             tst.push_back(13);
             for (int ind = 0; ind < 27; ++ind) {
                 const int nb = P.colleagues[b][ind];
@@ -350,18 +393,19 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                     st += kd * stride;
                     stride *= 3;
                 }
-                tslot.push_back((int)(P.pw_off[nb] / M));
+                check(pw_slot[nb] >= 0, "colleague plane waves");
+                tslot.push_back((int)pw_slot[nb]);
                 tst.push_back(st);
             }
             ts.push_back((int)tslot.size());
-            down.push_back(P.proxy_down_off[b]);
+            down.push_back(down_slot[b] * ncoef);
             if (!P.iftensprodeval[b]) {
                 for (int c = 0; c < 8; ++c) {
                     const int ch = P.children[b][c];
-                    if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch])) continue;
-                    check(P.proxy_down_off[ch] >= 0, "p2c child storage");
-                    pin.push_back(P.proxy_down_off[b]);
-                    pout.push_back(P.proxy_down_off[ch]);
+                    // children that neither receive incoming expansions nor evaluate read nothing
+                    if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch]) || down_slot[ch] < 0) continue;
+                    pin.push_back(down_slot[b] * ncoef);
+                    pout.push_back(down_slot[ch] * ncoef);
                     pmat.push_back((int64_t)c * 3 * p * p);
                 }
             }
@@ -387,9 +431,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         std::vector<int> slot, t0, tc;
         std::vector<double4> cs;
         for (int b = 0; b < P.nboxes; ++b) {
-            if (!P.iftensprodeval[b] || P.trg_count[b] == 0) continue;
-            check(P.proxy_down_off[b] >= 0, "leaf proxy_down");
-            slot.push_back((int)(P.proxy_down_off[b] / ncoef));
+            if (!leaf_eval[b]) continue;
+            slot.push_back((int)down_slot[b]);
             t0.push_back(P.trg_start[b]);
             tc.push_back(P.trg_count[b]);
             cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / P.boxsize[P.depth[b]]));
@@ -418,8 +461,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             int64_t nd = 0, np = 0;
             for (int b : P.level_boxes[l]) {
                 check(P.depth[b] == l, "level box depth");
-                if (P.proxy_down_off[b] >= 0) loc_down[b] = nd++;
-                if (P.pw_off[b] >= 0) loc_pw[b] = np++;
+                if (down_slot[b] >= 0) loc_down[b] = nd++;
+                if (pw_slot[b] >= 0) loc_pw[b] = np++;
             }
             f64_levels_[l].level = l;
             f64_levels_[l].n_down = nd;
@@ -431,9 +474,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             const double bs = P.boxsize[l];
             std::vector<int64_t> pin, pout;
             for (int b : P.level_boxes[l]) {
-                if (P.pw_off[b] < 0) continue;
-                check(P.proxy_up_off[b] >= 0, "pw box without proxy");
-                pin.push_back(P.proxy_up_off[b]);
+                if (pw_slot[b] < 0) continue;
+                pin.push_back(up_slot[b] * ncoef);
                 pout.push_back(loc_pw[b] * M);
             }
             F.n_pw = (int)pin.size();
@@ -446,15 +488,13 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             std::vector<int> slot, t0, tc;
             std::vector<double4> cs;
             for (int b : P.level_boxes[l]) {
-                if (P.iftensprodeval[b] && P.trg_count[b] > 0) {
-                    check(loc_down[b] >= 0, "leaf proxy_down");
+                if (leaf_eval[b]) {
                     slot.push_back((int)loc_down[b]);
                     t0.push_back(P.trg_start[b]);
                     tc.push_back(P.trg_count[b]);
                     cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / bs));
                 }
-                if (!(P.ifpwexp[b] && P.src_count[b] + P.trg_count[b] > 0 && P.trg_count[b] > 0)) continue;
-                check(loc_pw[b] >= 0 && loc_down[b] >= 0, "form-eval box storage");
+                if (!incoming[b]) continue;
                 tslot.push_back((int)loc_pw[b]);
                 tst.push_back(13);
                 for (int ind = 0; ind < 27; ++ind) {
@@ -462,7 +502,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                     if (nb < 0 || nb == b) continue;
                     if (P.is_leaf[b] && P.is_leaf[nb]) continue;
                     if (P.pw_off[nb] < 0) continue;
-                    check(P.depth[nb] == l, "colleague level");
+                    check(P.depth[nb] == l && loc_pw[nb] >= 0, "colleague plane waves");
                     int st = 0, stride = 1;
                     for (int d = 0; d < 3; ++d) {
                         const int kd = (int)std::lround((P.centers[3 * b + d] - P.centers[3 * nb + d]) / bs) + 1;
@@ -478,8 +518,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                 if (!P.iftensprodeval[b]) {
                     for (int c = 0; c < 8; ++c) {
                         const int ch = P.children[b][c];
-                        if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch])) continue;
-                        check(loc_down[ch] >= 0 && P.depth[ch] == l + 1 && l + 1 < P.nlevels, "p2c child storage");
+                        if (ch < 0 || !(P.src_count[ch] + P.trg_count[ch]) || loc_down[ch] < 0) continue;
+                        check(P.depth[ch] == l + 1 && l + 1 < P.nlevels, "p2c child level");
                         cin.push_back(loc_down[b] * ncoef);
                         cout.push_back(loc_down[ch] * ncoef);
                         cmat.push_back((int64_t)c * 3 * p * p);
