@@ -855,7 +855,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
     // child -> parent translation of real (p,p,p) tensors: one fused kernel, or
     // three contractions through scratch in chunks of C.c2p translations
     auto translate = [&](const double* in, const int64_t* in_off, double* out, const int64_t* out_off,
-                         const double* mat, const int64_t* mat_off, int count) {
+                         const double* mat, const int64_t* mat_off, int count, int structure) {
         if (fused_c2p) {
             dev::Sep3 f{};
             f.in = in; f.in_off = in_off; f.out = out; f.out_off = out_off; f.mat = mat; f.mat_off = mat_off;
@@ -872,7 +872,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             // x: in (i,j,k) -> s1 (j,k,a); y: s1 -> s2 (k,a,b); z: s2 -> out (a,b,c), accumulated
             a.in = in; a.in_off = in_off + c0; a.out = s1; a.out_stride = ncoef;
             a.mat = mat; a.mat_off = mat_off ? mat_off + c0 : nullptr; a.ni = p; a.na = p; a.R = p * p;
-            a.mode = dev::kStore;
+            a.mode = dev::kStore; a.structure = structure;
             dev::launch_contract(a, dev::kRRR, s);
             a.in = s1; a.in_off = nullptr; a.in_stride = ncoef; a.out = s2; a.mat = mat + p * p;
             dev::launch_contract(a, dev::kRRR, s);
@@ -883,7 +883,8 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
     };
     // upward
     for (const auto& g : c2p_groups_)
-        translate(proxy_up_, g.in_off, proxy_up_, g.out_off, c2p_ + (int64_t)g.child * 3 * p * p, nullptr, g.n);
+        translate(proxy_up_, g.in_off, proxy_up_, g.out_off, c2p_ + (int64_t)g.child * 3 * p * p, nullptr, g.n,
+                  dev::kTriUpper);
     // downward, one level at a time
     if (!f64_levels_.empty())
         PDMK_CUDA_CHECK(cudaMemsetAsync(down_level_[0], 0, sizeof(double) * std::max<int64_t>(f64_levels_[0].n_down * ncoef, 1), s));
@@ -904,7 +905,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
                 dev::ContractArgs a{};
                 a.n_entries = std::min(C.pw_out, F.n_pw - c0);
                 a.in = proxy_up_; a.in_off = F.pw_in_off + c0; a.out = s1; a.out_stride = (int64_t)p * p * n;
-                a.mat = L.poly2pw; a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore;
+                a.mat = L.poly2pw; a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore; a.structure = dev::kParIn;
                 dev::launch_contract(a, dev::kRCC, s);
                 a.in = s1; a.in_off = nullptr; a.in_stride = (int64_t)p * p * n; a.out = s2;
                 a.out_stride = (int64_t)p * n * n; a.R = p * n;
@@ -938,7 +939,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
                 dev::ContractArgs a{};
                 a.n_entries = ne;
                 a.in = pin; a.in_stride = M; a.out = s1; a.out_stride = (int64_t)n * n2 * p;
-                a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
+                a.mat = L.pw2polyT; a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore; a.structure = dev::kParOut;
                 dev::launch_contract(a, dev::kCCC, s);
                 a.in = s1; a.in_stride = (int64_t)n * n2 * p; a.out = s2; a.out_stride = (int64_t)n2 * p * p;
                 a.R = n2 * p;
@@ -961,7 +962,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             double* next = down_level_[(F.level + 1) & 1];
             const int64_t nd = f64_levels_[F.level + 1].n_down;
             PDMK_CUDA_CHECK(cudaMemsetAsync(next, 0, sizeof(double) * std::max<int64_t>(nd * ncoef, 1), s));
-            if (F.n_p2c) translate(down, F.p2c_in, next, F.p2c_out, p2c_, F.p2c_mat, F.n_p2c);
+            if (F.n_p2c) translate(down, F.p2c_in, next, F.p2c_out, p2c_, F.p2c_mat, F.n_p2c, dev::kTriLower);
         }
     }
     return nl;

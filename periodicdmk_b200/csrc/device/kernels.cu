@@ -12,6 +12,9 @@
 //   k_finalize    self correction + desort + far field add (pbc_tree.cpp:1759-1805, periodic_dmk.cpp:177-183)
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace pdmkb {
@@ -135,69 +138,358 @@ __device__ __forceinline__ void store_out<cd>(cd* p, double2 v, int mode, double
     }
 }
 
-__device__ __forceinline__ double2 to2(double v) { return make_double2(v, 0.0); }
-__device__ __forceinline__ double2 to2(cd v) { return make_double2(v.x, v.y); }
+// out = old + v (kAdd) or old + scale * Re v (kAddRealScaled)
+template <typename TO>
+__device__ __forceinline__ void store_acc(TO* p, TO old, double2 v, int mode, double scale);
+template <>
+__device__ __forceinline__ void store_acc<double>(double* p, double old, double2 v, int mode, double scale) {
+    *p = mode == kAdd ? old + v.x : old + scale * v.x;
+}
+template <>
+__device__ __forceinline__ void store_acc<cd>(cd* p, cd old, double2 v, int, double) {
+    *p = cd{old.x + v.x, old.y + v.y};
+}
 
-template <typename TI, typename TM, typename TO, int RT, int AB>
-__global__ void __launch_bounds__(256) k_contract(ContractArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    using TA = decltype(mac(TM(), TI(), TM()));  // accumulator type: complex if either is
-    const int ni = a.ni, na = a.na, R = a.R;
-    const int e = blockIdx.x, r0 = blockIdx.y * RT;
-    TM* sM = reinterpret_cast<TM*>(smem_raw);
-    const size_t moff = ((size_t)na * ni * sizeof(TM) + 15) / 16 * 16;
-    TI* sIn = reinterpret_cast<TI*>(smem_raw + moff);
-    const TI* in = reinterpret_cast<const TI*>(a.in) + (a.in_off ? a.in_off[e] : (int64_t)e * a.in_stride);
-    TO* out = reinterpret_cast<TO*>(a.out) + (a.out_off ? a.out_off[e] : (int64_t)e * a.out_stride);
-    const TM* mat = reinterpret_cast<const TM*>(a.mat) + (a.mat_off ? a.mat_off[e] : 0);
-    for (int idx = threadIdx.x; idx < na * ni; idx += blockDim.x) sM[idx] = mat[idx];
-    const int nr = min(RT, R - r0);
-    const TI* inb = in + (int64_t)ni * r0;
-    for (int idx = threadIdx.x; idx < ni * nr; idx += blockDim.x) {
-        const int i = idx % ni, rr = idx / ni;
-        sIn[rr + RT * i] = inb[idx];
+// Asynchronous global -> shared copy of one 8- or 16-byte element.
+template <int B>
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem);
+template <>
+__device__ __forceinline__ void cp_async_elem<8>(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+                 : "memory");
+}
+template <>
+__device__ __forceinline__ void cp_async_elem<16>(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+                 : "memory");
+}
+
+// Accumulator and multiply-add of each (input, matrix, output) type triple.
+// CCR keeps only the real part, the only one it stores.  mac_re / mac_im
+// multiply by a matrix entry that is real (m) or imaginary (i m).
+template <typename TI, typename TM, typename TO>
+struct CPol;
+template <>
+struct CPol<double, double, double> {
+    using A = double;
+    static __device__ __forceinline__ A zero() { return 0.0; }
+    static __device__ __forceinline__ void mac(A& c, double m, double x) { c = fma(m, x, c); }
+    static __device__ __forceinline__ double2 out(A c) { return make_double2(c, 0.0); }
+};
+template <>
+struct CPol<double, cd, cd> {
+    using A = double2;
+    static __device__ __forceinline__ A zero() { return make_double2(0.0, 0.0); }
+    static __device__ __forceinline__ void mac(A& c, cd m, double x) {
+        c.x = fma(m.x, x, c.x);
+        c.y = fma(m.y, x, c.y);
     }
-    __syncthreads();
-    const int rr = threadIdx.x % RT, ag = threadIdx.x / RT, nag = blockDim.x / RT;
-    if (rr >= nr) return;
-    for (int a0 = ag * AB; a0 < na; a0 += nag * AB) {
-        TA acc[AB];
+    static __device__ __forceinline__ void mac_re(A& c, double m, double x) { c.x = fma(m, x, c.x); }
+    static __device__ __forceinline__ void mac_im(A& c, double m, double x) { c.y = fma(m, x, c.y); }
+    static __device__ __forceinline__ double2 out(A c) { return c; }
+};
+template <>
+struct CPol<cd, cd, cd> {
+    using A = double2;
+    static __device__ __forceinline__ A zero() { return make_double2(0.0, 0.0); }
+    static __device__ __forceinline__ void mac(A& c, cd m, cd x) {
+        c.x = fma(m.x, x.x, c.x);
+        c.x = fma(-m.y, x.y, c.x);
+        c.y = fma(m.x, x.y, c.y);
+        c.y = fma(m.y, x.x, c.y);
+    }
+    static __device__ __forceinline__ void mac_re(A& c, double m, cd x) {
+        c.x = fma(m, x.x, c.x);
+        c.y = fma(m, x.y, c.y);
+    }
+    static __device__ __forceinline__ void mac_im(A& c, double m, cd x) {
+        c.x = fma(-m, x.y, c.x);
+        c.y = fma(m, x.x, c.y);
+    }
+    static __device__ __forceinline__ double2 out(A c) { return c; }
+};
+template <>
+struct CPol<cd, cd, double> {
+    using A = double;
+    static __device__ __forceinline__ A zero() { return 0.0; }
+    static __device__ __forceinline__ void mac(A& c, cd m, cd x) {
+        c = fma(m.x, x.x, c);
+        c = fma(-m.y, x.y, c);
+    }
+    static __device__ __forceinline__ void mac_re(A& c, double m, cd x) { c = fma(m, x.x, c); }
+    static __device__ __forceinline__ void mac_im(A& c, double m, cd x) { c = fma(-m, x.y, c); }
+    static __device__ __forceinline__ double2 out(A c) { return make_double2(c, 0.0); }
+};
+
+// Loads TA consecutive matrix values of one row of the shared tile.
+template <typename T, int TA>
+__device__ __forceinline__ void load_row(T (&m)[TA], const T* row) {
+    if constexpr (sizeof(T) == 8 && TA % 2 == 0) {
 #pragma unroll
-        for (int b = 0; b < AB; ++b) acc[b] = zero<TA>();
-        for (int i = 0; i < ni; ++i) {
-            const TI x = sIn[rr + RT * i];
-#pragma unroll
-            for (int b = 0; b < AB; ++b)
-                if (a0 + b < na) acc[b] = mac(sM[a0 + b + na * i], x, acc[b]);
+        for (int t = 0; t < TA; t += 2) {
+            const double2 v = reinterpret_cast<const double2*>(row)[t / 2];
+            m[t] = v.x;
+            m[t + 1] = v.y;
         }
+    } else {
 #pragma unroll
-        for (int b = 0; b < AB; ++b)
-            if (a0 + b < na) store_out<TO>(out + (r0 + rr) + (int64_t)R * (a0 + b), to2(acc[b]), a.mode, a.scale);
+        for (int t = 0; t < TA; ++t) m[t] = row[t];
     }
 }
 
-template <typename TI, typename TM, typename TO>
-static void launch_contract_t(const ContractArgs& a, cudaStream_t s) {
-    constexpr int RT = 32, AB = 4;
-    const size_t smem = ((size_t)a.na * a.ni * sizeof(TM) + 15) / 16 * 16 + (size_t)a.ni * RT * sizeof(TI);
+// One CTA = one entry x a tile of RB = WR*32*TR rows; 8 warps as WA column
+// groups x WR row groups.  Lane l of a warp owns rows l + 32 j (j < TR) of its
+// row group; column group g owns the output columns a = k*WA*TA + g + WA*t
+// (t < TA) of column chunk k, stored contiguously in the shared matrix tile.
+// Per step of the contracted index a lane loads TR inputs (consecutive across
+// lanes) and TA matrix values (one broadcast per pair), then does TR*TA
+// multiply-adds from registers.  S selects the matrix structure used (see
+// ContractStruct): the skipped entries are the rounding-level zeros of the
+// triangular parent/child matrices and of the real/imaginary plane-wave tables.
+template <typename TI, typename TM, typename TO, int TR, int TA, int WA, int S, bool ACC>
+__device__ __forceinline__ void contract_body(const ContractArgs& a, unsigned char* smem_raw) {
+    using Pol = CPol<TI, TM, TO>;
+    using Acc = typename Pol::A;
+    constexpr bool PAR = (S == kParIn || S == kParOut);
+    using SMT = typename std::conditional<PAR, double, TM>::type;
+    constexpr int WR = 8 / WA;
+    constexpr int RB = WR * 32 * TR;
+    constexpr int LD = RB + 1;  // odd stride: the transposing stores spread over the banks
+    constexpr int CW = WA * TA;
+    const int ni = a.ni, na = a.na, R = a.R;
+    const int napad = (na + CW - 1) / CW * CW;
+    const int e = blockIdx.x, r0 = blockIdx.y * RB;
+    SMT* sM = reinterpret_cast<SMT*>(smem_raw);  // [ni][napad], permuted columns, zero beyond na
+    TI* sIn = reinterpret_cast<TI*>(smem_raw + ((size_t)ni * napad * sizeof(SMT) + 15) / 16 * 16);  // [ni][LD]
+    const TI* in = reinterpret_cast<const TI*>(a.in) + (a.in_off ? a.in_off[e] : (int64_t)e * a.in_stride);
+    TO* out = reinterpret_cast<TO*>(a.out) + (a.out_off ? a.out_off[e] : (int64_t)e * a.out_stride);
+    const TM* mat = reinterpret_cast<const TM*>(a.mat) + (a.mat_off ? a.mat_off[e] : 0);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // fill: asynchronous element copies, all in flight at once (the transpose
+    // of the input tile and the column permutation of the matrix happen in
+    // the copies' destination addresses)
+    for (int i = w; i < ni; i += 8)
+        for (int c = lane; c < napad; c += 32) {
+            const int kk = c / CW, rem = c - kk * CW, g = rem / TA, t = rem - g * TA;
+            const int col = kk * CW + g + WA * t;
+            SMT* dst = sM + i * napad + c;
+            if (col >= na) {
+                *dst = SMT{};
+            } else if constexpr (PAR) {
+                const bool re = S == kParIn ? (i & 1) == 0 : (col & 1) == 0;
+                cp_async_elem<8>(dst, reinterpret_cast<const double*>(mat + col + (int64_t)na * i) + (re ? 0 : 1));
+            } else {
+                cp_async_elem<sizeof(TM)>(dst, mat + col + (int64_t)na * i);
+            }
+        }
+    const int nr = min(RB, R - r0);
+    const TI* inb = in + (int64_t)ni * r0;
+    for (int rr = w; rr < RB; rr += 8)
+        for (int i = lane; i < ni; i += 32) {
+            if (rr < nr)
+                cp_async_elem<sizeof(TI)>(sIn + i * LD + rr, inb + (int64_t)rr * ni + i);
+            else
+                sIn[i * LD + rr] = TI{};
+        }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const int wa = w % WA, wr = w / WA;
+    const int rbase = wr * 32 * TR + lane;
+    for (int k0 = 0; k0 < na; k0 += CW) {
+        if (k0 + wa >= na) break;
+        Acc acc[TR][TA];
+#pragma unroll
+        for (int j = 0; j < TR; ++j)
+#pragma unroll
+            for (int t = 0; t < TA; ++t) acc[j][t] = Pol::zero();
+        const SMT* mcol = sM + k0 + wa * TA;
+        if constexpr (S == kTriUpper || S == kTriLower) {
+            // square matrix in one chunk (ni <= CW): the contracted indices
+            // i in [WA s, WA s + WA) meet the columns a_t = wa + WA t with
+            // t >= s (upper: M(a,i) = 0 for i > a) or t <= s (lower: 0 for i < a)
+#pragma unroll
+            for (int sg = 0; sg < TA; ++sg) {
+#pragma unroll
+                for (int q = 0; q < WA; ++q) {
+                    const int i = WA * sg + q;
+                    if (i >= ni) break;
+                    TI x[TR];
+#pragma unroll
+                    for (int j = 0; j < TR; ++j) x[j] = sIn[i * LD + rbase + 32 * j];
+                    SMT m[TA];
+                    load_row<SMT, TA>(m, mcol + (size_t)i * napad);
+#pragma unroll
+                    for (int t = 0; t < TA; ++t) {
+                        if (S == kTriUpper ? t < sg : t > sg) continue;
+#pragma unroll
+                        for (int j = 0; j < TR; ++j) Pol::mac(acc[j][t], m[t], x[j]);
+                    }
+                }
+            }
+        } else if constexpr (S == kParIn) {
+            // entry real for even contracted index, imaginary for odd
+            for (int i = 0; i < ni; ++i) {
+                TI x[TR];
+#pragma unroll
+                for (int j = 0; j < TR; ++j) x[j] = sIn[i * LD + rbase + 32 * j];
+                SMT m[TA];
+                load_row<SMT, TA>(m, mcol + (size_t)i * napad);
+                if ((i & 1) == 0) {
+#pragma unroll
+                    for (int t = 0; t < TA; ++t)
+#pragma unroll
+                        for (int j = 0; j < TR; ++j) Pol::mac_re(acc[j][t], m[t], x[j]);
+                } else {
+#pragma unroll
+                    for (int t = 0; t < TA; ++t)
+#pragma unroll
+                        for (int j = 0; j < TR; ++j) Pol::mac_im(acc[j][t], m[t], x[j]);
+                }
+            }
+        } else if constexpr (S == kParOut) {
+            // entry real for even output column, imaginary for odd: all the
+            // columns of a group share the parity of k0 + wa (WA, CW even)
+            const bool re = ((k0 + wa) & 1) == 0;
+            for (int i = 0; i < ni; ++i) {
+                TI x[TR];
+#pragma unroll
+                for (int j = 0; j < TR; ++j) x[j] = sIn[i * LD + rbase + 32 * j];
+                SMT m[TA];
+                load_row<SMT, TA>(m, mcol + (size_t)i * napad);
+                if (re) {
+#pragma unroll
+                    for (int t = 0; t < TA; ++t)
+#pragma unroll
+                        for (int j = 0; j < TR; ++j) Pol::mac_re(acc[j][t], m[t], x[j]);
+                } else {
+#pragma unroll
+                    for (int t = 0; t < TA; ++t)
+#pragma unroll
+                        for (int j = 0; j < TR; ++j) Pol::mac_im(acc[j][t], m[t], x[j]);
+                }
+            }
+        } else {
+#pragma unroll 2
+            for (int i = 0; i < ni; ++i) {
+                TI x[TR];
+#pragma unroll
+                for (int j = 0; j < TR; ++j) x[j] = sIn[i * LD + rbase + 32 * j];
+                SMT m[TA];
+                load_row<SMT, TA>(m, mcol + (size_t)i * napad);
+#pragma unroll
+                for (int t = 0; t < TA; ++t)
+#pragma unroll
+                    for (int j = 0; j < TR; ++j) Pol::mac(acc[j][t], m[t], x[j]);
+            }
+        }
+        if constexpr (!ACC) {
+#pragma unroll
+            for (int t = 0; t < TA; ++t) {
+                const int col = k0 + wa + WA * t;
+                if (col >= na) break;
+#pragma unroll
+                for (int j = 0; j < TR; ++j) {
+                    const int r = rbase + 32 * j;
+                    if (r < nr) store_out<TO>(out + (r0 + r) + (int64_t)R * col, Pol::out(acc[j][t]), kStore, 1.0);
+                }
+            }
+        } else {
+            // accumulate: all the old values are loaded before the first store
+            TO old[TA][TR];
+#pragma unroll
+            for (int t = 0; t < TA; ++t)
+#pragma unroll
+                for (int j = 0; j < TR; ++j) {
+                    const int col = k0 + wa + WA * t, r = rbase + 32 * j;
+                    old[t][j] = (col < na && r < nr) ? out[(r0 + r) + (int64_t)R * col] : TO{};
+                }
+#pragma unroll
+            for (int t = 0; t < TA; ++t) {
+                const int col = k0 + wa + WA * t;
+                if (col >= na) break;
+#pragma unroll
+                for (int j = 0; j < TR; ++j) {
+                    const int r = rbase + 32 * j;
+                    if (r < nr) store_acc<TO>(out + (r0 + r) + (int64_t)R * col, old[t][j], Pol::out(acc[j][t]), a.mode, a.scale);
+                }
+            }
+        }
+    }
+}
+
+template <typename TI, typename TM, typename TO, int TR, int TA, int WA, int S, bool ACC>
+__global__ void __launch_bounds__(256) k_contract(ContractArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    contract_body<TI, TM, TO, TR, TA, WA, S, ACC>(a, smem_raw);
+}
+
+template <typename TI, typename TM, typename TO, int TR, int TA, int WA, int S, bool ACC>
+static void launch_contract_a(const ContractArgs& a, cudaStream_t s) {
+    constexpr int RB = (8 / WA) * 32 * TR;
+    constexpr bool PAR = (S == kParIn || S == kParOut);
+    const int napad = (a.na + WA * TA - 1) / (WA * TA) * (WA * TA);
+    const size_t msz = PAR ? sizeof(double) : sizeof(TM);
+    const size_t smem = ((size_t)a.ni * napad * msz + 15) / 16 * 16 + (size_t)a.ni * (RB + 1) * sizeof(TI);
     static bool configured = false;
     if (!configured) {
-        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_contract<TI, TM, TO, RT, AB>,
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_contract<TI, TM, TO, TR, TA, WA, S, ACC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         configured = true;
     }
     if (smem > 200 * 1024) throw std::runtime_error("contraction tile exceeds shared memory");
-    const dim3 grid(a.n_entries, (a.R + RT - 1) / RT);
-    k_contract<TI, TM, TO, RT, AB><<<grid, 256, smem, s>>>(a);
+    const dim3 grid(a.n_entries, (a.R + RB - 1) / RB);
+    k_contract<TI, TM, TO, TR, TA, WA, S, ACC><<<grid, 256, smem, s>>>(a);
+}
+
+template <typename TI, typename TM, typename TO, int TR, int TA, int WA, int S>
+static void launch_contract_s(const ContractArgs& a, cudaStream_t s) {
+    if (a.mode == kStore) return launch_contract_a<TI, TM, TO, TR, TA, WA, S, false>(a, s);
+    return launch_contract_a<TI, TM, TO, TR, TA, WA, S, true>(a, s);
+}
+
+// Structure dispatch: triangular only for real square matrices that fit one
+// column chunk, parity only for complex matrices; anything else runs dense.
+template <typename TI, typename TM, typename TO, int TR, int TA, int WA>
+static void launch_contract_k(const ContractArgs& a, cudaStream_t s) {
+    constexpr bool real = sizeof(TM) == sizeof(double);
+    const int st = a.structure;
+    if constexpr (real) {
+        if ((st == kTriUpper || st == kTriLower) && a.ni == a.na && a.ni <= WA * TA) {
+            if (st == kTriUpper) return launch_contract_s<TI, TM, TO, TR, TA, WA, kTriUpper>(a, s);
+            return launch_contract_s<TI, TM, TO, TR, TA, WA, kTriLower>(a, s);
+        }
+    } else {
+        if (st == kParIn) return launch_contract_s<TI, TM, TO, TR, TA, WA, kParIn>(a, s);
+        if (st == kParOut) return launch_contract_s<TI, TM, TO, TR, TA, WA, kParOut>(a, s);
+    }
+    return launch_contract_s<TI, TM, TO, TR, TA, WA, kDense>(a, s);
+}
+
+// Column tile TA: the smallest of the instantiated widths that covers na in
+// one pass of the WA column groups (the largest otherwise, looping over na).
+template <typename TI, typename TM, typename TO, int TR, int WA>
+static void launch_contract_t(const ContractArgs& a, cudaStream_t s) {
+    switch (std::min((a.na + WA - 1) / WA, 10)) {
+        case 0:
+        case 1:
+        case 2: return launch_contract_k<TI, TM, TO, TR, 2, WA>(a, s);
+        case 3: return launch_contract_k<TI, TM, TO, TR, 3, WA>(a, s);
+        case 4: return launch_contract_k<TI, TM, TO, TR, 4, WA>(a, s);
+        case 5: return launch_contract_k<TI, TM, TO, TR, 5, WA>(a, s);
+        case 6: return launch_contract_k<TI, TM, TO, TR, 6, WA>(a, s);
+        case 7: return launch_contract_k<TI, TM, TO, TR, 7, WA>(a, s);
+        case 8: return launch_contract_k<TI, TM, TO, TR, 8, WA>(a, s);
+        default: return launch_contract_k<TI, TM, TO, TR, 10, WA>(a, s);
+    }
 }
 
 void launch_contract(const ContractArgs& a, ContractType t, cudaStream_t s) {
     if (a.n_entries <= 0) return;
     switch (t) {
-        case kRRR: launch_contract_t<double, double, double>(a, s); break;
-        case kRCC: launch_contract_t<double, cd, cd>(a, s); break;
-        case kCCC: launch_contract_t<cd, cd, cd>(a, s); break;
-        case kCCR: launch_contract_t<cd, cd, double>(a, s); break;
+        case kRRR: launch_contract_t<double, double, double, 2, 4>(a, s); break;
+        case kRCC: launch_contract_t<double, cd, cd, 2, 8>(a, s); break;
+        case kCCC: launch_contract_t<cd, cd, cd, 2, 8>(a, s); break;
+        case kCCR: launch_contract_t<cd, cd, double, 2, 4>(a, s); break;
     }
 }
 

@@ -33,6 +33,13 @@ void launch_c2proxy(const C2ProxyArgs& a, int p, cudaStream_t s);
 // out = out_base + out_off[e] (or e*out_stride), M = mat_base + mat_off[e] (or 0).
 enum ContractMode { kStore = 0, kAdd = 1, kAddRealScaled = 2 };
 enum ContractType { kRRR = 0, kRCC = 1, kCCC = 2, kCCR = 3 };  // (in, mat, out): R real, C complex
+// Structure of M the contraction may exploit (the entries it skips are zero up
+// to rounding in the tables it is used with):
+//   kTriUpper  M[a + na*i] = 0 for i > a   (child -> parent translation)
+//   kTriLower  M[a + na*i] = 0 for i < a   (parent -> child translation)
+//   kParIn     M real for even i, imaginary for odd i   (polynomial -> plane wave)
+//   kParOut    M real for even a, imaginary for odd a   (plane wave -> polynomial)
+enum ContractStruct { kDense = 0, kTriUpper = 1, kTriLower = 2, kParIn = 3, kParOut = 4 };
 struct ContractArgs {
     const void* in;
     const int64_t* in_off;
@@ -45,6 +52,7 @@ struct ContractArgs {
     int ni, na, R, n_entries;
     int mode;
     double scale;
+    int structure;  // ContractStruct (0: dense)
 };
 void launch_contract(const ContractArgs& a, ContractType t, cudaStream_t s);
 
