@@ -101,14 +101,115 @@ __global__ void __launch_bounds__(128) k_c2proxy(C2ProxyArgs a) {
     }
 }
 
+// Same sum for the large orders, register-tiled: a thread owns the 8 x 4
+// coefficients (i in 8-block ib, j in 4-block jb) at one z-order k.  Per
+// source it loads 8 x-values and 4 y-values (shared by the warp, broadcast)
+// and one z-value, then does 32 multiply-adds.
+template <int P>
+__global__ void __launch_bounds__(128) k_c2proxy_tiled(C2ProxyArgs a) {
+    constexpr int TI = 8, TJ = 4, TS = 32;
+    constexpr int NIB = (P + TI - 1) / TI, NJB = (P + TJ - 1) / TJ;
+    constexpr int PI = NIB * TI, PJ = NJB * TJ;  // padded rows (zeros beyond P)
+    constexpr int NTASK = P * NJB * NIB;
+    __shared__ __align__(16) double sx[TS][PI];
+    __shared__ __align__(16) double sy[TS][PJ];
+    __shared__ double sz[TS][P];
+    const int e = blockIdx.x;
+    const int task = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool active = task < NTASK;
+    const int k = task % P, jb = (task / P) % NJB, ib = task / (P * NJB);
+    double acc[TI][TJ];
+#pragma unroll
+    for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int t = 0; t < TJ; ++t) acc[i][t] = 0.0;
+    const double4 cs = a.center_scale[e];
+    for (int r = a.rng_start[e]; r < a.rng_start[e + 1]; ++r) {
+        const int s0 = a.src_start[r], ns = a.src_count[r];
+        for (int base = 0; base < ns; base += TS) {
+            const int nt = min(TS, ns - base);
+            __syncthreads();
+            if (threadIdx.x < 3 * TS) {
+                const int si = threadIdx.x % TS, d = threadIdx.x / TS;
+                double* dst = d == 0 ? sx[si] : (d == 1 ? sy[si] : sz[si]);
+                const int len = d == 0 ? PI : (d == 1 ? PJ : P);
+                if (si < nt) {
+                    const double4 pt = a.src[s0 + base + si];
+                    const double x = (d == 0 ? pt.x - cs.x : (d == 1 ? pt.y - cs.y : pt.z - cs.z)) * cs.w;
+                    const double mult = d == 2 ? pt.w : 1.0;  // fold the charge into the z factor
+                    double t0 = 1.0, t1 = x;
+                    dst[0] = mult;
+                    if (P > 1) dst[1] = mult * x;
+                    for (int n = 2; n < P; ++n) {
+                        const double t2 = 2.0 * x * t1 - t0;
+                        dst[n] = mult * t2;
+                        t0 = t1;
+                        t1 = t2;
+                    }
+                    for (int n = P; n < len; ++n) dst[n] = 0.0;
+                } else {
+                    for (int n = 0; n < len; ++n) dst[n] = 0.0;
+                }
+            }
+            __syncthreads();
+            if (active) {
+#pragma unroll 2
+                for (int s = 0; s < nt; ++s) {
+                    double xv[TI], yz[TJ];
+                    const double2* xr = reinterpret_cast<const double2*>(&sx[s][ib * TI]);
+#pragma unroll
+                    for (int i = 0; i < TI / 2; ++i) {
+                        const double2 v = xr[i];
+                        xv[2 * i] = v.x;
+                        xv[2 * i + 1] = v.y;
+                    }
+                    const double z = sz[s][k];
+                    const double2* yr = reinterpret_cast<const double2*>(&sy[s][jb * TJ]);
+#pragma unroll
+                    for (int t = 0; t < TJ / 2; ++t) {
+                        const double2 v = yr[t];
+                        yz[2 * t] = v.x * z;
+                        yz[2 * t + 1] = v.y * z;
+                    }
+#pragma unroll
+                    for (int i = 0; i < TI; ++i)
+#pragma unroll
+                        for (int t = 0; t < TJ; ++t) acc[i][t] = fma(xv[i], yz[t], acc[i][t]);
+                }
+            }
+        }
+    }
+    if (!active) return;
+    double* out = a.proxy_up + (int64_t)a.slot[e] * (P * P * P) + (int64_t)P * P * k;
+    double old[TI][TJ];
+#pragma unroll
+    for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int t = 0; t < TJ; ++t) {
+            const int ii = ib * TI + i, jj = jb * TJ + t;
+            old[i][t] = (ii < P && jj < P) ? out[ii + P * jj] : 0.0;
+        }
+#pragma unroll
+    for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int t = 0; t < TJ; ++t) {
+            const int ii = ib * TI + i, jj = jb * TJ + t;
+            if (ii < P && jj < P) out[ii + P * jj] = old[i][t] + acc[i][t];
+        }
+}
+
 void launch_c2proxy(const C2ProxyArgs& a, int p, cudaStream_t s) {
     if (a.n_centers <= 0) return;
     const dim3 grid(a.n_centers, (p * p + 127) / 128);
+    auto tiled_grid = [&](int q) {
+        const int ntask = q * ((q + 3) / 4) * ((q + 7) / 8);
+        return dim3(a.n_centers, (ntask + 127) / 128);
+    };
     switch (p) {
         case 9: k_c2proxy<9><<<grid, 128, 0, s>>>(a); break;
         case 18: k_c2proxy<18><<<grid, 128, 0, s>>>(a); break;
-        case 28: k_c2proxy<28><<<grid, 128, 0, s>>>(a); break;
-        case 38: k_c2proxy<38><<<grid, 128, 0, s>>>(a); break;
+        case 28: k_c2proxy_tiled<28><<<tiled_grid(28), 128, 0, s>>>(a); break;
+        case 38: k_c2proxy_tiled<38><<<tiled_grid(38), 128, 0, s>>>(a); break;
         default: throw std::runtime_error("unsupported expansion order");
     }
 }
