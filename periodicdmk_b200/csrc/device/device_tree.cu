@@ -855,11 +855,12 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
     // child -> parent translation of real (p,p,p) tensors: one fused kernel, or
     // three contractions through scratch in chunks of C.c2p translations
     auto translate = [&](const double* in, const int64_t* in_off, double* out, const int64_t* out_off,
-                         const double* mat, const int64_t* mat_off, int count, int structure) {
+                         const double* mat, const int64_t* mat_off, int count, int structure, bool accumulate) {
         if (fused_c2p) {
             dev::Sep3 f{};
             f.in = in; f.in_off = in_off; f.out = out; f.out_off = out_off; f.mat = mat; f.mat_off = mat_off;
-            f.rhs = 1; f.accumulate = 1;
+            f.tri = structure == dev::kTriUpper ? 1 : (structure == dev::kTriLower ? 2 : 0);
+            f.rhs = 1; f.accumulate = accumulate ? 1 : 0;
             dev::launch_sep3<double>(f, p, count, s);
             ++nl;
             return;
@@ -876,7 +877,8 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             dev::launch_contract(a, dev::kRRR, s);
             a.in = s1; a.in_off = nullptr; a.in_stride = ncoef; a.out = s2; a.mat = mat + p * p;
             dev::launch_contract(a, dev::kRRR, s);
-            a.in = s2; a.out = out; a.out_off = out_off + c0; a.mat = mat + 2 * p * p; a.mode = dev::kAdd;
+            a.in = s2; a.out = out; a.out_off = out_off + c0; a.mat = mat + 2 * p * p;
+            a.mode = accumulate ? dev::kAdd : dev::kStore;
             dev::launch_contract(a, dev::kRRR, s);
             nl += 3;
         }
@@ -884,7 +886,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
     // upward
     for (const auto& g : c2p_groups_)
         translate(proxy_up_, g.in_off, proxy_up_, g.out_off, c2p_ + (int64_t)g.child * 3 * p * p, nullptr, g.n,
-                  dev::kTriUpper);
+                  dev::kTriUpper, true);
     // downward, one level at a time
     if (!f64_levels_.empty())
         PDMK_CUDA_CHECK(cudaMemsetAsync(down_level_[0], 0, sizeof(double) * std::max<int64_t>(f64_levels_[0].n_down * ncoef, 1), s));
@@ -962,7 +964,8 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             double* next = down_level_[(F.level + 1) & 1];
             const int64_t nd = f64_levels_[F.level + 1].n_down;
             PDMK_CUDA_CHECK(cudaMemsetAsync(next, 0, sizeof(double) * std::max<int64_t>(nd * ncoef, 1), s));
-            if (F.n_p2c) translate(down, F.p2c_in, next, F.p2c_out, p2c_, F.p2c_mat, F.n_p2c, dev::kTriLower);
+            // first write of each child's coefficients (one parent each): store
+            if (F.n_p2c) translate(down, F.p2c_in, next, F.p2c_out, p2c_, F.p2c_mat, F.n_p2c, dev::kTriLower, false);
         }
     }
     return nl;

@@ -564,24 +564,46 @@ static void launch_near_m32_kb(const NearM& a, const float4* th, const float4* t
 // ---------------------------------------------------------------------------
 
 
-template <typename T, int P>
+// TRI: 0 dense; 1 U(a,i) = 0 for i > a (child -> parent); 2 U(a,i) = 0 for
+// i < a (parent -> child).  The skipped entries are rounding-level zeros of
+// the reference's triangular Chebyshev translation matrices.
+// Column range [lo, hi) that segment s (contracted indices i in [SEG s,
+// SEG s + SEG)) touches: all columns, or those a triangular matrix can have
+// non-zero (a >= i for TRI 1, a <= i for TRI 2), widened to the segment.
+template <int P, int TRI, int SEG>
+__device__ __forceinline__ constexpr int seg_lo(int sg) { return TRI == 1 ? SEG * sg : 0; }
+template <int P, int TRI, int SEG>
+__device__ __forceinline__ constexpr int seg_hi(int sg) {
+    return TRI == 2 ? (SEG * sg + SEG < P ? SEG * sg + SEG : P) : P;
+}
+
+// dst[r + P*P*a] = sum_i Ut[i*P + a] * src[i + P*r], two columns r per thread.
+// The contracted index runs in segments of SEG (segment index unrolled, so
+// each segment's column range is a compile-time constant; loop inside a
+// segment kept rolled, which bounds the registers).
+template <typename T, int P, int TRI>
 __device__ __forceinline__ void sep3_step(const T* __restrict__ src, T* __restrict__ dst, const T* __restrict__ Ut,
                                           int nthr) {
-    // dst[r + P*P*a] = sum_i Ut[i*P + a] * src[i + P*r], two columns r per thread
+    constexpr int SEG = 3, NSEG = (P + SEG - 1) / SEG;
     for (int r = threadIdx.x; r < P * P; r += 2 * nthr) {
         const int r2 = r + nthr;
         const bool two = r2 < P * P;
         T acc0[P], acc1[P];
 #pragma unroll
         for (int a = 0; a < P; ++a) acc0[a] = acc1[a] = T(0);
-        for (int i = 0; i < P; ++i) {
-            const T x0 = src[i + P * r];
-            const T x1 = two ? src[i + P * r2] : T(0);
 #pragma unroll
-            for (int a = 0; a < P; ++a) {
-                const T u = Ut[i * P + a];
-                acc0[a] = fma(u, x0, acc0[a]);
-                acc1[a] = fma(u, x1, acc1[a]);
+        for (int sg = 0; sg < NSEG; ++sg) {
+            const int i1 = SEG * sg + SEG < P ? SEG * sg + SEG : P;
+#pragma unroll 1
+            for (int i = SEG * sg; i < i1; ++i) {
+                const T x0 = src[i + P * r];
+                const T x1 = two ? src[i + P * r2] : T(0);
+#pragma unroll
+                for (int a = seg_lo<P, TRI, SEG>(sg); a < seg_hi<P, TRI, SEG>(sg); ++a) {
+                    const T u = Ut[i * P + a];
+                    acc0[a] = fma(u, x0, acc0[a]);
+                    acc1[a] = fma(u, x1, acc1[a]);
+                }
             }
         }
 #pragma unroll
@@ -592,7 +614,7 @@ __device__ __forceinline__ void sep3_step(const T* __restrict__ src, T* __restri
     }
 }
 
-template <typename T, int P>
+template <typename T, int P, int TRI>
 __global__ void k_sep3(Sep3 a) {
     extern __shared__ __align__(16) unsigned char smem_s3[];
     constexpr int P3 = P * P * P;
@@ -613,44 +635,54 @@ __global__ void k_sep3(Sep3 a) {
         Ut[d * P * P + i * P + aa] = mat[d * P * P + aa + P * i];
     }
     __syncthreads();
-    sep3_step<T, P>(b0, b1, Ut, nthr);
+    sep3_step<T, P, TRI>(b0, b1, Ut, nthr);
     __syncthreads();
-    sep3_step<T, P>(b1, b0, Ut + P * P, nthr);
+    sep3_step<T, P, TRI>(b1, b0, Ut + P * P, nthr);
     __syncthreads();
-    // last step straight into the output (coalesced along r)
+    // last step straight into the output (coalesced along r); with
+    // accumulation all old values are loaded before the first store
     const T* Uz = Ut + 2 * P * P;
+    constexpr int SEG = 3, NSEG = (P + SEG - 1) / SEG;
     for (int r = threadIdx.x; r < P * P; r += nthr) {
         T acc[P];
 #pragma unroll
-        for (int c = 0; c < P; ++c) acc[c] = T(0);
-        for (int k = 0; k < P; ++k) {
-            const T x = b0[k + P * r];
+        for (int c = 0; c < P; ++c) acc[c] = a.accumulate ? out[r + P * P * c] : T(0);
 #pragma unroll
-            for (int c = 0; c < P; ++c) acc[c] = fma(Uz[k * P + c], x, acc[c]);
+        for (int sg = 0; sg < NSEG; ++sg) {
+            const int k1 = SEG * sg + SEG < P ? SEG * sg + SEG : P;
+#pragma unroll 1
+            for (int k = SEG * sg; k < k1; ++k) {
+                const T x = b0[k + P * r];
+#pragma unroll
+                for (int c = seg_lo<P, TRI, SEG>(sg); c < seg_hi<P, TRI, SEG>(sg); ++c)
+                    acc[c] = fma(Uz[k * P + c], x, acc[c]);
+            }
         }
 #pragma unroll
-        for (int c = 0; c < P; ++c) {
-            if (a.accumulate)
-                out[r + P * P * c] += acc[c];
-            else
-                out[r + P * P * c] = acc[c];
-        }
+        for (int c = 0; c < P; ++c) out[r + P * P * c] = acc[c];
     }
 }
 
 template <typename T, int P>
 static size_t sep3_smem() { return sizeof(T) * (2 * (size_t)P * P * P + 3 * (size_t)P * P); }
 
-template <typename T, int P>
-static void launch_sep3_p(const Sep3& a, int n_entries, cudaStream_t s) {
+template <typename T, int P, int TRI>
+static void launch_sep3_t(const Sep3& a, int n_entries, cudaStream_t s) {
     static bool configured = false;
     const size_t smem = sep3_smem<T, P>();
     if (!configured) {
-        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_sep3<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_sep3<T, P, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = true;
     }
     const int thr = std::max(32, ((P * P + 1) / 2 + 31) / 32 * 32);
-    k_sep3<T, P><<<n_entries, thr, smem, s>>>(a);
+    k_sep3<T, P, TRI><<<n_entries, thr, smem, s>>>(a);
+}
+
+template <typename T, int P>
+static void launch_sep3_p(const Sep3& a, int n_entries, cudaStream_t s) {
+    if (P <= 18 && a.tri == 1) return launch_sep3_t<T, P, (P <= 18 ? 1 : 0)>(a, n_entries, s);
+    if (P <= 18 && a.tri == 2) return launch_sep3_t<T, P, (P <= 18 ? 2 : 0)>(a, n_entries, s);
+    launch_sep3_t<T, P, 0>(a, n_entries, s);
 }
 
 // true if the fused kernel handles (T, P) (tensor pair fits in shared memory)
@@ -998,7 +1030,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         if (fused) {
             dev::Sep3 f{};
             f.in = up; f.in_off = g.in_off; f.out = up; f.out_off = g.out_off; f.mat = mx; f.rhs = kb;
-            f.accumulate = 1;
+            f.accumulate = 1; f.tri = 1;
             dev::launch_sep3<T>(f, p, g.n * kb, s); ++nl;
             continue;
         }
@@ -1073,7 +1105,9 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         if (E.n_p2c && fused) {
             dev::Sep3 f{};
             f.in = down; f.in_off = E.p2c_in; f.out = down; f.out_off = E.p2c_out; f.mat = p2cm;
-            f.mat_off = E.p2c_mat; f.rhs = kb; f.accumulate = 1;
+            // first write of the children's coefficients (one parent each; their
+            // own incoming expansions are added at the next level): store
+            f.mat_off = E.p2c_mat; f.rhs = kb; f.accumulate = 0; f.tri = 2;
             dev::launch_sep3<T>(f, p, E.n_p2c * kb, s); ++nl;
         } else if (E.n_p2c) {
             chunked(E.n_p2c, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {

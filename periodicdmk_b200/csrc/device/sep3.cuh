@@ -22,6 +22,7 @@ struct Sep3 {
     int rhs;
     int64_t e0;
     int accumulate;
+    int tri;  // 0 dense; 1 U(a,i) = 0 for i > a (child -> parent); 2 U(a,i) = 0 for i < a (parent -> child)
 };
 
 // true if the fused kernel handles (T, p) (the tensor pair fits in shared memory)

@@ -121,10 +121,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     float* sT = reinterpret_cast<float*>(sm + S::OFF_T);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int e = blockIdx.x;
+    // flat grid, centre-major: the row tiles and column splits of one centre
+    // run next to each other and share its sources in L2
+    const int ntile = (P * kb + 127) / 128;
+    const int e = blockIdx.x / (ntile * S::NSPLIT);
+    const int tsel = blockIdx.x % (ntile * S::NSPLIT);
     const int rows = P * kb;
-    const int row0 = blockIdx.y * 128;
-    const int col0 = blockIdx.z * S::CW;                 // first (i, j) column of this CTA
+    const int row0 = (tsel % ntile) * 128;
+    const int col0 = (tsel / ntile) * S::CW;             // first (i, j) column of this CTA
     const int ncol = min(S::CW, S::P2 - col0);
     const int r0 = a.rng_start[e], r1 = a.rng_start[e + 1];
     int nchunks = 0;
@@ -367,8 +371,9 @@ void launch_c2proxy_tc_p(const C2ProxyArgs& a, const float* src_q, float* up, in
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_c2proxy_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
         configured[dev] = true;
     }
-    const dim3 grid(a.n_centers, (P * kb + 127) / 128, S::NSPLIT);
-    k_c2proxy_tc<P><<<grid, kThreads, S::SMEM, s>>>(a, src_q, up, kb, err);
+    const int64_t nblocks = (int64_t)a.n_centers * ((P * kb + 127) / 128) * S::NSPLIT;
+    if (nblocks > INT32_MAX) throw std::runtime_error("too many proxy-moment tiles for one launch");
+    k_c2proxy_tc<P><<<(unsigned)nblocks, kThreads, S::SMEM, s>>>(a, src_q, up, kb, err);
 }
 
 }  // namespace
@@ -427,9 +432,12 @@ __global__ void __launch_bounds__(kNThreads, 1)
               const float4* __restrict__ src_hi, const float4* __restrict__ src_lo, const float* __restrict__ src_q,
               double* __restrict__ pot, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    const int e = blockIdx.x;
+    // flat grid, leaf-major: the target tiles of one leaf run next to each
+    // other and share its neighbours' sources in L2
+    const int ntile = (a.max_trg + 127) / 128;
+    const int e = blockIdx.x / ntile;
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
-    const int m0 = blockIdx.y * 128;
+    const int m0 = (blockIdx.x % ntile) * 128;
     if (m0 >= nt) return;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kN_OFF_BAR);  // [0,1] stage free, [2,3] segment accumulated
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kN_OFF_BAR + 32);
@@ -758,8 +766,9 @@ void launch_near_tc_nc(const NearTc& a, const float4* th, const float4* tl, cons
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_near_tc<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNSmem));
         configured[dev] = true;
     }
-    const dim3 grid(a.n_leaves, (a.max_trg + 127) / 128);
-    k_near_tc<NC><<<grid, kNThreads, kNSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
+    const int64_t nblocks = (int64_t)a.n_leaves * ((a.max_trg + 127) / 128);
+    if (nblocks > INT32_MAX) throw std::runtime_error("too many near-field tiles for one launch");
+    k_near_tc<NC><<<(unsigned)nblocks, kNThreads, kNSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
 }
 
 }  // namespace
@@ -823,9 +832,12 @@ template <int P, int KB>
 __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restrict__ err) {
     using S = EvShape<P, KB>;
     extern __shared__ __align__(1024) unsigned char sm[];
-    const int e = blockIdx.x;
+    // flat grid, leaf-major: the target tiles of one leaf run next to each
+    // other and share its downward coefficients in L2
+    const int ntile = (a.max_trg + 127) / 128;
+    const int e = blockIdx.x / ntile;
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
-    const int m0 = blockIdx.y * 128;
+    const int m0 = (blockIdx.x % ntile) * 128;
     if (m0 >= nt) return;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);  // [0,1] stage free, [2,3] segment done
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + S::OFF_BAR + 32);
@@ -1050,8 +1062,9 @@ void launch_eval_tc_pk(const EvalTc& a, int* err, cudaStream_t s) {
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_eval_tc<P, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
         configured[dev] = true;
     }
-    const dim3 grid(a.n_leaves, (a.max_trg + 127) / 128);
-    k_eval_tc<P, KB><<<grid, kEThreads, S::SMEM, s>>>(a, err);
+    const int64_t nblocks = (int64_t)a.n_leaves * ((a.max_trg + 127) / 128);
+    if (nblocks > INT32_MAX) throw std::runtime_error("too many leaf-evaluation tiles for one launch");
+    k_eval_tc<P, KB><<<(unsigned)nblocks, kEThreads, S::SMEM, s>>>(a, err);
 }
 
 }  // namespace
