@@ -156,8 +156,8 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                     int64_t kx = (l0[i][0] - lo[0]) / B, ky = (l0[i][1] - lo[1]) / B, kz = (l0[i][2] - lo[2]) / B;
                     key[i] = (kx * 4096 + ky) * 4096 + kz;
                 }
-                std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
             }
+            if (split) std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
             // apply the within-leaf permutation
             std::vector<double> pos_tmp(3 * (size_t)nt);
             std::vector<int> perm_tmp(nt);
@@ -785,6 +785,21 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         nufft_.sub_extent = upload(be);
         nufft_.pt_t = upload(pt_t);
         nufft_.pt_l0 = upload(pt_l0);
+        {
+            // interpolation order: inside each bin, targets by window cell
+            // (x, y, z), stable; the tree keeps its own target order
+            std::vector<int> order(n_);
+            std::iota(order.begin(), order.end(), 0);
+            for (auto& bn : bins) {
+                auto key = [&](int t) {
+                    const int4 l = pt_l0[t];
+                    return (((int64_t)(l.x - bn.org.x) << 20) | ((int64_t)(l.y - bn.org.y) << 10)) + (l.z - bn.org.z);
+                };
+                std::stable_sort(order.begin() + bn.start, order.begin() + bn.start + bn.count,
+                                 [&](int x, int y) { return key(x) < key(y); });
+            }
+            nufft_.interp_order = upload(order);
+        }
         nufft_.q_sorted = q_sorted_;
         nufft_.grid = grid_;
         nufft_.far = far_sorted_;

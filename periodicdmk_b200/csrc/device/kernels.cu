@@ -970,7 +970,8 @@ __global__ void __launch_bounds__(128) k_interp(NufftArgs a) {
     const double hw = 0.5 * W;
     const double* __restrict__ grid = a.grid + blockIdx.z * a.rhs_grid_stride;
     double* __restrict__ far = a.far + blockIdx.z * a.rhs_far_stride;
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    for (int tl = threadIdx.x; tl < nt; tl += blockDim.x) {
+        const int t = (a.interp_order ? a.interp_order[t0 + tl] : t0 + tl) - t0;
         const double4 tt = a.pt_t[t0 + t];
         const int4 l0 = a.pt_l0[t0 + t];
         double kx[W], ky[W], kz[W];

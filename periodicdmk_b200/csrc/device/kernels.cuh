@@ -129,6 +129,10 @@ struct NufftArgs {
     const double* q_sorted;  // per sorted target charge (user charge gathered)
     double* grid;            // n1*n2*n3 real
     double* far;             // per sorted target output
+    // Order in which the interpolation visits the sorted targets: inside each
+    // bin, targets grouped by the grid cell their window starts at, so that
+    // neighbouring threads read the same grid values (null: sorted order).
+    const int* interp_order = nullptr;
     int n1, n2, n3;
     int w;
     double es_beta;

@@ -131,8 +131,9 @@ __global__ void __launch_bounds__(128) k_spread_m(NufftArgs a, const double* __r
 
 template <int W, int CB>
 __global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __restrict__ esw, int64_t n) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+    const int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n) return;
+    const int64_t t = a.interp_order ? a.interp_order[it] : it;
     const int c0 = blockIdx.y * CB;
     const int4 l0 = a.pt_l0[t];
     const double* wt = esw + t * 3 * W;
