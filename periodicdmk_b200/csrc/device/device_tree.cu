@@ -779,6 +779,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             nufft_max_cells_ = std::max(nufft_max_cells_, bn.ext.x * bn.ext.y * bn.ext.z);
         }
         nufft_.n_leaves = (int)bins.size();
+        nufft_.max_cells = nufft_max_cells_;
         nufft_.trg_start = upload(bs);
         nufft_.trg_count = upload(bc);
         nufft_.sub_origin = upload(bo);
@@ -799,6 +800,39 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                                  [&](int x, int y) { return key(x) < key(y); });
             }
             nufft_.interp_order = upload(order);
+            // spreading runs: inside each bin, targets by (y, z, x) window start;
+            // a run = equal (y, z), x offsets within kSpreadRunDx of its first
+            std::vector<int> sorder(n_);
+            std::iota(sorder.begin(), sorder.end(), 0);
+            std::vector<int4> runs;
+            std::vector<int> bin_run{0};
+            for (auto& bn : bins) {
+                auto key = [&](int t) {
+                    const int4 l = pt_l0[t];
+                    return (((int64_t)(l.y - bn.org.y) << 20) | ((int64_t)(l.z - bn.org.z) << 10)) + (l.x - bn.org.x);
+                };
+                std::stable_sort(sorder.begin() + bn.start, sorder.begin() + bn.start + bn.count,
+                                 [&](int x, int y) { return key(x) < key(y); });
+                for (int i = bn.start; i < bn.start + bn.count;) {
+                    const int4 l = pt_l0[sorder[i]];
+                    int j = i;
+                    while (j < bn.start + bn.count) {
+                        const int4 m = pt_l0[sorder[j]];
+                        if (m.y != l.y || m.z != l.z || m.x - l.x > dev::kSpreadRunDx) break;
+                        ++j;
+                    }
+                    check(l.y - bn.org.y >= 0 && l.y - bn.org.y < 0x8000 && l.z - bn.org.z >= 0 &&
+                              l.z - bn.org.z < 0x8000 && l.x >= bn.org.x,
+                          "spreading run offsets");
+                    runs.push_back(make_int4(i, j - i, (l.y - bn.org.y) | ((l.z - bn.org.z) << 16), l.x - bn.org.x));
+                    i = j;
+                }
+                bin_run.push_back((int)runs.size());
+            }
+            if (runs.empty()) runs.push_back(make_int4(0, 0, 0, 0));
+            nufft_.spread_order = upload(sorder);
+            nufft_.spread_run = upload(runs);
+            nufft_.bin_run = upload(bin_run);
         }
         nufft_.q_sorted = q_sorted_;
         nufft_.grid = grid_;

@@ -118,6 +118,7 @@ void launch_desort_parts(const double* pot_sorted, const double* far_sorted, con
                          const double* q_user, double* tree_part, double* far_part, int n, cudaStream_t s);
 
 // ---- NUFFT far field (ES kernel, sigma = 2)
+constexpr int kSpreadRunDx = 4;
 struct NufftArgs {
     int n_leaves;
     const int* trg_start;
@@ -133,6 +134,15 @@ struct NufftArgs {
     // bin, targets grouped by the grid cell their window starts at, so that
     // neighbouring threads read the same grid values (null: sorted order).
     const int* interp_order = nullptr;
+    // Spreading by runs: inside each bin, targets whose windows start at the
+    // same (y, z) cell form a run (ordered by x; x offsets within a run at
+    // most kSpreadRunDx).  run = (first index into spread_order, count,
+    // y | z << 16 relative to the bin origin, smallest x relative to it);
+    // bin e owns runs bin_run[e] .. bin_run[e + 1] - 1.  Null: no run lists.
+    const int4* spread_run = nullptr;
+    const int* bin_run = nullptr;
+    const int* spread_order = nullptr;
+    int max_cells = 0;  // largest bin subgrid (cells)
     int n1, n2, n3;
     int w;
     double es_beta;
