@@ -69,14 +69,34 @@ __global__ void k_split_positions(const double4* __restrict__ in, float4* __rest
     lo[i] = make_float4((float)(p.x - (double)hx), (float)(p.y - (double)hy), (float)(p.z - (double)hz), 0.0f);
 }
 
+// Q (N x kb column-major, user order; RHS c >= kvalid read as zero) ->
+// Qr (N x kb row-major): 32 x 32 tiles through shared memory, coalesced on
+// both sides.  Gathering rows of Qr reads one contiguous kb-vector per source.
+__global__ void k_transpose_q(const double* __restrict__ Q, double* __restrict__ Qr, int64_t N, int kb, int kvalid) {
+    __shared__ double tile[32][33];
+    const int64_t r0 = (int64_t)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int c = c0 + j;
+        const int64_t r = r0 + threadIdx.x;
+        tile[j][threadIdx.x] = (c < kvalid && r < N) ? Q[(int64_t)c * N + r] : 0.0;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t r = r0 + j;
+        const int c = c0 + threadIdx.x;
+        if (r < N && c < kb) Qr[r * kb + c] = tile[threadIdx.x][j];
+    }
+}
+
 template <typename T>
-__global__ void k_gather_src_m(T* __restrict__ src_q, const int* __restrict__ idx, const double* __restrict__ Q,
-                               int64_t n_all, int64_t N, int kb, int kvalid) {
+__global__ void k_gather_src_rows(T* __restrict__ src_q, const int* __restrict__ idx, const double* __restrict__ Qr,
+                                  int64_t n_all, int kb) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_all * kb) return;
     const int64_t s = i / kb;
-    const int c = (int)(i % kb);
-    src_q[i] = c < kvalid ? (T)Q[(int64_t)c * N + idx[s]] : T(0);
+    const int c = (int)(i - s * kb);
+    src_q[i] = (T)Qr[(int64_t)idx[s] * kb + c];
 }
 
 __global__ void k_gather_trg_m(double* __restrict__ q_t, const int* __restrict__ perm, const double* __restrict__ Q,
@@ -991,9 +1011,13 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     PDMK_CUDA_CHECK(cudaMemsetAsync(up, 0, sizeof(T) * std::max<int64_t>(n_up_ * ncoef * kb, 1), s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(down, 0, sizeof(T) * std::max<int64_t>(n_down_ * ncoef * kb, 1), s));
     {
+        // charges to row-major (the far-field output buffer is free until the
+        // interpolation writes it), then one contiguous row per source
         const int64_t tot = (int64_t)n_all_ * kb;
-        dev::k_gather_src_m<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src_q, src_charge_idx_, Q, n_all_, n_, kb,
-                                                                             kvalid); ++nl;
+        const dim3 tgrid((unsigned)((n_ + 31) / 32), (unsigned)((kb + 31) / 32));
+        dev::k_transpose_q<<<tgrid, dim3(32, 8), 0, s>>>(Q, m.far, n_, kb, kvalid); ++nl;
+        dev::k_gather_src_rows<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src_q, src_charge_idx_, m.far, n_all_,
+                                                                                kb); ++nl;
         const int64_t tt = (int64_t)n_ * kb;
         dev::k_gather_trg_m<<<(unsigned)((tt + 255) / 256), 256, 0, s>>>(m.q_t, trg_perm_, Q, n_, kb, kvalid); ++nl;
     }
