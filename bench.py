@@ -7,7 +7,10 @@ Workload (one step = one batched evaluate of 64 charge vectors on a resident tre
   n_per_leaf = 300, nz = 4, mixed-precision path.  The plain FP64 evaluate of
   one charge vector on the same tree is measured beside it.  Synthetic data;
   the trees are built once (untimed), as in the reference's build-once /
-  evaluate-many contract.
+  evaluate-many contract.  Extra fragments of the same JSON line: the
+  many-systems batch (--batch-systems) and the plain FP64 evaluate of a
+  clustered triclinic system of 2e6 points at 9 and 12 digits
+  (--clustered-digits, --clustered-n).
 
 Metric: Mpts*RHS/s = N * RHS / t_evaluate / 1e6 (whole job: summed over ranks).
 
@@ -68,6 +71,74 @@ def batch_systems(nsys, seed):
         pos.append(rng.uniform(0.0, 1.0, (n, 3)) @ cell.T)
         qs.append(q)
     return cells, pos, qs
+
+
+def clustered_system(n, seed=3):
+    """High-accuracy workload: triclinic cell with columns (1,0,0), (0.3,0.9,0),
+    (0.2,0.25,0.85); half the points uniform in fractional coordinates, half
+    from 64 isotropic Gaussian clusters (sigma 0.01 Cartesian, centres uniform
+    in the cell, wrapped back into the cell); +-1 neutral charges."""
+    rng = np.random.default_rng(seed)
+    cell = np.array([[1.0, 0.3, 0.2], [0.0, 0.9, 0.25], [0.0, 0.0, 0.85]])  # columns = lattice vectors
+    inv = np.linalg.inv(cell)
+    nu = n // 2
+    frac_u = rng.uniform(0.0, 1.0, (nu, 3))
+    centres = rng.uniform(0.0, 1.0, (64, 3)) @ cell.T
+    which = rng.integers(0, 64, n - nu)
+    pts = centres[which] + rng.normal(0.0, 0.01, (n - nu, 3))
+    frac_c = (pts @ inv.T) % 1.0
+    pos = np.vstack([frac_u, frac_c]) @ cell.T
+    q = np.ones(n)
+    q[: n // 2] = -1.0
+    rng.shuffle(q)
+    return cell, pos, q
+
+
+def run_clustered(pd, args, world, dev, flush, barrier, max_over_ranks):
+    """Plain FP64 evaluate of the clustered triclinic workload at each digit
+    count of --clustered-digits (device-resident charges, L2 flushed, CUDA-event
+    stage times); the highest digit count is the accuracy reference."""
+    import torch
+    digits = [int(x) for x in args.clustered_digits.split(",") if x.strip()]
+    n = args.clustered_n
+    cell, pos, q = clustered_system(n)
+    q_d = torch.from_numpy(q).to(dev)
+    pot_d = torch.empty(n, dtype=torch.float64, device=dev)
+    out = {"workload": "triclinic cell (1,0,0),(0.3,0.9,0),(0.2,0.25,0.85); N=%d, 50%% fractional-uniform, "
+                       "50%% in 64 Gaussian clusters (sigma 0.01), +-1 charges; npl 300, nz 4; plain FP64 "
+                       "evaluate, one charge vector" % n,
+           "n_points": n, "digits": {}}
+    pots = {}
+    for nd in digits:
+        t0 = time.perf_counter()
+        tree = pd.PeriodicDMKTree(cell, pos, n_digits=nd, n_per_leaf=300, nz=4, precision="double")
+        tb = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            tree.evaluate_device(q_d.data_ptr(), pot_d.data_ptr())
+        torch.cuda.synchronize()
+        st = []
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            tree.evaluate_device(q_d.data_ptr(), pot_d.data_ptr())
+            st.append(tree.stage_times())
+        torch.cuda.synchronize()
+        barrier()
+        t = max_over_ranks(sum(x["total_ms"] for x in st) / 1e3) / args.steps
+        info = tree.info()
+        out["digits"][str(nd)] = {
+            "ms_per_evaluate": t * 1e3, "value": world * n / t / 1e6, "unit": "Mpts/s",
+            "stage_ms_median": {kk: statistics.median(x[kk] for x in st)
+                                for kk in ("dmk_ms", "near_ms", "nufft_ms", "total_ms")},
+            "device_bytes": info["device_bytes"], "tree_build_s": tb, "p": info["p"], "n_pw": info["n_pw"]}
+        pots[nd] = pot_d.cpu().numpy()
+        tree.close()
+    if len(pots) > 1:
+        ref = pots[max(pots)]
+        out["rel_l2_vs_highest_digits"] = {str(nd): float(np.linalg.norm(v - ref) / np.linalg.norm(ref))
+                                           for nd, v in pots.items() if nd != max(pots)}
+    return out
 
 
 def lpt_partition(costs, parts):
@@ -372,6 +443,8 @@ def run_ours(args):
     tree_f.close()
     if args.batch_systems > 0:
         line["batch"] = run_batch(pd, args, world, rank, barrier, max_over_ranks)
+    if args.clustered_digits.strip():
+        line["clustered_triclinic"] = run_clustered(pd, args, world, dev, flush, barrier, max_over_ranks)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, desc, _ = cpu_baseline(n, 3, threads)
@@ -395,6 +468,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="systems of the many-systems measurement (0 skips it)")
+    ap.add_argument("--clustered-digits", default="9,12",
+                    help="digit counts of the clustered triclinic FP64 measurement ('' skips it)")
+    ap.add_argument("--clustered-n", type=int, default=2000000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
