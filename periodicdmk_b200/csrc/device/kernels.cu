@@ -671,13 +671,154 @@ __global__ void __launch_bounds__(128) k_eval(EvalArgs a) {
     }
 }
 
+// Large orders, register-tiled: per leaf, D[t][(j,k)] = sum_i T_i(x_t) C[i,(j,k)]
+// is a small GEMM.  Warp w takes 4 targets of the 32-target pass, lane l the 4
+// columns (j,k) = cbase + 4 l .. +3 of the 128-column pass: per i it loads 4
+// x-values (broadcast) and 4 coefficients, then does 16 multiply-adds.  The
+// y and z factors are applied per column, and the 32 lanes' partial sums of
+// a target are added by a warp reduction.
+template <int P>
+__global__ void __launch_bounds__(256) k_eval_tiled(EvalArgs a) {
+    constexpr int TT = 4, TC = 4, NW = 8;
+    constexpr int TB = NW * TT;   // targets per pass
+    constexpr int CB = 32 * TC;   // columns per pass
+    constexpr int LDC = CB + 2;   // padded row (16-byte aligned rows, fewer bank conflicts on the fill)
+    constexpr int P2 = P * P;
+    extern __shared__ __align__(16) unsigned char smem_ev[];
+    // two coefficient tiles [P][LDC] (the next column pass loads while this one computes)
+    auto sCb = reinterpret_cast<double(*)[LDC]>(smem_ev);
+    auto sX = reinterpret_cast<double(*)[TB]>(smem_ev + sizeof(double) * 2 * P * LDC);           // [P][TB]
+    auto sY = reinterpret_cast<double(*)[P + 1]>(smem_ev + sizeof(double) * P * (2 * LDC + TB));  // [TB][P + 1]
+    auto sZ = sY + TB;                                                                             // [TB][P + 1]
+    const int e = blockIdx.x;
+    const int t0 = a.trg_start[e], nt = a.trg_count[e];
+    const double4 cs = a.center_scale[e];
+    const double* C = a.proxy_down + (int64_t)a.slot[e] * (P * P * P);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // asynchronous fill of the column pass starting at cbase into tile buf
+    auto fill = [&](int buf, int cbase) {
+        const int ncol = min(CB, P2 - cbase);
+        const double* Cb = C + (int64_t)P * cbase;
+        double(*sC)[LDC] = sCb + buf * P;
+        for (int idx = threadIdx.x; idx < P * CB; idx += blockDim.x) {
+            const int c = idx / P, i = idx - c * P;
+            if (c < ncol)
+                cp_async_elem<8>(&sC[i][c], Cb + idx);
+            else
+                sC[i][c] = 0.0;
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    for (int tbase = 0; tbase < nt; tbase += TB) {
+        __syncthreads();
+        if (tid < TB) {
+            const int t = tbase + tid;
+            double x = 0.0, y = 0.0, z = 0.0;
+            const bool act = t < nt;
+            if (act) {
+                const double4 pt = a.trg[t0 + t];
+                x = (pt.x - cs.x) * cs.w;
+                y = (pt.y - cs.y) * cs.w;
+                z = (pt.z - cs.z) * cs.w;
+            }
+            double x0 = 1.0, x1 = x, y0 = 1.0, y1 = y, z0 = 1.0, z1 = z;
+            const double m = act ? 1.0 : 0.0;  // inactive targets: all-zero rows
+            sX[0][tid] = m;
+            sY[tid][0] = 1.0;
+            sZ[tid][0] = 1.0;
+            if (P > 1) {
+                sX[1][tid] = m * x;
+                sY[tid][1] = y;
+                sZ[tid][1] = z;
+            }
+#pragma unroll 4
+            for (int n = 2; n < P; ++n) {
+                const double x2 = 2.0 * x * x1 - x0, y2 = 2.0 * y * y1 - y0, z2 = 2.0 * z * z1 - z0;
+                sX[n][tid] = m * x2;
+                sY[tid][n] = y2;
+                sZ[tid][n] = z2;
+                x0 = x1;
+                x1 = x2;
+                y0 = y1;
+                y1 = y2;
+                z0 = z1;
+                z1 = z2;
+            }
+        }
+        double part[TT];
+#pragma unroll
+        for (int q = 0; q < TT; ++q) part[q] = 0.0;
+        __syncthreads();  // previous target pass done with both tiles
+        fill(0, 0);
+        for (int pass = 0, cbase = 0; cbase < P2; ++pass, cbase += CB) {
+            if (cbase + CB < P2) {
+                fill((pass + 1) & 1, cbase + CB);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+            __syncthreads();  // this pass's tile (and the Chebyshev rows) visible to all
+            double(*sC)[LDC] = sCb + (pass & 1) * P;
+            double d[TT][TC];
+#pragma unroll
+            for (int q = 0; q < TT; ++q)
+#pragma unroll
+                for (int r = 0; r < TC; ++r) d[q][r] = 0.0;
+#pragma unroll 2
+            for (int i = 0; i < P; ++i) {
+                const double2 xa = *reinterpret_cast<const double2*>(&sX[i][w * TT]);
+                const double2 xb = *reinterpret_cast<const double2*>(&sX[i][w * TT + 2]);
+                const double2 ca = *reinterpret_cast<const double2*>(&sC[i][lane * TC]);
+                const double2 cb = *reinterpret_cast<const double2*>(&sC[i][lane * TC + 2]);
+                const double xv[TT] = {xa.x, xa.y, xb.x, xb.y};
+                const double cv[TC] = {ca.x, ca.y, cb.x, cb.y};
+#pragma unroll
+                for (int q = 0; q < TT; ++q)
+#pragma unroll
+                    for (int r = 0; r < TC; ++r) d[q][r] = fma(xv[q], cv[r], d[q][r]);
+            }
+#pragma unroll
+            for (int r = 0; r < TC; ++r) {
+                const int col = cbase + lane * TC + r;
+                if (col >= P2) break;
+                const int j = col % P, k = col / P;
+#pragma unroll
+                for (int q = 0; q < TT; ++q) part[q] = fma(d[q][r], sY[w * TT + q][j] * sZ[w * TT + q][k], part[q]);
+            }
+            __syncthreads();  // every warp done with this tile before it is refilled
+        }
+#pragma unroll
+        for (int q = 0; q < TT; ++q) {
+            double v = part[q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            const int t = tbase + w * TT + q;
+            if (lane == 0 && t < nt) a.pot[t0 + t] += v;
+        }
+    }
+}
+
+template <int P>
+static void launch_eval_tiled(const EvalArgs& a, cudaStream_t s) {
+    constexpr int TB = 32, LDC = 130;
+    constexpr size_t smem = sizeof(double) * ((size_t)P * (2 * LDC + TB) + 2 * (size_t)TB * (P + 1));
+    static bool configured[64] = {};
+    int dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_eval_tiled<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured[dev] = true;
+    }
+    k_eval_tiled<P><<<a.n_leaves, 256, smem, s>>>(a);
+}
+
 void launch_eval(const EvalArgs& a, int p, cudaStream_t s) {
     if (a.n_leaves <= 0) return;
     switch (p) {
         case 9: k_eval<9><<<a.n_leaves, 128, 0, s>>>(a); break;
         case 18: k_eval<18><<<a.n_leaves, 128, 0, s>>>(a); break;
-        case 28: k_eval<28><<<a.n_leaves, 128, 0, s>>>(a); break;
-        case 38: k_eval<38><<<a.n_leaves, 128, 0, s>>>(a); break;
+        case 28: launch_eval_tiled<28>(a, s); break;
+        case 38: launch_eval_tiled<38>(a, s); break;
         default: throw std::runtime_error("unsupported expansion order");
     }
 }
