@@ -234,6 +234,60 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     // Skipping the rest changes no arithmetic on the expansions that are read.
     std::vector<int64_t> up_slot(P.nboxes, -1), down_slot(P.nboxes, -1), pw_slot(P.nboxes, -1);
     std::vector<char> incoming(P.nboxes, 0), leaf_eval(P.nboxes, 0);
+    // Image boxes that are exact lattice translates of an original box of the
+    // same level: every source is the image of a source of that box under one
+    // lattice vector D, the counts agree and the centres differ by D.  Proxy
+    // moments and outgoing expansions are taken about the box centre, so such
+    // a box shares the original's (they differ only by the rounding of the
+    // image positions); it gets no storage and no work of its own.  With a
+    // cell whose lattice vectors are multiples of the box size (cubes) this
+    // covers every image-only box; triclinic images straddle boxes and none
+    // qualify.
+    std::vector<int> alias(P.nboxes, -1);
+    {
+        std::vector<int> orig_of(n_, -1);
+        std::vector<double> disp(3 * (size_t)n_all_);
+        std::vector<char> is_orig(n_all_, 0);
+        for (int s = 0; s < n_all_; ++s) {
+            const int q = P.src_charge_idx[s];
+            double m = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                disp[3 * (size_t)s + d] = P.src_sorted[3 * (size_t)s + d] - P.r_user[3 * (size_t)q + d];
+                m = std::max(m, std::abs(disp[3 * (size_t)s + d]));
+            }
+            if (m <= 1e-12) {
+                is_orig[s] = 1;
+                orig_of[q] = s;
+            }
+        }
+        std::vector<int> box_at(n_all_, -1);
+        for (int l = 0; l < P.nlevels; ++l) {
+            for (int b : P.level_boxes[l])
+                for (int s = P.src_start[b]; s < P.src_start[b] + P.src_count[b]; ++s) box_at[s] = b;
+            for (int b : P.level_boxes[l]) {
+                const int s0 = P.src_start[b], ns = P.src_count[b];
+                if (ns <= 0) continue;
+                const double* D = &disp[3 * (size_t)s0];
+                bool ok = !is_orig[s0];
+                const int o0 = orig_of[P.src_charge_idx[s0]];
+                const int B = o0 >= 0 ? box_at[o0] : -1;
+                ok = ok && B >= 0 && B != b && P.depth[B] == l && P.src_count[B] == ns;
+                for (int s = s0; s < s0 + ns && ok; ++s) {
+                    const int o = orig_of[P.src_charge_idx[s]];
+                    ok = !is_orig[s] && o >= 0 && box_at[o] == B;
+                    for (int d = 0; d < 3 && ok; ++d)
+                        ok = std::abs(disp[3 * (size_t)s + d] - D[d]) <= 1e-9 * (1.0 + std::abs(D[d]));
+                }
+                for (int d = 0; d < 3 && ok; ++d)
+                    ok = std::abs(P.centers[3 * b + d] - P.centers[3 * B + d] - D[d]) <= 1e-9 * (1.0 + std::abs(D[d]));
+                if (ok) alias[b] = B;
+            }
+            // box_at of this level's sources is overwritten by the next level
+            for (int b : P.level_boxes[l])
+                for (int s = P.src_start[b]; s < P.src_start[b] + P.src_count[b]; ++s) box_at[s] = -1;
+        }
+        for (int b = 0; b < P.nboxes; ++b) n_alias_ += alias[b] >= 0;
+    }
     {
         std::vector<char> need_pw(P.nboxes, 0), need_up(P.nboxes, 0);
         for (int b = 0; b < P.nboxes; ++b) {
@@ -251,22 +305,39 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                 need_pw[nb] = 1;
             }
         }
+        // a translate's plane waves are its original's
+        for (int b = 0; b < P.nboxes; ++b)
+            if (need_pw[b] && alias[b] >= 0) need_pw[alias[b]] = 1;
         // top-down: a box's proxy_up is read by its own outgoing transform or
-        // through the translation into a parent whose proxy_up is read
-        for (int l = 0; l < P.nlevels; ++l)
+        // through the translation into a parent whose proxy_up is read (and
+        // formed here: a translate parent borrows its original's)
+        for (int l = 0; l < P.nlevels; ++l) {
             for (int b : P.level_boxes[l]) {
                 const int par = P.parent[b];
-                const bool via = par >= 0 && need_up[par] && P.has_proxy_from_children[par] && P.src_count[b] > 0 &&
-                                 P.ifpwexp[b];
+                const bool via = par >= 0 && need_up[par] && alias[par] < 0 && P.has_proxy_from_children[par] &&
+                                 P.src_count[b] > 0 && P.ifpwexp[b];
                 need_up[b] = need_pw[b] || via;
-                if (need_up[b]) check(P.proxy_up_off[b] >= 0, "proxy_up storage");
             }
-        for (int l = 0; l < P.nlevels; ++l)
+            for (int b : P.level_boxes[l])
+                if (need_up[b] && alias[b] >= 0) need_up[alias[b]] = 1;
+            for (int b : P.level_boxes[l])
+                if (need_up[b]) check(P.proxy_up_off[b] >= 0, "proxy_up storage");
+        }
+        for (int l = 0; l < P.nlevels; ++l) {
             for (int b : P.level_boxes[l]) {
+                if (alias[b] >= 0) continue;
                 if (need_up[b]) up_slot[b] = n_up_++;
                 if (need_pw[b]) pw_slot[b] = n_pw_++;
-                if (incoming[b] || leaf_eval[b]) down_slot[b] = n_down_++;
             }
+            for (int b : P.level_boxes[l]) {
+                if (alias[b] < 0) continue;
+                if (need_up[b]) up_slot[b] = up_slot[alias[b]];
+                if (need_pw[b]) pw_slot[b] = pw_slot[alias[b]];
+                check((!need_up[b] || up_slot[b] >= 0) && (!need_pw[b] || pw_slot[b] >= 0), "translate storage");
+            }
+            for (int b : P.level_boxes[l])
+                if (incoming[b] || leaf_eval[b]) down_slot[b] = n_down_++;
+        }
     }
 
     // ------------------------------------------------------------------ tables
@@ -310,7 +381,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         std::vector<int> slot, rng{0}, s0, sc;
         std::vector<double4> cs;
         for (int b = 0; b < P.nboxes; ++b) {
-            if (by_center[b].empty() || up_slot[b] < 0) continue;
+            if (by_center[b].empty() || up_slot[b] < 0 || alias[b] >= 0) continue;
             slot.push_back((int)up_slot[b]);
             const int lvl = P.c2proxy_work[by_center[b][0]].level;
             cs.push_back(make_double4(P.centers[3 * b], P.centers[3 * b + 1], P.centers[3 * b + 2], 2.0 / P.boxsize[lvl]));
@@ -339,7 +410,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         for (int c = 0; c < 8; ++c) {
             std::vector<int64_t> in, out;
             for (int b : P.level_boxes[l]) {
-                if (!P.has_proxy_from_children[b] || up_slot[b] < 0) continue;
+                if (!P.has_proxy_from_children[b] || up_slot[b] < 0 || alias[b] >= 0) continue;
                 const int ch = P.children[b][c];
                 if (ch < 0 || !(P.src_count[ch] > 0 && P.ifpwexp[ch])) continue;
                 check(up_slot[ch] >= 0, "c2p offsets");
@@ -359,7 +430,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     for (int l = 0; l < P.nlevels; ++l) {
         std::vector<int64_t> in, out;
         for (int b : P.level_boxes[l]) {
-            if (pw_slot[b] < 0) continue;
+            if (pw_slot[b] < 0 || alias[b] >= 0) continue;
             check(up_slot[b] >= 0, "pw box without proxy");
             in.push_back(up_slot[b] * ncoef);
             out.push_back(pw_slot[b] * M);
@@ -462,8 +533,10 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             for (int b : P.level_boxes[l]) {
                 check(P.depth[b] == l, "level box depth");
                 if (down_slot[b] >= 0) loc_down[b] = nd++;
-                if (pw_slot[b] >= 0) loc_pw[b] = np++;
+                if (pw_slot[b] >= 0 && alias[b] < 0) loc_pw[b] = np++;
             }
+            for (int b : P.level_boxes[l])
+                if (pw_slot[b] >= 0 && alias[b] >= 0) loc_pw[b] = loc_pw[alias[b]];
             f64_levels_[l].level = l;
             f64_levels_[l].n_down = nd;
             down_level_boxes_[l & 1] = std::max(down_level_boxes_[l & 1], nd);
@@ -474,7 +547,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             const double bs = P.boxsize[l];
             std::vector<int64_t> pin, pout;
             for (int b : P.level_boxes[l]) {
-                if (pw_slot[b] < 0) continue;
+                if (pw_slot[b] < 0 || alias[b] >= 0) continue;
                 pin.push_back(up_slot[b] * ncoef);
                 pout.push_back(loc_pw[b] * M);
             }

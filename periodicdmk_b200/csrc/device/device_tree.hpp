@@ -158,6 +158,7 @@ class DeviceTree {
     // expansions
     double* proxy_up_ = nullptr;
     int64_t n_up_ = 0, n_down_ = 0, n_pw_ = 0;
+    int64_t n_alias_ = 0;  // image boxes sharing an original box's expansions (exact lattice translates)
     // tables
     double* c2p_ = nullptr;
     double* p2c_ = nullptr;
