@@ -854,6 +854,7 @@ struct DeviceTree::MultiState {
     float4 *src_hi = nullptr, *src_lo = nullptr, *trg_hi = nullptr, *trg_lo = nullptr;
     int* err = nullptr;  // set by tensor-core kernels whose pipeline wait timed out
     double* esw = nullptr;  // NUFFT spreading weights per sorted target (3 x W)
+    float* esw32 = nullptr;  // the same in float (mixed-precision state: spreading)
 
     template <typename T>
     T* alloc(size_t n) {
@@ -937,6 +938,10 @@ DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
     PDMK_CUDA_CHECK(cudaMemsetAsync(m->err, 0, sizeof(int), stream_));
     m->esw = m->alloc<double>((size_t)n_ * 3 * nufft_.w);
     dev::launch_es_weights(nufft_, n_, m->esw, stream_);
+    if (fp32) {
+        m->esw32 = m->alloc<float>((size_t)n_ * 3 * nufft_.w);
+        dev::launch_to_float(m->esw, m->esw32, (int64_t)n_ * 3 * nufft_.w, stream_);
+    }
     m->spec = m->alloc<cd>((size_t)(n_spec_ * kb));
     {
         int dims[3] = {nufft_.n1, nufft_.n2, nufft_.n3};
@@ -1226,7 +1231,13 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         na.rhs_grid_stride = n_grid_;
         na.rhs_far_stride = n_;
         PDMK_CUDA_CHECK(cudaMemsetAsync(m.grid, 0, sizeof(double) * n_grid_ * kb, s));
-        dev::launch_spread_multi(na, m.esw, nufft_max_jk_, nufft_max_ex_, kb, s); ++nl;
+        // mixed precision: spreading with single-precision taps and partial
+        // sums into the FP64 grid; transforms and interpolation stay FP64
+        // (single-precision interpolation sums lost accuracy for no speed)
+        bool spread32 = false;
+        if constexpr (f32) spread32 = dev::launch_spread_multi_f32(na, m.esw32, kb, s);
+        if (!spread32) dev::launch_spread_multi(na, m.esw, nufft_max_jk_, nufft_max_ex_, kb, s);
+        ++nl;
         if (cufftExecD2Z(m.fwd, m.grid, reinterpret_cast<cufftDoubleComplex*>(m.spec)) != CUFFT_SUCCESS)
             throw std::runtime_error("cuFFT error in the batched forward transform");
         dev::launch_multiply(m.spec, mult_, n_spec_, s, kb); ++nl;

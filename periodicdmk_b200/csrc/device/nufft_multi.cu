@@ -136,40 +136,43 @@ __global__ void __launch_bounds__(128) k_spread_m(NufftArgs a, const double* __r
 // register window), then adds them to the bin subgrid in shared memory; at
 // the end the subgrid is added to the global grid.  Every multiply-add
 // belongs to a (target, tap) pair.
-template <int W, int CB, int XO>
-__device__ __forceinline__ void spread_run_add(double (&acc)[W + kSpreadRunDx][CB], const double* __restrict__ wx,
-                                               const double (&f)[CB]) {
+template <int W, int CB, int XO, typename TW>
+__device__ __forceinline__ void spread_run_add(TW (&acc)[W + kSpreadRunDx][CB], const TW* __restrict__ wx,
+                                               const TW (&f)[CB]) {
 #pragma unroll
     for (int ia = 0; ia < W; ++ia) {
-        const double w = wx[ia];
+        const TW w = wx[ia];
 #pragma unroll
         for (int c = 0; c < CB; ++c) acc[XO + ia][c] = fma(f[c], w, acc[XO + ia][c]);
     }
 }
 
-template <int W, int CB>
-__global__ void __launch_bounds__((W * W + 31) / 32 * 32) k_spread_r(NufftArgs a, const double* __restrict__ esw) {
+// TW: type of the weights, the run accumulators and the bin subgrid (double,
+// or float in the mixed-precision path); the global grid stays FP64.
+template <int W, int CB, typename TW>
+__global__ void __launch_bounds__((W * W + 31) / 32 * 32) k_spread_r(NufftArgs a, const TW* __restrict__ esw) {
     constexpr int NXR = W + kSpreadRunDx;
     constexpr int TS = 32;                  // targets staged at a time
     constexpr int NT = (W * W + 31) / 32 * 32;
-    __shared__ double sW[TS][3 * W];        // weights of the staged targets
-    __shared__ double sQ[TS][CB];           // their charges
+    __shared__ TW sW[TS][3 * W];            // weights of the staged targets
+    __shared__ TW sQ[TS][CB];               // their charges
     __shared__ int sXo[TS];                 // their x offset in the run
-    extern __shared__ double sub[];         // [c][x][y][z] over the bin's extents
+    extern __shared__ __align__(16) unsigned char sub_raw[];
+    TW* sub = reinterpret_cast<TW*>(sub_raw);  // [c][x][y][z] over the bin's extents
     const int e = blockIdx.x;
     const int c0 = blockIdx.y * CB;
     const int4 org = a.sub_origin[e], ext = a.sub_extent[e];
     const int ncell = ext.x * ext.y * ext.z;
-    for (int i = threadIdx.x; i < ncell * CB; i += NT) sub[i] = 0.0;
+    for (int i = threadIdx.x; i < ncell * CB; i += NT) sub[i] = TW(0);
     const bool active = threadIdx.x < W * W;
     const int dy = threadIdx.x / W, dz = threadIdx.x % W;
     for (int r = a.bin_run[e]; r < a.bin_run[e + 1]; ++r) {
         const int4 R = a.spread_run[r];
-        double acc[NXR][CB];
+        TW acc[NXR][CB];
 #pragma unroll
         for (int i = 0; i < NXR; ++i)
 #pragma unroll
-            for (int c = 0; c < CB; ++c) acc[i][c] = 0.0;
+            for (int c = 0; c < CB; ++c) acc[i][c] = TW(0);
         for (int base = 0; base < R.y; base += TS) {
             const int m = min(TS, R.y - base);
             __syncthreads();  // previous chunk (or subgrid flush) done
@@ -181,22 +184,22 @@ __global__ void __launch_bounds__((W * W + 31) / 32 * 32) k_spread_r(NufftArgs a
             for (int i = threadIdx.x; i < m * CB; i += NT) {
                 const int k = i / CB, c = i - k * CB;
                 const int t = a.spread_order[R.x + base + k];
-                sQ[k][c] = a.q_sorted[(int64_t)(c0 + c) * a.rhs_q_stride + t];
+                sQ[k][c] = (TW)a.q_sorted[(int64_t)(c0 + c) * a.rhs_q_stride + t];
             }
             for (int k = threadIdx.x; k < m; k += NT) sXo[k] = a.pt_l0[a.spread_order[R.x + base + k]].x - org.x - R.w;
             __syncthreads();
             if (active) {
                 for (int k = 0; k < m; ++k) {
-                    const double wyz = sW[k][W + dy] * sW[k][2 * W + dz];
-                    double f[CB];
+                    const TW wyz = sW[k][W + dy] * sW[k][2 * W + dz];
+                    TW f[CB];
 #pragma unroll
                     for (int c = 0; c < CB; ++c) f[c] = wyz * sQ[k][c];
                     switch (sXo[k]) {
-                        case 0: spread_run_add<W, CB, 0>(acc, sW[k], f); break;
-                        case 1: spread_run_add<W, CB, 1>(acc, sW[k], f); break;
-                        case 2: spread_run_add<W, CB, 2>(acc, sW[k], f); break;
-                        case 3: spread_run_add<W, CB, 3>(acc, sW[k], f); break;
-                        default: spread_run_add<W, CB, 4>(acc, sW[k], f); break;
+                        case 0: spread_run_add<W, CB, 0, TW>(acc, sW[k], f); break;
+                        case 1: spread_run_add<W, CB, 1, TW>(acc, sW[k], f); break;
+                        case 2: spread_run_add<W, CB, 2, TW>(acc, sW[k], f); break;
+                        case 3: spread_run_add<W, CB, 3, TW>(acc, sW[k], f); break;
+                        default: spread_run_add<W, CB, 4, TW>(acc, sW[k], f); break;
                     }
                 }
             }
@@ -215,7 +218,7 @@ __global__ void __launch_bounds__((W * W + 31) / 32 * 32) k_spread_r(NufftArgs a
     }
     __syncthreads();
     for (int i = threadIdx.x; i < ncell * CB; i += NT) {
-        const double v = sub[i];
+        const double v = (double)sub[i];
         if (v == 0.0) continue;
         const int c = i / ncell, cell = i - c * ncell;
         const int x = cell / (ext.y * ext.z), yz = cell - x * (ext.y * ext.z);
@@ -271,21 +274,25 @@ __global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __r
 
 constexpr size_t kSpreadRunSmem = 100 * 1024;
 
+template <int W, typename TW>
+bool spread_run_w(const NufftArgs& a, const TW* esw, int nrhs, cudaStream_t s) {
+    if (!(a.spread_run && nrhs % 4 == 0 && (size_t)a.max_cells * 4 * sizeof(TW) <= kSpreadRunSmem)) return false;
+    static bool configured[64] = {};
+    int dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_spread_r<W, 4, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSpreadRunSmem));
+        configured[dev] = true;
+    }
+    const size_t smem = (size_t)a.max_cells * 4 * sizeof(TW);
+    k_spread_r<W, 4, TW><<<dim3(a.n_leaves, nrhs / 4), (W * W + 31) / 32 * 32, smem, s>>>(a, esw);
+    return true;
+}
+
 template <int W>
 void spread_w(const NufftArgs& a, const double* esw, int max_jk, int max_ex, int nrhs, cudaStream_t s) {
-    if (a.spread_run && nrhs % 4 == 0 && (size_t)a.max_cells * 4 * sizeof(double) <= kSpreadRunSmem) {
-        static bool configured[64] = {};
-        int dev = 0;
-        PDMK_CUDA_CHECK(cudaGetDevice(&dev));
-        if (dev >= 0 && dev < 64 && !configured[dev]) {
-            PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_spread_r<W, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)kSpreadRunSmem));
-            configured[dev] = true;
-        }
-        const size_t smem = (size_t)a.max_cells * 4 * sizeof(double);
-        k_spread_r<W, 4><<<dim3(a.n_leaves, nrhs / 4), (W * W + 31) / 32 * 32, smem, s>>>(a, esw);
-        return;
-    }
+    if (spread_run_w<W, double>(a, esw, nrhs, s)) return;
     const int yb = (max_jk + 127) / 128;
     if (max_ex <= 12) {
         if (nrhs % 4 == 0) {
@@ -359,6 +366,15 @@ void launch_interp_multi(const NufftArgs& a, const double* esw, int64_t n, int n
 #define PDMK_INW(W) interp_w<W>(a, esw, n, nrhs, s)
     PDMK_NUFFT_W_SWITCH(a.w, PDMK_INW)
 #undef PDMK_INW
+}
+
+bool launch_spread_multi_f32(const NufftArgs& a, const float* esw32, int nrhs, cudaStream_t s) {
+    if (a.n_leaves <= 0 || nrhs <= 0) return true;
+    bool done = false;
+#define PDMK_SPF(W) done = spread_run_w<W, float>(a, esw32, nrhs, s)
+    PDMK_NUFFT_W_SWITCH(a.w, PDMK_SPF)
+#undef PDMK_SPF
+    return done;
 }
 
 #undef PDMK_NUFFT_W_SWITCH

@@ -13,6 +13,9 @@ void launch_es_weights(const NufftArgs& a, int64_t n, double* w, cudaStream_t s)
 void launch_spread_multi(const NufftArgs& a, const double* esw, int max_jk, int max_ex, int nrhs, cudaStream_t s);
 // far[c][t] = interpolation of grid[c] at sorted target t, c < nrhs
 void launch_interp_multi(const NufftArgs& a, const double* esw, int64_t n, int nrhs, cudaStream_t s);
+// Spreading with single-precision weights and partial sums into the FP64
+// grid (mixed-precision path); false: not applicable, use launch_spread_multi.
+bool launch_spread_multi_f32(const NufftArgs& a, const float* esw32, int nrhs, cudaStream_t s);
 
 }  // namespace dev
 }  // namespace pdmkb
