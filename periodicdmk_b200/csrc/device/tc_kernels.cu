@@ -788,23 +788,26 @@ bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4*
 
 // ===========================================================================
 // Leaf evaluation on the tensor cores.  Rows (l, c) of the proxy coefficients
-// are processed in passes of up to 256 (whole l values); K = (i, j) in chunks
-// of 16.  The A operand (T_i(x) T_j(y) of the tile's targets) is regenerated
-// per pass from tables in shared memory; B is loaded from the coefficients and
-// split.  Every kESeg chunks the accumulator (two alternating 256-column
-// buffers) is folded with T_l(z) into per-target FP32 sums of the kb RHS by all
-// eight warps (lane quarter = targets, half = l range), so no tensor-memory
-// accumulation runs over more than a few MMA steps.
+// are processed in passes of up to kEN = 128 (whole l values); K = (i, j) in
+// chunks of 16.  The A operand (T_i(x) T_j(y) of the tile's targets) is
+// regenerated per pass from tables in shared memory; B is loaded from the
+// coefficients and split.  Every kESeg chunks the accumulator (two alternating
+// 128-column buffers) is folded with T_l(z) into per-target FP32 sums of the kb
+// RHS by all eight warps (lane quarter = targets, half = l range), so no
+// tensor-memory accumulation runs over more than a few MMA steps.  A CTA takes
+// 256 tensor-memory columns and under 100 KB of shared memory, so two CTAs share
+// an SM (16 warps: the operand generation is latency-bound with 8).
 // ===========================================================================
 namespace {
 
 constexpr int kEKC = 16;
 constexpr int kEKCH = kEKC / 4;
+constexpr int kEN = 128;  // accumulator columns of one buffer (MMA N)
 constexpr int kESeg = 4;
 constexpr int kEThreads = 256;
 constexpr int kESBO = kEKCH * 128;
 constexpr int kEA = 128 * kEKC * 4;
-constexpr int kEB = 256 * kEKC * 4;
+constexpr int kEB = kEN * kEKC * 4;
 constexpr int kE_OFF_AH = 0, kE_OFF_AL = kEA, kE_OFF_BH = 2 * kEA, kE_OFF_BL = 2 * kEA + kEB;
 constexpr int kEStage = 2 * kEA + 2 * kEB;
 
@@ -813,7 +816,7 @@ struct EvShape {
     static constexpr int P2 = P * P;
     static constexpr int P3 = P * P * P;
     static constexpr int NKC = (P2 + kEKC - 1) / kEKC;
-    static constexpr int LP = (256 / KB) < P ? (256 / KB) : P;  // l values per pass
+    static constexpr int LP = (kEN / KB) < P ? (kEN / KB) : P;  // l values per pass
     static constexpr int NPASS = (P + LP - 1) / LP;
     static constexpr int NSEGP = (NKC + kESeg - 1) / kESeg;     // segments per pass
     static constexpr int TSTR = P | 1;  // odd row stride of the T tables (bank spread)
@@ -821,15 +824,15 @@ struct EvShape {
     static constexpr int T_BYTES = 3 * 128 * TSTR * 4;
     static constexpr int OFF_BAR = (OFF_T + T_BYTES + 15) / 16 * 16;
     static constexpr int SMEM_USED = OFF_BAR + 64;
-    static constexpr int SMEM = SMEM_USED < 120 * 1024 ? 120 * 1024 : SMEM_USED;  // one CTA per SM (512 TMEM cols)
-    static constexpr int B_ITEMS = 256 * kEKCH / kEThreads;
+    static constexpr int SMEM = SMEM_USED;  // two CTAs per SM (2 x 256 TMEM columns)
+    static constexpr int B_ITEMS = kEN * kEKCH / kEThreads;
     static_assert(SMEM <= 227 * 1024, "eval smem");
     static_assert(KB % 16 == 0 && KB <= 64, "RHS block");
     static_assert(128 * KB * 4 <= kEStage, "half-sum exchange buffer");
 };
 
 template <int P, int KB>
-__global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restrict__ err) {
+__global__ void __launch_bounds__(kEThreads, 2) k_eval_tc(EvalTc a, int* __restrict__ err) {
     using S = EvShape<P, KB>;
     extern __shared__ __align__(1024) unsigned char sm[];
     // flat grid, leaf-major: the target tiles of one leaf run next to each
@@ -846,7 +849,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     if (warp == 0) {
-        tc::tmem_alloc(s_tmem, 512);
+        tc::tmem_alloc(s_tmem, 2 * kEN);
         tc::tmem_relinquish();
     }
     if (tid == 0) {
@@ -936,7 +939,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
         const int hl = (nl + 1) / 2;
         const int lb = dh * hl, le = min(nl, lb + hl);
         const float* Tz = sT + (2 * 128 + dq * 32 + lane) * S::TSTR;
-        const uint32_t lane_base = tmem + ((uint32_t)(dq * 32) << 16) + (uint32_t)((gg & 1) * 256);
+        const uint32_t lane_base = tmem + ((uint32_t)(dq * 32) << 16) + (uint32_t)((gg & 1) * kEN);
         for (int li = lb; li < le; ++li) {
             const float tz = Tz[l0 + li];
 #pragma unroll
@@ -997,7 +1000,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
             const int nrows = min(S::LP, P - pass * S::LP) * KB;
             const uint32_t base = tc::smem_u32(stage);
             const uint32_t idesc = tc::idesc_tf32(128, nrows);
-            const uint32_t d = tmem + (uint32_t)((seg & 1) * 256);
+            const uint32_t d = tmem + (uint32_t)((seg & 1) * kEN);
 #pragma unroll
             for (int ks = 0; ks < kEKC / 8; ++ks) {
                 const uint32_t kofs = ks * 256;
@@ -1046,7 +1049,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_eval_tc(EvalTc a, int* __restr
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, 512);
+        tc::tmem_dealloc(tmem, 2 * kEN);
     }
     if (!ok && tid == 0) atomicExch(err, 1);
 }
