@@ -258,8 +258,8 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    for _ in range(max(0, args.warmup - 1)):
-        pass
+    # cpu_baseline runs one untimed evaluate first (the CPU oracle keeps no
+    # state between evaluates beyond its thread pool and touched pages)
     v, desc, t = cpu_baseline(args.n, max(1, args.steps), threads)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpts*RHS/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
