@@ -109,11 +109,15 @@ template <int P>
 __global__ void __launch_bounds__(128) k_c2proxy_tiled(C2ProxyArgs a) {
     constexpr int TI = 8, TJ = 4, TS = 32;
     constexpr int NIB = (P + TI - 1) / TI, NJB = (P + TJ - 1) / TJ;
-    constexpr int PI = NIB * TI, PJ = NJB * TJ;  // padded rows (zeros beyond P)
+    constexpr int PI = NIB * TI, PJ = NJB * TJ;  // used widths (zeros beyond P)
+    // row strides: even (16-byte rows for the paired loads) and 2 mod 4
+    // doubles, so the Chebyshev writes of 32 sources at one degree spread
+    // over 8 bank groups instead of 2
+    constexpr int LX = (PI % 4 == 2) ? PI : PI + 2, LY = (PJ % 4 == 2) ? PJ : PJ + 2;
     constexpr int NTASK = P * NJB * NIB;
-    __shared__ __align__(16) double sx[TS][PI];
-    __shared__ __align__(16) double sy[TS][PJ];
-    __shared__ double sz[TS][P];
+    __shared__ __align__(16) double sx[TS][LX];
+    __shared__ __align__(16) double sy[TS][LY];
+    __shared__ double sz[TS][P | 1];
     const int e = blockIdx.x;
     const int task = blockIdx.y * blockDim.x + threadIdx.x;
     const bool active = task < NTASK;
@@ -180,21 +184,15 @@ __global__ void __launch_bounds__(128) k_c2proxy_tiled(C2ProxyArgs a) {
         }
     }
     if (!active) return;
+    // a centre's moments are written here first (its children's translations
+    // are added afterwards) and every coefficient by exactly one thread: store
     double* out = a.proxy_up + (int64_t)a.slot[e] * (P * P * P) + (int64_t)P * P * k;
-    double old[TI][TJ];
 #pragma unroll
     for (int i = 0; i < TI; ++i)
 #pragma unroll
         for (int t = 0; t < TJ; ++t) {
             const int ii = ib * TI + i, jj = jb * TJ + t;
-            old[i][t] = (ii < P && jj < P) ? out[ii + P * jj] : 0.0;
-        }
-#pragma unroll
-    for (int i = 0; i < TI; ++i)
-#pragma unroll
-        for (int t = 0; t < TJ; ++t) {
-            const int ii = ib * TI + i, jj = jb * TJ + t;
-            if (ii < P && jj < P) out[ii + P * jj] = old[i][t] + acc[i][t];
+            if (ii < P && jj < P) out[ii + P * jj] = acc[i][t];
         }
 }
 
