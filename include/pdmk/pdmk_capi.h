@@ -85,7 +85,8 @@ int pdmk_evaluate_parts_double(void* h, const double* charges, double* tree_part
  * target leaves, expansion order p, plane waves per axis, kernel launches per
  * single-RHS evaluate, device bytes, far-field modes (ms, mt, mu product),
  * near-field box pairs, plane-wave boxes, kernel launches of the last
- * multi-RHS evaluate, tree digit count, mixed path available (1/0), 0. */
+ * multi-RHS evaluate, tree digit count, mixed path available (1/0), image
+ * boxes that share an original box's expansions (exact lattice translates). */
 int pdmk_info_double(void* h, int64_t* out16);
 int pdmk_info_float(void* h, int64_t* out16);
 

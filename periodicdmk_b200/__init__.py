@@ -140,7 +140,7 @@ class PeriodicDMKTree:
 
     INFO_KEYS = ["n_points", "n_all", "n_boxes", "n_levels", "n_target_leaves", "p", "n_pw",
                  "launches_per_evaluate", "device_bytes", "far_modes", "near_pairs", "pw_boxes",
-                 "launches_last_multi", "n_digits_tree", "mixed_available", "reserved"]
+                 "launches_last_multi", "n_digits_tree", "mixed_available", "translate_boxes"]
 
     def __init__(self, cell, positions, n_digits=6, n_per_leaf=300, nz=4, precision="double"):
         if precision not in ("double", "float"):

@@ -157,7 +157,7 @@ int info_impl(void* h, int64_t* out) {
     out[12] = im->dev->multi_launches_;
     out[13] = P.dp.n_digits_tree;
     out[14] = im->dev->mixed_allowed() ? 1 : 0;
-    out[15] = 0;
+    out[15] = im->dev->translate_boxes();
     return 0;
 }
 

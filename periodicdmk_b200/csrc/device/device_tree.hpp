@@ -77,6 +77,8 @@ class DeviceTree {
     int64_t near_pairs_nominal() const { return near_pairs_nominal_; }
     int near_coeffs() const { return near_.nc; }
     size_t device_bytes() const { return bytes_; }
+    // image boxes sharing an original box's proxy moments and outgoing expansions
+    int64_t translate_boxes() const { return n_alias_; }
 
   private:
     struct MultiState;

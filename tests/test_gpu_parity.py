@@ -109,6 +109,21 @@ def test_fp64_level_chunks_agree_with_one_chunk(nd, monkeypatch):
         assert rel_l2(ref, oracle.evaluate(cell, pos, q, nd, 40, 4)) < 0.2 * 10.0 ** -nd
 
 
+def test_translate_image_boxes_share_expansions():
+    # In a cube the box grid is aligned with the lattice, so image boxes that
+    # hold exact translates of an original box's sources share its moments and
+    # outgoing plane waves; triclinic images straddle boxes and none qualify.
+    (cell, pos, q), npl = SYSTEMS["cube_deep"]()
+    t = _tree(cell, pos, 6, npl)
+    assert t.info()["translate_boxes"] > 0
+    assert rel_l2(t.evaluate(q), oracle.evaluate(cell, pos, q, 6, npl, 4)) < 0.2e-6
+    t.close()
+    (cell, pos, q), npl = SYSTEMS["triclinic_clustered"]()
+    t = _tree(cell, pos, 6, npl)
+    assert t.info()["translate_boxes"] == 0
+    t.close()
+
+
 def test_multi_rhs_equals_single_calls():
     (cell, pos, q), npl = SYSTEMS["cube_deep"]()
     rng = np.random.default_rng(5)
