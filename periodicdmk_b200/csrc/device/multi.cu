@@ -11,6 +11,8 @@
 // far field (NUFFT), self term and final accumulation.
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -648,12 +650,25 @@ __global__ void k_sep3(Sep3 a) {
     T* out = reinterpret_cast<T*>(a.out) + a.out_off[eb] * rhs + ec * P3;
     const T* mat = reinterpret_cast<const T*>(a.mat) + (a.mat_off ? a.mat_off[eb] : 0);
     const int nthr = blockDim.x;
-    for (int idx = threadIdx.x; idx < P3; idx += nthr) b0[idx] = in[idx];
+    // input tensor: asynchronous 16-byte copies (all in flight at once) when
+    // the source is 16-byte aligned, element loads otherwise
+    if ((reinterpret_cast<uintptr_t>(in) & 15) == 0) {
+        constexpr int NV = (int)(P3 * sizeof(T) / 16);
+        for (int v = threadIdx.x; v < NV; v += nthr)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(b0 + v * (16 / sizeof(T)))),
+                         "l"(in + v * (16 / sizeof(T)))
+                         : "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        for (int idx = NV * (int)(16 / sizeof(T)) + threadIdx.x; idx < P3; idx += nthr) b0[idx] = in[idx];
+    } else {
+        for (int idx = threadIdx.x; idx < P3; idx += nthr) b0[idx] = in[idx];
+    }
     for (int idx = threadIdx.x; idx < 3 * P * P; idx += nthr) {
         const int d = idx / (P * P), w = idx % (P * P);
         const int i = w / P, aa = w % P;
         Ut[d * P * P + i * P + aa] = mat[d * P * P + aa + P * i];
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     sep3_step<T, P, TRI>(b0, b1, Ut, nthr);
     __syncthreads();
