@@ -186,6 +186,36 @@ def run_batch(pd, args, world, rank, barrier, max_over_ranks):
             "host_build_s": t_build, "device_bytes_rank0": info["device_bytes"]}
 
 
+def smi_id(local):
+    """nvidia-smi / NVML identifier of CUDA device `local` (its UUID: nvidia-smi
+    indexes ignore CUDA_VISIBLE_DEVICES); the index if the UUID is unknown."""
+    try:
+        import torch
+        return "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        return str(local)
+
+
+def bind_host_to_gpu(local):
+    """Restrict this process to the CPUs NVML reports as local to the GPU (the
+    pinned host buffers are then first touched on the GPU's NUMA node).
+    Returns the previous affinity, or None if nothing changed."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByUUID(smi_id(local))
+        old = os.sched_getaffinity(0)
+        words = (max(max(old), os.cpu_count() or 1) + 64) // 64
+        masks = pynvml.nvmlDeviceGetCpuAffinity(h, words)
+        cpus = {64 * w + b for w, m in enumerate(masks) for b in range(64) if (int(m) >> b) & 1} & old
+        if not cpus or cpus == old:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return old
+    except Exception:
+        return None
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -200,7 +230,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                ["nvidia-smi", "-i", smi_id(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -279,6 +309,7 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    host_affinity = bind_host_to_gpu(local)
     dist = None
     if world > 1:
         import datetime
@@ -466,6 +497,8 @@ def run_ours(args):
         line["batch"] = run_batch(pd, args, world, rank, barrier, max_over_ranks)
     if args.clustered_digits.strip():
         line["clustered_triclinic"] = run_clustered(pd, args, world, dev, flush, barrier, max_over_ranks)
+    if host_affinity is not None:
+        os.sched_setaffinity(0, host_affinity)  # the CPU baseline gets every host core
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, desc, _ = cpu_baseline(n, 3, threads)
