@@ -873,6 +873,25 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                                  [&](int x, int y) { return key(x) < key(y); });
             }
             nufft_.interp_order = upload(order);
+            std::vector<int2> ipair;
+            std::vector<int> bin_pair{0};
+            for (auto& bn : bins) {
+                for (int i = bn.start; i < bn.start + bn.count;) {
+                    const int ta = order[i];
+                    int tb = -1;
+                    if (i + 1 < bn.start + bn.count) {
+                        const int4 la = pt_l0[ta], lb = pt_l0[order[i + 1]];
+                        if (la.x == lb.x && la.y == lb.y && la.z == lb.z) tb = order[i + 1];
+                    }
+                    ipair.push_back(make_int2(ta, tb));
+                    i += tb >= 0 ? 2 : 1;
+                }
+                bin_pair.push_back((int)ipair.size());
+                nufft_.max_pairs = std::max(nufft_.max_pairs, bin_pair.back() - bin_pair[bin_pair.size() - 2]);
+            }
+            if (ipair.empty()) ipair.push_back(make_int2(0, -1));
+            nufft_.interp_pair = upload(ipair);
+            nufft_.bin_pair = upload(bin_pair);
             // spreading runs: inside each bin, targets by (y, z, x) window start;
             // a run = equal (y, z), x offsets within kSpreadRunDx of its first
             std::vector<int> sorder(n_);

@@ -134,6 +134,13 @@ struct NufftArgs {
     // bin, targets grouped by the grid cell their window starts at, so that
     // neighbouring threads read the same grid values (null: sorted order).
     const int* interp_order = nullptr;
+    // Interpolation pairs: consecutive targets of the interpolation order
+    // whose windows start at the same cell, interpolated by one thread (y = -1
+    // for a target without a partner); bin e owns pairs bin_pair[e] ..
+    // bin_pair[e + 1] - 1.  Null: no pair lists.
+    const int2* interp_pair = nullptr;
+    const int* bin_pair = nullptr;
+    int max_pairs = 0;  // most pairs in one bin
     // Spreading by runs: inside each bin, targets whose windows start at the
     // same (y, z) cell form a run (ordered by x; x offsets within a run at
     // most kSpreadRunDx).  run = (first index into spread_order, count,

@@ -272,6 +272,129 @@ __global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __r
     for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + t] = u[c];
 }
 
+// Interpolation from each bin's subgrid in shared memory: grid (bins, RHS
+// blocks of CB).  The CTA copies the ext.x x ext.y x ext.z cells of its CB RHS
+// planes around the bin into shared memory as [RHS pair][cell][2], and each
+// thread interpolates one pair of targets whose windows start at the same
+// cell: every 16-byte load (two RHS) feeds four FMAs, half the bytes per FMA
+// of one target per thread (shared-memory and L1 delivery, 128 B per clock,
+// bound the one-target kernel).  Taps and FMA order per target are those of
+// k_interp_m, so the results agree bit for bit.  A bin with more cells than
+// cap_cells reads the grid directly.
+template <int W, int CB>
+__device__ __forceinline__ void interp_direct(const NufftArgs& a, const double* esw, const double* g0, int t,
+                                              double (&u)[CB]) {
+    const int4 l0 = a.pt_l0[t];
+    const double* wt = esw + (int64_t)t * 3 * W;
+    double wy[W], wz[W];
+    int iy[W], iz[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+        wy[c] = wt[W + c];
+        wz[c] = wt[2 * W + c];
+        iy[c] = wrap_index(l0.y + c, a.n2);
+        iz[c] = wrap_index(l0.z + c, a.n3);
+    }
+#pragma unroll
+    for (int c = 0; c < CB; ++c) u[c] = 0.0;
+#pragma unroll 1
+    for (int ia = 0; ia < W; ++ia) {
+        const double wxa = wt[ia];
+        const int64_t gx = (int64_t)wrap_index(l0.x + ia, a.n1) * a.n2;
+#pragma unroll
+        for (int ib = 0; ib < W; ++ib) {
+            const double wxy = wxa * wy[ib];
+            const double* row = g0 + (gx + iy[ib]) * a.n3;
+#pragma unroll
+            for (int ic = 0; ic < W; ++ic) {
+                const double w = wxy * wz[ic];
+                const double* p = row + iz[ic];
+#pragma unroll
+                for (int c = 0; c < CB; ++c) u[c] = fma(w, __ldg(p + (int64_t)c * a.rhs_grid_stride), u[c]);
+            }
+        }
+    }
+}
+
+template <int W, int CB>
+__global__ void __launch_bounds__(256, 2) k_interp_s(NufftArgs a, const double* __restrict__ esw, int cap_cells) {
+    static_assert(CB % 2 == 0, "RHS pairs");
+    extern __shared__ __align__(16) double sub[];
+    const int e = blockIdx.x, c0 = blockIdx.y * CB;
+    const int4 org = a.sub_origin[e], ext = a.sub_extent[e];
+    const int ncell = ext.x * ext.y * ext.z;
+    const bool staged = ncell <= cap_cells;
+    const double* g0 = a.grid + (int64_t)c0 * a.rhs_grid_stride;
+    if (staged) {
+        const int eyz = ext.y * ext.z;
+        for (int i = threadIdx.x; i < CB * ncell; i += blockDim.x) {
+            const int h = i & 1, r = i >> 1;
+            const int j = r / ncell, cell = r - j * ncell;
+            const int x = cell / eyz, yz = cell - x * eyz;
+            const int y = yz / ext.z, z = yz - y * ext.z;
+            const int64_t g = ((int64_t)wrap_index(org.x + x, a.n1) * a.n2 + wrap_index(org.y + y, a.n2)) * a.n3 +
+                              wrap_index(org.z + z, a.n3);
+            sub[i] = g0[(int64_t)(2 * j + h) * a.rhs_grid_stride + g];
+        }
+        __syncthreads();
+    }
+    const double2* s2 = reinterpret_cast<const double2*>(sub);
+    for (int ip = a.bin_pair[e] + (int)threadIdx.x; ip < a.bin_pair[e + 1]; ip += blockDim.x) {
+        const int2 tp = a.interp_pair[ip];
+        const bool two = tp.y >= 0;
+        double ua[CB], ub[CB];
+        if (staged) {
+            const int4 l0 = a.pt_l0[tp.x];
+            const double* wa = esw + (int64_t)tp.x * 3 * W;
+            const double* wb = esw + (int64_t)(two ? tp.y : tp.x) * 3 * W;
+            double wya[W], wza[W], wyb[W], wzb[W];
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+                wya[c] = wa[W + c];
+                wza[c] = wa[2 * W + c];
+                wyb[c] = two ? wb[W + c] : 0.0;
+                wzb[c] = wb[2 * W + c];
+            }
+#pragma unroll
+            for (int c = 0; c < CB; ++c) ua[c] = ub[c] = 0.0;
+            const int lx = l0.x - org.x, ly = l0.y - org.y, lz = l0.z - org.z;
+#pragma unroll 1
+            for (int ia = 0; ia < W; ++ia) {
+                const double wxa = wa[ia], wxb = wb[ia];
+                const int rx = (lx + ia) * ext.y + ly;
+#pragma unroll
+                for (int ib = 0; ib < W; ++ib) {
+                    const double wxya = wxa * wya[ib], wxyb = wxb * wyb[ib];
+                    const int row = (rx + ib) * ext.z + lz;
+#pragma unroll
+                    for (int ic = 0; ic < W; ++ic) {
+                        const double w0 = wxya * wza[ic], w1 = wxyb * wzb[ic];
+#pragma unroll
+                        for (int j = 0; j < CB / 2; ++j) {
+                            const double2 v = s2[j * ncell + row + ic];
+                            ua[2 * j] = fma(w0, v.x, ua[2 * j]);
+                            ua[2 * j + 1] = fma(w0, v.y, ua[2 * j + 1]);
+                            ub[2 * j] = fma(w1, v.x, ub[2 * j]);
+                            ub[2 * j + 1] = fma(w1, v.y, ub[2 * j + 1]);
+                        }
+                    }
+                }
+            }
+        } else {
+            interp_direct<W, CB>(a, esw, g0, tp.x, ua);
+            if (two) interp_direct<W, CB>(a, esw, g0, tp.y, ub);
+        }
+#pragma unroll
+        for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + tp.x] = ua[c];
+        if (two)
+#pragma unroll
+            for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + tp.y] = ub[c];
+    }
+}
+
+constexpr int kInterpCB = 4;                     // RHS per shared-memory interpolation CTA
+constexpr size_t kInterpSmemMax = 96 * 1024;     // subgrid bytes per CTA
+
 constexpr size_t kSpreadRunSmem = 100 * 1024;
 
 template <int W, typename TW>
@@ -321,6 +444,23 @@ void spread_w(const NufftArgs& a, const double* esw, int max_jk, int max_ex, int
 
 template <int W>
 void interp_w(const NufftArgs& a, const double* esw, int64_t n, int nrhs, cudaStream_t s) {
+    // windows up to 9 taps keep the staged kernel within 128 registers (two CTAs per SM)
+    if constexpr (W <= 9) if (nrhs % kInterpCB == 0 && a.interp_pair && a.bin_pair && a.n_leaves > 0 && a.max_cells > 0) {
+        const int cap = (int)std::min<int64_t>(a.max_cells, kInterpSmemMax / (kInterpCB * sizeof(double)));
+        static bool configured[64] = {};
+        int dev = 0;
+        PDMK_CUDA_CHECK(cudaGetDevice(&dev));
+        if (dev >= 0 && dev < 64 && !configured[dev]) {
+            PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_interp_s<W, kInterpCB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)kInterpSmemMax));
+            configured[dev] = true;
+        }
+        const size_t smem = (size_t)cap * kInterpCB * sizeof(double);
+        // one pass over a bin's pairs: threads = its pair count, whole warps, at most 256
+        const int nt = std::min(256, std::max(64, (a.max_pairs + 31) / 32 * 32));
+        k_interp_s<W, kInterpCB><<<dim3(a.n_leaves, nrhs / kInterpCB), nt, smem, s>>>(a, esw, cap);
+        return;
+    }
     const unsigned bx = (unsigned)((n + 127) / 128);
     if (nrhs % 8 == 0)
         k_interp_m<W, 8><<<dim3(bx, nrhs / 8), 128, 0, s>>>(a, esw, n);
