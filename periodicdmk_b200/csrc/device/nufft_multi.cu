@@ -272,15 +272,29 @@ __global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __r
     for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + t] = u[c];
 }
 
-// Interpolation from each bin's subgrid in shared memory: grid (bins, RHS
-// blocks of CB).  The CTA copies the ext.x x ext.y x ext.z cells of its CB RHS
-// planes around the bin into shared memory as [RHS pair][cell][2], and each
-// thread interpolates one pair of targets whose windows start at the same
-// cell: every 16-byte load (two RHS) feeds four FMAs, half the bytes per FMA
-// of one target per thread (shared-memory and L1 delivery, 128 B per clock,
-// bound the one-target kernel).  Taps and FMA order per target are those of
-// k_interp_m, so the results agree bit for bit.  A bin with more cells than
-// cap_cells reads the grid directly.
+// Interpolation from each bin's subgrid in shared memory: one CTA per bin,
+// looping over the RHS in blocks of CB.  The CTA copies the ext.x x ext.y x
+// ext.z cells of a block's CB RHS planes into shared memory as [RHS pair]
+// [cell][2] with asynchronous 8-byte copies, the next block's copies in flight
+// while the current block is interpolated (two buffers).  Each thread owns one
+// pair of targets whose windows start at the same cell and keeps their y/z
+// weights in registers across the blocks: every 16-byte load (two RHS) feeds
+// four FMAs, half the bytes per FMA of one target per thread (shared-memory
+// and L1 delivery, 128 B per clock, bound the one-target kernel).  Taps and
+// FMA order per target are those of k_interp_m, so the results agree bit for
+// bit.  Bins with more cells than cap_cells are left to k_interp_big, which
+// reads the grid directly.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <int W, int CB>
 __device__ __forceinline__ void interp_direct(const NufftArgs& a, const double* esw, const double* g0, int t,
                                               double (&u)[CB]) {
@@ -317,16 +331,19 @@ __device__ __forceinline__ void interp_direct(const NufftArgs& a, const double* 
 }
 
 template <int W, int CB>
-__global__ void __launch_bounds__(256, 2) k_interp_s(NufftArgs a, const double* __restrict__ esw, int cap_cells) {
+__global__ void __launch_bounds__(256, 2)
+    k_interp_s(NufftArgs a, const double* __restrict__ esw, int cap_cells, int nblocks) {
     static_assert(CB % 2 == 0, "RHS pairs");
-    extern __shared__ __align__(16) double sub[];
-    const int e = blockIdx.x, c0 = blockIdx.y * CB;
+    extern __shared__ __align__(16) double sub[];  // [2 buffers][CB / 2][cap_cells][2]
+    const int e = blockIdx.x;
     const int4 org = a.sub_origin[e], ext = a.sub_extent[e];
-    const int ncell = ext.x * ext.y * ext.z;
-    const bool staged = ncell <= cap_cells;
-    const double* g0 = a.grid + (int64_t)c0 * a.rhs_grid_stride;
-    if (staged) {
-        const int eyz = ext.y * ext.z;
+    const int eyz = ext.y * ext.z, ncell = ext.x * eyz;
+    if (ncell > cap_cells) return;
+    const int bufsz = CB * cap_cells;
+    // asynchronous copies of RHS block b into buffer b & 1 (one commit group)
+    auto stage = [&](int b) {
+        const double* gb = a.grid + (int64_t)b * CB * a.rhs_grid_stride;
+        double* dst = sub + (b & 1) * bufsz;
         for (int i = threadIdx.x; i < CB * ncell; i += blockDim.x) {
             const int h = i & 1, r = i >> 1;
             const int j = r / ncell, cell = r - j * ncell;
@@ -334,20 +351,29 @@ __global__ void __launch_bounds__(256, 2) k_interp_s(NufftArgs a, const double* 
             const int y = yz / ext.z, z = yz - y * ext.z;
             const int64_t g = ((int64_t)wrap_index(org.x + x, a.n1) * a.n2 + wrap_index(org.y + y, a.n2)) * a.n3 +
                               wrap_index(org.z + z, a.n3);
-            sub[i] = g0[(int64_t)(2 * j + h) * a.rhs_grid_stride + g];
+            cp_async8(dst + i, gb + (int64_t)(2 * j + h) * a.rhs_grid_stride + g);
         }
-        __syncthreads();
-    }
-    const double2* s2 = reinterpret_cast<const double2*>(sub);
-    for (int ip = a.bin_pair[e] + (int)threadIdx.x; ip < a.bin_pair[e + 1]; ip += blockDim.x) {
-        const int2 tp = a.interp_pair[ip];
+        cp_async_commit_group();
+    };
+    const int p0 = a.bin_pair[e], p1 = a.bin_pair[e + 1];
+    for (int base = p0; base < p1; base += blockDim.x) {  // the same trip count for all threads
+        const int ip = base + (int)threadIdx.x;
+        const bool act = ip < p1;
+        const int2 tp = act ? a.interp_pair[ip] : make_int2(0, -1);
         const bool two = tp.y >= 0;
-        double ua[CB], ub[CB];
-        if (staged) {
+        int lx = 0, ly = 0, lz = 0;
+        const double* wa = esw;
+        const double* wb = esw;
+        double wya[W], wza[W], wyb[W], wzb[W];
+#pragma unroll
+        for (int c = 0; c < W; ++c) wya[c] = wza[c] = wyb[c] = wzb[c] = 0.0;
+        if (act) {
             const int4 l0 = a.pt_l0[tp.x];
-            const double* wa = esw + (int64_t)tp.x * 3 * W;
-            const double* wb = esw + (int64_t)(two ? tp.y : tp.x) * 3 * W;
-            double wya[W], wza[W], wyb[W], wzb[W];
+            lx = l0.x - org.x;
+            ly = l0.y - org.y;
+            lz = l0.z - org.z;
+            wa = esw + (int64_t)tp.x * 3 * W;
+            wb = esw + (int64_t)(two ? tp.y : tp.x) * 3 * W;
 #pragma unroll
             for (int c = 0; c < W; ++c) {
                 wya[c] = wa[W + c];
@@ -355,40 +381,74 @@ __global__ void __launch_bounds__(256, 2) k_interp_s(NufftArgs a, const double* 
                 wyb[c] = two ? wb[W + c] : 0.0;
                 wzb[c] = wb[2 * W + c];
             }
+        }
+        stage(0);
+        for (int b = 0; b < nblocks; ++b) {
+            if (b + 1 < nblocks) {
+                stage(b + 1);
+                cp_async_wait_group<1>();
+            } else {
+                cp_async_wait_group<0>();
+            }
+            __syncthreads();
+            if (act) {
+                const double2* s2 = reinterpret_cast<const double2*>(sub + (b & 1) * bufsz);
+                double ua[CB], ub[CB];
 #pragma unroll
-            for (int c = 0; c < CB; ++c) ua[c] = ub[c] = 0.0;
-            const int lx = l0.x - org.x, ly = l0.y - org.y, lz = l0.z - org.z;
+                for (int c = 0; c < CB; ++c) ua[c] = ub[c] = 0.0;
 #pragma unroll 1
-            for (int ia = 0; ia < W; ++ia) {
-                const double wxa = wa[ia], wxb = wb[ia];
-                const int rx = (lx + ia) * ext.y + ly;
+                for (int ia = 0; ia < W; ++ia) {
+                    const double wxa = wa[ia], wxb = wb[ia];
+                    const int rx = (lx + ia) * ext.y + ly;
 #pragma unroll
-                for (int ib = 0; ib < W; ++ib) {
-                    const double wxya = wxa * wya[ib], wxyb = wxb * wyb[ib];
-                    const int row = (rx + ib) * ext.z + lz;
+                    for (int ib = 0; ib < W; ++ib) {
+                        const double wxya = wxa * wya[ib], wxyb = wxb * wyb[ib];
+                        const int row = (rx + ib) * ext.z + lz;
 #pragma unroll
-                    for (int ic = 0; ic < W; ++ic) {
-                        const double w0 = wxya * wza[ic], w1 = wxyb * wzb[ic];
+                        for (int ic = 0; ic < W; ++ic) {
+                            const double w0 = wxya * wza[ic], w1 = wxyb * wzb[ic];
 #pragma unroll
-                        for (int j = 0; j < CB / 2; ++j) {
-                            const double2 v = s2[j * ncell + row + ic];
-                            ua[2 * j] = fma(w0, v.x, ua[2 * j]);
-                            ua[2 * j + 1] = fma(w0, v.y, ua[2 * j + 1]);
-                            ub[2 * j] = fma(w1, v.x, ub[2 * j]);
-                            ub[2 * j + 1] = fma(w1, v.y, ub[2 * j + 1]);
+                            for (int j = 0; j < CB / 2; ++j) {
+                                const double2 v = s2[j * ncell + row + ic];
+                                ua[2 * j] = fma(w0, v.x, ua[2 * j]);
+                                ua[2 * j + 1] = fma(w0, v.y, ua[2 * j + 1]);
+                                ub[2 * j] = fma(w1, v.x, ub[2 * j]);
+                                ub[2 * j + 1] = fma(w1, v.y, ub[2 * j + 1]);
+                            }
                         }
                     }
                 }
+                const int c0 = b * CB;
+#pragma unroll
+                for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + tp.x] = ua[c];
+                if (two)
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + tp.y] = ub[c];
             }
-        } else {
-            interp_direct<W, CB>(a, esw, g0, tp.x, ua);
-            if (two) interp_direct<W, CB>(a, esw, g0, tp.y, ub);
+            __syncthreads();
         }
+    }
+}
+
+// The bins that k_interp_s leaves (more cells than cap_cells): each thread
+// interpolates its pair's targets from the grid in global memory.
+template <int W, int CB>
+__global__ void __launch_bounds__(256) k_interp_big(NufftArgs a, const double* __restrict__ esw, int cap_cells) {
+    const int e = blockIdx.x, c0 = blockIdx.y * CB;
+    const int4 ext = a.sub_extent[e];
+    if (ext.x * ext.y * ext.z <= cap_cells) return;
+    const double* g0 = a.grid + (int64_t)c0 * a.rhs_grid_stride;
+    for (int ip = a.bin_pair[e] + (int)threadIdx.x; ip < a.bin_pair[e + 1]; ip += blockDim.x) {
+        const int2 tp = a.interp_pair[ip];
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            const int t = k == 0 ? tp.x : tp.y;
+            if (t < 0) break;
+            double u[CB];
+            interp_direct<W, CB>(a, esw, g0, t, u);
 #pragma unroll
-        for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + tp.x] = ua[c];
-        if (two)
-#pragma unroll
-            for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + tp.y] = ub[c];
+            for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + t] = u[c];
+        }
     }
 }
 
@@ -446,7 +506,7 @@ template <int W>
 void interp_w(const NufftArgs& a, const double* esw, int64_t n, int nrhs, cudaStream_t s) {
     // windows up to 9 taps keep the staged kernel within 128 registers (two CTAs per SM)
     if constexpr (W <= 9) if (nrhs % kInterpCB == 0 && a.interp_pair && a.bin_pair && a.n_leaves > 0 && a.max_cells > 0) {
-        const int cap = (int)std::min<int64_t>(a.max_cells, kInterpSmemMax / (kInterpCB * sizeof(double)));
+        const int cap = (int)std::min<int64_t>(a.max_cells, kInterpSmemMax / (2 * kInterpCB * sizeof(double)));
         static bool configured[64] = {};
         int dev = 0;
         PDMK_CUDA_CHECK(cudaGetDevice(&dev));
@@ -455,10 +515,11 @@ void interp_w(const NufftArgs& a, const double* esw, int64_t n, int nrhs, cudaSt
                                                  (int)kInterpSmemMax));
             configured[dev] = true;
         }
-        const size_t smem = (size_t)cap * kInterpCB * sizeof(double);
+        const size_t smem = 2 * (size_t)cap * kInterpCB * sizeof(double);
         // one pass over a bin's pairs: threads = its pair count, whole warps, at most 256
         const int nt = std::min(256, std::max(64, (a.max_pairs + 31) / 32 * 32));
-        k_interp_s<W, kInterpCB><<<dim3(a.n_leaves, nrhs / kInterpCB), nt, smem, s>>>(a, esw, cap);
+        k_interp_s<W, kInterpCB><<<a.n_leaves, nt, smem, s>>>(a, esw, cap, nrhs / kInterpCB);
+        if (a.max_cells > cap) k_interp_big<W, kInterpCB><<<dim3(a.n_leaves, nrhs / kInterpCB), nt, 0, s>>>(a, esw, cap);
         return;
     }
     const unsigned bx = (unsigned)((n + 127) / 128);
