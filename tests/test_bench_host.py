@@ -18,3 +18,18 @@ def test_clustered_system_matches_its_description():
     assert nn_c < 0.5 * nn_u
     cell2, pos2, q2 = bench.clustered_system(4000, seed=3)
     assert np.array_equal(pos, pos2) and np.array_equal(q, q2)
+
+
+def test_host_binding_helpers_without_a_gpu():
+    """Without a usable GPU or NVML the bench keeps the process affinity and
+    still names a device for nvidia-smi (its index)."""
+    import os
+
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    before = os.sched_getaffinity(0)
+    assert bench.bind_host_to_gpu(0) is None
+    assert os.sched_getaffinity(0) == before
+    assert bench.smi_id(0) == "0"
