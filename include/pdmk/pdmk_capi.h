@@ -108,11 +108,14 @@ int pdmk_fma_peak(int fp64, double* tflops);
  * loop that cannot take the device-wide synchronisation of cudaMalloc/cudaFree.
  * The tree is created beforehand (pdmk_create_double allocates its buffers);
  * charges_dev / pot_dev are N doubles on the tree's device, owned by the caller.
- * Transform scratch lives in one static 32 MiB device array held by every GPU
- * that loads the library until exit; trees needing more per box are rejected
- * (-1).  The first call on a device looks up that array's address: make it
- * before any stream capture.  Calls share the array, so calls that overlap on
- * the GPU race and must be serialised by the caller.  Synchronous. */
+ * Transform scratch lives in one static 32 MiB device array, held until exit by
+ * every GPU it has been reserved on; trees needing more per box are rejected
+ * (-1).  CUDA loads the array lazily: pdmk_create_double reserves it on the
+ * tree's device (so the reservation belongs to the caller's set-up, before its
+ * allocator takes the pool); if that fails, the first call here retries and
+ * returns -2 when the device has no room.  Make the first call before any
+ * stream capture.  Calls share the array, so calls that overlap on the GPU
+ * race and must be serialised by the caller.  Synchronous. */
 int pdmk_evaluate_device_noalloc_double(void* h, const double* charges_dev, double* pot_dev);
 
 /* ---- batches of independent systems ------------------------------------ */

@@ -4,8 +4,9 @@
     python -m periodicdmk_b200.build --clean  # rebuild everything
 
 CUDA sources are compiled by nvcc for ``-gencode arch=compute_100a,code=sm_100a``;
-host C++ by g++.  cudart and cuFFT are linked statically so the library does
-not depend on whichever CUDA runtime the host process (e.g. torch) loaded.
+host C++ by g++.  cudart is linked statically, so the library does not depend
+on whichever CUDA runtime the host process (e.g. torch) loaded; cuFFT is linked
+dynamically (libcufft from the CUDA toolkit's lib64, found through an rpath).
 """
 import concurrent.futures as cf
 import os

@@ -319,6 +319,21 @@ int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, doub
     }
 }
 
+int pdmk_evaluate_device_noalloc_double(void* h, const double* q_dev, double* pot_dev) {
+    if (!h) {
+        set_error("pdmk_evaluate_device_noalloc_double", "null handle");
+        return -1;
+    }
+    try {
+        if (!q_dev || !pot_dev) throw std::invalid_argument("null device pointer");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h);
+        t->impl()->dev->evaluate_device_noalloc(q_dev, pot_dev);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_device_noalloc_double", e);
+    }
+}
+
 int pdmk_info_double(void* h, int64_t* out) { return info_impl<double>(h, out); }
 
 int pdmk_stage_times_double(void* h, double* out8) { return stage_times_impl<double>(h, out8); }

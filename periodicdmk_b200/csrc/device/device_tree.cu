@@ -775,7 +775,10 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             if (F.eval.n_leaves) launches_ += 1;
         }
     }
-    if (fp64_working_set) ensure_fp64_working_set();
+    if (fp64_working_set) {
+        ensure_fp64_working_set();
+        noalloc_reserve(device_);  // double trees may use the no-allocation evaluate
+    }
 
     // ------------------------------------------------------------------ far field
     {

@@ -21,6 +21,11 @@ struct StageTimes {
     double finalize_ms = 0;
 };
 
+// Looks up (and so, under lazy module loading, reserves) the static scratch
+// array of the no-allocation evaluate on `device`; failures are left to that
+// evaluate to report.  Defined in noalloc.cu.
+void noalloc_reserve(int device);
+
 class DeviceTree {
   public:
     // fp64_working_set: allocate the single-RHS FP64 expansion and transform

@@ -19,9 +19,16 @@
 // box needs more scratch than the array holds is rejected with an error.
 //
 // Rules for callers:
-//   * The first call on a device looks up the array's device address (set-up
-//     done once per device, with that device current).  Make that first call
-//     before any CUDA stream capture.
+//   * The array belongs to this file's device code, which CUDA loads onto a
+//     device lazily (CUDA_MODULE_LOADING=LAZY is the default): the 32 MiB are
+//     reserved on a device when its address is first looked up.  Creating a
+//     double tree (pdmk_create_double) does that look-up, with the tree's
+//     device current, so the reservation happens during the caller's set-up,
+//     together with the tree's own buffers, before the caller's allocator
+//     takes the memory pool.  If that look-up fails at creation (the device
+//     has no 32 MiB left), the first no-allocation call repeats it and fails
+//     with -2 if it still cannot reserve the array.  Either way the first
+//     call on a device should come before any CUDA stream capture.
 //   * All calls share the one array and it keeps the last call's contents
 //     (every value is written before it is read, so nothing needs clearing).
 //     Calls that overlap on the GPU -- two trees evaluated concurrently on
@@ -35,9 +42,7 @@
 #include <stdexcept>
 #include <string>
 
-#include "../api/impl.hpp"
 #include "device_tree.hpp"
-#include "pdmk/pdmk_capi.h"
 
 namespace pdmkb {
 
@@ -71,8 +76,17 @@ dev::cd* scratch_address(int device) {
 
 }  // namespace
 
+void noalloc_reserve(int device) {
+    try {
+        scratch_address(device);
+    } catch (const std::exception&) {
+        cudaGetLastError();  // not sticky; the no-allocation call retries and reports it
+    }
+}
+
 void DeviceTree::evaluate_device_noalloc(const double* q, double* pot) {
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    last_was_multi_ = false;
     if (!proxy_up_)
         throw std::invalid_argument("the no-allocation evaluate needs a tree built with its FP64 buffers (double tree)");
     dev::cd* scratch = scratch_address(device_);
@@ -105,20 +119,3 @@ void DeviceTree::evaluate_device_noalloc(const double* q, double* pot) {
 }
 
 }  // namespace pdmkb
-
-extern "C" int pdmk_evaluate_device_noalloc_double(void* h, const double* charges_dev, double* pot_dev) {
-    if (!h) {
-        std::fprintf(stderr, "pdmk_evaluate_device_noalloc_double: null handle\n");
-        return -1;
-    }
-    try {
-        if (!charges_dev || !pot_dev) throw std::invalid_argument("null device pointer");
-        auto* t = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h);
-        t->impl()->dev->evaluate_device_noalloc(charges_dev, pot_dev);
-        return 0;
-    } catch (const std::exception& e) {
-        std::fprintf(stderr, "pdmk_evaluate_device_noalloc_double: %s\n", e.what());
-        const std::string m = e.what();
-        return (m.rfind("CUDA error", 0) == 0 || m.rfind("cuFFT error", 0) == 0) ? -2 : -1;
-    }
-}

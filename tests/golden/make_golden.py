@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own code.
 
-Runs only where the reference source tree is present: it builds
+Runs only where the reference source tree is present (PDMK_REFERENCE_DIR names
+the reference project's root): it builds
 oracle/_ref/libref.so from the reference's standalone sources
 (cpp/src/dmk/prolate.cpp, cpp/src/dmk/legeexps.cpp, cpp/include/dmk/pbc.hpp,
 cpp/include/pdmk/image_layout.hpp) with `make -C oracle ref` and records:
@@ -12,7 +13,7 @@ cpp/include/pdmk/image_layout.hpp) with `make -C oracle ref` and records:
 The fixtures are committed; tests compare the oracle and the product's host
 code against them without needing the reference.
 
-    python tests/golden/make_golden.py
+    PDMK_REFERENCE_DIR=<reference project> python tests/golden/make_golden.py
 """
 import ctypes
 import hashlib
