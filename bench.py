@@ -282,6 +282,30 @@ def cpu_baseline(n_target, steps, threads):
     return n / t / 1e6, desc, t
 
 
+def parity_vs_oracle(cell, pos, Q, P_mixed, pot_plain, cols):
+    """Accuracy of the timed results against the CPU oracle at the full
+    workload size (part of the CPU-baseline leg: the oracle is the checker
+    here, nothing timed runs through it).  Q: (N, k) charges; P_mixed: (k, N)
+    mixed-precision potentials; pot_plain: FP64 potentials of column 0.
+    Relative L2 and max error, max|u - u_ref| / max|u_ref|."""
+    import oracle
+    t0 = time.perf_counter()
+    ref = oracle.evaluate_multi(cell, pos, Q[:, list(cols)], 6, 300, 4)
+
+    def rl2(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    def mx(a, b):
+        return float(np.abs(a - b).max() / np.abs(b).max())
+    out = {"columns": list(cols),
+           "mixed_rel_l2": [rl2(P_mixed[c], ref[:, j]) for j, c in enumerate(cols)],
+           "mixed_max_err": [mx(P_mixed[c], ref[:, j]) for j, c in enumerate(cols)],
+           "plain_fp64_rel_l2": rl2(pot_plain, ref[:, 0]), "plain_fp64_max_err": mx(pot_plain, ref[:, 0]),
+           "oracle": "CPU DMK restatement (FP64, exact reciprocal-lattice far field) at N=%d" % len(pos),
+           "oracle_s": time.perf_counter() - t0}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -503,6 +527,10 @@ def run_ours(args):
         threads = os.cpu_count() or 1
         v, desc, _ = cpu_baseline(n, 3, threads)
         line["cpu_baseline"] = {"value": v, "unit": "Mpts*RHS/s", "cores": threads, "kind": "port", "sample": desc}
+        par = parity_vs_oracle(cell, pos, Q, P_mixed, pot_plain, (0, k - 1))
+        line["parity_vs_oracle"] = par
+        line["rel_l2_vs_oracle"] = max(par["mixed_rel_l2"])
+        line["max_err_vs_oracle"] = max(par["mixed_max_err"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -38,6 +38,13 @@ def lib():
         _lib.oracle_plan_stats.restype = ctypes.c_int
         _lib.oracle_ewald_direct.argtypes = [d, ctypes.c_int, d, d, ctypes.c_double, d, d]
         _lib.oracle_ewald_direct.restype = ctypes.c_int
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.oracle_ewald_targets.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ip, ctypes.c_double,
+                                              ctypes.c_double, d]
+        _lib.oracle_ewald_targets.restype = ctypes.c_int
+        _lib.oracle_evaluate_multi.argtypes = [d, ctypes.c_int, d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, d]
+        _lib.oracle_evaluate_multi.restype = ctypes.c_int
         _lib.oracle_pswf.argtypes = [ctypes.c_double, ctypes.c_int, d, d, d]
         _lib.oracle_legendre.argtypes = [ctypes.c_int, d, d]
         ip = ctypes.POINTER(ctypes.c_int)
@@ -100,6 +107,37 @@ def ewald_direct(cell, pos, q, s=5.0):
     if lib().oracle_ewald_direct(_dp(c), len(q), _dp(pos), _dp(q), s, _dp(pot), _dp(e)) != 0:
         raise RuntimeError("oracle_ewald_direct failed")
     return pot, float(e[0])
+
+
+def ewald_targets(cell, pos, q, targets, s=6.0, alpha=0.0):
+    """Ewald potentials at the given target indices (all sources, all images).
+
+    s sets the accuracy (real-space terms below erfc(s), reciprocal terms
+    below exp(-s^2)); alpha <= 0 balances the real- and reciprocal-space work.
+    Cost ~ len(targets) * (sources within s/alpha) + N * (modes within 2 s alpha).
+    """
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.int32)
+    out = np.zeros(len(t))
+    c = _cell(cell)
+    ip = ctypes.POINTER(ctypes.c_int)
+    if lib().oracle_ewald_targets(_dp(c), len(q), _dp(pos), _dp(q), len(t), t.ctypes.data_as(ip), s, alpha,
+                                  _dp(out)) != 0:
+        raise RuntimeError("oracle_ewald_targets failed")
+    return out
+
+
+def evaluate_multi(cell, pos, Q, n_digits=6, n_per_leaf=300, nz=4):
+    """Oracle potentials of k charge vectors Q (N, k) on one plan (exact far field)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    Qc = np.ascontiguousarray(np.asarray(Q, dtype=np.float64).T)  # column-major N x k
+    n, k = Qc.shape[1], Qc.shape[0]
+    out = np.zeros_like(Qc)
+    c = _cell(cell)
+    if lib().oracle_evaluate_multi(_dp(c), n, _dp(pos), k, _dp(Qc), n_digits, n_per_leaf, nz, _dp(out)) != 0:
+        raise RuntimeError("oracle_evaluate_multi failed")
+    return out.T
 
 
 def pswf(beta, x):

@@ -723,4 +723,227 @@ int oracle_ewald_direct(const double* cell, int n, const double* pos, const doub
     return 0;
 }
 
+// Ewald sum at a subset of targets (neutral-gauge potentials, k = 0 dropped),
+// for checks at sizes where the all-pairs sum above cannot finish:
+//   phi(x_t) = sum_{j,n}' q_j erfc(alpha r)/r            (r = |x_t - x_j + R_n| < s/alpha)
+//            + sum_{0 < |k| <= 2 s alpha} (4 pi / V) e^{-k^2/(4 alpha^2)} / k^2 Re[S(k) e^{i k.x_t}]
+//            - 2 alpha/sqrt(pi) q_t,          S(k) = sum_j q_j e^{-i k.x_j}
+// (the splitting of cpp/src/ewald_nufft.cpp:777-910, evaluated at m targets).
+// Real space: sources binned in fractional coordinates; a pair closer than
+// rcut differs by less than rcut/h_d in fractional coordinate d (h_d the
+// lattice-plane spacing), which bounds the bins visited.  Reciprocal space:
+// k.x = 2 pi (m . f) with f the fractional coordinates, so e^{-i k.x}
+// factorises over the three axes and S(k) is accumulated per source over the
+// modes of the sphere.  alpha <= 0 picks alpha from an estimate of the two
+// costs.  Sums are compensated (Neumaier) so rounding stays near 1e-15 of the
+// potential at 10^6 sources.
+int oracle_ewald_targets(const double* cell, int n, const double* pos, const double* q, int m, const int* tidx,
+                         double s, double alpha, double* pot) {
+    try {
+        const double* a[3] = {cell, cell + 3, cell + 6};
+        auto cross = [](const double* u, const double* v, double* w) {
+            w[0] = u[1] * v[2] - u[2] * v[1];
+            w[1] = u[2] * v[0] - u[0] * v[2];
+            w[2] = u[0] * v[1] - u[1] * v[0];
+        };
+        auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+        double c[3][3];
+        cross(a[1], a[2], c[0]);
+        cross(a[2], a[0], c[1]);
+        cross(a[0], a[1], c[2]);
+        const double V = std::fabs(dot(a[0], c[0]));
+        if (!(V > 0) || n <= 0 || m <= 0) return -1;
+        double h[3];
+        for (int d = 0; d < 3; ++d) h[d] = V / std::sqrt(dot(c[d], c[d]));
+        // fractional coordinates f = A^-1 x: rows of A^-1 are c_d / V (sign of det folded in)
+        const double sgn = dot(a[0], c[0]) > 0 ? 1.0 : -1.0;
+        double ainv[3][3];
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 3; ++e) ainv[d][e] = sgn * c[d][e] / V;
+        if (!(alpha > 0)) {
+            // real-space pairs ~ m * (n/V) * (4/3) pi rcut^3 * 10 (erfc, bins), reciprocal
+            // modes ~ n * (4/3) pi kmax^3 V / (2 pi)^3
+            const double A = m * (n / V) * 4.18879 * s * s * s * 10.0;
+            const double B = n * 4.18879 * 8.0 * s * s * s * V / (8.0 * M_PI * M_PI * M_PI);
+            alpha = std::pow(A / B, 1.0 / 6.0);
+        }
+        const double rcut = s / alpha, kmax = 2.0 * s * alpha, rc2 = rcut * rcut;
+        std::vector<double> f((size_t)3 * n);
+        for (int j = 0; j < n; ++j)
+            for (int d = 0; d < 3; ++d) {
+                const double* x = pos + 3 * (size_t)j;
+                double v = ainv[d][0] * x[0] + ainv[d][1] * x[1] + ainv[d][2] * x[2];
+                v -= std::floor(v);
+                if (v >= 1.0) v = 0.0;
+                f[3 * (size_t)j + d] = v;
+            }
+        // ---- real space
+        int G[3], reach[3];
+        const double per_bin = 8.0;  // target sources per bin
+        const double nb = std::max(1.0, std::cbrt(n / per_bin));
+        for (int d = 0; d < 3; ++d) {
+            G[d] = std::max(1, std::min(512, (int)std::lround(nb)));
+            reach[d] = (int)std::ceil(rcut / h[d] * G[d]) + 1;
+        }
+        const size_t nbins = (size_t)G[0] * G[1] * G[2];
+        std::vector<int> bstart(nbins + 1, 0), border(n);
+        auto bin_of = [&](int j) {
+            int b[3];
+            for (int d = 0; d < 3; ++d) b[d] = std::min(G[d] - 1, (int)(f[3 * (size_t)j + d] * G[d]));
+            return ((size_t)b[2] * G[1] + b[1]) * G[0] + b[0];
+        };
+        for (int j = 0; j < n; ++j) bstart[bin_of(j) + 1]++;
+        for (size_t b = 0; b < nbins; ++b) bstart[b + 1] += bstart[b];
+        {
+            std::vector<int> fill(bstart.begin(), bstart.end() - 1);
+            for (int j = 0; j < n; ++j) border[fill[bin_of(j)]++] = j;
+        }
+        std::vector<double> phi(m, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int ti = 0; ti < m; ++ti) {
+            const int t = tidx[ti];
+            const double* ft = &f[3 * (size_t)t];
+            int bt[3];
+            for (int d = 0; d < 3; ++d) bt[d] = std::min(G[d] - 1, (int)(ft[d] * G[d]));
+            double sum = 0, comp = 0;
+            for (int o2 = -reach[2]; o2 <= reach[2]; ++o2)
+                for (int o1 = -reach[1]; o1 <= reach[1]; ++o1)
+                    for (int o0 = -reach[0]; o0 <= reach[0]; ++o0) {
+                        const int raw[3] = {bt[0] + o0, bt[1] + o1, bt[2] + o2};
+                        int bi[3], sh[3];
+                        for (int d = 0; d < 3; ++d) {
+                            sh[d] = (int)std::floor((double)raw[d] / G[d]);
+                            bi[d] = raw[d] - sh[d] * G[d];
+                        }
+                        const size_t b = ((size_t)bi[2] * G[1] + bi[1]) * G[0] + bi[0];
+                        for (int k = bstart[b]; k < bstart[b + 1]; ++k) {
+                            const int j = border[k];
+                            if (j == t && !sh[0] && !sh[1] && !sh[2]) continue;
+                            double df[3];
+                            for (int d = 0; d < 3; ++d) df[d] = ft[d] - (f[3 * (size_t)j + d] + sh[d]);
+                            double dr[3];
+                            for (int e = 0; e < 3; ++e) dr[e] = a[0][e] * df[0] + a[1][e] * df[1] + a[2][e] * df[2];
+                            const double r2 = dot(dr, dr);
+                            if (r2 >= rc2) continue;
+                            const double r = std::sqrt(r2);
+                            const double v = q[j] * std::erfc(alpha * r) / r;
+                            const double tsum = sum + v;
+                            comp += std::fabs(sum) >= std::fabs(v) ? (sum - tsum) + v : (v - tsum) + sum;
+                            sum = tsum;
+                        }
+                    }
+            phi[ti] = sum + comp - 2.0 * alpha / std::sqrt(M_PI) * q[t];
+        }
+        // ---- reciprocal space: modes m with |m1 b1 + m2 b2 + m3 b3| <= kmax
+        double b[3][3];
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 3; ++e) b[d][e] = 2 * M_PI * ainv[d][e];
+        int mm[3];
+        for (int d = 0; d < 3; ++d) mm[d] = (int)std::ceil(kmax * std::sqrt(dot(a[d], a[d])) / (2 * M_PI));
+        struct Row {
+            int m2, m3, lo, hi;  // m1 in [lo, hi]
+            size_t off;
+        };
+        std::vector<Row> rows;
+        std::vector<double> w;
+        const double km2 = kmax * kmax, inv4a2 = 1.0 / (4 * alpha * alpha), pref = 4 * M_PI / V;
+        size_t nk = 0;
+        for (int m3 = 0; m3 <= mm[2]; ++m3)
+            for (int m2 = -mm[1]; m2 <= mm[1]; ++m2) {
+                if (m3 == 0 && m2 < 0) continue;  // half space: (m3 > 0) or (m3 = 0, m2 > 0) or (m3 = m2 = 0, m1 > 0)
+                int lo = -mm[0], hi = mm[0];
+                if (m3 == 0 && m2 == 0) lo = 1;
+                Row r{m2, m3, 0, -1, nk};
+                for (int m1 = lo; m1 <= hi; ++m1) {
+                    double kv[3];
+                    for (int e = 0; e < 3; ++e) kv[e] = m1 * b[0][e] + m2 * b[1][e] + m3 * b[2][e];
+                    const double k2 = dot(kv, kv);
+                    if (k2 > km2) continue;
+                    if (r.hi < r.lo) r.lo = m1;
+                    r.hi = m1;
+                }
+                if (r.hi < r.lo) continue;
+                for (int m1 = r.lo; m1 <= r.hi; ++m1) {
+                    double kv[3];
+                    for (int e = 0; e < 3; ++e) kv[e] = m1 * b[0][e] + m2 * b[1][e] + m3 * b[2][e];
+                    const double k2 = dot(kv, kv);
+                    w.push_back(k2 <= km2 ? 2.0 * pref * std::exp(-k2 * inv4a2) / k2 : 0.0);  // x2: the -k half
+                }
+                nk += r.hi - r.lo + 1;
+                rows.push_back(r);
+            }
+        std::vector<cplx> S(nk, cplx(0));
+        const int nthreads = omp_get_max_threads();
+        const int chunk = 512;
+#pragma omp parallel num_threads(nthreads)
+        {
+            std::vector<cplx> acc(nk, cplx(0)), part(nk, cplx(0));
+            std::vector<cplx> e1(2 * mm[0] + 1), e2(2 * mm[1] + 1), e3(mm[2] + 1);
+#pragma omp for schedule(static)
+            for (int c0 = 0; c0 < n; c0 += chunk) {
+                std::fill(part.begin(), part.end(), cplx(0));
+                for (int j = c0; j < std::min(n, c0 + chunk); ++j) {
+                    const double* fj = &f[3 * (size_t)j];
+                    for (int k = -mm[0]; k <= mm[0]; ++k)
+                        e1[k + mm[0]] = std::polar(1.0, -2 * M_PI * k * fj[0]);
+                    for (int k = -mm[1]; k <= mm[1]; ++k)
+                        e2[k + mm[1]] = std::polar(1.0, -2 * M_PI * k * fj[1]);
+                    for (int k = 0; k <= mm[2]; ++k) e3[k] = std::polar(1.0, -2 * M_PI * k * fj[2]);
+                    for (const Row& r : rows) {
+                        const cplx g = q[j] * e3[r.m3] * e2[r.m2 + mm[1]];
+                        cplx* pp = &part[r.off];
+                        const cplx* ee = &e1[r.lo + mm[0]];
+                        for (int k = 0; k <= r.hi - r.lo; ++k) pp[k] += g * ee[k];
+                    }
+                }
+                for (size_t k = 0; k < nk; ++k) acc[k] += part[k];
+            }
+#pragma omp critical
+            for (size_t k = 0; k < nk; ++k) S[k] += acc[k];
+        }
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int ti = 0; ti < m; ++ti) {
+            const double* ft = &f[3 * (size_t)tidx[ti]];
+            std::vector<cplx> e1(2 * mm[0] + 1), e2(2 * mm[1] + 1), e3(mm[2] + 1);
+            for (int k = -mm[0]; k <= mm[0]; ++k) e1[k + mm[0]] = std::polar(1.0, 2 * M_PI * k * ft[0]);
+            for (int k = -mm[1]; k <= mm[1]; ++k) e2[k + mm[1]] = std::polar(1.0, 2 * M_PI * k * ft[1]);
+            for (int k = 0; k <= mm[2]; ++k) e3[k] = std::polar(1.0, 2 * M_PI * k * ft[2]);
+            double sum = 0, comp = 0;
+            for (const Row& r : rows) {
+                const cplx g = e3[r.m3] * e2[r.m2 + mm[1]];
+                for (int k = 0; k <= r.hi - r.lo; ++k) {
+                    const double v = w[r.off + k] * (S[r.off + k] * g * e1[r.lo + k + mm[0]]).real();
+                    const double tsum = sum + v;
+                    comp += std::fabs(sum) >= std::fabs(v) ? (sum - tsum) + v : (v - tsum) + sum;
+                    sum = tsum;
+                }
+            }
+            pot[ti] = phi[ti] + sum + comp;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_ewald_targets: %s\n", e.what());
+        return -1;
+    }
+}
+
+// k charge vectors on one plan (charges and potentials N x k column-major);
+// the exact far field, as oracle_evaluate.
+int oracle_evaluate_multi(const double* cell, int n, const double* pos, int k, const double* Q, int n_digits,
+                          int n_per_leaf, int nz, double* pot) {
+    try {
+        Plan P = pdmkb::build_plan(cell, n, pos, n_digits, n_per_leaf, nz);
+        for (int c = 0; c < k; ++c) {
+            Components C;
+            oracle_eval(P, Q + (size_t)n * c, C, true, false);
+            double* out = pot + (size_t)n * c;
+            for (int i = 0; i < n; ++i) out[i] = C.near[i] + C.mid[i] + C.self[i] + C.far[i];
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_evaluate_multi: %s\n", e.what());
+        return -1;
+    }
+}
+
 }  // extern "C"

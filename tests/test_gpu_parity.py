@@ -47,6 +47,9 @@ def test_parts_match_oracle(name, nd):
 
 
 def test_cfg1_matches_oracle_and_ewald():
+    # N = 20,000 cube, +-1 charges, 6 digits, npl 300: the reference's own
+    # CPU-runnable case.  Against the DMK oracle (same algorithm) and against
+    # an Ewald sum at every target (the physics): the drop-in bar is 2e-6.
     (cell, pos, q), npl = SYSTEMS["cube_cfg1"]()
     t = _tree(cell, pos, 6, npl)
     info = t.info()
@@ -54,6 +57,9 @@ def test_cfg1_matches_oracle_and_ewald():
     pot = t.evaluate(q)
     ref = oracle.evaluate(cell, pos, q, 6, npl, 4)
     assert rel_l2(pot, ref) < 2e-7
+    ew = oracle.ewald_targets(cell, pos, q, np.arange(len(q)), s=6.0)
+    assert rel_l2(pot, ew) < 2e-6
+    assert np.abs(pot - ew).max() < 2e-6 * np.abs(ew).max()
     t.close()
 
 
