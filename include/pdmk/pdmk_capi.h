@@ -102,6 +102,13 @@ int pdmk_stage_times_float(void* h, double* out8);
  * else FP32), 2 flops per FMA; the denominator of CUDA-core rooflines. */
 int pdmk_fma_peak(int fp64, double* tflops);
 
+/* Measured tensor-core throughput of the current device in TFLOP/s (2 flops
+ * per multiply-add): kind 0 = tcgen05 TF32 MMA with the operands in shared
+ * memory (one of the three products of a 3xTF32 split), kind 1 = FP64 DMMA
+ * (mma.sync m8n8k4, the FP64 tensor-core form of sm_100a).  The denominators
+ * of tensor-core rooflines.  Returns -1 for an unknown kind. */
+int pdmk_tc_peak(int kind, double* tflops);
+
 /* Evaluate that allocates no device memory (no counterpart in the reference).
  * For callers that cannot allocate device memory while they run -- e.g. an
  * engine whose caching allocator owns the GPU memory pool, or a time-step

@@ -45,6 +45,9 @@ def lib():
         _lib.oracle_evaluate_multi.argtypes = [d, ctypes.c_int, d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, d]
         _lib.oracle_evaluate_multi.restype = ctypes.c_int
+        _lib.oracle_tree_compare.argtypes = [d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_longlong)]
+        _lib.oracle_tree_compare.restype = ctypes.c_int
         _lib.oracle_pswf.argtypes = [ctypes.c_double, ctypes.c_int, d, d, d]
         _lib.oracle_legendre.argtypes = [ctypes.c_int, d, d]
         ip = ctypes.POINTER(ctypes.c_int)
@@ -107,6 +110,20 @@ def ewald_direct(cell, pos, q, s=5.0):
     if lib().oracle_ewald_direct(_dp(c), len(q), _dp(pos), _dp(q), s, _dp(pot), _dp(e)) != 0:
         raise RuntimeError("oracle_ewald_direct failed")
     return pot, float(e[0])
+
+
+def tree_compare(cell, pos, n_digits=6, n_per_leaf=300, nz=4):
+    """Build the tree with the oracle's independent builder (oracle_tree.cpp)
+    and compare it with the product's host plan; returns counts and mismatches."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    out = (ctypes.c_longlong * 16)()
+    c = _cell(cell)
+    if lib().oracle_tree_compare(_dp(c), len(pos), _dp(pos), n_digits, n_per_leaf, nz, out) != 0:
+        raise RuntimeError("oracle_tree_compare failed")
+    keys = ["boxes", "levels", "leaves_with_sources", "box_mismatch", "leaf_source_mismatch",
+            "leaf_target_mismatch", "pwexp_mismatch", "list1_mismatch", "list1_entries", "c2proxy_mismatch",
+            "direct_work_mismatch", "image_count_mismatch", "geometry_mismatch", "boxes_l0", "boxes_l1", "boxes_l2"]
+    return dict(zip(keys, list(out)))
 
 
 def ewald_targets(cell, pos, q, targets, s=6.0, alpha=0.0):

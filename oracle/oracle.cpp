@@ -19,7 +19,11 @@
 //     weights (the reference uses a NUFFT at tolerance eps/4);
 //   * the near field masks pairs by distance instead of culling them by box
 //     contact geometry first (culled pairs all have r >= b and contribute 0).
-// The tree, lists and tables come from the host plan builder.
+// The tree, lists and tables come from the host plan builder; the tree and
+// lists are checked box for box against the oracle's own independent builder
+// (oracle_tree.cpp, tests/test_oracle_pins.py), the tables end to end against
+// the Ewald sums below and against the reference's own PSWF / quadrature /
+// image code (golden fixtures).
 //
 // Also: a direct O(N^2) Ewald sum (cpp/src/ewald_nufft.cpp:777-910) as the
 // independent physics check.

@@ -30,7 +30,8 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
     "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float",
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
-    "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_evaluate_device_noalloc_double",
+    "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_tc_peak",
+    "pdmk_evaluate_device_noalloc_double",
     "pdmk_batch_create", "pdmk_batch_create_double", "pdmk_batch_evaluate", "pdmk_batch_evaluate_float",
     "pdmk_batch_info", "pdmk_batch_destroy",
     "pdmk_last_error",
@@ -96,6 +97,8 @@ def library():
     lib.pdmk_evaluate_device_noalloc_double.restype = ctypes.c_int
     lib.pdmk_fma_peak.argtypes = [ctypes.c_int, _D]
     lib.pdmk_fma_peak.restype = ctypes.c_int
+    lib.pdmk_tc_peak.argtypes = [ctypes.c_int, _D]
+    lib.pdmk_tc_peak.restype = ctypes.c_int
     lib.pdmk_batch_create.argtypes = [ctypes.c_int, _D, _I, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.pdmk_batch_create.restype = v
     lib.pdmk_batch_create_double.argtypes = lib.pdmk_batch_create.argtypes
@@ -374,6 +377,16 @@ def optimize_cubic_cover(cell, nz=4):
     if rc != 0:
         raise RuntimeError("pdmk_optimize_cubic_cover failed (code %d)" % rc)
     return dict(m=m.value, n=n.value, p=p.value, e1=e1, e2=e2, e3=e3, s=float(s[0]), cost=float(cost[0]))
+
+
+def tc_peak_tflops(kind="tf32"):
+    """Measured tensor-core throughput of the current CUDA device (TFLOP/s):
+    "tf32" = tcgen05 TF32 MMA, "fp64" = FP64 DMMA (mma.sync m8n8k4)."""
+    k = {"tf32": 0, "fp64": 1}[kind]
+    out = np.zeros(1)
+    if library().pdmk_tc_peak(k, _ptr(out)) != 0:
+        raise RuntimeError("pdmk_tc_peak failed: " + _last_error())
+    return float(out[0])
 
 
 def fma_peak_tflops(fp64=True):

@@ -348,6 +348,15 @@ int pdmk_fma_peak(int fp64, double* tflops) {
         return fail("pdmk_fma_peak", e);
     }
 }
+int pdmk_tc_peak(int kind, double* tflops) {
+    try {
+        if (!tflops) throw std::invalid_argument("null output");
+        *tflops = pdmkb::dev::tc_probe_tflops(kind);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_tc_peak", e);
+    }
+}
 int pdmk_info_float(void* h, int64_t* out) { return info_impl<float>(h, out); }
 
 // ---------------------------------------------------------------------------

@@ -112,6 +112,10 @@ void launch_to_float(const double* in, float* out, int64_t n, cudaStream_t s);
 
 // ---- FMA throughput probe of the current device, TFLOP/s (2 flops per FMA)
 double fma_probe_tflops(bool fp64);
+// Measured tensor-core throughput (TFLOP/s, 2 flops per multiply-add) of the
+// current device: kind 0 tcgen05 TF32 MMA (M 128, N 256, operands in shared
+// memory), kind 1 FP64 DMMA (mma.sync m8n8k4).  Defined in peaks.cu.
+double tc_probe_tflops(int kind);
 
 // ---- the two parts of the potential in user order (tests / diagnostics)
 void launch_desort_parts(const double* pot_sorted, const double* far_sorted, const double4* trg, const int* trg_perm,

@@ -70,6 +70,7 @@ struct Plan {
     std::vector<int> img_src_idx;      // image j -> originating user index
     std::vector<double> src_sorted;    // 3*n_all
     std::vector<int> src_charge_idx;   // sorted source -> user charge index
+    std::vector<int> src_perm;         // sorted source -> index in (originals ++ images)
     std::vector<double> trg_sorted;    // 3*N
     std::vector<int> trg_perm;         // sorted target -> user index
 

@@ -536,6 +536,7 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
     P.trg_sorted = std::move(B.tpos);
     P.trg_perm = std::move(B.tperm);
     P.src_charge_idx.resize(nsall);
+    P.src_perm = B.sperm;
     for (int i = 0; i < nsall; ++i) {
         const int j = B.sperm[i];
         P.src_charge_idx[i] = j < n ? j : P.img_src_idx[j - n];

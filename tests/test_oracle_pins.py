@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import TRICLINIC, clustered_system, rel_l2, uniform_system
+from conftest import TRICLINIC, batch_systems, clustered_system, rel_l2, uniform_system
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -176,3 +176,39 @@ def test_oracle_multi_equals_single_columns():
     P = oracle.evaluate_multi(cell, pos, Q, 6, 40, 4)
     for c in range(3):
         assert rel_l2(P[:, c], oracle.evaluate(cell, pos, Q[:, c], 6, 40, 4)) < 1e-14
+
+
+def _assert_same_tree(r):
+    bad = {k: v for k, v in r.items() if k.endswith("_mismatch") and v != 0}
+    assert not bad, (bad, r)
+
+
+@pytest.mark.parametrize("case", range(5))
+@pytest.mark.parametrize("npl", [20, 300])
+def test_independent_tree_matches_plan_golden_systems(case, npl):
+    # The oracle's own tree builder (oracle/oracle_tree.cpp: integer box keys,
+    # per-point descent, 2:1 balance as a fixed point) and the product's host
+    # plan give the same boxes, leaf point sets, plane-wave flags, near lists
+    # with their cutoffs, moment work and direct work on the golden systems.
+    g = _load("images.json")[case]
+    cell, pos, _ = _golden_system(g["name"])
+    r = oracle.tree_compare(cell, pos, 6, npl, g["nz"])
+    _assert_same_tree(r)
+    assert r["boxes"] >= r["boxes_l0"] > 0
+
+
+def test_independent_tree_matches_plan_clustered_triclinic():
+    # the clustered triclinic workload's shape (half the points in 64 Gaussian
+    # clusters of sigma 0.01) at 2e5 points: deep, 2:1-balanced trees
+    cell, pos, _ = clustered_system(200000, 3, TRICLINIC, n_clusters=64, sigma=0.01)
+    r = oracle.tree_compare(cell, pos, 9, 300, 4)
+    _assert_same_tree(r)
+    assert r["levels"] >= 4
+
+
+def test_independent_tree_matches_plan_batch_cells():
+    # random triclinic cells of the many-systems workload (axis sorting in the
+    # lattice QR, oblique images)
+    cells, pos, _ = batch_systems(6, 17, n_min=1000, n_max=20000)
+    for c, p in zip(cells, pos):
+        _assert_same_tree(oracle.tree_compare(c, p, 6, 300, 4))
