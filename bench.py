@@ -282,6 +282,26 @@ def cpu_baseline(n_target, steps, threads):
     return n / t / 1e6, desc, t
 
 
+def near_traffic_per_launch(pairs_full):
+    """DRAM bytes per k_near_tc launch at the bench workload, from the committed
+    ncu summary of a smaller case of the same workload (its dram__bytes read +
+    write per launch, scaled by the culled pair count: the kernel streams its
+    sources once per target tile and kept chunk, which grows with the pairs)."""
+    import re
+    path = os.path.join(ROOT, "profiles", "k_near_tc_cube2e5_6digits_64rhs.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    b = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    pr = re.search(r"culled_pairs:\s*([0-9.eE+]+)", text)
+    if not b or not pr:
+        return None
+    v = float(b.group(1)) * pairs_full / float(pr.group(1))
+    return {"bytes": v, "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_near_tc launch at "
+                                  "N=2e5 (profiles/k_near_tc_cube2e5_6digits_64rhs.md), scaled by culled pairs"}
+
+
 def parity_vs_oracle(cell, pos, Q, P_mixed, pot_plain, cols):
     """Accuracy of the timed results against the CPU oracle at the full
     workload size (part of the CPU-baseline leg: the oracle is the checker
@@ -465,9 +485,18 @@ def run_ours(args):
     e2e_value = world * n * k / (t_e2e / args.steps) / 1e6
     assert np.allclose(Ph.numpy()[0], P_mixed[0], rtol=1e-5, atol=1e-5)
 
-    # ---------------- rooflines: dominant kernel of each path (CUDA-core FMA bound)
+    # ---------------- rooflines: dominant kernel of each path
+    # k_near_tc (mixed): the kernel values run on the CUDA cores (FP32 FMA pipe),
+    # the products with the k charge vectors on the tensor cores (tcgen05 TF32),
+    # so the ideal time is split by pipe: t_ideal = F_cuda / P_fma32 + F_tc / P_tf32,
+    # F_cuda = culled pairs x (2*NC + 14), F_tc = culled pairs x 2k (each product
+    # counted once, though a 3xTF32 split issues three MMAs for it);
+    # frac = t_ideal / t_measured; achieved / peak are the same ratio expressed
+    # as rates over F_cuda + F_tc.
     pk64 = pd.fma_peak_tflops(fp64=True)
     pk32 = pd.fma_peak_tflops(fp64=False)
+    pk_tf32 = pd.tc_peak_tflops("tf32")
+    pk_dmma = pd.tc_peak_tflops("fp64")
 
     def med(sts, key):
         return statistics.median(s[key] for s in sts)
@@ -475,17 +504,31 @@ def run_ours(args):
     ncoef = int(plain_st[0]["near_ncoef"])
     pairs = plain_st[0]["near_pairs_culled"]
     near_flop_plain = pairs * (2 * ncoef + 14)
-    near_flop_mixed = pairs * (2 * ncoef + 14 + 2 * k)
+    f_cuda = pairs * (2 * ncoef + 14)
+    f_tc = pairs * 2 * k
+    t_near_mixed = med(mixed_st, "near_ms") * 1e-3
+    t_ideal = f_cuda / (pk32 * 1e12) + f_tc / (pk_tf32 * 1e12)
     ach_plain = near_flop_plain / (med(plain_st, "near_ms") * 1e-3) / 1e12
-    ach_mixed = near_flop_mixed / (med(mixed_st, "near_ms") * 1e-3) / 1e12
+    ach_mixed = (f_cuda + f_tc) / t_near_mixed / 1e12
+    peak_mixed = (f_cuda + f_tc) / t_ideal / 1e12
+    traffic = near_traffic_per_launch(pairs)
     stage_keys = ("dmk_ms", "near_ms", "nufft_ms", "finalize_ms", "total_ms")
-    roofline = {"bound": "fp32", "kernel": "k_near_tc (residual near field, %d RHS per call: FP32 kernel values on "
-                                           "the CUDA cores, TF32 hi/lo products on the tensor cores)" % k,
-                "achieved": ach_mixed, "peak": pk32, "unit": "TFLOP/s", "frac": ach_mixed / pk32,
-                "traffic": None, "peak_source": "measured FP32 FMA probe on this GPU (pdmk_fma_peak)",
-                "algorithmic_flop_per_launch": near_flop_mixed,
-                "flop_convention": "culled pairs x (2*NC + 14 + 2*k)",
+    roofline = {"bound": "tensor", "kernel": "k_near_tc (residual near field, %d RHS per call: FP32 kernel values on "
+                                             "the CUDA cores, TF32 hi/lo products on the tensor cores)" % k,
+                "achieved": ach_mixed, "peak": peak_mixed, "unit": "TFLOP/s", "frac": t_ideal / t_near_mixed,
+                "traffic": traffic["bytes"] if traffic else None,
+                "traffic_source": traffic["source"] if traffic else "no ncu summary found",
+                "split": {"f_cuda_flop": f_cuda, "f_tc_flop": f_tc, "p_fma32_tflops": pk32,
+                          "p_tf32_tflops": pk_tf32, "t_ideal_ms": t_ideal * 1e3, "t_measured_ms": t_near_mixed * 1e3,
+                          "frac_counting_three_tf32_products": (f_cuda / (pk32 * 1e12) + 3 * f_tc / (pk_tf32 * 1e12))
+                          / t_near_mixed},
+                "peak_source": "of measured: FP32 FMA probe (pdmk_fma_peak) and tcgen05 TF32 MMA probe "
+                               "(pdmk_tc_peak) on this GPU, combined by pipe",
+                "flop_convention": "culled pairs x (2*NC + 14) on the CUDA cores + culled pairs x 2k on the tensor "
+                                   "cores",
                 "stage_ms_median": {kk: med(mixed_st, kk) for kk in stage_keys}}
+    measured_peaks = {"fma_fp32_tflops": pk32, "fma_fp64_tflops": pk64, "tcgen05_tf32_tflops": pk_tf32,
+                      "dmma_fp64_tflops": pk_dmma}
     plain = {"value": plain_value, "unit": "Mpts*RHS/s", "ms_per_step": t_plain / args.steps * 1e3,
              "gpu_launches": info["launches_per_evaluate"] * args.steps,
              "roofline": {"bound": "fp64", "kernel": "k_near (residual near field)", "achieved": ach_plain,
@@ -514,7 +557,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": 4 * n * k, "ms_per_step": t_e2e / args.steps * 1e3,
                     "api": "pdmk_evaluate_multi_float (pinned host buffers)"},
             "gpu_launches": finfo["launches_last_multi"] * args.steps,
-            "roofline": roofline, "clocks": clk2.summary()}
+            "roofline": roofline, "measured_peaks": measured_peaks, "clocks": clk2.summary()}
     tree_d.close()
     tree_f.close()
     if args.batch_systems > 0:

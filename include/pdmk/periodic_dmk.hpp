@@ -15,6 +15,7 @@
 #include <array>
 #include <memory>
 #include <optional>
+#include <variant>
 #include <vector>
 
 #include "eval_timing.hpp"
@@ -60,6 +61,34 @@ class PeriodicDMKTreeT {
 };
 
 using PeriodicDMKTree = PeriodicDMKTreeT<double, 3>;
+
+/// Float / double selection by digit count (drop-in for the reference's
+/// AutoPeriodicDMKTree, cpp/include/pdmk/periodic_dmk.hpp:79-106, selection
+/// rule cpp/src/periodic_dmk.cpp:326-336): the float tree (mixed-precision
+/// path) for n_digits <= 6, the double tree (plain FP64 path) above.
+using AnyPDMKTree = std::variant<std::unique_ptr<PeriodicDMKTreeT<float, 3>>,
+                                 std::unique_ptr<PeriodicDMKTreeT<double, 3>>>;
+
+class AutoPeriodicDMKTree {
+  public:
+    AutoPeriodicDMKTree(const Mat3& cell, const std::vector<Vec3>& positions, int n_digits, int n_per_leaf = 300,
+                        int nz = 4);
+    AutoPeriodicDMKTree(const AutoPeriodicDMKTree&) = delete;
+    AutoPeriodicDMKTree& operator=(const AutoPeriodicDMKTree&) = delete;
+    AutoPeriodicDMKTree(AutoPeriodicDMKTree&&) = default;
+    AutoPeriodicDMKTree& operator=(AutoPeriodicDMKTree&&) = default;
+
+    bool is_single_precision() const { return single_precision_; }
+    /// float potentials from the float tree, double from the double tree
+    std::variant<std::vector<float>, std::vector<double>> evaluate(const std::vector<double>& charges);
+
+  private:
+    AnyPDMKTree impl_;
+    bool single_precision_ = false;
+};
+
+AutoPeriodicDMKTree make_periodic_dmk_tree(const Mat3& cell, const std::vector<Vec3>& positions, int n_digits,
+                                           int n_per_leaf = 300, int nz = 4);
 
 extern template class PeriodicDMKTreeT<double, 3>;
 extern template class PeriodicDMKTreeT<float, 3>;

@@ -77,4 +77,23 @@ std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_multi(const std::vector<
 template class PeriodicDMKTreeT<double, 3>;
 template class PeriodicDMKTreeT<float, 3>;
 
+AutoPeriodicDMKTree::AutoPeriodicDMKTree(const Mat3& cell, const std::vector<Vec3>& positions, int n_digits,
+                                         int n_per_leaf, int nz) {
+    single_precision_ = n_digits <= 6;
+    if (single_precision_)
+        impl_ = std::make_unique<PeriodicDMKTreeT<float, 3>>(cell, positions, n_digits, n_per_leaf, nz);
+    else
+        impl_ = std::make_unique<PeriodicDMKTreeT<double, 3>>(cell, positions, n_digits, n_per_leaf, nz);
+}
+
+std::variant<std::vector<float>, std::vector<double>> AutoPeriodicDMKTree::evaluate(const std::vector<double>& charges) {
+    if (single_precision_) return std::get<std::unique_ptr<PeriodicDMKTreeT<float, 3>>>(impl_)->evaluate(charges);
+    return std::get<std::unique_ptr<PeriodicDMKTreeT<double, 3>>>(impl_)->evaluate(charges);
+}
+
+AutoPeriodicDMKTree make_periodic_dmk_tree(const Mat3& cell, const std::vector<Vec3>& positions, int n_digits,
+                                           int n_per_leaf, int nz) {
+    return AutoPeriodicDMKTree(cell, positions, n_digits, n_per_leaf, nz);
+}
+
 }  // namespace pdmk
