@@ -485,6 +485,24 @@ def run_ours(args):
     e2e_value = world * n * k / (t_e2e / args.steps) / 1e6
     assert np.allclose(Ph.numpy()[0], P_mixed[0], rtol=1e-5, atol=1e-5)
 
+    # the same, with the charges stored in float32 (pdmk_evaluate_multi_float_qf32:
+    # half the bytes in, widened to double on the device)
+    Qh32 = torch.from_numpy(np.ascontiguousarray(Q.T).astype(np.float32)).pin_memory()
+    qp32 = ctypes.cast(Qh32.data_ptr(), F)
+    e2e32 = []
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = lib.pdmk_evaluate_multi_float_qf32(tree_f._h, n, k, qp32, pp)
+        e2e32.append(time.perf_counter() - t0)
+        if rc != 0:
+            raise RuntimeError("pdmk_evaluate_multi_float_qf32 failed: " + pd._last_error())
+    barrier()
+    t_e2e32 = max_over_ranks(sum(e2e32))
+    e2e32_value = world * n * k / (t_e2e32 / args.steps) / 1e6
+
     # ---------------- rooflines: dominant kernel of each path
     # k_near_tc (mixed): the kernel values run on the CUDA cores (FP32 FMA pipe),
     # the products with the k charge vectors on the tensor cores (tcgen05 TF32),
@@ -556,6 +574,10 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "Mpts*RHS/s", "h2d_bytes_per_step": 8 * n * k,
                     "d2h_bytes_per_step": 4 * n * k, "ms_per_step": t_e2e / args.steps * 1e3,
                     "api": "pdmk_evaluate_multi_float (pinned host buffers)"},
+            "e2e_float32_charges": {"value": e2e32_value, "unit": "Mpts*RHS/s", "h2d_bytes_per_step": 4 * n * k,
+                                    "d2h_bytes_per_step": 4 * n * k, "ms_per_step": t_e2e32 / args.steps * 1e3,
+                                    "api": "pdmk_evaluate_multi_float_qf32 (charges stored in float32, pinned "
+                                           "host buffers)"},
             "gpu_launches": finfo["launches_last_multi"] * args.steps,
             "roofline": roofline, "measured_peaks": measured_peaks, "clocks": clk2.summary()}
     tree_d.close()

@@ -77,6 +77,15 @@ int pdmk_evaluate_device_float(void* h, const double* charges_dev, float* pot_de
 int pdmk_evaluate_multi_device_double(void* h, int k, const double* Q_dev, double* pot_dev, int mixed);
 int pdmk_evaluate_multi_device_float(void* h, int k, const double* Q_dev, double* pot_dev);
 
+/* Charges stored in float32 (N x k column-major, charges_Nxk[i + N*c]) on a
+ * float tree (mixed-precision path): the host variant copies half the bytes of
+ * the double form in and float potentials out; the device variant takes a
+ * float charge buffer and writes double potentials.  The charges are widened
+ * to double on the device, so the results equal the double-charge calls on
+ * the same (float-representable) charges. */
+int pdmk_evaluate_multi_float_qf32(void* h, int N, int k, const float* charges_Nxk, float* pot_Nxk);
+int pdmk_evaluate_multi_device_float_qf32(void* h, int k, const float* Q_dev, double* pot_dev);
+
 /* The two parts of the potential in user order: the tree part (near field +
  * plane-wave levels - self term) and the periodic far field. */
 int pdmk_evaluate_parts_double(void* h, const double* charges, double* tree_part, double* far_part);

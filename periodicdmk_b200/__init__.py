@@ -29,6 +29,7 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
     "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
     "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float",
+    "pdmk_evaluate_multi_float_qf32", "pdmk_evaluate_multi_device_float_qf32",
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
     "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_tc_peak",
     "pdmk_evaluate_device_noalloc_double",
@@ -73,13 +74,16 @@ def library():
     lib.pdmk_evaluate_multi_device_double.restype = ctypes.c_int
     lib.pdmk_evaluate_multi_device_float.argtypes = [v, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_evaluate_multi_device_float.restype = ctypes.c_int
+    lib.pdmk_evaluate_multi_float_qf32.argtypes = [v, ctypes.c_int, ctypes.c_int, _F, _F]
+    lib.pdmk_evaluate_multi_device_float_qf32.argtypes = [v, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_info_double.argtypes = [v, _I64]
     lib.pdmk_info_float.argtypes = [v, _I64]
     for f in ("pdmk_evaluate_double", "pdmk_evaluate_float", "pdmk_evaluate_timed_double",
               "pdmk_evaluate_timed_float", "pdmk_evaluate_multi_double", "pdmk_evaluate_multi_float",
               "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
-    "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float", "pdmk_evaluate_parts_double",
-              "pdmk_info_double", "pdmk_info_float"):
+              "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float",
+              "pdmk_evaluate_multi_float_qf32", "pdmk_evaluate_multi_device_float_qf32",
+              "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float"):
         getattr(lib, f).restype = ctypes.c_int
     lib.pdmk_destroy_double.argtypes = [v]
     lib.pdmk_destroy_double.restype = None
@@ -244,6 +248,27 @@ class PeriodicDMKTree:
             rc = self._lib.pdmk_evaluate_multi_device_float(self._h, int(k), ctypes.c_void_p(q_ptr),
                                                             ctypes.c_void_p(pot_ptr))
         self._check(rc, "pdmk_evaluate_multi_device")
+
+    def evaluate_multi_f32(self, charges):
+        """k charge vectors stored as float32 (N, k) on a float tree: float32 in,
+        float32 potentials (N, k) out (pdmk_evaluate_multi_float_qf32)."""
+        if self.precision != "float":
+            raise ValueError("float32 charges are taken by float trees (mixed-precision path)")
+        Q = np.asarray(charges, dtype=np.float32)
+        if Q.ndim != 2 or Q.shape[0] != self.N:
+            raise ValueError("charges must be (N, k)")
+        k = Q.shape[1]
+        Qc = np.ascontiguousarray(Q.T)  # column-major N x k
+        out = np.empty((k, self.N), dtype=np.float32)
+        rc = self._lib.pdmk_evaluate_multi_float_qf32(self._h, self.N, k, _ptr(Qc, _F), _ptr(out, _F))
+        self._check(rc, "pdmk_evaluate_multi_float_qf32")
+        return out.T
+
+    def evaluate_multi_device_f32(self, k, q_ptr, pot_ptr):
+        """float32 charges (N x k column-major, device) -> double potentials (device); float trees."""
+        rc = self._lib.pdmk_evaluate_multi_device_float_qf32(self._h, int(k), ctypes.c_void_p(q_ptr),
+                                                             ctypes.c_void_p(pot_ptr))
+        self._check(rc, "pdmk_evaluate_multi_device_float_qf32")
 
     def evaluate_parts(self, charges):
         """(tree part, far-field part), both user order; double trees only."""

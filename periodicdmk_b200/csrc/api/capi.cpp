@@ -304,6 +304,39 @@ int pdmk_evaluate_multi_device_float(void* h, int k, const double* Q_dev, double
     return multi_device_impl<float>(h, k, Q_dev, pot_dev, true);
 }
 
+int pdmk_evaluate_multi_float_qf32(void* h, int, int k, const float* q, float* pot) {
+    if (!h) {
+        set_error("pdmk_evaluate_multi_float_qf32", "null handle");
+        return -1;
+    }
+    try {
+        if (!q || !pot) throw std::invalid_argument("null charges or output");
+        if (k <= 0) throw std::invalid_argument("k must be positive");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<float, 3>*>(h);
+        t->impl()->dev->evaluate_multi_host_f32(q, k, pot, /*fp32=*/true);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_multi_float_qf32", e);
+    }
+}
+
+int pdmk_evaluate_multi_device_float_qf32(void* h, int k, const float* Q_dev, double* pot_dev) {
+    if (!h) {
+        set_error("pdmk_evaluate_multi_device_float_qf32", "null handle");
+        return -1;
+    }
+    try {
+        if (!Q_dev || !pot_dev) throw std::invalid_argument("null device pointer");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<float, 3>*>(h);
+        auto* dv = t->impl()->dev.get();
+        dv->evaluate_multi_device_f32(Q_dev, k, pot_dev, /*fp32=*/true, nullptr);
+        PDMK_CUDA_CHECK(cudaStreamSynchronize(dv->stream()));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_multi_device_float_qf32", e);
+    }
+}
+
 int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, double* far_part) {
     if (!h) {
         set_error("pdmk_evaluate_parts", "null handle");

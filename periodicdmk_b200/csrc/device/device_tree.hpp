@@ -61,6 +61,12 @@ class DeviceTree {
     // float* (converted on the device before the copy back).
     void evaluate_multi_host(const double* Q, int k, void* pot, bool pot_float, bool fp32,
                              StageTimes* times = nullptr);
+    // Same with float charges (N x k column-major): the host variant copies
+    // float charges in and float potentials out; the device variant takes a
+    // float charge buffer on this tree's device and writes double potentials.
+    // The charges are widened to double on the device before the evaluate.
+    void evaluate_multi_host_f32(const float* Q, int k, float* pot, bool fp32);
+    void evaluate_multi_device_f32(const float* Q, int k, double* pot, bool fp32, StageTimes* times = nullptr);
     // Whether the mixed-precision path is used for this tree's digit count
     // (it is for n_digits <= 6; above that the FP64 path runs).
     bool mixed_allowed() const { return n_digits_ <= 6; }
@@ -102,6 +108,7 @@ class DeviceTree {
     double* stage_q_ = nullptr;
     double* stage_p_ = nullptr;
     size_t stage_elems_ = 0;
+    void ensure_stage(int64_t n);  // grow both staging buffers to n doubles
 
   public:
     bool last_was_multi_ = false;

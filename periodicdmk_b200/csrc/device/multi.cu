@@ -1350,22 +1350,59 @@ void launch_to_float(const double* in, float* out, int64_t n, cudaStream_t s) {
 }
 }  // namespace dev
 
+namespace dev {
+__global__ void k_to_double_in(const float* __restrict__ in, double* __restrict__ out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)in[i];
+}
+}  // namespace dev
+
+void DeviceTree::ensure_stage(int64_t n) {
+    if ((size_t)n <= stage_elems_) return;
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    if (stage_q_) cudaFree(stage_q_);
+    if (stage_p_) cudaFree(stage_p_);
+    stage_q_ = stage_p_ = nullptr;
+    stage_elems_ = 0;
+    PDMK_CUDA_CHECK(cudaMalloc(&stage_q_, sizeof(double) * (size_t)n));
+    PDMK_CUDA_CHECK(cudaMalloc(&stage_p_, sizeof(double) * (size_t)n));
+    stage_elems_ = (size_t)n;
+}
+
+void DeviceTree::evaluate_multi_device_f32(const float* Q, int k, double* pot, bool fp32, StageTimes* times) {
+    if (k <= 0) throw std::invalid_argument("k must be positive");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    const int64_t n = (int64_t)n_ * k;
+    ensure_stage(n);
+    dev::k_to_double_in<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(Q, stage_q_, n);
+    evaluate_multi_device(stage_q_, k, pot, fp32, times);
+}
+
+void DeviceTree::evaluate_multi_host_f32(const float* Q, int k, float* pot, bool fp32) {
+    if (k <= 0) throw std::invalid_argument("k must be positive");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    const int64_t n = (int64_t)n_ * k;
+    ensure_stage(n);
+    // float charges land in the upper half of the potential staging buffer,
+    // are widened into the charge staging buffer, and the float potentials
+    // are narrowed into the charge buffer after the evaluate
+    float* qf = reinterpret_cast<float*>(stage_p_) + n;
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(qf, Q, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, stream_));
+    dev::k_to_double_in<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(qf, stage_q_, n);
+    evaluate_multi_device(stage_q_, k, stage_p_, fp32, nullptr);
+    float* pf = reinterpret_cast<float*>(stage_q_);
+    dev::k_to_float_out<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(stage_p_, pf, n);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pf, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
 void DeviceTree::evaluate_multi_host(const double* Q, int k, void* pot, bool pot_float, bool fp32,
                                      StageTimes* times) {
     if (k <= 0) throw std::invalid_argument("k must be positive");
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
     const int64_t n = (int64_t)n_ * k;
     const size_t bytes = sizeof(double) * (size_t)n;
-    if ((size_t)n > stage_elems_) {
-        PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
-        if (stage_q_) cudaFree(stage_q_);
-        if (stage_p_) cudaFree(stage_p_);
-        stage_q_ = stage_p_ = nullptr;
-        stage_elems_ = 0;
-        PDMK_CUDA_CHECK(cudaMalloc(&stage_q_, bytes));
-        PDMK_CUDA_CHECK(cudaMalloc(&stage_p_, bytes));
-        stage_elems_ = (size_t)n;
-    }
+    ensure_stage(n);
     double* qd = stage_q_;
     double* pd = stage_p_;
     PDMK_CUDA_CHECK(cudaMemcpyAsync(qd, Q, bytes, cudaMemcpyHostToDevice, stream_));

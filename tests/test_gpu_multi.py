@@ -144,3 +144,27 @@ def test_mixed_accuracy_many_sources_per_box():
         assert rel_l2(Pm[:, c], ref) < 1e-6, (c, rel_l2(Pm[:, c], ref))
     tf.close()
     td.close()
+
+
+def test_float32_charges_equal_double_charges():
+    # charges stored in float32 (the 64-RHS workload keeps them in float32 and
+    # float64): widened on the device, so on float-representable charges the
+    # result equals the double-charge call
+    import torch
+
+    cell, pos, _ = uniform_system(4000, 50)
+    Q = _charges(len(pos), 16, 8).astype(np.float32)
+    t = pd.PeriodicDMKTree(cell, pos, 6, 40, 4, precision="float")
+    ref = _multi_device(t, Q.astype(np.float64), mixed=True)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    q_d = torch.from_numpy(np.ascontiguousarray(Q.T)).to(dev)
+    p_d = torch.empty((16, len(pos)), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    t.evaluate_multi_device_f32(16, q_d.data_ptr(), p_d.data_ptr())
+    P = p_d.cpu().numpy().T
+    H = t.evaluate_multi_f32(Q)
+    assert H.dtype == np.float32
+    for c in range(16):
+        assert rel_l2(P[:, c], ref[:, c]) < 1e-12
+        assert rel_l2(H[:, c], ref[:, c]) < 1e-7
+    t.close()
