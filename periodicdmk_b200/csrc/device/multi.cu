@@ -1212,6 +1212,17 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                 t.pair_chunk_base = near_pair_chunk_base_; t.chunk_lo = near_chunk_lo_; t.chunk_hi = near_chunk_hi_;
                 t.N = n_; t.kb = kb;
                 for (int i = 0; i < near_.nc; ++i) t.coef[i] = near_.coef[i];
+                // Test hook of the failure detection (never set in normal use):
+                // PDMK_TEST_WITHHOLD_NEAR_CHUNK=j makes the first tile withhold
+                // chunk j's MMAs and commits; its next pipeline wait then runs
+                // out after ~10 ms, the kernel aborts cleanly and sets the error
+                // word, and the evaluate returns -2.
+                t.withhold_chunk = -1;
+                t.wait_cycles = 4000000000LL;
+                if (const char* w = std::getenv("PDMK_TEST_WITHHOLD_NEAR_CHUNK")) {
+                    t.withhold_chunk = std::atoi(w);
+                    t.wait_cycles = 20000000LL;
+                }
                 tc_done = dev::launch_near_tc(t, near_.nc, m.trg_hi, m.trg_lo, m.src_hi, m.src_lo,
                                               reinterpret_cast<const float*>(src_q), m.pot, m.err, s);
             }

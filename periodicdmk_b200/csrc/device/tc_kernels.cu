@@ -447,6 +447,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
     int* s_kept = reinterpret_cast<int*>(sm + kN_OFF_BAR + 56);  // chunks kept after the cull
     float* s_tbox = reinterpret_cast<float*>(sm + kN_OFF_BAR + 64);   // [4 warps][6], then tile box [6]
     int* s_wcnt = reinterpret_cast<int*>(sm + kN_OFF_BAR + 192);      // [16] kept per warp
+    int* s_last_commit = reinterpret_cast<int*>(sm + kN_OFF_BAR + 60);  // last chunk whose MMAs were committed
     NearPair* pairs = reinterpret_cast<NearPair*>(sm + kN_OFF_PAIR);
     int* pref = reinterpret_cast<int*>(sm + kN_OFF_PREF);
     int* list = reinterpret_cast<int*>(sm + kN_OFF_LIST);
@@ -466,6 +467,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
         tc::mbar_init(&bar[2], 1);
         tc::mbar_init(&bar[3], 1);
         s_abort[0] = s_abort[1] = s_abort[2] = 0;
+        *s_last_commit = -1;
         int np = 0, nch = 0;
         pref[0] = 0;
         for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
@@ -611,7 +613,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
     // Add segment gg's accumulator (TMEM buffer gg & 1) to the FP64 sums.  Warp w
     // reads TMEM lanes 32 (w % 4) .. +31 (targets) and columns 16 (w / 4) .. +15 (RHS).
     auto drain = [&](int gg) -> bool {
-        const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1);
+        const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1, a.wait_cycles);
         if (!__all_sync(0xffffffffu, waited)) return false;  // keep the warp-collective loads uniform
         tc::fence_after_sync();
         const int lq = warp & 3, cg = warp >> 2;
@@ -656,7 +658,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
                 if (q + 2 < nchunks) pnext = load_pos(q + 2);
             }
         }
-        if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1)) s_abort[st] = 1;
+        if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1, a.wait_cycles)) s_abort[st] = 1;
         unsigned char* stage = sm + st * kNStage;
         const float4* sh = reinterpret_cast<const float4*>(sm + kN_OFF_SRC + st * kNSrc);
         const float4* sl = sh + kNKC;
@@ -704,7 +706,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
         tc::fence_proxy_async();
         __syncthreads();
         if (s_abort[st]) break;
-        if (tid == 0) {
+        if (tid == 0 && !(blockIdx.x == 0 && q == a.withhold_chunk)) {
             tc::fence_after_sync();
             const uint32_t base = tc::smem_u32(stage);
             const uint32_t idesc = tc::idesc_tf32(128, NBp);
@@ -722,6 +724,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
             }
             tc::commit(&bar[st]);
             if (last) tc::commit(&bar[2 + (seg & 1)]);
+            *s_last_commit = q;
         }
         issued = q + 1;
         // fold the previous segment while this one runs on the tensor core
@@ -734,12 +737,16 @@ __global__ void __launch_bounds__(kNThreads, 1)
     bool ok = s_abort[0] == 0 && s_abort[1] == 0;
     if (ok && issued > 0) {
         if (!drain((issued - 1) / kNSeg)) s_abort[2] = 1;
-    } else if (!ok && issued > 0) {
-        const int ql = issued - 1;
-        tc::mbar_wait(&bar[ql & 1], (ql >> 1) & 1);
     }
     __syncthreads();
     ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;
+    if (!ok) {
+        // wait (bounded) until this CTA's MMAs in flight are done before the
+        // tensor memory is freed: tensor-core ops complete in issue order, so
+        // the last committed chunk's barrier covers all of them
+        const int lc = *s_last_commit;
+        if (lc >= 0) tc::mbar_wait(&bar[lc & 1], (lc >> 1) & 1);
+    }
     if (ok) {
         for (int i = tid; i < kb * 128; i += kNThreads) {
             const int c = i >> 7, mm = i & 127;

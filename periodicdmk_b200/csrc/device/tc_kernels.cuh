@@ -43,6 +43,12 @@ struct NearTc {
     int max_trg;  // largest trg_count (grid extent over 128-target tiles)
     int64_t N;
     int kb;
+    // Failure-detection test hook: CTA 0 issues neither the MMAs nor the
+    // commits of chunk withhold_chunk (-1: none), so a later bounded wait on
+    // that chunk's barrier runs out; wait_cycles bounds the pipeline waits
+    // inside the chunk loop (SM clock cycles).
+    int withhold_chunk;
+    long long wait_cycles;
 };
 constexpr int kNearTcMaxPairs = 128;
 constexpr int kNearTcChunk = 32;        // sources per chunk
