@@ -117,6 +117,9 @@ class DeviceTree {
     // moments, bit 1 near field, bit 2 leaf evaluation); the CUDA-core
     // kernels cover the rest.  Initialised from PDMK_TC_MASK (default 7).
     int tc_mask_ = 7;
+    // Near-field tensor-core kernel shape: 1 = 1024 threads per CTA (32 warps
+    // per SM), 0 = 512 threads.  Initialised from PDMK_NEAR_TC_WIDE (default 0).
+    int near_tc_wide_ = 0;
 
   private:
     void init(const Plan& P, int device, bool fp64_working_set);
