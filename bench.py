@@ -176,6 +176,27 @@ def run_batch(pd, args, world, rank, barrier, max_over_ranks):
     total = sum(len(q) for q in qs)
     info = b.info()
     b.close()
+    # the same systems as a loop of plain per-system calls (one float tree per
+    # system, pdmk_evaluate_float with host buffers, one after another); trees
+    # built on host threads (the ctypes calls release the GIL)
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        singles = list(ex.map(lambda i: pd.PeriodicDMKTree(cells[i], pos[i], n_digits=6, n_per_leaf=300, nz=4,
+                                                           precision="float"), mine))
+    for tr, q in zip(singles, q_mine):
+        tr.evaluate(q)
+        tr.evaluate(q)
+    barrier()
+    tl = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        for tr, q in zip(singles, q_mine):
+            tr.evaluate(q)
+        tl.append(time.perf_counter() - t0)
+    barrier()
+    t_loop = max_over_ranks(statistics.median(tl))
+    for tr in singles:
+        tr.close()
     return {"workload": "%d independent periodic systems: triclinic cells (lengths U[0.8,1.2], angles "
                         "U[75,105] deg), N log-uniform in [1e3,1e5] (total %d points), +-1 charges, 6 digits, "
                         "npl 300, nz 4, float trees (mixed precision), one RHS" % (len(qs), total),
@@ -183,6 +204,9 @@ def run_batch(pd, args, world, rank, barrier, max_over_ranks):
             "timing": "host wall clock of the synchronous pdmk_batch_evaluate call (charges H2D and potentials "
                       "D2H included), median of steps, max over ranks",
             "partition": "LPT on point counts over %d rank(s)" % world,
+            "loop_of_plain_calls": {"value": total / t_loop / 1e6, "unit": "Mpts/s", "ms_per_step": t_loop * 1e3,
+                                    "api": "pdmk_evaluate_float per system, one after another (host buffers)"},
+            "batch_vs_loop": t_loop / t,
             "host_build_s": t_build, "device_bytes_rank0": info["device_bytes"]}
 
 

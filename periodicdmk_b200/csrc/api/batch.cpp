@@ -5,16 +5,25 @@
 // Construction: the host plans (tree, lists, tables) of all systems are built
 // on all host threads, then uploaded one by one.  Evaluate: one host->device
 // copy of all charges, every system's evaluate enqueued on its own stream
-// after that copy, one device->host copy of all potentials after every
-// system's stream has finished.
+// after that copy (replayed from a CUDA graph from the second evaluate on), one
+// device->host copy of all potentials after every system has finished.
+// Float trees (one charge vector per system) leave their near field and final
+// gather out of the per-system sequences: after all systems' other stages one
+// persistent kernel pulls (system, leaf) items from a device queue, largest
+// first, and writes every system's potentials (batch_near.cu).  Its targets per
+// thread are chosen at the first evaluate by timing the candidates (an
+// autotuner whose choice is cached per batch shape for the process).
 #include "batch.hpp"
 
 #include <algorithm>
 #include <atomic>
 #include <exception>
+#include <map>
 #include <mutex>
+#include <numeric>
 #include <stdexcept>
 #include <thread>
+#include <tuple>
 
 #include "../host/plan.hpp"
 
@@ -70,6 +79,25 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         PDMK_CUDA_CHECK(cudaMalloc(&potf_dev_, sizeof(float) * n));
         PDMK_CUDA_CHECK(cudaMallocHost(&err_host_, sizeof(int) * nsys));
         graphs_.assign(nsys, nullptr);
+        if (single_) {
+            for (auto& t : trees_) t->defer_near_ = true;
+            // queue items: every system's near-field leaves, largest work first
+            std::vector<std::tuple<int64_t, int, int>> items;
+            for (int i = 0; i < nsys; ++i) {
+                const auto& cost = trees_[i]->near_leaf_cost();
+                for (int e = 0; e < trees_[i]->near_leaves(); ++e) items.emplace_back(-cost[e], i, e);
+            }
+            std::stable_sort(items.begin(), items.end());
+            std::vector<int2> it(items.size());
+            for (size_t k = 0; k < items.size(); ++k) it[k] = make_int2(std::get<1>(items[k]), std::get<2>(items[k]));
+            n_items_ = (int)it.size();
+            PDMK_CUDA_CHECK(cudaMalloc(&items_dev_, sizeof(int2) * std::max<size_t>(it.size(), 1)));
+            PDMK_CUDA_CHECK(cudaMemcpy(items_dev_, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
+            PDMK_CUDA_CHECK(cudaMalloc(&sys_dev_, sizeof(dev::NearLeafSys) * nsys));
+            PDMK_CUDA_CHECK(cudaMalloc(&head_dev_, sizeof(int)));
+            nc_ = trees_[0]->near_coeffs();
+            for (int i = 0; i < nc_; ++i) coef32_[i] = (float)trees_[0]->near_coef()[i];
+        }
     } catch (...) {
         release();
         throw;
@@ -93,6 +121,12 @@ void TreeBatch::release() {
     if (q_dev_) cudaFree(q_dev_);
     if (pot_dev_) cudaFree(pot_dev_);
     if (potf_dev_) cudaFree(potf_dev_);
+    if (sys_dev_) cudaFree(sys_dev_);
+    if (items_dev_) cudaFree(items_dev_);
+    if (head_dev_) cudaFree(head_dev_);
+    sys_dev_ = nullptr;
+    items_dev_ = nullptr;
+    head_dev_ = nullptr;
     ready_ = nullptr;
     stream_ = nullptr;
     q_dev_ = pot_dev_ = nullptr;
@@ -153,6 +187,7 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
         PDMK_CUDA_CHECK(cudaEventRecord(done_[i], ts));
         PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
     }
+    if (single_) run_queue();
     if (pot_float) {
         dev::launch_to_float(pot_dev_, potf_dev_, n, stream_);
         PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, potf_dev_, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_));
@@ -177,6 +212,69 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
     if (n_err)
         for (size_t i = 0; i < trees_.size(); ++i)
             if (err_host_[i]) trees_[i]->check_device_error();  // clears the word and throws
+}
+
+void TreeBatch::build_queue() {
+    // descriptors of every system's buffers (its single-RHS float state exists
+    // after the first deferred evaluate)
+    std::vector<dev::NearLeafSys> d(trees_.size());
+    for (size_t i = 0; i < trees_.size(); ++i) trees_[i]->near_leaf_sys(d[i], pot_dev_ + off_[i]);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(sys_dev_, d.data(), sizeof(dev::NearLeafSys) * d.size(), cudaMemcpyHostToDevice,
+                                    stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    queue_built_ = true;
+}
+
+namespace {
+// autotuner cache: (items, total points, polynomial length, device) -> targets per thread
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int64_t, int, int>, int> g_tune;
+}  // namespace
+
+void TreeBatch::run_queue() {
+    if (!queue_built_) build_queue();
+    dev::BatchNearArgs a{};
+    a.sys = sys_dev_;
+    a.items = items_dev_;
+    a.n_items = n_items_;
+    a.head = head_dev_;
+    for (int i = 0; i < 32; ++i) a.coef32[i] = coef32_[i];
+    if (tpt_ == 0) {
+        const auto key = std::make_tuple(n_items_, total_points(), nc_, device_);
+        {
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            auto it = g_tune.find(key);
+            if (it != g_tune.end()) tpt_ = it->second;
+        }
+        if (tpt_ == 0) {
+            // time each candidate once on this batch (the kernel writes the
+            // potentials from inputs it does not modify, so repeats are harmless)
+            cudaEvent_t e0, e1;
+            PDMK_CUDA_CHECK(cudaEventCreate(&e0));
+            PDMK_CUDA_CHECK(cudaEventCreate(&e1));
+            float best = 1e30f;
+            for (int tpt : {1, 2, 4}) {
+                const int ctas = dev::batch_near_ctas(nc_, tpt);
+                PDMK_CUDA_CHECK(cudaEventRecord(e0, stream_));
+                dev::launch_batch_near(a, nc_, tpt, ctas, stream_);
+                PDMK_CUDA_CHECK(cudaEventRecord(e1, stream_));
+                PDMK_CUDA_CHECK(cudaEventSynchronize(e1));
+                float ms = 0;
+                PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    tpt_ = tpt;
+                }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            g_tune[key] = tpt_;
+        }
+        ctas_ = dev::batch_near_ctas(nc_, tpt_);
+    }
+    dev::launch_batch_near(a, nc_, tpt_, ctas_, stream_);
+    PDMK_CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace pdmkb

@@ -44,6 +44,22 @@ class TreeBatch {
     std::vector<cudaGraphExec_t> graphs_;
     int* err_host_ = nullptr;  // pinned, one word per system
     int evaluates_ = 0;
+    // Float trees: the near field and final gather of all systems run as one
+    // persistent launch over a device queue of (system, leaf) items.
+    void build_queue();
+    void run_queue();
+    dev::NearLeafSys* sys_dev_ = nullptr;
+    int2* items_dev_ = nullptr;
+    int* head_dev_ = nullptr;
+    int n_items_ = 0;
+    int nc_ = 0;
+    float coef32_[32] = {};
+    bool queue_built_ = false;
+    int tpt_ = 0, ctas_ = 0;  // targets per thread and grid of the queue kernel (autotuned)
+
+  public:
+    // targets per thread chosen by the autotuner (0 before the first evaluate)
+    int queue_targets_per_thread() const { return tpt_; }
 };
 
 }  // namespace pdmkb

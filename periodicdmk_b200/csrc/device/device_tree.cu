@@ -721,6 +721,15 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             }
             ps.push_back((int)s0.size());
         }
+        near_leaf_cost_.assign(tc.size(), 0);
+        int64_t near_targets = 0;
+        for (size_t i = 0; i < tc.size(); ++i) {
+            int64_t ns = 0;
+            for (int k = ps[i]; k < ps[i + 1]; ++k) ns += sc[k];
+            near_leaf_cost_[i] = (int64_t)tc[i] * ns;
+            near_targets += tc[i];
+        }
+        check(near_targets == n_, "near-field leaves cover every target once");
         for (size_t i = 0; i < tc.size(); ++i) {
             near_max_trg_ = std::max(near_max_trg_, tc[i]);
             near_max_pairs_ = std::max(near_max_pairs_, ps[i + 1] - ps[i]);

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../host/plan.hpp"
+#include "batch_near.cuh"
 #include "kernels.cuh"
 
 namespace pdmkb {
@@ -112,6 +113,19 @@ class DeviceTree {
 
   public:
     bool last_was_multi_ = false;
+    // Set by a batch of systems: single-RHS float evaluates leave out the near
+    // field and the final gather, which the batch's queue kernel does for all
+    // systems in one launch (batch_near.cu).
+    bool defer_near_ = false;
+    // Descriptor of this tree's buffers for the batch near-field kernel (the
+    // single-RHS float state must exist: one deferred evaluate has run);
+    // out = this system's potentials in user order.
+    void near_leaf_sys(dev::NearLeafSys& d, double* out) const;
+    // Near-field leaves (target leaves) and their estimated work (targets x
+    // sources over the leaf's near pairs), host copies.
+    int near_leaves() const { return near_.n_leaves; }
+    const std::vector<int64_t>& near_leaf_cost() const { return near_leaf_cost_; }
+    const double* near_coef() const { return near_.coef; }
     int multi_launches_ = 0;  // kernels launched by the last multi-RHS evaluate
     // Tensor-core kernels the mixed-precision path may use (bit 0 proxy
     // moments, bit 1 near field, bit 2 leaf evaluation); the CUDA-core
@@ -154,6 +168,7 @@ class DeviceTree {
     int64_t near_pairs_culled_ = 0, near_pairs_nominal_ = 0;
     int near_max_trg_ = 0, near_max_pairs_ = 0;  // largest target count / source-box count of a near-field leaf
     int near_max_chunks_ = 0;                     // largest number of 32-source chunks of a near-field leaf
+    std::vector<int64_t> near_leaf_cost_;         // per near-field leaf: targets x near sources
     int* near_pair_chunk_base_ = nullptr;         // per near pair: first chunk bounding box of its source box
     float4* near_chunk_lo_ = nullptr;
     float4* near_chunk_hi_ = nullptr;

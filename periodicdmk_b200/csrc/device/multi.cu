@@ -1192,8 +1192,9 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         }
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
-    // near field
-    if (near_.n_leaves > 0) {
+    // near field (left to the batch's queue kernel when deferred)
+    const bool deferred = f32 && defer_near_ && kb == 1;
+    if (near_.n_leaves > 0 && !deferred) {
         dev::NearM a{};
         a.trg_start = near_.trg_start; a.trg_count = near_.trg_count; a.pair_start = near_.pair_start;
         a.pair_src_start = near_.pair_src_start; a.pair_src_count = near_.pair_src_count;
@@ -1276,7 +1277,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         dev::launch_interp_multi(na, m.esw, n_, kb, s); ++nl;
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
-    {
+    if (!deferred) {
         const int64_t tot = (int64_t)n_ * kvalid;
         dev::k_finalize_m<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m.pot, m.far, trg_, trg_perm_, m.q_t, pot_user,
                                                                         n_, kvalid); ++nl;
@@ -1284,6 +1285,28 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[4], s));
     PDMK_CUDA_CHECK(cudaGetLastError());
     multi_launches_ += nl;
+}
+
+void DeviceTree::near_leaf_sys(dev::NearLeafSys& d, double* out) const {
+    const MultiState* m = multi_[1].get();
+    if (!m || m->kb != 1) throw std::logic_error("near_leaf_sys: no single-RHS float state");
+    d.trg_start = near_.trg_start;
+    d.trg_count = near_.trg_count;
+    d.pair_start = near_.pair_start;
+    d.pair_src_start = near_.pair_src_start;
+    d.pair_src_count = near_.pair_src_count;
+    d.pair_bsize = near_.pair_bsize;
+    d.trg_hi = m->trg_hi;
+    d.trg_lo = m->trg_lo;
+    d.src_hi = m->src_hi;
+    d.src_lo = m->src_lo;
+    d.src_q = static_cast<const float*>(m->src_q);
+    d.pot = m->pot;
+    d.far = m->far;
+    d.trg = trg_;
+    d.perm = trg_perm_;
+    d.q_t = m->q_t;
+    d.out = out;
 }
 
 void DeviceTree::evaluate_multi_device(const double* Q, int k, double* pot, bool fp32, StageTimes* times) {
