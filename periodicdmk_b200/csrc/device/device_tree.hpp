@@ -128,8 +128,9 @@ class DeviceTree {
     const double* near_coef() const { return near_.coef; }
     int multi_launches_ = 0;  // kernels launched by the last multi-RHS evaluate
     // Tensor-core kernels the mixed-precision path may use (bit 0 proxy
-    // moments, bit 1 near field, bit 2 leaf evaluation); the CUDA-core
-    // kernels cover the rest.  Initialised from PDMK_TC_MASK (default 7).
+    // moments, bit 1 near field, bit 2 leaf evaluation, bit 3 the separable
+    // translation and plane-wave transform steps); the CUDA-core kernels cover
+    // the rest.  Initialised from PDMK_TC_MASK (default 7).
     int tc_mask_ = 7;
     // Near-field tensor-core kernel shape: 1 = 1024 threads per CTA (32 warps
     // per SM), 0 = 512 threads.  Initialised from PDMK_NEAR_TC_WIDE (default 0).

@@ -21,6 +21,7 @@
 #include "nufft_multi.cuh"
 #include "pw_fused.cuh"
 #include "sep3.cuh"
+#include "contract_tc.cuh"
 #include "tc_kernels.cuh"
 
 namespace pdmkb {
@@ -1061,13 +1062,36 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             ++nl;
         }
     }
+    // Transforms on the tensor cores (FP32 blocks, PDMK_TC_MASK bit 3): every
+    // separable step is one tcgen05 contraction (contract_tc.cu); the chunks
+    // of (box, RHS) entries are sized so that the step intermediates stay in L2.
+    const bool tc_tr = f32 && (tc_mask_ & 8) && dev::contract_tc_supported(n, n, 2, 2) &&
+                       dev::contract_tc_supported(p, p, 1, 1);
+    const int64_t l2_scratch = 64ll << 20;
     // chunked batched contraction helper over (box, rhs) entries
     auto chunked = [&](int n_boxes, int64_t per_entry_bytes, auto&& body) {
         const int64_t total = (int64_t)n_boxes * kb;
-        const int64_t C = std::max<int64_t>(1, sbytes / std::max<int64_t>(per_entry_bytes, 1));
+        int64_t C = std::max<int64_t>(1, sbytes / std::max<int64_t>(per_entry_bytes, 1));
+        if (tc_tr) C = std::max<int64_t>(1, std::min<int64_t>(C, l2_scratch / std::max<int64_t>(per_entry_bytes, 1)));
         for (int64_t e0 = 0; e0 < total; e0 += C) body(e0, (int)std::min<int64_t>(C, total - e0));
     };
-    const bool fused = dev::sep3_supported<T>(p);
+    // one contraction step: tensor cores when selected, else the CUDA-core kernel
+    // (ci / co: 1 real, 2 complex input / output; cm: complex matrix)
+    auto step = [&](const dev::ContractM& c, int ci, int co, bool cm, auto launch_cuda_core) {
+        if (tc_tr) {
+            dev::ContractTc t{};
+            t.in = static_cast<const float*>(c.in); t.in_off = c.in_off; t.in_stride = c.in_stride; t.in_unit = c.in_unit;
+            t.out = static_cast<float*>(c.out); t.out_off = c.out_off; t.out_stride = c.out_stride; t.out_unit = c.out_unit;
+            t.mat = static_cast<const float*>(c.mat); t.mat_off = c.mat_off; t.mat_complex = cm ? 1 : 0;
+            t.ni = c.ni; t.na = c.na; t.R = c.R; t.ci = ci; t.co = co; t.rhs = c.rhs; t.e0 = c.e0;
+            t.n_entries = c.n_entries; t.accumulate = c.mode != dev::kStore ? 1 : 0;
+            t.scale = c.mode == dev::kAddRealScaled ? (float)c.scale : 1.0f; t.err = m.err;
+            dev::launch_contract_tc(t, s);
+        } else {
+            launch_cuda_core(c);
+        }
+    };
+    const bool fused = dev::sep3_supported<T>(p) && !tc_tr;
     // upward children -> parents
     for (const auto& g : c2p_groups_) {
         const T* mx = c2pm + (int64_t)g.child * 3 * p * p;
@@ -1078,20 +1102,21 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             dev::launch_sep3<T>(f, p, g.n * kb, s); ++nl;
             continue;
         }
-        chunked(g.n, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {
+        chunked(g.n, (int64_t)sizeof(T) * ncoef * 2, [&](int64_t e0, int ne) {
+            auto rrr = [&](const dev::ContractM& c) { dev::launch_contract_m<T, T, T>(c, s); };
             dev::ContractM a{};
             a.rhs = kb; a.e0 = e0; a.n_entries = ne;
             a.in = up; a.in_off = g.in_off; a.in_unit = ncoef; a.out = m.s1; a.out_stride = ncoef;
             a.mat = mx; a.ni = p; a.na = p; a.R = p * p; a.mode = dev::kStore;
-            dev::launch_contract_m<T, T, T>(a, s); ++nl;
+            step(a, 1, 1, false, rrr); ++nl;
             a.in = m.s1; a.in_off = nullptr; a.in_stride = ncoef; a.out = m.s2; a.mat = mx + p * p;
-            dev::launch_contract_m<T, T, T>(a, s); ++nl;
+            step(a, 1, 1, false, rrr); ++nl;
             a.in = m.s2; a.out = up; a.out_off = g.out_off; a.out_unit = ncoef; a.mat = mx + 2 * p * p; a.mode = dev::kAdd;
-            dev::launch_contract_m<T, T, T>(a, s); ++nl;
+            step(a, 1, 1, false, rrr); ++nl;
         });
     }
     // outgoing plane waves
-    const bool pw_fused = dev::pw_fused_supported<T>(p, n, n2);
+    const bool pw_fused = dev::pw_fused_supported<T>(p, n, n2) && !tc_tr;
     for (const auto& g : pw_groups_) {
         if (pw_fused) {
             dev::PwFused f{};
@@ -1101,17 +1126,19 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             continue;
         }
         const int64_t e1 = (int64_t)p * p * n, e2 = (int64_t)p * n * n;
-        chunked(g.n, (int64_t)sizeof(C) * std::max(e1, e2), [&](int64_t e0, int ne) {
+        chunked(g.n, (int64_t)sizeof(C) * (tc_tr ? e1 + e2 : std::max(e1, e2)), [&](int64_t e0, int ne) {
+            auto rcc = [&](const dev::ContractM& c) { dev::launch_contract_m<T, C, C>(c, s); };
+            auto ccc = [&](const dev::ContractM& c) { dev::launch_contract_m<C, C, C>(c, s); };
             dev::ContractM a{};
             a.rhs = kb; a.e0 = e0; a.n_entries = ne;
             a.in = up; a.in_off = g.in_off; a.in_unit = ncoef; a.out = m.s1; a.out_stride = e1;
             a.mat = levtab(g.level, 0); a.ni = p; a.na = n; a.R = p * p; a.mode = dev::kStore;
-            dev::launch_contract_m<T, C, C>(a, s); ++nl;
+            step(a, 1, 2, true, rcc); ++nl;
             a.in = m.s1; a.in_off = nullptr; a.in_stride = e1; a.out = m.s2; a.out_stride = e2; a.R = p * n;
-            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            step(a, 2, 2, true, ccc); ++nl;
             a.in = m.s2; a.in_stride = e2; a.out = pw; a.out_off = g.out_off; a.out_unit = M;
             a.mat = levtab(g.level, 1); a.na = n2; a.R = n * n;
-            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            step(a, 2, 2, true, ccc); ++nl;
         });
     }
     // downward per level
@@ -1135,16 +1162,18 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                 dev::launch_pw_in_fused<T>(f, p, n, n2, nb * kb, s); ++nl;
                 continue;
             }
+            auto ccc = [&](const dev::ContractM& c) { dev::launch_contract_m<C, C, C>(c, s); };
+            auto ccr = [&](const dev::ContractM& c) { dev::launch_contract_m<C, C, T>(c, s); };
             dev::ContractM a{};
             a.rhs = kb; a.e0 = (int64_t)b0 * kb; a.n_entries = nb * kb;
             a.in = m.pw_in; a.in_stride = M; a.out = m.s1; a.out_stride = e1;
             a.mat = levtab(E.level, 2); a.ni = n; a.na = p; a.R = n * n2; a.mode = dev::kStore;
-            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            step(a, 2, 2, true, ccc); ++nl;
             a.in = m.s1; a.in_stride = e1; a.out = m.s2; a.out_stride = e2; a.R = n2 * p;
-            dev::launch_contract_m<C, C, C>(a, s); ++nl;
+            step(a, 2, 2, true, ccc); ++nl;
             a.in = m.s2; a.in_stride = e2; a.out = down; a.out_off = E.down_off; a.out_unit = ncoef;
             a.mat = levtab(E.level, 3); a.ni = n2; a.R = p * p; a.mode = dev::kAddRealScaled; a.scale = 2.0;
-            dev::launch_contract_m<C, C, T>(a, s); ++nl;
+            step(a, 2, 1, true, ccr); ++nl;
         }
         if (E.n_p2c && fused) {
             dev::Sep3 f{};
@@ -1154,17 +1183,19 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             f.mat_off = E.p2c_mat; f.rhs = kb; f.accumulate = 0; f.tri = 2;
             dev::launch_sep3<T>(f, p, E.n_p2c * kb, s); ++nl;
         } else if (E.n_p2c) {
-            chunked(E.n_p2c, (int64_t)sizeof(T) * ncoef, [&](int64_t e0, int ne) {
+            chunked(E.n_p2c, (int64_t)sizeof(T) * ncoef * 2, [&](int64_t e0, int ne) {
+                auto rrr = [&](const dev::ContractM& c) { dev::launch_contract_m<T, T, T>(c, s); };
                 dev::ContractM b{};
                 b.rhs = kb; b.e0 = e0; b.n_entries = ne;
                 b.in = down; b.in_off = E.p2c_in; b.in_unit = ncoef; b.out = m.s1; b.out_stride = ncoef;
                 b.mat = p2cm; b.mat_off = E.p2c_mat; b.ni = p; b.na = p; b.R = p * p; b.mode = dev::kStore;
-                dev::launch_contract_m<T, T, T>(b, s); ++nl;
+                step(b, 1, 1, false, rrr); ++nl;
                 b.in = m.s1; b.in_off = nullptr; b.in_stride = ncoef; b.out = m.s2; b.mat = p2cm + p * p;
-                dev::launch_contract_m<T, T, T>(b, s); ++nl;
+                b.mat_off = E.p2c_mat;
+                step(b, 1, 1, false, rrr); ++nl;
                 b.in = m.s2; b.out = down; b.out_off = E.p2c_out; b.out_unit = ncoef; b.mat = p2cm + 2 * p * p;
                 b.mode = dev::kAdd;
-                dev::launch_contract_m<T, T, T>(b, s); ++nl;
+                step(b, 1, 1, false, rrr); ++nl;
             });
         }
     }

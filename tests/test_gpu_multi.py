@@ -168,3 +168,21 @@ def test_float32_charges_equal_double_charges():
         assert rel_l2(P[:, c], ref[:, c]) < 1e-12
         assert rel_l2(H[:, c], ref[:, c]) < 1e-7
     t.close()
+
+
+@pytest.mark.parametrize("nd,tol", [(6, 1e-6), (3, 2e-4)])
+def test_tensor_core_transforms(nd, tol, monkeypatch):
+    # PDMK_TC_MASK bit 3 (read when the tree is built) runs the translation and
+    # plane-wave transform steps as tcgen05 contractions (3xTF32); same bars as
+    # the CUDA-core transforms, against the FP64 path
+    cell, pos, _ = clustered_system(6000, 48, TRICLINIC, n_clusters=4, sigma=0.03)
+    Q = _charges(len(pos), 64, 6)
+    td = pd.PeriodicDMKTree(cell, pos, nd, 40, 4)
+    Pd = _multi_device(td, Q, mixed=False)
+    td.close()
+    monkeypatch.setenv("PDMK_TC_MASK", "15")
+    t = pd.PeriodicDMKTree(cell, pos, nd, 40, 4)
+    Pm = _multi_device(t, Q, mixed=True)
+    t.close()
+    errs = [rel_l2(Pm[:, c], Pd[:, c]) for c in range(64)]
+    assert max(errs) < tol, (int(np.argmax(errs)), max(errs))
