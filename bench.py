@@ -293,16 +293,19 @@ def cpu_baseline(n_target, steps, threads):
     n = 100000
     scale = (n / float(n_target)) ** (1.0 / 3.0)
     cell, pos, q = make_system(n, seed=2, scale=scale)
-    oracle.evaluate(cell, pos, q, 6, 300, 4, with_far=True, fast_far=True)  # warm-up
+    pl = oracle.Plan(cell, pos, 6, 300, 4)  # build once (not timed), as the reference's tree
+    pl.evaluate(q, fast_far=True)  # warm-up
     ts = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        oracle.evaluate(cell, pos, q, 6, 300, 4, with_far=True, fast_far=True)
+        pl.evaluate(q, fast_far=True)
         ts.append(time.perf_counter() - t0)
+    pl.close()
     t = statistics.median(ts)
     desc = ("CPU oracle (FP64 restatement of the reference evaluate: upward/plane-wave/near/self stages + "
-            "CPU NUFFT far field), N=%d uniform in a cube of side %.4f (same density as the N=%d workload), "
-            "6 digits, npl 300, nz 4, %d OpenMP threads, median of %d" % (n, scale, n_target, threads, steps))
+            "CPU NUFFT far field; plan built once, not timed), N=%d uniform in a cube of side %.4f (same density "
+            "as the N=%d workload), 6 digits, npl 300, nz 4, %d OpenMP threads, median of %d"
+            % (n, scale, n_target, threads, steps))
     return n / t / 1e6, desc, t
 
 
@@ -348,6 +351,68 @@ def parity_vs_oracle(cell, pos, Q, P_mixed, pot_plain, cols):
            "oracle": "CPU DMK restatement (FP64, exact reciprocal-lattice far field) at N=%d" % len(pos),
            "oracle_s": time.perf_counter() - t0}
     return out
+
+
+def run_cpu_configs(args):
+    """CPU baseline per workload: the oracle (FP64 restatement of the reference
+    evaluate with its CPU NUFFT far field) timed on all host cores on a bounded
+    sample of each configuration (same density, digits, n_per_leaf and nz;
+    tree build excluded).  Prints one JSON line."""
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+
+    def timed(cell, pos, q, nd, reps=2):
+        pl = oracle.Plan(cell, pos, nd, 300, 4)
+        pl.evaluate(q, fast_far=True)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            pl.evaluate(q, fast_far=True)
+            ts.append(time.perf_counter() - t0)
+        pl.close()
+        return statistics.median(ts)
+
+    out = {"cpu_configs": {}, "cores": threads, "omp_num_threads": threads,
+           "kind": "port (FP64 oracle restatement, CPU NUFFT far field; plan build not timed)"}
+    rows = out["cpu_configs"]
+    # cube workloads at their full size are timed on N = 1e5 samples at the same density
+    n = 100000
+    for nd in (6, 3):
+        scale = (n / 1e6) ** (1.0 / 3.0)
+        cell, pos, q = make_system(n, seed=1, scale=scale)
+        t = timed(cell, pos, q, nd)
+        rows["cube_1e6_%d_digits" % nd] = {"sample_n": n, "s_per_evaluate": t, "mpts_per_s": n / t / 1e6,
+                                           "note": "N=1e5 in a cube of the 1e6 workload's density"}
+    rows["cube_1e6_64rhs_6_digits"] = dict(rows["cube_1e6_6_digits"],
+                                           note="per charge vector: the CPU path evaluates the 64 vectors one "
+                                                "after another, so its Mpts*RHS/s equals the 1-RHS rate")
+    cell, pos, q = make_system(20000, seed=1)
+    t = timed(cell, pos, q, 6)
+    rows["cube_2e4_6_digits"] = {"sample_n": 20000, "s_per_evaluate": t, "mpts_per_s": 20000 / t / 1e6,
+                                 "note": "the full workload"}
+    # clustered triclinic: N = 2e5 sample with the same cell and cluster shape
+    cl_cell, cl_pos, cl_q = clustered_system(200000)
+    for nd in (9, 12):
+        t = timed(cl_cell, cl_pos, cl_q, nd, reps=1)
+        rows["clustered_triclinic_2e6_%d_digits" % nd] = {
+            "sample_n": 200000, "s_per_evaluate": t, "mpts_per_s": 200000 / t / 1e6,
+            "note": "N=2e5 with the workload's cell, 64 clusters of sigma 0.01 and half uniform"}
+    # many systems: a loop of per-system evaluates over the first 64 of the 512
+    cells, bpos, qs = batch_systems(64, seed=11)
+    plans = [oracle.Plan(c, p, 6, 300, 4) for c, p in zip(cells, bpos)]
+    t0 = time.perf_counter()
+    for pl, qq in zip(plans, qs):
+        pl.evaluate(qq, fast_far=True)
+    t = time.perf_counter() - t0
+    for pl in plans:
+        pl.close()
+    npts = sum(len(qq) for qq in qs)
+    rows["batch_512_systems_6_digits"] = {"sample_n": npts, "s_per_evaluate": t, "mpts_per_s": npts / t / 1e6,
+                                          "note": "loop of per-system evaluates over 64 of the 512 systems "
+                                                  "(plans built beforehand, not timed)"}
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 def run_reference(args):
@@ -642,11 +707,15 @@ def main():
     ap.add_argument("--clustered-digits", default="9,12",
                     help="digit counts of the clustered triclinic FP64 measurement ('' skips it)")
     ap.add_argument("--clustered-n", type=int, default=2000000)
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="time only the CPU oracle on bounded samples of every workload (JSON line)")
     ap.add_argument("--clustered-only", action="store_true",
                     help="run only the clustered triclinic FP64 measurement (its JSON fragment alone)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.cpu_configs:
+        return run_cpu_configs(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -48,6 +48,12 @@ def lib():
         _lib.oracle_tree_compare.argtypes = [d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_longlong)]
         _lib.oracle_tree_compare.restype = ctypes.c_int
+        _lib.oracle_plan_new.argtypes = [d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _lib.oracle_plan_new.restype = ctypes.c_void_p
+        _lib.oracle_plan_eval.argtypes = [ctypes.c_void_p, d, ctypes.c_int, ctypes.c_int, d]
+        _lib.oracle_plan_eval.restype = ctypes.c_int
+        _lib.oracle_plan_free.argtypes = [ctypes.c_void_p]
+        _lib.oracle_plan_free.restype = None
         _lib.oracle_pswf.argtypes = [ctypes.c_double, ctypes.c_int, d, d, d]
         _lib.oracle_legendre.argtypes = [ctypes.c_int, d, d]
         ip = ctypes.POINTER(ctypes.c_int)
@@ -87,6 +93,37 @@ def evaluate(cell, pos, q, n_digits=6, n_per_leaf=300, nz=4, with_far=True, comp
         comp = comp.reshape(4, n)
         return pot, dict(near=comp[0], mid=comp[1], self=comp[2], far=comp[3])
     return pot
+
+
+class Plan:
+    """Build-once / evaluate-many oracle: the plan (tree, lists, tables) is built
+    at construction, evaluate(q) runs only the evaluate stages."""
+
+    def __init__(self, cell, pos, n_digits=6, n_per_leaf=300, nz=4):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        self.n = len(pos)
+        c = _cell(cell)
+        self._h = lib().oracle_plan_new(_dp(c), self.n, _dp(pos), n_digits, n_per_leaf, nz)
+        if not self._h:
+            raise RuntimeError("oracle_plan_new failed")
+
+    def evaluate(self, q, with_far=True, fast_far=False):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        pot = np.zeros(self.n)
+        if lib().oracle_plan_eval(self._h, _dp(q), 1 if with_far else 0, 1 if fast_far else 0, _dp(pot)) != 0:
+            raise RuntimeError("oracle_plan_eval failed")
+        return pot
+
+    def close(self):
+        if self._h:
+            lib().oracle_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def plan_stats(cell, pos, n_digits=6, n_per_leaf=300, nz=4):

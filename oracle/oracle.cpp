@@ -564,6 +564,32 @@ int oracle_evaluate2(const double* cell, int n, const double* pos, const double*
     }
 }
 
+// Build-once / evaluate-many form (for timing the evaluate alone, as the
+// reference's PeriodicDMKTreeT separates construction from evaluate).
+void* oracle_plan_new(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz) {
+    try {
+        return new Plan(pdmkb::build_plan(cell, n, pos, n_digits, n_per_leaf, nz));
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_plan_new: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+int oracle_plan_eval(void* h, const double* q, int with_far, int fast_far, double* pot) {
+    try {
+        const Plan& P = *static_cast<Plan*>(h);
+        Components C;
+        oracle_eval(P, q, C, with_far != 0, fast_far != 0);
+        for (int i = 0; i < P.n_src; ++i) pot[i] = C.near[i] + C.mid[i] + C.self[i] + C.far[i];
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_plan_eval: %s\n", e.what());
+        return -1;
+    }
+}
+
+void oracle_plan_free(void* h) { delete static_cast<Plan*>(h); }
+
 // Plan statistics for tests: out[0..9] = n_all, nboxes, nlevels, n_target_leaves,
 // n_pw_boxes, n_c2proxy_work, list1 total, ms, mt, mu.
 int oracle_plan_stats(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz,
