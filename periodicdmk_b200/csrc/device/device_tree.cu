@@ -19,6 +19,7 @@
 
 #include "../host/pswf.hpp"
 #include "device_tree.hpp"
+#include "dmma.cuh"
 #include "pw_fused.cuh"
 #include "sep3.cuh"
 #include "tc_kernels.cuh"
@@ -87,6 +88,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
 
     if (const char* tm = std::getenv("PDMK_TC_MASK")) tc_mask_ = std::atoi(tm) & 15;
     if (const char* tw = std::getenv("PDMK_NEAR_TC_WIDE")) near_tc_wide_ = std::atoi(tw) != 0;
+    if (const char* dm = std::getenv("PDMK_FP64_DMMA")) fp64_dmma_ = std::atoi(dm) != 0;
     n_ = P.n_src;
     n_digits_ = P.dp.n_digits_tree;
     n_all_ = P.n_all;
@@ -1028,12 +1030,17 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             a.in = in; a.in_off = in_off + c0; a.out = s1; a.out_stride = ncoef;
             a.mat = mat; a.mat_off = mat_off ? mat_off + c0 : nullptr; a.ni = p; a.na = p; a.R = p * p;
             a.mode = dev::kStore; a.structure = structure;
-            dev::launch_contract(a, dev::kRRR, s);
+            // FP64 tensor cores (DMMA) when selected, else the CUDA-core contraction
+            auto rrr = [&](const dev::ContractArgs& c) {
+                if (fp64_dmma_ && dev::translate_dmma_supported(c.ni, c.na)) dev::launch_translate_dmma(c, s);
+                else dev::launch_contract(c, dev::kRRR, s);
+            };
+            rrr(a);
             a.in = s1; a.in_off = nullptr; a.in_stride = ncoef; a.out = s2; a.mat = mat + p * p;
-            dev::launch_contract(a, dev::kRRR, s);
+            rrr(a);
             a.in = s2; a.out = out; a.out_off = out_off + c0; a.mat = mat + 2 * p * p;
             a.mode = accumulate ? dev::kAdd : dev::kStore;
-            dev::launch_contract(a, dev::kRRR, s);
+            rrr(a);
             nl += 3;
         }
     };

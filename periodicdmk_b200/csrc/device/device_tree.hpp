@@ -135,6 +135,9 @@ class DeviceTree {
     // Near-field tensor-core kernel shape: 1 = 1024 threads per CTA (32 warps
     // per SM), 0 = 512 threads.  Initialised from PDMK_NEAR_TC_WIDE (default 0).
     int near_tc_wide_ = 0;
+    // FP64 child <-> parent translations on the FP64 tensor cores (DMMA)
+    // instead of the CUDA cores.  Initialised from PDMK_FP64_DMMA (default 0).
+    int fp64_dmma_ = 0;
 
   private:
     void init(const Plan& P, int device, bool fp64_working_set);

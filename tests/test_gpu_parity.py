@@ -183,3 +183,19 @@ def test_errors_on_device_tree():
     t.close()
     with pytest.raises(RuntimeError, match="bloch|outside|n_digits|nz"):
         _tree(cell, pos + 5.0, 6, 30)
+
+
+@pytest.mark.parametrize("nd", [9, 12])
+def test_fp64_translations_on_dmma(nd, monkeypatch):
+    # PDMK_FP64_DMMA=1 (read when the tree is built) runs the child <-> parent
+    # translations on mma.sync.m8n8k4.f64; same arithmetic up to the order of
+    # the FP64 sums, so it agrees with the CUDA-core path to rounding and with
+    # the oracle as before
+    cell, pos, q = clustered_system(20000, 41, TRICLINIC, n_clusters=8, sigma=0.03)
+    ref_tree = _tree(cell, pos, nd, 40)
+    ref = ref_tree.evaluate(q)
+    ref_tree.close()
+    monkeypatch.setenv("PDMK_FP64_DMMA", "1")
+    t = _tree(cell, pos, nd, 40)
+    assert rel_l2(t.evaluate(q), ref) < 1e-13
+    t.close()
