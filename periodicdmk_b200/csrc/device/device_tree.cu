@@ -87,7 +87,6 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     for (auto& e : ev_) PDMK_CUDA_CHECK(cudaEventCreate(&e));
 
     if (const char* tm = std::getenv("PDMK_TC_MASK")) tc_mask_ = std::atoi(tm) & 15;
-    if (const char* tw = std::getenv("PDMK_NEAR_TC_WIDE")) near_tc_wide_ = std::atoi(tw) != 0;
     if (const char* dm = std::getenv("PDMK_FP64_DMMA")) fp64_dmma_ = std::atoi(dm) != 0;
     n_ = P.n_src;
     n_digits_ = P.dp.n_digits_tree;

@@ -132,9 +132,6 @@ class DeviceTree {
     // translation and plane-wave transform steps); the CUDA-core kernels cover
     // the rest.  Initialised from PDMK_TC_MASK (default 7).
     int tc_mask_ = 7;
-    // Near-field tensor-core kernel shape: 1 = 1024 threads per CTA (32 warps
-    // per SM), 0 = 512 threads.  Initialised from PDMK_NEAR_TC_WIDE (default 0).
-    int near_tc_wide_ = 0;
     // FP64 child <-> parent translations on the FP64 tensor cores (DMMA)
     // instead of the CUDA cores.  Initialised from PDMK_FP64_DMMA (default 0).
     int fp64_dmma_ = 0;

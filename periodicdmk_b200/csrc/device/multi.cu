@@ -1243,11 +1243,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                 t.pair_bsize = near_.pair_bsize; t.n_leaves = near_.n_leaves; t.max_trg = near_max_trg_;
                 t.pair_chunk_base = near_pair_chunk_base_; t.chunk_lo = near_chunk_lo_; t.chunk_hi = near_chunk_hi_;
                 t.N = n_; t.kb = kb;
-                for (int i = 0; i < near_.nc; ++i) {
-                    t.coef[i] = near_.coef[i];
-                    t.coef32[i] = (float)near_.coef[i];
-                }
-                t.wide = near_tc_wide_;
+                for (int i = 0; i < near_.nc; ++i) t.coef[i] = near_.coef[i];
                 // Test hook of the failure detection (never set in normal use):
                 // PDMK_TEST_WITHHOLD_NEAR_CHUNK=j makes the first tile withhold
                 // chunk j's MMAs and commits; its next pipeline wait then runs

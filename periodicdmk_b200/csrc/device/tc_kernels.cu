@@ -779,372 +779,11 @@ void launch_near_tc_nc(const NearTc& a, const float4* th, const float4* tl, cons
 }
 
 
-// ---------------------------------------------------------------------------
-// The same near-field product with 1024 threads per CTA (32 warps per SM, at
-// most 64 registers per thread): each thread forms the kernel values of one
-// target and one group of 4 sources per chunk (the residual-polynomial
-// coefficients are read from the kernel's constant parameter bank, not held in
-// registers), 2 charges of the B operand, and drains 8 accumulator columns.
-// Chunk loop, cull, pipeline and abort logic as k_near_tc.
-// ---------------------------------------------------------------------------
-constexpr int kWThreads = 1024;
-constexpr int kW_OFF_BAR = kN_OFF_LIST + kNearTcMaxChunks * 4;
-constexpr int kWSmem = kW_OFF_BAR + 384;
-static_assert(kWSmem <= 227 * 1024, "near smem (wide)");
-
-__device__ __forceinline__ void split_store2(const float2 v, unsigned char* hi_p, unsigned char* lo_p) {
-    uint2 hi, lo;
-    tc::split_tf32(v.x, hi.x, lo.x);
-    tc::split_tf32(v.y, hi.y, lo.y);
-    *reinterpret_cast<uint2*>(hi_p) = hi;
-    *reinterpret_cast<uint2*>(lo_p) = lo;
-}
-
-template <int NC>
-__global__ void __launch_bounds__(kWThreads, 1)
-    k_near_tc_w(NearTc a, const float4* __restrict__ trg_hi, const float4* __restrict__ trg_lo,
-                const float4* __restrict__ src_hi, const float4* __restrict__ src_lo, const float* __restrict__ src_q,
-                double* __restrict__ pot, int* __restrict__ err) {
-    extern __shared__ __align__(1024) unsigned char sm[];
-    const int ntile = (a.max_trg + 127) / 128;
-    const int e = blockIdx.x / ntile;
-    const int t0 = a.trg_start[e], nt = a.trg_count[e];
-    const int m0 = (blockIdx.x % ntile) * 128;
-    if (m0 >= nt) return;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kW_OFF_BAR);  // [0,1] stage free, [2,3] segment accumulated
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kW_OFF_BAR + 32);
-    volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kW_OFF_BAR + 36);  // [3]
-    int* s_np = reinterpret_cast<int*>(sm + kW_OFF_BAR + 48);
-    int* s_nch = reinterpret_cast<int*>(sm + kW_OFF_BAR + 52);
-    int* s_kept = reinterpret_cast<int*>(sm + kW_OFF_BAR + 56);
-    int* s_last_commit = reinterpret_cast<int*>(sm + kW_OFF_BAR + 60);
-    float* s_tbox = reinterpret_cast<float*>(sm + kW_OFF_BAR + 64);   // [4 warps][6], then tile box [6] (120 B)
-    int* s_wcnt = reinterpret_cast<int*>(sm + kW_OFF_BAR + 192);      // [32] kept per warp
-    NearPair* pairs = reinterpret_cast<NearPair*>(sm + kN_OFF_PAIR);
-    int* pref = reinterpret_cast<int*>(sm + kN_OFF_PREF);
-    int* list = reinterpret_cast<int*>(sm + kN_OFF_LIST);
-    double* acc64 = reinterpret_cast<double*>(sm + kN_OFF_ACC);
-
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int kb = a.kb;
-    const int NBp = (kb + 15) & ~15;
-
-    if (warp == 0) {
-        tc::tmem_alloc(s_tmem, 128);
-        tc::tmem_relinquish();
-    }
-    if (tid == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
-        tc::mbar_init(&bar[2], 1);
-        tc::mbar_init(&bar[3], 1);
-        s_abort[0] = s_abort[1] = s_abort[2] = 0;
-        *s_last_commit = -1;
-        int np = 0, nch = 0;
-        pref[0] = 0;
-        for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
-            const int cnt = a.pair_src_count[pr];
-            if (cnt <= 0 || np >= kNearTcMaxPairs) continue;
-            const double b = a.pair_bsize[pr];
-            NearPair q;
-            q.start = a.pair_src_start[pr];
-            q.count = cnt;
-            q.nch = (cnt + kNKC - 1) / kNKC;
-            q.cb = a.pair_chunk_base[pr];
-            q.d2max = (float)(b * b);
-            q.rsc = (float)(2.0 / b);
-            q.cen = (float)(-0.5 * b);
-            pairs[np++] = q;
-            nch += q.nch;
-            pref[np] = nch;
-        }
-        *s_np = np;
-        *s_nch = min(nch, kNearTcMaxChunks);
-        tc::fence_mbar_init();
-    }
-    for (int i = tid; i < 64 * 128; i += kWThreads) acc64[i] = 0.0;
-
-    // A role: target row am, source group ag (sources 4 ag .. 4 ag + 3)
-    const int am = tid & 127, ag = tid >> 7;
-    const bool tval = m0 + am < nt;
-    const float4 th = tval ? trg_hi[t0 + m0 + am] : make_float4(1e30f, 1e30f, 1e30f, 0.0f);
-    const float4 tl = tval ? trg_lo[t0 + m0 + am] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (warp < 4) {
-        float lo[3] = {tval ? th.x : 3e38f, tval ? th.y : 3e38f, tval ? th.z : 3e38f};
-        float hi[3] = {tval ? th.x : -3e38f, tval ? th.y : -3e38f, tval ? th.z : -3e38f};
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-                hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
-            }
-        if (lane == 0)
-            for (int d = 0; d < 3; ++d) {
-                s_tbox[warp * 6 + d] = lo[d];
-                s_tbox[warp * 6 + 3 + d] = hi[d];
-            }
-    }
-    // B role: RHS row bc, sources 2 bs2, 2 bs2 + 1
-    const int bc = tid & 63, bs2 = tid >> 6;
-    // position prefetch role (warps 8-9): source tid-256 (hi) or tid-288 (lo)
-    const bool prole = tid >= 256 && tid < 256 + 2 * kNKC;
-    const int ps_ = (tid - 256) & (kNKC - 1);
-    const bool plo = tid >= 256 + kNKC;
-
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *s_tmem;
-    const int np = *s_np, ncand = *s_nch;
-    if (tid == 0) {
-        for (int d = 0; d < 3; ++d) {
-            float lo = s_tbox[d], hi = s_tbox[3 + d];
-            for (int w = 1; w < 4; ++w) {
-                lo = fminf(lo, s_tbox[w * 6 + d]);
-                hi = fmaxf(hi, s_tbox[w * 6 + 3 + d]);
-            }
-            const float pad = 2.5e-7f * fmaxf(fabsf(lo), fabsf(hi)) + 1e-30f;
-            s_tbox[24 + d] = lo - pad;
-            s_tbox[27 + d] = hi + pad;
-        }
-        *s_kept = 0;
-    }
-    __syncthreads();
-    {
-        const float tlo[3] = {s_tbox[24], s_tbox[25], s_tbox[26]};
-        const float thi[3] = {s_tbox[27], s_tbox[28], s_tbox[29]};
-        for (int base = 0; base < ncand; base += kWThreads) {
-            const int c = base + tid;
-            bool keep = false;
-            int code = 0;
-            if (c < ncand) {
-                int lo = 0, hi = np - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (pref[mid] <= c) lo = mid; else hi = mid - 1;
-                }
-                const int j = c - pref[lo];
-                const NearPair& q = pairs[lo];
-                const float4 clo = __ldg(a.chunk_lo + q.cb + j), chi = __ldg(a.chunk_hi + q.cb + j);
-                const float gx = fmaxf(0.0f, fmaxf(clo.x - thi[0], tlo[0] - chi.x));
-                const float gy = fmaxf(0.0f, fmaxf(clo.y - thi[1], tlo[1] - chi.y));
-                const float gz = fmaxf(0.0f, fmaxf(clo.z - thi[2], tlo[2] - chi.z));
-                keep = fmaf(gx, gx, fmaf(gy, gy, gz * gz)) <= q.d2max * 1.00001f;
-                code = (lo << 16) | j;
-            }
-            const unsigned ball = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) s_wcnt[warp] = __popc(ball);
-            __syncthreads();
-            int off = *s_kept;
-            for (int w = 0; w < warp; ++w) off += s_wcnt[w];
-            if (keep) list[off + __popc(ball & ((1u << lane) - 1u))] = code;
-            __syncthreads();
-            if (tid == 0) {
-                int tot = 0;
-                for (int w = 0; w < kWThreads / 32; ++w) tot += s_wcnt[w];
-                *s_kept += tot;
-            }
-            __syncthreads();
-        }
-    }
-    const int nchunks = *s_kept;
-
-    auto chunk_src = [&](int q, int& p, int& g0, int& n) {
-        const int v = list[q];
-        p = v >> 16;
-        const int j = v & 0xFFFF;
-        g0 = pairs[p].start + j * kNKC;
-        n = min(kNKC, pairs[p].count - j * kNKC);
-    };
-    auto load_q = [&](int q, float (&qv)[2]) {
-        int p, g0, n;
-        chunk_src(q, p, g0, n);
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const int s = bs2 * 2 + u;
-            qv[u] = (s < n && bc < kb) ? __ldg(src_q + (int64_t)(g0 + s) * kb + bc) : 0.0f;
-        }
-    };
-    auto load_pos = [&](int q) -> float4 {
-        int p, g0, n;
-        chunk_src(q, p, g0, n);
-        if (ps_ >= n) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        return plo ? __ldg(src_lo + g0 + ps_) : __ldg(src_hi + g0 + ps_);
-    };
-    auto store_pos = [&](int buf, float4 v) {
-        float4* dst = reinterpret_cast<float4*>(sm + kN_OFF_SRC + buf * kNSrc);
-        dst[(plo ? kNKC : 0) + ps_] = v;
-    };
-    // Warp w reads TMEM lanes 32 (w % 4) .. +31 (targets) and columns 8 (w / 4) .. +7 (RHS).
-    auto drain = [&](int gg) -> bool {
-        const bool waited = tc::mbar_wait(&bar[2 + (gg & 1)], (gg >> 1) & 1, a.wait_cycles);
-        if (!__all_sync(0xffffffffu, waited)) return false;
-        tc::fence_after_sync();
-        const int lq = warp & 3, cg = warp >> 2;
-        if (8 * cg < NBp) {
-            const uint32_t base = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((gg & 1) * 64 + 8 * cg);
-            float v[8];
-            tc::tmem_ld_x8(base, v);
-            tc::tmem_wait_ld();
-            const int m = lq * 32 + lane;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) acc64[(8 * cg + i) * 128 + m] += (double)v[i];
-        }
-        tc::fence_before_sync();
-        return true;
-    };
-
-    float qcur[2], qnext[2];
-    float4 pnext = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (nchunks > 0) {
-        load_q(0, qcur);
-        if (prole) store_pos(0, load_pos(0));
-        if (nchunks > 1 && prole) pnext = load_pos(1);
-    }
-    __syncthreads();
-
-    int issued = 0;
-    for (int q = 0; q < nchunks; ++q) {
-        const int st = q & 1;
-        const int seg = q / kNSeg;
-        const bool first = q % kNSeg == 0, last = q % kNSeg == kNSeg - 1 || q == nchunks - 1;
-        int pidx, g0c, nv;
-        chunk_src(q, pidx, g0c, nv);
-        const float d2max = pairs[pidx].d2max, rsc = pairs[pidx].rsc, cen = pairs[pidx].cen;
-        if (q + 1 < nchunks) {
-            load_q(q + 1, qnext);
-            if (prole) {
-                store_pos(st ^ 1, pnext);
-                if (q + 2 < nchunks) pnext = load_pos(q + 2);
-            }
-        }
-        if (q >= 2 && !tc::mbar_wait(&bar[st], ((q - 2) >> 1) & 1, a.wait_cycles)) s_abort[st] = 1;
-        unsigned char* stage = sm + st * kNStage;
-        const float4* sh = reinterpret_cast<const float4*>(sm + kN_OFF_SRC + st * kNSrc);
-        const float4* sl = sh + kNKC;
-        {
-            float r2v[4];
-            bool anyin = false;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int s = 4 * ag + k;
-                const float4 yh = sh[s], yl = sl[s];
-                const float dx = (th.x - yh.x) + (tl.x - yl.x);
-                const float dy = (th.y - yh.y) + (tl.y - yl.y);
-                const float dz = (th.z - yh.z) + (tl.z - yl.z);
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool in = s < nv && r2 > 1e-30f && r2 < d2max;
-                r2v[k] = in ? r2 : -1.0f;
-                anyin |= in;
-            }
-            float w[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            if (__any_sync(0xffffffffu, anyin)) {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float r2 = r2v[k] > 0.0f ? r2v[k] : 1.0f;
-                    const float rinv = rsqrtf(r2);
-                    const float x = fmaf(r2, rinv, cen) * rsc;
-                    float pv = a.coef32[NC - 1];
-#pragma unroll
-                    for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, a.coef32[i]);
-                    w[k] = r2v[k] > 0.0f ? pv * rinv : 0.0f;
-                }
-            }
-            const uint32_t off = tc::kmajor_offset(am, 4 * ag, kNKCH);
-            split_store(make_float4(w[0], w[1], w[2], w[3]), stage + kN_OFF_AH + off, stage + kN_OFF_AL + off);
-        }
-        {
-            const uint32_t off = tc::kmajor_offset(bc, 2 * bs2, kNKCH);
-            split_store2(make_float2(qcur[0], qcur[1]), stage + kN_OFF_BH + off, stage + kN_OFF_BL + off);
-        }
-        tc::fence_proxy_async();
-        __syncthreads();
-        if (s_abort[st]) break;
-        if (tid == 0 && !(blockIdx.x == 0 && q == a.withhold_chunk)) {
-            tc::fence_after_sync();
-            const uint32_t base = tc::smem_u32(stage);
-            const uint32_t idesc = tc::idesc_tf32(128, NBp);
-            const uint32_t d = tmem + (uint32_t)((seg & 1) * 64);
-#pragma unroll
-            for (int ks = 0; ks < kNKC / 8; ++ks) {
-                const uint32_t kofs = ks * 256;
-                const uint64_t ah = tc::smem_desc_k_noswizzle(base + kN_OFF_AH + kofs, 128, kNSBO);
-                const uint64_t alo = tc::smem_desc_k_noswizzle(base + kN_OFF_AL + kofs, 128, kNSBO);
-                const uint64_t bh = tc::smem_desc_k_noswizzle(base + kN_OFF_BH + kofs, 128, kNSBO);
-                const uint64_t blo = tc::smem_desc_k_noswizzle(base + kN_OFF_BL + kofs, 128, kNSBO);
-                tc::mma_tf32(d, ah, bh, idesc, (first && ks == 0) ? 0u : 1u);
-                tc::mma_tf32(d, ah, blo, idesc, 1u);
-                tc::mma_tf32(d, alo, bh, idesc, 1u);
-            }
-            tc::commit(&bar[st]);
-            if (last) tc::commit(&bar[2 + (seg & 1)]);
-            *s_last_commit = q;
-        }
-        issued = q + 1;
-        if (first && seg > 0) {
-            if (!drain(seg - 1)) s_abort[st ^ 1] = 1;
-        }
-        qcur[0] = qnext[0];
-        qcur[1] = qnext[1];
-    }
-    bool ok = s_abort[0] == 0 && s_abort[1] == 0;
-    if (ok && issued > 0) {
-        if (!drain((issued - 1) / kNSeg)) s_abort[2] = 1;
-    }
-    __syncthreads();
-    ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;
-    if (!ok) {
-        const int lc = *s_last_commit;
-        if (lc >= 0) tc::mbar_wait(&bar[lc & 1], (lc >> 1) & 1);
-    }
-    __syncthreads();
-    if (ok) {
-        for (int i = tid; i < kb * 128; i += kWThreads) {
-            const int c = i >> 7, mm = i & 127;
-            if (m0 + mm < nt) pot[(int64_t)c * a.N + t0 + m0 + mm] += acc64[c * 128 + mm];
-        }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) {
-        tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, 128);
-    }
-    if (!ok && tid == 0) atomicExch(err, 1);
-}
-
-template <int NC>
-void launch_near_tc_w_nc(const NearTc& a, const float4* th, const float4* tl, const float4* sh, const float4* sl,
-                         const float* q, double* pot, int* err, cudaStream_t s) {
-    static bool configured[64] = {};
-    int dev = 0;
-    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
-    if (!configured[dev]) {
-        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_near_tc_w<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWSmem));
-        configured[dev] = true;
-    }
-    const int64_t nblocks = (int64_t)a.n_leaves * ((a.max_trg + 127) / 128);
-    if (nblocks > INT32_MAX) throw std::runtime_error("too many near-field tiles for one launch");
-    k_near_tc_w<NC><<<(unsigned)nblocks, kWThreads, kWSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
-}
-
 }  // namespace
 
 bool launch_near_tc(const NearTc& a, int nc, const float4* trg_hi, const float4* trg_lo, const float4* src_hi,
                     const float4* src_lo, const float* src_q, double* pot, int* err, cudaStream_t s) {
     if (a.kb < 1 || a.kb > 64 || a.n_leaves <= 0 || a.max_trg <= 0) return false;
-    if (a.wide) {
-        switch (nc) {
-#define PDMK_NTCW(NC)                                                                       \
-    case NC: launch_near_tc_w_nc<NC>(a, trg_hi, trg_lo, src_hi, src_lo, src_q, pot, err, s); \
-        return true;
-            PDMK_NTCW(5) PDMK_NTCW(6) PDMK_NTCW(9) PDMK_NTCW(11) PDMK_NTCW(12)
-#undef PDMK_NTCW
-            default: return false;
-        }
-    }
     switch (nc) {
 #define PDMK_NTC(NC)                                                                  \
     case NC: launch_near_tc_nc<NC>(a, trg_hi, trg_lo, src_hi, src_lo, src_q, pot, err, s); \

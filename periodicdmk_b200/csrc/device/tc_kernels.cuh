@@ -39,7 +39,6 @@ struct NearTc {
     const float4* chunk_lo;
     const float4* chunk_hi;
     double coef[32];
-    float coef32[32];  // the same coefficients in FP32 (read from the constant bank by the kernel)
     int n_leaves;
     int max_trg;  // largest trg_count (grid extent over 128-target tiles)
     int64_t N;
@@ -50,7 +49,6 @@ struct NearTc {
     // inside the chunk loop (SM clock cycles).
     int withhold_chunk;
     long long wait_cycles;
-    int wide;  // 1: the 1024-thread kernel (32 warps per SM), 0: the 512-thread kernel
 };
 constexpr int kNearTcMaxPairs = 128;
 constexpr int kNearTcChunk = 32;        // sources per chunk
