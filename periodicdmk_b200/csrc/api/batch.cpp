@@ -64,11 +64,28 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
     if (first_error) std::rethrow_exception(first_error);
     try {
         PDMK_CUDA_CHECK(cudaGetDevice(&device_));
-        trees_.reserve(nsys);
-        for (int i = 0; i < nsys; ++i) {
-            trees_.push_back(std::make_unique<DeviceTree>(*plans[i], device_, /*fp64_working_set=*/!single_));
-            plans[i].reset();  // the device tree keeps what it needs
-        }
+        // device trees (uploads, cuFFT plans) on host threads too: each system's
+        // upload is a sequence of small allocations and copies
+        trees_.resize(nsys);
+        next = 0;
+        auto upload = [&]() {
+            cudaSetDevice(device_);
+            for (;;) {
+                const int i = next.fetch_add(1);
+                if (i >= nsys) return;
+                try {
+                    trees_[i] = std::make_unique<DeviceTree>(*plans[i], device_, /*fp64_working_set=*/!single_);
+                    plans[i].reset();  // the device tree keeps what it needs
+                } catch (...) {
+                    std::lock_guard<std::mutex> g(err_mu);
+                    if (!first_error) first_error = std::current_exception();
+                }
+            }
+        };
+        std::vector<std::thread> up;
+        for (int t = 0; t < nthr; ++t) up.emplace_back(upload);
+        for (auto& t : up) t.join();
+        if (first_error) std::rethrow_exception(first_error);
         PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
         done_.assign(nsys, nullptr);

@@ -100,7 +100,10 @@ void launch_s(const ContractArgs& a, cudaStream_t s) {
     int BS = 8 * NT;
     while (BS % 16 != 8) ++BS;
     const size_t smem = sizeof(double) * ((size_t)kDRows * RS + (size_t)4 * KS * BS);
-    static bool configured = false;
+    static bool configured_dev[64] = {};
+    int cur_dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&cur_dev));
+    bool& configured = configured_dev[cur_dev & 63];
     if (!configured) {
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_translate_dmma<S, NT, false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));

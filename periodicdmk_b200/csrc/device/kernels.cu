@@ -529,7 +529,10 @@ static void launch_contract_a(const ContractArgs& a, cudaStream_t s) {
     const int napad = (a.na + WA * TA - 1) / (WA * TA) * (WA * TA);
     const size_t msz = PAR ? sizeof(double) : sizeof(TM);
     const size_t smem = ((size_t)a.ni * napad * msz + 15) / 16 * 16 + (size_t)a.ni * (RB + 1) * sizeof(TI);
-    static bool configured = false;
+    static bool configured_dev[64] = {};
+    int cur_dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&cur_dev));
+    bool& configured = configured_dev[cur_dev & 63];
     if (!configured) {
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_contract<TI, TM, TO, TR, TA, WA, S, ACC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));

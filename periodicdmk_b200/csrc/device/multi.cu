@@ -273,7 +273,10 @@ void launch_contract_m(const ContractM& a, cudaStream_t s) {
     constexpr int RT = 32, AB = 4;
     if (a.n_entries <= 0) return;
     const size_t smem = ((size_t)a.na * a.ni * sizeof(TM) + 15) / 16 * 16 + (size_t)a.ni * RT * sizeof(TI);
-    static bool configured = false;
+    static bool configured_dev[64] = {};
+    int cur_dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&cur_dev));
+    bool& configured = configured_dev[cur_dev & 63];
     if (!configured) {
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_contract_m<TI, TM, TO, RT, AB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -704,7 +707,10 @@ static size_t sep3_smem() { return sizeof(T) * (2 * (size_t)P * P * P + 3 * (siz
 
 template <typename T, int P, int TRI>
 static void launch_sep3_t(const Sep3& a, int n_entries, cudaStream_t s) {
-    static bool configured = false;
+    static bool configured_dev[64] = {};
+    int cur_dev = 0;
+    PDMK_CUDA_CHECK(cudaGetDevice(&cur_dev));
+    bool& configured = configured_dev[cur_dev & 63];
     const size_t smem = sep3_smem<T, P>();
     if (!configured) {
         PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_sep3<T, P, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
