@@ -1255,6 +1255,9 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                 // chunk j's MMAs and commits; its next pipeline wait then runs
                 // out after ~10 ms, the kernel aborts cleanly and sets the error
                 // word, and the evaluate returns -2.
+                // segment length between FP64 drains (tuning: PDMK_NEAR_SEG)
+                t.seg_chunks = 0;
+                if (const char* sg = std::getenv("PDMK_NEAR_SEG")) t.seg_chunks = std::atoi(sg);
                 t.withhold_chunk = -1;
                 t.wait_cycles = 4000000000LL;
                 if (const char* w = std::getenv("PDMK_TEST_WITHHOLD_NEAR_CHUNK")) {

@@ -401,7 +401,7 @@ bool launch_c2proxy_tc(const C2ProxyArgs& a, const float* src_q, float* proxy_up
 namespace {
 
 constexpr int kNKC = 32;            // sources per chunk
-constexpr int kNSeg = 2;            // chunks accumulated in tensor memory before a drain
+constexpr int kNSeg = 2;            // default chunks accumulated in tensor memory before a drain
 constexpr int kNKCH = kNKC / 4;     // 16-byte K chunks per operand row
 constexpr int kNThreads = 512;
 constexpr int kNSBO = kNKCH * 128;  // bytes between 8-row groups
@@ -640,14 +640,15 @@ __global__ void __launch_bounds__(kNThreads, 1)
     }
     __syncthreads();
 
-    // The accumulator is drained every kNSeg chunks: the tensor-core FP32
+    // The accumulator is drained every nseg chunks: the tensor-core FP32
     // accumulation loses low bits on every MMA step, so each segment stays
     // short and the sums continue in FP64 on the CUDA cores.
+    const int nseg = a.seg_chunks > 0 ? a.seg_chunks : kNSeg;
     int issued = 0;
     for (int q = 0; q < nchunks; ++q) {
         const int st = q & 1;
-        const int seg = q / kNSeg;
-        const bool first = q % kNSeg == 0, last = q % kNSeg == kNSeg - 1 || q == nchunks - 1;
+        const int seg = q / nseg;
+        const bool first = q % nseg == 0, last = q % nseg == nseg - 1 || q == nchunks - 1;
         int pidx, g0c, nv;
         chunk_src(q, pidx, g0c, nv);
         const NearPair pr = pairs[pidx];
@@ -736,7 +737,7 @@ __global__ void __launch_bounds__(kNThreads, 1)
     }
     bool ok = s_abort[0] == 0 && s_abort[1] == 0;
     if (ok && issued > 0) {
-        if (!drain((issued - 1) / kNSeg)) s_abort[2] = 1;
+        if (!drain((issued - 1) / nseg)) s_abort[2] = 1;
     }
     __syncthreads();
     ok = s_abort[0] == 0 && s_abort[1] == 0 && s_abort[2] == 0;

@@ -49,6 +49,9 @@ struct NearTc {
     // inside the chunk loop (SM clock cycles).
     int withhold_chunk;
     long long wait_cycles;
+    // chunks of 32 sources accumulated in tensor memory between two FP64 drains
+    // (<= 0: the default, 2)
+    int seg_chunks;
 };
 constexpr int kNearTcMaxPairs = 128;
 constexpr int kNearTcChunk = 32;        // sources per chunk
