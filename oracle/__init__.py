@@ -42,6 +42,9 @@ def lib():
         _lib.oracle_ewald_targets.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ip, ctypes.c_double,
                                               ctypes.c_double, d]
         _lib.oracle_ewald_targets.restype = ctypes.c_int
+        _lib.oracle_ewald_targets_grad.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ip, ctypes.c_double,
+                                                   ctypes.c_double, d, d]
+        _lib.oracle_ewald_targets_grad.restype = ctypes.c_int
         _lib.oracle_evaluate_multi.argtypes = [d, ctypes.c_int, d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, d]
         _lib.oracle_evaluate_multi.restype = ctypes.c_int
@@ -180,6 +183,22 @@ def ewald_targets(cell, pos, q, targets, s=6.0, alpha=0.0):
                                   _dp(out)) != 0:
         raise RuntimeError("oracle_ewald_targets failed")
     return out
+
+
+def ewald_targets_grad(cell, pos, q, targets, s=6.0, alpha=0.0):
+    """(potentials, gradients (m, 3)) at the target indices: Ewald, all sources and
+    images; gradient = d phi / d x (Cartesian)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.int32)
+    out = np.zeros(len(t))
+    g = np.zeros(3 * len(t))
+    c = _cell(cell)
+    ip = ctypes.POINTER(ctypes.c_int)
+    if lib().oracle_ewald_targets_grad(_dp(c), len(q), _dp(pos), _dp(q), len(t), t.ctypes.data_as(ip), s, alpha,
+                                       _dp(out), _dp(g)) != 0:
+        raise RuntimeError("oracle_ewald_targets_grad failed")
+    return out, g.reshape(-1, 3)
 
 
 def evaluate_multi(cell, pos, Q, n_digits=6, n_per_leaf=300, nz=4):

@@ -767,8 +767,20 @@ int oracle_ewald_direct(const double* cell, int n, const double* pos, const doub
 // modes of the sphere.  alpha <= 0 picks alpha from an estimate of the two
 // costs.  Sums are compensated (Neumaier) so rounding stays near 1e-15 of the
 // potential at 10^6 sources.
+int oracle_ewald_targets_grad(const double* cell, int n, const double* pos, const double* q, int m, const int* tidx,
+                              double s, double alpha, double* pot, double* grad);
+
 int oracle_ewald_targets(const double* cell, int n, const double* pos, const double* q, int m, const int* tidx,
                          double s, double alpha, double* pot) {
+    return oracle_ewald_targets_grad(cell, n, pos, q, m, tidx, s, alpha, pot, nullptr);
+}
+
+// The same with the potential's gradient at the targets: grad[3 ti + d] =
+// d phi / d x_d (Cartesian; the field is -grad, the force on q_t is -q_t grad).
+// Real space: d/dr [erfc(alpha r)/r] = -erfc(alpha r)/r^2 - 2 alpha/sqrt(pi) e^{-alpha^2 r^2}/r
+// along (x_t - x_j)/r; reciprocal space: -sum w(k) k Im[S(k) e^{i k.x_t}].
+int oracle_ewald_targets_grad(const double* cell, int n, const double* pos, const double* q, int m, const int* tidx,
+                              double s, double alpha, double* pot, double* grad) {
     try {
         const double* a[3] = {cell, cell + 3, cell + 6};
         auto cross = [](const double* u, const double* v, double* w) {
@@ -828,14 +840,15 @@ int oracle_ewald_targets(const double* cell, int n, const double* pos, const dou
             std::vector<int> fill(bstart.begin(), bstart.end() - 1);
             for (int j = 0; j < n; ++j) border[fill[bin_of(j)]++] = j;
         }
-        std::vector<double> phi(m, 0.0);
+        std::vector<double> phi(m, 0.0), gr((size_t)3 * m, 0.0);
+        const double twoa_sqpi = 2.0 * alpha / std::sqrt(M_PI);
 #pragma omp parallel for schedule(dynamic, 1)
         for (int ti = 0; ti < m; ++ti) {
             const int t = tidx[ti];
             const double* ft = &f[3 * (size_t)t];
             int bt[3];
             for (int d = 0; d < 3; ++d) bt[d] = std::min(G[d] - 1, (int)(ft[d] * G[d]));
-            double sum = 0, comp = 0;
+            double sum = 0, comp = 0, g0 = 0, g1 = 0, g2 = 0;
             for (int o2 = -reach[2]; o2 <= reach[2]; ++o2)
                 for (int o1 = -reach[1]; o1 <= reach[1]; ++o1)
                     for (int o0 = -reach[0]; o0 <= reach[0]; ++o0) {
@@ -856,13 +869,23 @@ int oracle_ewald_targets(const double* cell, int n, const double* pos, const dou
                             const double r2 = dot(dr, dr);
                             if (r2 >= rc2) continue;
                             const double r = std::sqrt(r2);
-                            const double v = q[j] * std::erfc(alpha * r) / r;
+                            const double ec = std::erfc(alpha * r);
+                            const double v = q[j] * ec / r;
                             const double tsum = sum + v;
                             comp += std::fabs(sum) >= std::fabs(v) ? (sum - tsum) + v : (v - tsum) + sum;
                             sum = tsum;
+                            if (grad) {
+                                const double dvdr = -q[j] * (ec / r2 + twoa_sqpi * std::exp(-alpha * alpha * r2) / r);
+                                g0 += dvdr * dr[0] / r;
+                                g1 += dvdr * dr[1] / r;
+                                g2 += dvdr * dr[2] / r;
+                            }
                         }
                     }
             phi[ti] = sum + comp - 2.0 * alpha / std::sqrt(M_PI) * q[t];
+            gr[3 * (size_t)ti] = g0;
+            gr[3 * (size_t)ti + 1] = g1;
+            gr[3 * (size_t)ti + 2] = g2;
         }
         // ---- reciprocal space: modes m with |m1 b1 + m2 b2 + m3 b3| <= kmax
         double b[3][3];
@@ -938,17 +961,30 @@ int oracle_ewald_targets(const double* cell, int n, const double* pos, const dou
             for (int k = -mm[0]; k <= mm[0]; ++k) e1[k + mm[0]] = std::polar(1.0, 2 * M_PI * k * ft[0]);
             for (int k = -mm[1]; k <= mm[1]; ++k) e2[k + mm[1]] = std::polar(1.0, 2 * M_PI * k * ft[1]);
             for (int k = 0; k <= mm[2]; ++k) e3[k] = std::polar(1.0, 2 * M_PI * k * ft[2]);
-            double sum = 0, comp = 0;
+            double sum = 0, comp = 0, g0 = 0, g1 = 0, g2 = 0;
             for (const Row& r : rows) {
                 const cplx g = e3[r.m3] * e2[r.m2 + mm[1]];
                 for (int k = 0; k <= r.hi - r.lo; ++k) {
-                    const double v = w[r.off + k] * (S[r.off + k] * g * e1[r.lo + k + mm[0]]).real();
+                    const cplx zv = S[r.off + k] * g * e1[r.lo + k + mm[0]];
+                    const double v = w[r.off + k] * zv.real();
                     const double tsum = sum + v;
                     comp += std::fabs(sum) >= std::fabs(v) ? (sum - tsum) + v : (v - tsum) + sum;
                     sum = tsum;
+                    if (grad) {
+                        const int m1 = r.lo + k;
+                        const double wi = -w[r.off + k] * zv.imag();
+                        g0 += wi * (m1 * b[0][0] + r.m2 * b[1][0] + r.m3 * b[2][0]);
+                        g1 += wi * (m1 * b[0][1] + r.m2 * b[1][1] + r.m3 * b[2][1]);
+                        g2 += wi * (m1 * b[0][2] + r.m2 * b[1][2] + r.m3 * b[2][2]);
+                    }
                 }
             }
             pot[ti] = phi[ti] + sum + comp;
+            if (grad) {
+                grad[3 * (size_t)ti] = gr[3 * (size_t)ti] + g0;
+                grad[3 * (size_t)ti + 1] = gr[3 * (size_t)ti + 1] + g1;
+                grad[3 * (size_t)ti + 2] = gr[3 * (size_t)ti + 2] + g2;
+            }
         }
         return 0;
     } catch (const std::exception& e) {

@@ -212,3 +212,24 @@ def test_independent_tree_matches_plan_batch_cells():
     cells, pos, _ = batch_systems(6, 17, n_min=1000, n_max=20000)
     for c, p in zip(cells, pos):
         _assert_same_tree(oracle.tree_compare(c, p, 6, 300, 4))
+
+
+def test_ewald_gradient_matches_finite_differences():
+    # d phi_t / d x_t of the sampled-target Ewald sum against central
+    # differences (moving a point moves its charge: its own images and the self
+    # term do not depend on its position, so the derivative is the field of the
+    # other charges)
+    cell, pos, q = clustered_system(400, 9, TRICLINIC, n_clusters=3, sigma=0.05)
+    idx = np.array([0, 57, 203, 399])
+    _, g = oracle.ewald_targets_grad(cell, pos, q, idx, s=6.5)
+    h = 1e-5
+    for row, t in enumerate(idx):
+        for d in range(3):
+            pp, pm = pos.copy(), pos.copy()
+            pp[t, d] += h
+            pm[t, d] -= h
+            fd = (oracle.ewald_targets(cell, pp, q, [t], s=6.5)[0] - oracle.ewald_targets(cell, pm, q, [t], s=6.5)[0]) / (2 * h)
+            assert abs(fd - g[row, d]) < 1e-6 * max(1.0, np.abs(g[row]).max()), (t, d, fd, g[row, d])
+    # potentials unchanged by the gradient pass
+    v, _ = oracle.ewald_targets_grad(cell, pos, q, idx, s=6.5)
+    assert rel_l2(v, oracle.ewald_targets(cell, pos, q, idx, s=6.5)) < 1e-15
