@@ -86,6 +86,18 @@ int pdmk_evaluate_multi_device_float(void* h, int k, const double* Q_dev, double
 int pdmk_evaluate_multi_float_qf32(void* h, int N, int k, const float* charges_Nxk, float* pot_Nxk);
 int pdmk_evaluate_multi_device_float_qf32(void* h, int k, const float* Q_dev, double* pot_dev);
 
+/* Potentials and their gradients (the field is -grad; the force on charge i
+ * is -q_i grad_i) of a double tree, user order: grad_3xN[d + 3*i] = d u_i /
+ * d x_d in the caller's frame.  No counterpart in the reference's C ABI: its
+ * lower layers compute target gradients (pgh_trg = DMK_POTENTIAL_GRAD;
+ * cpp/src/dmk/proxy.cpp:307-448, cpp/include/dmk/vector_kernels.hpp:391-417)
+ * but PeriodicDMKTreeT exposes potentials only.  N and positions_3xN are
+ * ignored, as in pdmk_evaluate_double.  The device form takes device buffers
+ * (N, N and 3N doubles). */
+int pdmk_evaluate_grad_double(void* h, int N, const double* positions_3xN, const double* charges, double* pot_out,
+                              double* grad_3xN);
+int pdmk_evaluate_grad_device_double(void* h, const double* charges_dev, double* pot_dev, double* grad_dev);
+
 /* The two parts of the potential in user order: the tree part (near field +
  * plane-wave levels - self term) and the periodic far field. */
 int pdmk_evaluate_parts_double(void* h, const double* charges, double* tree_part, double* far_part);

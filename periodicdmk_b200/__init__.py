@@ -30,6 +30,7 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_device_double", "pdmk_evaluate_device_float",
     "pdmk_evaluate_multi_device_double", "pdmk_evaluate_multi_device_float",
     "pdmk_evaluate_multi_float_qf32", "pdmk_evaluate_multi_device_float_qf32",
+    "pdmk_evaluate_grad_double", "pdmk_evaluate_grad_device_double",
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
     "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_tc_peak",
     "pdmk_evaluate_device_noalloc_double",
@@ -75,6 +76,10 @@ def library():
     lib.pdmk_evaluate_multi_device_float.argtypes = [v, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_evaluate_multi_device_float.restype = ctypes.c_int
     lib.pdmk_evaluate_multi_float_qf32.argtypes = [v, ctypes.c_int, ctypes.c_int, _F, _F]
+    lib.pdmk_evaluate_grad_double.argtypes = [v, ctypes.c_int, _D, _D, _D, _D]
+    lib.pdmk_evaluate_grad_double.restype = ctypes.c_int
+    lib.pdmk_evaluate_grad_device_double.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pdmk_evaluate_grad_device_double.restype = ctypes.c_int
     lib.pdmk_evaluate_multi_device_float_qf32.argtypes = [v, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     lib.pdmk_info_double.argtypes = [v, _I64]
     lib.pdmk_info_float.argtypes = [v, _I64]
@@ -248,6 +253,19 @@ class PeriodicDMKTree:
             rc = self._lib.pdmk_evaluate_multi_device_float(self._h, int(k), ctypes.c_void_p(q_ptr),
                                                             ctypes.c_void_p(pot_ptr))
         self._check(rc, "pdmk_evaluate_multi_device")
+
+    def evaluate_grad(self, charges):
+        """(potentials (N,), gradients (N, 3)) of a double tree; gradient = d u / d x
+        (the field is -gradient)."""
+        if self.precision != "double":
+            raise ValueError("gradients are computed by double trees")
+        q = self._charges(charges)
+        pot = np.empty(self.N)
+        grad = np.empty((self.N, 3))
+        dummy = np.zeros(3, dtype=np.float64)
+        rc = self._lib.pdmk_evaluate_grad_double(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(pot), _ptr(grad))
+        self._check(rc, "pdmk_evaluate_grad_double")
+        return pot, grad
 
     def evaluate_multi_f32(self, charges):
         """k charge vectors stored as float32 (N, k) on a float tree: float32 in,

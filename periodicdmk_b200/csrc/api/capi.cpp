@@ -337,6 +337,36 @@ int pdmk_evaluate_multi_device_float_qf32(void* h, int k, const float* Q_dev, do
     }
 }
 
+int pdmk_evaluate_grad_double(void* h, int, const double*, const double* q, double* pot, double* grad) {
+    if (!h) {
+        set_error("pdmk_evaluate_grad_double", "null handle");
+        return -1;
+    }
+    try {
+        if (!q || !pot || !grad) throw std::invalid_argument("null charges or output");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h);
+        t->impl()->dev->evaluate_grad_host(q, pot, grad);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_grad_double", e);
+    }
+}
+
+int pdmk_evaluate_grad_device_double(void* h, const double* q_dev, double* pot_dev, double* grad_dev) {
+    if (!h) {
+        set_error("pdmk_evaluate_grad_device_double", "null handle");
+        return -1;
+    }
+    try {
+        if (!q_dev || !pot_dev || !grad_dev) throw std::invalid_argument("null device pointer");
+        auto* t = static_cast<pdmk::PeriodicDMKTreeT<double, 3>*>(h);
+        t->impl()->dev->evaluate_grad_device(q_dev, pot_dev, grad_dev);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_grad_device_double", e);
+    }
+}
+
 int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, double* far_part) {
     if (!h) {
         set_error("pdmk_evaluate_parts", "null handle");

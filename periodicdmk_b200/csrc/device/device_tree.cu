@@ -20,6 +20,7 @@
 #include "../host/pswf.hpp"
 #include "device_tree.hpp"
 #include "dmma.cuh"
+#include "grad.cuh"
 #include "pw_fused.cuh"
 #include "sep3.cuh"
 #include "tc_kernels.cuh"
@@ -849,6 +850,10 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                     mult[((size_t)i1 * ng[1] + i2) * n3h + i3] = frac * w * H * H / (Ps * Ps);
                 }
         mult_ = upload(mult);
+        for (int i = 0; i < 9; ++i) {
+            frame_.qmat[i] = P.qmat[i];
+            frame_.umatinv[i] = P.umatinv[i];
+        }
         CUFFT_CHECK(cufftPlan3d(&plan_fwd_, ng[0], ng[1], ng[2], CUFFT_D2Z));
         CUFFT_CHECK(cufftPlan3d(&plan_inv_, ng[0], ng[1], ng[2], CUFFT_Z2D));
         CUFFT_CHECK(cufftSetStream(plan_fwd_, stream_));
@@ -1118,6 +1123,10 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             e.proxy_down = down;
             dev::launch_eval(e, p, s);
             ++nl;
+            if (grad_on_) {
+                dev::launch_eval_grad(e, p, grad_sorted_, n_, s);
+                ++nl;
+            }
         }
         // parent -> child into the next level's buffer
         if (F.level + 1 < (int)f64_levels_.size()) {
@@ -1212,6 +1221,69 @@ void DeviceTree::evaluate_parts_host(const double* q_user, double* tree_part, do
     PDMK_CUDA_CHECK(cudaMemcpyAsync(far_part, fp, sizeof(double) * n_, cudaMemcpyDeviceToHost, stream_));
     PDMK_CUDA_CHECK(cudaFreeAsync(tp, stream_));
     PDMK_CUDA_CHECK(cudaFreeAsync(fp, stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+void DeviceTree::ensure_grad() {
+    if (grad_sorted_) return;
+    ensure_fp64_working_set();
+    grad_sorted_ = alloc<double>(3 * (size_t)n_);
+    far_grad_ = alloc<double>(3 * (size_t)n_);
+    grad_dev_ = alloc<double>(3 * (size_t)n_);
+    spec_save_ = alloc<dev::cd>(n_spec_);
+    spec_tmp_ = alloc<dev::cd>(n_spec_);
+}
+
+void DeviceTree::evaluate_grad_device(const double* q, double* pot, double* grad) {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    last_was_multi_ = false;
+    ensure_grad();
+    struct Flag {  // the leaf-evaluation gradients run only inside this call
+        bool& f;
+        explicit Flag(bool& x) : f(x) { f = true; }
+        ~Flag() { f = false; }
+    } on(grad_on_);
+    cudaStream_t s = stream_;
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(pot_sorted_, 0, sizeof(double) * n_, s));
+    PDMK_CUDA_CHECK(cudaMemsetAsync(grad_sorted_, 0, sizeof(double) * 3 * (size_t)n_, s));
+    run_fp64_tree(q, f64_scratch_, f64_scratch_elems_, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
+    dev::launch_near_pg(near_, grad_sorted_, n_, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[2], s));
+    // far field: potential, then the three spectral derivatives of the same spectrum
+    dev::launch_nufft_gather_q(trg_perm_, q, q_sorted_, n_, s);
+    PDMK_CUDA_CHECK(cudaMemsetAsync(grid_, 0, sizeof(double) * n_grid_, s));
+    dev::launch_spread(nufft_, nufft_max_jk_, nufft_max_ex_, s);
+    CUFFT_CHECK(cufftExecD2Z(plan_fwd_, grid_, reinterpret_cast<cufftDoubleComplex*>(spec_)));
+    dev::launch_multiply(spec_, mult_, n_spec_, s);
+    // the complex-to-real transform overwrites its input: keep a copy
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(spec_save_, spec_, sizeof(dev::cd) * n_spec_, cudaMemcpyDeviceToDevice, s));
+    CUFFT_CHECK(cufftExecZ2D(plan_inv_, reinterpret_cast<cufftDoubleComplex*>(spec_), grid_));
+    dev::launch_interp(nufft_, s);
+    for (int d = 0; d < 3; ++d) {
+        dev::launch_grad_multiply(spec_save_, spec_tmp_, nufft_.n1, nufft_.n2, nufft_.n3, d, frame_, s);
+        CUFFT_CHECK(cufftExecZ2D(plan_inv_, reinterpret_cast<cufftDoubleComplex*>(spec_tmp_), grid_));
+        dev::NufftArgs na = nufft_;
+        na.far = far_grad_ + (int64_t)d * n_;
+        dev::launch_interp(na, s);
+    }
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
+    dev::launch_finalize(pot_sorted_, far_sorted_, trg_, trg_perm_, q, pot, n_, s);
+    dev::launch_finalize_grad(grad_sorted_, far_grad_, trg_perm_, grad, n_, frame_, s);
+    PDMK_CUDA_CHECK(cudaEventRecord(ev_[4], s));
+    PDMK_CUDA_CHECK(cudaGetLastError());
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+void DeviceTree::evaluate_grad_host(const double* q_user, double* pot_user, double* grad_user) {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    ensure_grad();
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, q_user, sizeof(double) * n_, cudaMemcpyHostToDevice, stream_));
+    evaluate_grad_device(q_dev_, pot_dev_, grad_dev_);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(pot_user, pot_dev_, sizeof(double) * n_, cudaMemcpyDeviceToHost, stream_));
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(grad_user, grad_dev_, sizeof(double) * 3 * (size_t)n_, cudaMemcpyDeviceToHost,
+                                    stream_));
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 

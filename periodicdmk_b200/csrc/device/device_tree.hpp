@@ -10,6 +10,7 @@
 
 #include "../host/plan.hpp"
 #include "batch_near.cuh"
+#include "grad.cuh"
 #include "kernels.cuh"
 
 namespace pdmkb {
@@ -77,6 +78,12 @@ class DeviceTree {
     // static device array instead of the tree's buffers, and nothing is
     // allocated; synchronous.  Defined in noalloc.cu.
     void evaluate_device_noalloc(const double* q_user_d, double* pot_user_d);
+    // Potentials and their gradients d u / d x (user frame, grad[3 i + d], user
+    // order) of the plain FP64 path: device buffers (N, 3N doubles) or host
+    // buffers.  Synchronous.  Defined with the gradient kernels' drivers in
+    // device_tree.cu (kernels in grad.cu).
+    void evaluate_grad_device(const double* q_user_d, double* pot_user_d, double* grad_user_d);
+    void evaluate_grad_host(const double* q_user, double* pot_user, double* grad_user);
     // Tree part (near + plane-wave levels - self) and far field, user order, host buffers.
     void evaluate_parts_host(const double* q_user, double* tree_part, double* far_part);
     // Number of kernels one evaluate launches (for reporting).
@@ -268,6 +275,15 @@ class DeviceTree {
     double* mult_ = nullptr;
     int64_t n_spec_ = 0, n_grid_ = 0;
     cufftHandle plan_fwd_ = 0, plan_inv_ = 0;
+    // gradients (allocated on the first gradient evaluate)
+    void ensure_grad();
+    bool grad_on_ = false;          // leaf-evaluation gradients launched by run_fp64_tree
+    double* grad_sorted_ = nullptr; // near + local-expansion gradient, [3][n] sorted targets
+    double* far_grad_ = nullptr;    // far-field gradient, [3][n]
+    double* grad_dev_ = nullptr;    // staging for host-buffer gradient evaluates, [n][3]
+    dev::cd* spec_save_ = nullptr;  // far-field spectrum after the multiplier
+    dev::cd* spec_tmp_ = nullptr;   // i K_d times it
+    dev::GradFrame frame_{};
 };
 
 }  // namespace pdmkb
