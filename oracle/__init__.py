@@ -45,6 +45,9 @@ def lib():
         _lib.oracle_ewald_targets_grad.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ip, ctypes.c_double,
                                                    ctypes.c_double, d, d]
         _lib.oracle_ewald_targets_grad.restype = ctypes.c_int
+        _lib.oracle_ewald_targets_qp.argtypes = [d, ctypes.c_int, d, d, ctypes.c_int, ip, ctypes.c_double,
+                                                 ctypes.c_double, d, d, d]
+        _lib.oracle_ewald_targets_qp.restype = ctypes.c_int
         _lib.oracle_evaluate_multi.argtypes = [d, ctypes.c_int, d, ctypes.c_int, d, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, d]
         _lib.oracle_evaluate_multi.restype = ctypes.c_int
@@ -199,6 +202,22 @@ def ewald_targets_grad(cell, pos, q, targets, s=6.0, alpha=0.0):
                                        _dp(out), _dp(g)) != 0:
         raise RuntimeError("oracle_ewald_targets_grad failed")
     return out, g.reshape(-1, 3)
+
+
+def ewald_targets_qp(cell, pos, q, targets, bloch, s=6.0, alpha=0.0):
+    """Quasi-periodic Ewald potentials (complex) at the target indices: images at
+    x_j + R carry e^{i bloch.R} (bloch Cartesian, the caller's frame)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.int32)
+    b = np.ascontiguousarray(bloch, dtype=np.float64)
+    re, im = np.zeros(len(t)), np.zeros(len(t))
+    c = _cell(cell)
+    ip = ctypes.POINTER(ctypes.c_int)
+    if lib().oracle_ewald_targets_qp(_dp(c), len(q), _dp(pos), _dp(q), len(t), t.ctypes.data_as(ip), s, alpha,
+                                     _dp(b), _dp(re), _dp(im)) != 0:
+        raise RuntimeError("oracle_ewald_targets_qp failed")
+    return re + 1j * im
 
 
 def evaluate_multi(cell, pos, Q, n_digits=6, n_per_leaf=300, nz=4):

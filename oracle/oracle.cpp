@@ -1012,4 +1012,170 @@ int oracle_evaluate_multi(const double* cell, int n, const double* pos, int k, c
     }
 }
 
+// Quasi-periodic Ewald sum at a subset of targets: images at x_j + R carry the
+// phase e^{i beta.R} (beta the Bloch vector, Cartesian, the caller's frame):
+//   phi(x_t) = sum_{j,R}' q_j e^{i beta.R} G(x_t - x_j - R), G = 1/r,
+// split as erfc(alpha r)/r (real space, R = (x_t - x_j) - dr from the actual
+// positions) + the Bloch-periodised erf(alpha r)/r,
+//   (4 pi / V) sum_k e^{-|k+beta|^2/(4 alpha^2)} / |k+beta|^2 S(k) e^{i (k+beta).x_t},
+//   S(k) = sum_j q_j e^{-i (k+beta).x_j}   (all k; k + beta = 0 dropped)
+// - 2 alpha/sqrt(pi) q_t.  The periodic sum is the beta = 0 case.  Complex
+// output (pot_re, pot_im).
+int oracle_ewald_targets_qp(const double* cell, int n, const double* pos, const double* q, int m, const int* tidx,
+                            double s, double alpha, const double* bloch, double* pot_re, double* pot_im) {
+    try {
+        const double* a[3] = {cell, cell + 3, cell + 6};
+        auto cross = [](const double* u, const double* v, double* w) {
+            w[0] = u[1] * v[2] - u[2] * v[1];
+            w[1] = u[2] * v[0] - u[0] * v[2];
+            w[2] = u[0] * v[1] - u[1] * v[0];
+        };
+        auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+        double c[3][3];
+        cross(a[1], a[2], c[0]);
+        cross(a[2], a[0], c[1]);
+        cross(a[0], a[1], c[2]);
+        const double V = std::fabs(dot(a[0], c[0]));
+        if (!(V > 0) || n <= 0 || m <= 0) return -1;
+        double h[3];
+        for (int d = 0; d < 3; ++d) h[d] = V / std::sqrt(dot(c[d], c[d]));
+        const double sgn = dot(a[0], c[0]) > 0 ? 1.0 : -1.0;
+        double ainv[3][3];
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 3; ++e) ainv[d][e] = sgn * c[d][e] / V;
+        if (!(alpha > 0)) {
+            const double A = m * (n / V) * 4.18879 * s * s * s * 10.0;
+            const double B = 2.0 * n * 4.18879 * 8.0 * s * s * s * V / (8.0 * M_PI * M_PI * M_PI);
+            alpha = std::pow(A / B, 1.0 / 6.0);
+        }
+        const double rcut = s / alpha, kmax = 2.0 * s * alpha, rc2 = rcut * rcut;
+        std::vector<double> f((size_t)3 * n), fu((size_t)3 * n);
+        for (int j = 0; j < n; ++j)
+            for (int d = 0; d < 3; ++d) {
+                const double* x = pos + 3 * (size_t)j;
+                const double v = ainv[d][0] * x[0] + ainv[d][1] * x[1] + ainv[d][2] * x[2];
+                fu[3 * (size_t)j + d] = v;
+                double w = v - std::floor(v);
+                if (w >= 1.0) w = 0.0;
+                f[3 * (size_t)j + d] = w;
+            }
+        // ---- real space (cell list as oracle_ewald_targets)
+        int G[3], reach[3];
+        const double nb = std::max(1.0, std::cbrt(n / 8.0));
+        for (int d = 0; d < 3; ++d) {
+            G[d] = std::max(1, std::min(512, (int)std::lround(nb)));
+            reach[d] = (int)std::ceil(rcut / h[d] * G[d]) + 1;
+        }
+        const size_t nbins = (size_t)G[0] * G[1] * G[2];
+        std::vector<int> bstart(nbins + 1, 0), border(n);
+        auto bin_of = [&](int j) {
+            int b[3];
+            for (int d = 0; d < 3; ++d) b[d] = std::min(G[d] - 1, (int)(f[3 * (size_t)j + d] * G[d]));
+            return ((size_t)b[2] * G[1] + b[1]) * G[0] + b[0];
+        };
+        for (int j = 0; j < n; ++j) bstart[bin_of(j) + 1]++;
+        for (size_t b = 0; b < nbins; ++b) bstart[b + 1] += bstart[b];
+        {
+            std::vector<int> fill(bstart.begin(), bstart.end() - 1);
+            for (int j = 0; j < n; ++j) border[fill[bin_of(j)]++] = j;
+        }
+        std::vector<cplx> phi(m);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int ti = 0; ti < m; ++ti) {
+            const int t = tidx[ti];
+            const double* ft = &f[3 * (size_t)t];
+            const double* xt = pos + 3 * (size_t)t;
+            int bt[3];
+            for (int d = 0; d < 3; ++d) bt[d] = std::min(G[d] - 1, (int)(ft[d] * G[d]));
+            cplx sum(0);
+            for (int o2 = -reach[2]; o2 <= reach[2]; ++o2)
+                for (int o1 = -reach[1]; o1 <= reach[1]; ++o1)
+                    for (int o0 = -reach[0]; o0 <= reach[0]; ++o0) {
+                        const int raw[3] = {bt[0] + o0, bt[1] + o1, bt[2] + o2};
+                        int bi[3], sh[3];
+                        for (int d = 0; d < 3; ++d) {
+                            sh[d] = (int)std::floor((double)raw[d] / G[d]);
+                            bi[d] = raw[d] - sh[d] * G[d];
+                        }
+                        const size_t b = ((size_t)bi[2] * G[1] + bi[1]) * G[0] + bi[0];
+                        for (int k = bstart[b]; k < bstart[b + 1]; ++k) {
+                            const int j = border[k];
+                            if (j == t && !sh[0] && !sh[1] && !sh[2]) continue;
+                            double df[3];
+                            for (int d = 0; d < 3; ++d) df[d] = ft[d] - (f[3 * (size_t)j + d] + sh[d]);
+                            double dr[3];
+                            for (int e = 0; e < 3; ++e) dr[e] = a[0][e] * df[0] + a[1][e] * df[1] + a[2][e] * df[2];
+                            const double r2 = dot(dr, dr);
+                            if (r2 >= rc2) continue;
+                            const double r = std::sqrt(r2);
+                            const double* xj = pos + 3 * (size_t)j;
+                            double R[3];
+                            for (int e = 0; e < 3; ++e) R[e] = (xt[e] - xj[e]) - dr[e];
+                            const double ph = dot(bloch, R);
+                            sum += q[j] * std::erfc(alpha * r) / r * cplx(std::cos(ph), std::sin(ph));
+                        }
+                    }
+            phi[ti] = sum - 2.0 * alpha / std::sqrt(M_PI) * q[t];
+        }
+        // ---- reciprocal space: every mode m with |2 pi A^-T m + beta| <= kmax
+        double b[3][3];
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 3; ++e) b[d][e] = 2 * M_PI * ainv[d][e];
+        const double bn = std::sqrt(dot(bloch, bloch));
+        int mm[3];
+        for (int d = 0; d < 3; ++d) mm[d] = (int)std::ceil((kmax + bn) * std::sqrt(dot(a[d], a[d])) / (2 * M_PI));
+        std::vector<std::array<int, 3>> modes;
+        std::vector<double> w;
+        const double km2 = kmax * kmax, inv4a2 = 1.0 / (4 * alpha * alpha), pref = 4 * M_PI / V;
+        for (int m3 = -mm[2]; m3 <= mm[2]; ++m3)
+            for (int m2 = -mm[1]; m2 <= mm[1]; ++m2)
+                for (int m1 = -mm[0]; m1 <= mm[0]; ++m1) {
+                    double kv[3];
+                    for (int e = 0; e < 3; ++e) kv[e] = m1 * b[0][e] + m2 * b[1][e] + m3 * b[2][e] + bloch[e];
+                    const double k2 = dot(kv, kv);
+                    if (k2 > km2 || k2 < 1e-24) continue;
+                    modes.push_back({m1, m2, m3});
+                    w.push_back(pref * std::exp(-k2 * inv4a2) / k2);
+                }
+        const size_t nk = modes.size();
+        std::vector<cplx> S(nk, cplx(0));
+#pragma omp parallel
+        {
+            std::vector<cplx> acc(nk, cplx(0));
+            std::vector<cplx> e1(2 * mm[0] + 1), e2(2 * mm[1] + 1), e3(2 * mm[2] + 1);
+#pragma omp for schedule(static)
+            for (int j = 0; j < n; ++j) {
+                const double* fj = &fu[3 * (size_t)j];
+                const double bx = dot(bloch, pos + 3 * (size_t)j);
+                const cplx cj = q[j] * cplx(std::cos(bx), -std::sin(bx));
+                for (int k = -mm[0]; k <= mm[0]; ++k) e1[k + mm[0]] = std::polar(1.0, -2 * M_PI * k * fj[0]);
+                for (int k = -mm[1]; k <= mm[1]; ++k) e2[k + mm[1]] = std::polar(1.0, -2 * M_PI * k * fj[1]);
+                for (int k = -mm[2]; k <= mm[2]; ++k) e3[k + mm[2]] = std::polar(1.0, -2 * M_PI * k * fj[2]);
+                for (size_t k = 0; k < nk; ++k)
+                    acc[k] += cj * e1[modes[k][0] + mm[0]] * e2[modes[k][1] + mm[1]] * e3[modes[k][2] + mm[2]];
+            }
+#pragma omp critical
+            for (size_t k = 0; k < nk; ++k) S[k] += acc[k];
+        }
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int ti = 0; ti < m; ++ti) {
+            const int t = tidx[ti];
+            const double* ft = &fu[3 * (size_t)t];
+            cplx sum(0);
+            for (size_t k = 0; k < nk; ++k) {
+                const double ph = 2 * M_PI * (modes[k][0] * ft[0] + modes[k][1] * ft[1] + modes[k][2] * ft[2]);
+                sum += w[k] * S[k] * cplx(std::cos(ph), std::sin(ph));
+            }
+            const double bx = dot(bloch, pos + 3 * (size_t)t);
+            const cplx v = phi[ti] + sum * cplx(std::cos(bx), std::sin(bx));
+            pot_re[ti] = v.real();
+            pot_im[ti] = v.imag();
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle_ewald_targets_qp: %s\n", e.what());
+        return -1;
+    }
+}
+
 }  // extern "C"

@@ -233,3 +233,17 @@ def test_ewald_gradient_matches_finite_differences():
     # potentials unchanged by the gradient pass
     v, _ = oracle.ewald_targets_grad(cell, pos, q, idx, s=6.5)
     assert rel_l2(v, oracle.ewald_targets(cell, pos, q, idx, s=6.5)) < 1e-15
+
+
+def test_quasi_periodic_ewald_oracle():
+    # Bloch vector 0 reproduces the periodic Ewald sum; for a nonzero Bloch
+    # vector the result does not depend on the splitting parameter alpha
+    cell, pos, q = clustered_system(500, 5, TRICLINIC, n_clusters=3, sigma=0.05)
+    idx = np.arange(len(q))
+    ref = oracle.ewald_targets(cell, pos, q, idx, s=6.5)
+    z = oracle.ewald_targets_qp(cell, pos, q, idx, [0.0, 0.0, 0.0], s=6.5)
+    assert rel_l2(z.real, ref) < 1e-14 and np.abs(z.imag).max() < 1e-13 * np.abs(ref).max()
+    b = np.array([0.7, -1.1, 2.3])
+    z1 = oracle.ewald_targets_qp(cell, pos, q, idx, b, s=6.5)
+    z2 = oracle.ewald_targets_qp(cell, pos, q, idx, b, s=6.5, alpha=9.0)
+    assert np.linalg.norm(z1 - z2) / np.linalg.norm(z1) < 1e-13
