@@ -99,15 +99,24 @@ struct Plan {
     std::vector<double> resid;         // residual polynomial coefficients
     double psi0_at_zero = 0, c0 = 0;
 
+    // ---- quasi-periodic evaluation: images at x + R carry e^{i bloch.R}, the
+    // Bloch vector taken in the lattice-QR frame of the tree (as the reference's
+    // generate_images / far_field_nufft use it, cpp/include/dmk/pbc.hpp:142-256,
+    // cpp/src/dmk/pbc.cpp:250-357)
+    bool qp = false;
+    double bloch[3]{};
+
     // ---- periodic far field (windowed kernel W_rc)
-    int ms = 0, mt = 0, mu = 0;        // mode counts along the three reciprocal axes
+    int ms = 0, mt = 0, mu = 0;        // mode counts along the three reciprocal axes (|bloch| added when qp)
     std::vector<double> ff_weights;    // ms*mt*mu, ms fastest, modes -m/2 .. (m-1)/2
 
     std::string summary() const;
 };
 
 // Build a plan.  cell[j*3+i] = component i of lattice vector j; pos[3*i+d].
+// bloch (3 doubles, or null): quasi-periodic plan (see Plan::qp).
 // Throws std::invalid_argument on bad input.
-Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz);
+Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz,
+                const double* bloch = nullptr);
 
 }  // namespace pdmkb

@@ -185,7 +185,11 @@ void build_tables(Plan& P) {
     {
         const double twopi = 2.0 * M_PI;
         const double* u = P.umat;
-        const double dkmax = beta / P.rc;
+        // quasi-periodic: the modes reach |2 pi L^-T m + bloch| <= beta / rc
+        // (cpp/src/dmk/pbc.cpp:258-265)
+        const double bn = P.qp ? std::sqrt(P.bloch[0] * P.bloch[0] + P.bloch[1] * P.bloch[1] + P.bloch[2] * P.bloch[2])
+                               : 0.0;
+        const double dkmax = beta / P.rc + bn;
         const double an1 = u[0];
         const double an2 = std::sqrt(u[3] * u[3] + u[4] * u[4]);
         const double an3 = std::sqrt(u[6] * u[6] + u[7] * u[7] + u[8] * u[8]);
@@ -201,9 +205,10 @@ void build_tables(Plan& P) {
         for (int k = -P.mu / 2; k <= (P.mu - 1) / 2; ++k)
             for (int j = -P.mt / 2; j <= (P.mt - 1) / 2; ++j)
                 for (int i = -P.ms / 2; i <= (P.ms - 1) / 2; ++i, ++idx) {
-                    const double d1 = twopi * (a11 * i);
-                    const double d2 = twopi * (a21 * i + a22 * j);
-                    const double d3 = twopi * (a31 * i + a32 * j + a33 * k);
+                    // shifted wavenumbers 2 pi L^-T m + bloch (bloch = 0 when periodic)
+                    const double d1 = twopi * (a11 * i) + P.bloch[0];
+                    const double d2 = twopi * (a21 * i + a22 * j) + P.bloch[1];
+                    const double d3 = twopi * (a31 * i + a32 * j + a33 * k) + P.bloch[2];
                     const double k2 = d1 * d1 + d2 * d2 + d3 * d3;
                     if (k2 < 1e-30) continue;
                     const double xval = std::sqrt(k2) * P.rc / beta;

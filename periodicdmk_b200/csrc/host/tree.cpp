@@ -255,7 +255,8 @@ struct Builder {
 
 }  // namespace
 
-Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz) {
+Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz,
+                const double* bloch) {
     if (n <= 0) throw std::invalid_argument("number of points must be positive");
     if (n_per_leaf <= 0) throw std::invalid_argument("n_per_leaf must be positive");
     if (nz <= 0) throw std::invalid_argument("nz must be positive (the automatic rc choice is not supported)");
@@ -664,6 +665,10 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
         }
     }
 
+    if (bloch) {
+        P.qp = true;
+        for (int d = 0; d < 3; ++d) P.bloch[d] = bloch[d];
+    }
     build_tables(P);
     return P;
 }
