@@ -98,6 +98,24 @@ int pdmk_evaluate_grad_double(void* h, int N, const double* positions_3xN, const
                               double* grad_3xN);
 int pdmk_evaluate_grad_device_double(void* h, const double* charges_dev, double* pot_dev, double* grad_dev);
 
+/* Quasi-periodic trees (the reference's PeriodicDMKTreeT constructed with a
+ * Bloch vector and its evaluate_complex, cpp/src/periodic_dmk.cpp:41-47,
+ * 251-276; not in the reference's C ABI, whose create takes no Bloch vector).
+ * bloch3 is in the lattice-QR frame, as the reference takes it.  The complex
+ * potentials u_i = sum_j q_j sum_R e^{i bloch.R} G(x_i - x_j - R) come out
+ * interleaved, pot_2N[2 i] = Re u_i, pot_2N[2 i + 1] = Im u_i (the layout of
+ * the reference's pbcdmk_adaptive output), computed in FP64 for both tree
+ * types.  The real evaluates of a quasi-periodic tree, and the complex
+ * evaluate of a periodic one, fail with -1.  The device form takes device
+ * buffers (N charges, 2N doubles out). */
+void* pdmk_create_qp_double(const double* cell_3x3, int N, const double* positions_3xN, int n_digits, int n_per_leaf,
+                            int nz, const double* bloch3);
+void* pdmk_create_qp_float(const double* cell_3x3, int N, const double* positions_3xN, int n_digits, int n_per_leaf,
+                           int nz, const double* bloch3);
+int pdmk_evaluate_complex_double(void* h, int N, const double* positions_3xN, const double* charges, double* pot_2N);
+int pdmk_evaluate_complex_float(void* h, int N, const double* positions_3xN, const double* charges, float* pot_2N);
+int pdmk_evaluate_complex_device_double(void* h, const double* charges_dev, double* pot_2N_dev);
+
 /* The two parts of the potential in user order: the tree part (near field +
  * plane-wave levels - self term) and the periodic far field. */
 int pdmk_evaluate_parts_double(void* h, const double* charges, double* tree_part, double* far_part);

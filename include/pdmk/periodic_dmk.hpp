@@ -9,10 +9,15 @@
 //   Real = float  : mixed-precision path (FP32 near field and transforms where
 //                   the error budget allows, FP64 far field and accumulation),
 //                   float output as in the reference.
-// Only DIM = 3 is provided (the reference's 2D and quasi-periodic paths are
-// not part of this build).
+// With a Bloch vector (taken in the lattice-QR frame, as the reference takes
+// it) the tree is quasi-periodic: evaluate_complex returns
+// sum_j q_j sum_R e^{i bloch.R} G(x_i - x_j - R), computed in FP64 for both
+// Real types, and evaluate / evaluate_timed / evaluate_multi throw
+// std::logic_error.  Only DIM = 3 is provided (the reference's 2D path is not
+// part of this build).
 #pragma once
 #include <array>
+#include <complex>
 #include <memory>
 #include <optional>
 #include <variant>
@@ -47,6 +52,11 @@ class PeriodicDMKTreeT {
     /// k charge vectors on the same tree: charges is N x k column-major
     /// (charges[i + N*c]); returns N x k column-major potentials.
     std::vector<Real> evaluate_multi(const std::vector<double>& charges, int k);
+    /// Quasi-periodic potentials (trees built with a Bloch vector; the
+    /// reference's evaluate_complex, cpp/src/periodic_dmk.cpp:251-276).
+    /// Throws std::logic_error without a Bloch vector, std::invalid_argument if
+    /// charges.size() != n_points().
+    std::vector<std::complex<Real>> evaluate_complex(const std::vector<double>& charges);
 
     int n_points() const { return n_src_; }
     double cube_size() const { return rc_; }
@@ -58,6 +68,7 @@ class PeriodicDMKTreeT {
     std::unique_ptr<Impl> p_;
     int n_src_;
     double rc_;
+    bool qp_ = false;
 };
 
 using PeriodicDMKTree = PeriodicDMKTreeT<double, 3>;

@@ -34,6 +34,8 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_parts_double", "pdmk_info_double", "pdmk_info_float",
     "pdmk_stage_times_double", "pdmk_stage_times_float", "pdmk_fma_peak", "pdmk_tc_peak",
     "pdmk_evaluate_device_noalloc_double",
+    "pdmk_create_qp_double", "pdmk_create_qp_float", "pdmk_evaluate_complex_double",
+    "pdmk_evaluate_complex_float", "pdmk_evaluate_complex_device_double",
     "pdmk_batch_create", "pdmk_batch_create_double", "pdmk_batch_evaluate", "pdmk_batch_evaluate_float",
     "pdmk_batch_info", "pdmk_batch_destroy",
     "pdmk_last_error",
@@ -62,6 +64,16 @@ def library():
     lib.pdmk_create_double.restype = v
     lib.pdmk_create_float.argtypes = lib.pdmk_create_double.argtypes
     lib.pdmk_create_float.restype = v
+    lib.pdmk_create_qp_double.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
+    lib.pdmk_create_qp_double.restype = v
+    lib.pdmk_create_qp_float.argtypes = lib.pdmk_create_qp_double.argtypes
+    lib.pdmk_create_qp_float.restype = v
+    lib.pdmk_evaluate_complex_double.argtypes = [v, ctypes.c_int, _D, _D, _D]
+    lib.pdmk_evaluate_complex_double.restype = ctypes.c_int
+    lib.pdmk_evaluate_complex_float.argtypes = [v, ctypes.c_int, _D, _D, _F]
+    lib.pdmk_evaluate_complex_float.restype = ctypes.c_int
+    lib.pdmk_evaluate_complex_device_double.argtypes = [v, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pdmk_evaluate_complex_device_double.restype = ctypes.c_int
     lib.pdmk_evaluate_double.argtypes = [v, ctypes.c_int, _D, _D, _D]
     lib.pdmk_evaluate_float.argtypes = [v, ctypes.c_int, _D, _D, _F]
     lib.pdmk_evaluate_timed_double.argtypes = [v, ctypes.c_int, _D, _D, _D, _D]
@@ -148,13 +160,16 @@ class PeriodicDMKTree:
     cell: 3x3, columns are the lattice vectors.  positions: (N, 3) Cartesian.
     precision: "double" (plain FP64 path) or "float" (mixed-precision path,
     float output), as the reference's double / float instantiations.
+    bloch: optional Bloch vector (3,), in the lattice-QR frame as the
+    reference takes it; the tree is then quasi-periodic and evaluates with
+    evaluate_complex only (the real evaluates raise).
     """
 
     INFO_KEYS = ["n_points", "n_all", "n_boxes", "n_levels", "n_target_leaves", "p", "n_pw",
                  "launches_per_evaluate", "device_bytes", "far_modes", "near_pairs", "pw_boxes",
                  "launches_last_multi", "n_digits_tree", "mixed_available", "translate_boxes"]
 
-    def __init__(self, cell, positions, n_digits=6, n_per_leaf=300, nz=4, precision="double"):
+    def __init__(self, cell, positions, n_digits=6, n_per_leaf=300, nz=4, precision="double", bloch=None):
         if precision not in ("double", "float"):
             raise ValueError("precision must be 'double' or 'float'")
         pos = np.ascontiguousarray(positions, dtype=np.float64)
@@ -164,8 +179,17 @@ class PeriodicDMKTree:
         self.precision = precision
         self.N = pos.shape[0]
         c = _cell_colmajor(cell)
-        create = self._lib.pdmk_create_double if precision == "double" else self._lib.pdmk_create_float
-        self._h = create(_ptr(c), self.N, _ptr(pos), int(n_digits), int(n_per_leaf), int(nz))
+        self.bloch = None
+        if bloch is None:
+            create = self._lib.pdmk_create_double if precision == "double" else self._lib.pdmk_create_float
+            self._h = create(_ptr(c), self.N, _ptr(pos), int(n_digits), int(n_per_leaf), int(nz))
+        else:
+            b = np.ascontiguousarray(bloch, dtype=np.float64)
+            if b.shape != (3,):
+                raise ValueError("bloch must have shape (3,)")
+            self.bloch = b
+            create = self._lib.pdmk_create_qp_double if precision == "double" else self._lib.pdmk_create_qp_float
+            self._h = create(_ptr(c), self.N, _ptr(pos), int(n_digits), int(n_per_leaf), int(nz), _ptr(b))
         if not self._h:
             raise RuntimeError("pdmk_create failed: " + _last_error())
         self.n_digits = n_digits
@@ -253,6 +277,29 @@ class PeriodicDMKTree:
             rc = self._lib.pdmk_evaluate_multi_device_float(self._h, int(k), ctypes.c_void_p(q_ptr),
                                                             ctypes.c_void_p(pot_ptr))
         self._check(rc, "pdmk_evaluate_multi_device")
+
+    def evaluate_complex(self, charges):
+        """Quasi-periodic potentials sum_j q_j sum_R e^{i bloch.R} G(x_i - x_j - R)
+        of a tree built with a Bloch vector: complex128 (double trees) or
+        complex64 (float trees), computed in FP64."""
+        q = self._charges(charges)
+        dummy = np.zeros(3, dtype=np.float64)
+        if self.precision == "double":
+            out = np.empty(2 * self.N)
+            rc = self._lib.pdmk_evaluate_complex_double(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(out))
+        else:
+            out = np.empty(2 * self.N, dtype=np.float32)
+            rc = self._lib.pdmk_evaluate_complex_float(self._h, self.N, _ptr(dummy), _ptr(q), _ptr(out, _F))
+        self._check(rc, "pdmk_evaluate_complex")
+        return out.view(np.complex128 if self.precision == "double" else np.complex64)
+
+    def evaluate_complex_device(self, q_ptr, pot2_ptr):
+        """Quasi-periodic evaluate on device buffers (N charges; 2N doubles out,
+        (Re, Im) interleaved) of a double tree."""
+        if self.precision != "double":
+            raise RuntimeError("evaluate_complex_device is provided for double trees")
+        rc = self._lib.pdmk_evaluate_complex_device_double(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(pot2_ptr))
+        self._check(rc, "pdmk_evaluate_complex_device_double")
 
     def evaluate_grad(self, charges):
         """(potentials (N,), gradients (N, 3)) of a double tree; gradient = d u / d x

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -58,6 +59,45 @@ void* create_impl(const double* cell, int n, const double* pos, int nd, int npl,
     } catch (const std::exception& e) {
         set_error("pdmk_create", e.what());
         return nullptr;
+    }
+}
+
+template <typename Real>
+void* create_qp_impl(const double* cell, int n, const double* pos, int nd, int npl, int nz, const double* bloch) {
+    try {
+        if (!cell || !pos || !bloch) throw std::invalid_argument("null cell, positions or bloch");
+        if (n <= 0) throw std::invalid_argument("N must be positive");
+        g_last_error.clear();
+        return new pdmk::PeriodicDMKTreeT<Real, 3>(to_mat3(cell), to_positions(pos, n), nd, npl, nz,
+                                                   std::array<double, 3>{bloch[0], bloch[1], bloch[2]});
+    } catch (const std::exception& e) {
+        set_error("pdmk_create_qp", e.what());
+        return nullptr;
+    }
+}
+
+template <typename Real, typename Out>
+int evaluate_complex_impl(void* h, const double* q, Out* pot2, bool device) {
+    if (!h) {
+        set_error("pdmk_evaluate_complex", "null handle");
+        return -1;
+    }
+    try {
+        if (!q || !pot2) throw std::invalid_argument("null charges or output");
+        auto* dv = static_cast<pdmk::PeriodicDMKTreeT<Real, 3>*>(h)->impl()->dev.get();
+        if (device) {
+            dv->evaluate_complex_device(q, reinterpret_cast<double*>(pot2));
+            PDMK_CUDA_CHECK(cudaStreamSynchronize(dv->stream()));
+        } else if (std::is_same<Out, double>::value) {
+            dv->evaluate_complex_host(q, reinterpret_cast<double*>(pot2));
+        } else {
+            std::vector<double> tmp(2 * (size_t)dv->n_points());
+            dv->evaluate_complex_host(q, tmp.data());
+            for (size_t i = 0; i < tmp.size(); ++i) pot2[i] = (Out)tmp[i];
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_evaluate_complex", e);
     }
 }
 
@@ -365,6 +405,24 @@ int pdmk_evaluate_grad_device_double(void* h, const double* q_dev, double* pot_d
     } catch (const std::exception& e) {
         return fail("pdmk_evaluate_grad_device_double", e);
     }
+}
+
+void* pdmk_create_qp_double(const double* cell, int N, const double* pos, int nd, int npl, int nz,
+                            const double* bloch) {
+    return create_qp_impl<double>(cell, N, pos, nd, npl, nz, bloch);
+}
+void* pdmk_create_qp_float(const double* cell, int N, const double* pos, int nd, int npl, int nz,
+                           const double* bloch) {
+    return create_qp_impl<float>(cell, N, pos, nd, npl, nz, bloch);
+}
+int pdmk_evaluate_complex_double(void* h, int, const double*, const double* q, double* pot2) {
+    return evaluate_complex_impl<double, double>(h, q, pot2, false);
+}
+int pdmk_evaluate_complex_float(void* h, int, const double*, const double* q, float* pot2) {
+    return evaluate_complex_impl<float, float>(h, q, pot2, false);
+}
+int pdmk_evaluate_complex_device_double(void* h, const double* q_dev, double* pot2_dev) {
+    return evaluate_complex_impl<double, double>(h, q_dev, pot2_dev, true);
 }
 
 int pdmk_evaluate_parts_double(void* h, const double* q, double* tree_part, double* far_part) {

@@ -23,8 +23,6 @@ template <typename Real, int DIM>
 PeriodicDMKTreeT<Real, DIM>::PeriodicDMKTreeT(const MatND<DIM>& cell, const std::vector<VecND<DIM>>& positions,
                                               int n_digits, int n_per_leaf, int nz,
                                               std::optional<std::array<double, DIM>> bloch) {
-    if (bloch.has_value())
-        throw std::logic_error("PeriodicDMKTreeT: quasi-periodic (bloch) evaluation is not provided by this build");
     p_ = std::make_unique<Impl>();
     double c[9];
     for (int j = 0; j < 3; ++j)
@@ -32,8 +30,12 @@ PeriodicDMKTreeT<Real, DIM>::PeriodicDMKTreeT(const MatND<DIM>& cell, const std:
     std::vector<double> pos(3 * positions.size());
     for (size_t i = 0; i < positions.size(); ++i)
         for (int d = 0; d < 3; ++d) pos[3 * i + d] = positions[i][d];
+    double b[3] = {0.0, 0.0, 0.0};
+    if (bloch.has_value())
+        for (int d = 0; d < 3; ++d) b[d] = (*bloch)[d];
+    qp_ = bloch.has_value();
     p_->plan = std::make_unique<pdmkb::Plan>(
-        pdmkb::build_plan(c, (int)positions.size(), pos.data(), n_digits, n_per_leaf, nz));
+        pdmkb::build_plan(c, (int)positions.size(), pos.data(), n_digits, n_per_leaf, nz, qp_ ? b : nullptr));
     p_->single = std::is_same<Real, float>::value;
     p_->dev = std::make_unique<pdmkb::DeviceTree>(*p_->plan, -1, /*fp64_working_set=*/!p_->single);
     n_src_ = p_->plan->n_src;
@@ -45,12 +47,14 @@ PeriodicDMKTreeT<Real, DIM>::~PeriodicDMKTreeT() = default;
 
 template <typename Real, int DIM>
 std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate(const std::vector<double>& charges) {
+    if (qp_) throw std::logic_error("evaluate: bloch is set - use evaluate_complex()");
     EvalTiming t;
     return evaluate_timed(charges, t);
 }
 
 template <typename Real, int DIM>
 std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_timed(const std::vector<double>& charges, EvalTiming& timing) {
+    if (qp_) throw std::logic_error("evaluate_timed: bloch is set - use evaluate_complex()");
     if ((int)charges.size() != n_src_) throw std::invalid_argument("charges size != n_src");
     std::vector<double> pot(n_src_);
     pdmkb::StageTimes st;
@@ -67,11 +71,23 @@ std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_timed(const std::vector<
 
 template <typename Real, int DIM>
 std::vector<Real> PeriodicDMKTreeT<Real, DIM>::evaluate_multi(const std::vector<double>& charges, int k) {
+    if (qp_) throw std::logic_error("evaluate_multi: bloch is set - use evaluate_complex()");
     if (k <= 0 || (int64_t)charges.size() != (int64_t)n_src_ * k)
         throw std::invalid_argument("charges size != n_src * k");
     std::vector<double> pot((size_t)n_src_ * k);
     p_->dev->evaluate_multi_host(charges.data(), k, pot.data(), /*pot_float=*/false, /*fp32=*/p_->single, nullptr);
     return std::vector<Real>(pot.begin(), pot.end());
+}
+
+template <typename Real, int DIM>
+std::vector<std::complex<Real>> PeriodicDMKTreeT<Real, DIM>::evaluate_complex(const std::vector<double>& charges) {
+    if (!qp_) throw std::logic_error("evaluate_complex: bloch not set at construction");
+    if ((int)charges.size() != n_src_) throw std::invalid_argument("charges size != n_src");
+    std::vector<double> pot(2 * (size_t)n_src_);
+    p_->dev->evaluate_complex_host(charges.data(), pot.data());
+    std::vector<std::complex<Real>> out((size_t)n_src_);
+    for (int i = 0; i < n_src_; ++i) out[i] = std::complex<Real>((Real)pot[2 * (size_t)i], (Real)pot[2 * (size_t)i + 1]);
+    return out;
 }
 
 template class PeriodicDMKTreeT<double, 3>;

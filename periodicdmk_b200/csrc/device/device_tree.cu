@@ -245,9 +245,10 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     // image positions); it gets no storage and no work of its own.  With a
     // cell whose lattice vectors are multiples of the box size (cubes) this
     // covers every image-only box; triclinic images straddle boxes and none
-    // qualify.
+    // qualify.  Quasi-periodic trees share nothing: an image box's charges
+    // carry the Bloch phase of its lattice vector.
     std::vector<int> alias(P.nboxes, -1);
-    {
+    if (!P.qp) {
         std::vector<int> orig_of(n_, -1);
         std::vector<double> disp(3 * (size_t)n_all_);
         std::vector<char> is_orig(n_all_, 0);
@@ -787,7 +788,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             if (F.eval.n_leaves) launches_ += 1;
         }
     }
-    if (fp64_working_set) {
+    if (fp64_working_set && !P.qp) {  // quasi-periodic trees evaluate on the two-column state
         ensure_fp64_working_set();
         noalloc_reserve(device_);  // double trees may use the no-allocation evaluate
     }
@@ -850,6 +851,60 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
                     mult[((size_t)i1 * ng[1] + i2) * n3h + i3] = frac * w * H * H / (Ps * Ps);
                 }
         mult_ = upload(mult);
+        if (P.qp) {
+            // Quasi-periodic multiplier (cpp/src/dmk/pbc.cpp:289-318): the
+            // spectrum of the phased charges is weighted by w(2 pi L^-T k + bloch)
+            // over the mode box, which is not even in k.  Over the stored half
+            // spectrum of the two real transforms (real and imaginary part of
+            // the phased charges) it enters through its even and odd parts
+            // s = (w(k) + w(-k)) / 2 and d = (w(k) - w(-k)) / 2.
+            auto wq = [&](int k1, int k2, int k3) {
+                if (!inK(k1, k2, k3)) return 0.0;
+                const double d1 = twopi * (a11 * k1) + P.bloch[0];
+                const double d2 = twopi * (a21 * k1 + a22 * k2) + P.bloch[1];
+                const double d3 = twopi * (a31 * k1 + a32 * k2 + a33 * k3) + P.bloch[2];
+                const double kk = d1 * d1 + d2 * d2 + d3 * d3;
+                if (kk < 1e-30) return 0.0;
+                const double xval = std::sqrt(kk) * P.rc / P.dp.beta;
+                return xval > 1.0 ? 0.0 : dfac * pf(xval) / kk;
+            };
+            std::vector<double> qs(n_spec_, 0.0), qd(n_spec_, 0.0);
+            for (int i1 = 0; i1 < ng[0]; ++i1)
+                for (int i2 = 0; i2 < ng[1]; ++i2)
+                    for (int i3 = 0; i3 < n3h; ++i3) {
+                        const int k1 = i1 <= ng[0] / 2 ? i1 : i1 - ng[0];
+                        const int k2 = i2 <= ng[1] / 2 ? i2 : i2 - ng[1];
+                        const int k3 = i3;
+                        const double wp = wq(k1, k2, k3), wm = wq(-k1, -k2, -k3);
+                        if (wp == 0.0 && wm == 0.0) continue;
+                        const double Ps = ph[0][i1] * ph[1][i2] * ph[2][i3];
+                        const double c = H * H / (Ps * Ps);
+                        const size_t at = ((size_t)i1 * ng[1] + i2) * n3h + i3;
+                        qs[at] = 0.5 * (wp + wm) * c;
+                        qd[at] = 0.5 * (wp - wm) * c;
+                    }
+            qp_s_ = upload(qs);
+            qp_d_ = upload(qd);
+            // Bloch phases: e^{i bloch.R} of each sorted source (R = its lattice
+            // image vector) and e^{i bloch.x} of each sorted target
+            std::vector<double2> sp(n_all_), tp(n_);
+            for (int j = 0; j < n_all_; ++j) {
+                const int q = P.src_charge_idx[j];
+                double ph_j = 0.0;
+                for (int d = 0; d < 3; ++d)
+                    ph_j += P.bloch[d] * (P.src_sorted[3 * (size_t)j + d] - P.r_user[3 * (size_t)q + d]);
+                sp[j] = make_double2(std::cos(ph_j), std::sin(ph_j));
+            }
+            for (int t = 0; t < n_; ++t) {
+                const int u = P.trg_perm[t];
+                double th = 0.0;
+                for (int d = 0; d < 3; ++d) th += P.bloch[d] * P.r_user[3 * (size_t)u + d];
+                tp[t] = make_double2(std::cos(th), std::sin(th));
+            }
+            qp_src_phase_ = upload(sp);
+            qp_trg_phase_ = upload(tp);
+            qp_ = true;
+        }
         for (int i = 0; i < 9; ++i) {
             frame_.qmat[i] = P.qmat[i];
             frame_.umatinv[i] = P.umatinv[i];
@@ -1162,7 +1217,12 @@ void DeviceTree::release() {
     for (auto& e : ev_) e = nullptr;
 }
 
+void DeviceTree::require_periodic(const char* what) const {
+    if (qp_) throw std::logic_error(std::string(what) + ": bloch is set - use evaluate_complex()");
+}
+
 void DeviceTree::run(const double* q, double* pot) {
+    require_periodic("evaluate");
     ensure_fp64_working_set();
     cudaStream_t s = stream_;
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
@@ -1235,6 +1295,7 @@ void DeviceTree::ensure_grad() {
 }
 
 void DeviceTree::evaluate_grad_device(const double* q, double* pot, double* grad) {
+    require_periodic("evaluate_grad");
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
     last_was_multi_ = false;
     ensure_grad();

@@ -84,6 +84,16 @@ class DeviceTree {
     // device_tree.cu (kernels in grad.cu).
     void evaluate_grad_device(const double* q_user_d, double* pot_user_d, double* grad_user_d);
     void evaluate_grad_host(const double* q_user, double* pot_user, double* grad_user);
+    // Quasi-periodic trees (built from a plan with a Bloch vector): complex
+    // potentials u(x_i) = sum_j q_j sum_R e^{i bloch.R} G(x_i - x_j - R),
+    // interleaved (Re, Im) per point in user order (2N doubles), computed in
+    // FP64 as two real right-hand sides (the phased charges' real and
+    // imaginary parts) through the tree, and a two-transform quasi-periodic
+    // far field.  Device buffers, or host buffers.  Synchronous.  Defined in
+    // multi.cu (kernels in qp.cu).
+    bool quasi_periodic() const { return qp_; }
+    void evaluate_complex_device(const double* q_user_d, double* pot2_user_d, StageTimes* times = nullptr);
+    void evaluate_complex_host(const double* q_user, double* pot2_user, StageTimes* times = nullptr);
     // Tree part (near + plane-wave levels - self) and far field, user order, host buffers.
     void evaluate_parts_host(const double* q_user, double* tree_part, double* far_part);
     // Number of kernels one evaluate launches (for reporting).
@@ -284,6 +294,14 @@ class DeviceTree {
     dev::cd* spec_save_ = nullptr;  // far-field spectrum after the multiplier
     dev::cd* spec_tmp_ = nullptr;   // i K_d times it
     dev::GradFrame frame_{};
+    // quasi-periodic state (qp.cu)
+    bool qp_ = false;
+    bool qp_run_ = false;               // run_multi_block<double> computes the two QP columns
+    double2* qp_src_phase_ = nullptr;   // (cos, sin) of bloch.R per sorted source
+    double2* qp_trg_phase_ = nullptr;   // (cos, sin) of bloch.x per sorted target
+    double* qp_s_ = nullptr;            // even part of the far-field multiplier, half spectrum
+    double* qp_d_ = nullptr;            // odd part
+    void require_periodic(const char* what) const;  // throws std::logic_error on QP trees
 };
 
 }  // namespace pdmkb

@@ -18,6 +18,7 @@
 #include <stdexcept>
 
 #include "device_tree.hpp"
+#include "qp.cuh"
 #include "nufft_multi.cuh"
 #include "pw_fused.cuh"
 #include "sep3.cuh"
@@ -859,6 +860,7 @@ struct DeviceTree::MultiState {
     void* s2 = nullptr;
     void* pw_in = nullptr;
     int64_t scratch_bytes = 0;
+    bool step_scratch = false;  // s1 / s2 hold scratch_bytes (else 256-byte placeholders)
     double* pot = nullptr;
     double* far = nullptr;
     double* q_t = nullptr;
@@ -945,12 +947,16 @@ DeviceTree::MultiState& DeviceTree::multi_state(int kb, bool fp32) {
     for (const auto& g : pw_groups_) max_boxes = std::max<int64_t>(max_boxes, g.n);
     for (const auto& E : eval_levels_) max_boxes = std::max<int64_t>({max_boxes, (int64_t)E.n, (int64_t)E.n_p2c});
     m->scratch_bytes = std::max<int64_t>(per_entry * kb, std::min<int64_t>((int64_t)512 << 20, per_entry * kb * max_boxes));
-    // s1 / s2 hold step-by-step transform intermediates; the fused transforms need none
+    // s1 / s2 hold step-by-step transform intermediates; the fused transforms need
+    // none, but the tensor-core transforms (PDMK_TC_MASK bit 3) run step by step
+    // in place of the fused kernels and need them at full size
     const bool fused_all = fp32 ? (dev::sep3_supported<float>(p_) && dev::pw_fused_supported<float>(p_, npw_, npw2_))
                                 : (dev::sep3_supported<double>(p_) && dev::pw_fused_supported<double>(p_, npw_, npw2_));
-    const size_t s12 = fused_all ? 256 : (size_t)m->scratch_bytes;
+    const bool tc_steps = fp32 && (tc_mask_ & 8);
+    const size_t s12 = fused_all && !tc_steps ? 256 : (size_t)m->scratch_bytes;
     m->s1 = m->alloc<unsigned char>(s12);
     m->s2 = m->alloc<unsigned char>(s12);
+    m->step_scratch = s12 == (size_t)m->scratch_bytes;
     m->pw_in = m->alloc<unsigned char>((size_t)m->scratch_bytes);
     m->pot = m->alloc<double>((size_t)n_ * kb);
     m->far = m->alloc<double>((size_t)n_ * kb);
@@ -1032,12 +1038,22 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     };
     const int64_t sbytes = m.scratch_bytes;
 
+    // quasi-periodic trees run only the two-column form (qp.cu)
+    const bool qp = !f32 && qp_run_;
+    if (qp_ && !qp) require_periodic("evaluate_multi");
+    if (qp && (kb != 2 || kvalid != 1)) throw std::logic_error("quasi-periodic evaluate: two-column state expected");
     int nl = 0;
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(m.pot, 0, sizeof(double) * n_ * kb, s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(up, 0, sizeof(T) * std::max<int64_t>(n_up_ * ncoef * kb, 1), s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(down, 0, sizeof(T) * std::max<int64_t>(n_down_ * ncoef * kb, 1), s));
-    {
+    if (qp) {
+        // the phased charges q e^{i bloch.R} per sorted source (two columns, rows
+        // per source) and q e^{-i bloch.x} per sorted target for the far field
+        dev::launch_qp_charges(reinterpret_cast<double*>(src_q), src_charge_idx_, qp_src_phase_, n_all_, m.q_t,
+                               trg_perm_, qp_trg_phase_, n_, Q, s);
+        nl += 2;
+    } else {
         // charges to row-major (the far-field output buffer is free until the
         // interpolation writes it), then one contiguous row per source
         const int64_t tot = (int64_t)n_all_ * kb;
@@ -1071,7 +1087,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     // Transforms on the tensor cores (FP32 blocks, PDMK_TC_MASK bit 3): every
     // separable step is one tcgen05 contraction (contract_tc.cu); the chunks
     // of (box, RHS) entries are sized so that the step intermediates stay in L2.
-    const bool tc_tr = f32 && (tc_mask_ & 8) && dev::contract_tc_supported(n, n, 2, 2) &&
+    const bool tc_tr = f32 && (tc_mask_ & 8) && m.step_scratch && dev::contract_tc_supported(n, n, 2, 2) &&
                        dev::contract_tc_supported(p, p, 1, 1);
     const int64_t l2_scratch = 64ll << 20;
     // chunked batched contraction helper over (box, rhs) entries
@@ -1098,6 +1114,8 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         }
     };
     const bool fused = dev::sep3_supported<T>(p) && !tc_tr;
+    if (!m.step_scratch && (!fused || !dev::pw_fused_supported<T>(p, n, n2)))
+        throw std::logic_error("multi-RHS state without step scratch");
     // upward children -> parents
     for (const auto& g : c2p_groups_) {
         const T* mx = c2pm + (int64_t)g.child * 3 * p * p;
@@ -1307,13 +1325,19 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         ++nl;
         if (cufftExecD2Z(m.fwd, m.grid, reinterpret_cast<cufftDoubleComplex*>(m.spec)) != CUFFT_SUCCESS)
             throw std::runtime_error("cuFFT error in the batched forward transform");
-        dev::launch_multiply(m.spec, mult_, n_spec_, s, kb); ++nl;
+        if (qp)
+            dev::launch_qp_combine(m.spec, qp_s_, qp_d_, n_spec_, s);
+        else
+            dev::launch_multiply(m.spec, mult_, n_spec_, s, kb);
+        ++nl;
         if (cufftExecZ2D(m.inv, reinterpret_cast<cufftDoubleComplex*>(m.spec), m.grid) != CUFFT_SUCCESS)
             throw std::runtime_error("cuFFT error in the batched inverse transform");
         dev::launch_interp_multi(na, m.esw, n_, kb, s); ++nl;
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
-    if (!deferred) {
+    if (qp) {
+        dev::launch_qp_finalize(m.pot, m.far, trg_, trg_perm_, Q, qp_trg_phase_, pot_user, n_, s); ++nl;
+    } else if (!deferred) {
         const int64_t tot = (int64_t)n_ * kvalid;
         dev::k_finalize_m<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m.pot, m.far, trg_, trg_perm_, m.q_t, pot_user,
                                                                         n_, kvalid); ++nl;
@@ -1376,6 +1400,32 @@ void DeviceTree::evaluate_multi_device(const double* Q, int k, double* pot, bool
     if (times) *times = acc;
     last_multi_ = acc;
     last_was_multi_ = true;
+}
+
+void DeviceTree::evaluate_complex_device(const double* q, double* pot2, StageTimes* times) {
+    if (!qp_) throw std::logic_error("evaluate_complex: bloch not set at construction");
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    MultiState& m = multi_state(2, false);
+    struct Flag {  // run_multi_block computes the quasi-periodic columns only inside this call
+        bool& f;
+        explicit Flag(bool& x) : f(x) { f = true; }
+        ~Flag() { f = false; }
+    } on(qp_run_);
+    multi_launches_ = 0;
+    run_multi_block<double>(m, q, 1, pot2);
+    const StageTimes t = last_times();
+    if (times) *times = t;
+    last_multi_ = t;
+    last_was_multi_ = true;
+}
+
+void DeviceTree::evaluate_complex_host(const double* q, double* pot2, StageTimes* times) {
+    PDMK_CUDA_CHECK(cudaSetDevice(device_));
+    ensure_stage(2 * (int64_t)n_);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(stage_q_, q, sizeof(double) * n_, cudaMemcpyHostToDevice, stream_));
+    evaluate_complex_device(stage_q_, stage_p_, times);
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(pot2, stage_p_, sizeof(double) * 2 * (size_t)n_, cudaMemcpyDeviceToHost, stream_));
+    PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 
 void DeviceTree::enqueue_multi_device(const double* Q, int k, double* pot, bool fp32) {

@@ -85,6 +85,7 @@ void noalloc_reserve(int device) {
 }
 
 void DeviceTree::evaluate_device_noalloc(const double* q, double* pot) {
+    require_periodic("evaluate");
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
     last_was_multi_ = false;
     if (!proxy_up_)

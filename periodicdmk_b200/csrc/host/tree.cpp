@@ -666,6 +666,8 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
     }
 
     if (bloch) {
+        for (int d = 0; d < 3; ++d)
+            if (!std::isfinite(bloch[d])) throw std::invalid_argument("bloch must be finite");
         P.qp = true;
         for (int d = 0; d < 3; ++d) P.bloch[d] = bloch[d];
     }
