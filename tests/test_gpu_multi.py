@@ -12,6 +12,8 @@ the same tolerances.
 """
 import ctypes
 
+import json
+
 import numpy as np
 import pytest
 
@@ -170,19 +172,27 @@ def test_float32_charges_equal_double_charges():
     t.close()
 
 
-@pytest.mark.parametrize("nd,tol", [(6, 1e-6), (3, 2e-4)])
+@pytest.mark.parametrize("nd,tol", [(6, 5e-6), (3, 2e-4)])
 def test_tensor_core_transforms(nd, tol, monkeypatch):
     # PDMK_TC_MASK bit 3 (read when the tree is built) runs the translation and
-    # plane-wave transform steps as tcgen05 contractions (3xTF32); same bars as
-    # the CUDA-core transforms, against the FP64 path
+    # plane-wave transform steps as tcgen05 contractions (3xTF32), against the
+    # FP64 path.  3xTF32 keeps about 22 bits of each operand (an 11-bit hi part
+    # and an 11-bit rounding of the remainder) against FP32's 24, so its error is
+    # a few times that of the CUDA-core FP32 transforms (which keep the 1e-6 bar,
+    # test_mixed_multi_accuracy); the 6-digit bar here is 5e-6.  The path is off
+    # by default: it is also slower.
     cell, pos, _ = clustered_system(6000, 48, TRICLINIC, n_clusters=4, sigma=0.03)
     Q = _charges(len(pos), 64, 6)
     td = pd.PeriodicDMKTree(cell, pos, nd, 40, 4)
     Pd = _multi_device(td, Q, mixed=False)
+    Pc = _multi_device(td, Q, mixed=True)
     td.close()
     monkeypatch.setenv("PDMK_TC_MASK", "15")
     t = pd.PeriodicDMKTree(cell, pos, nd, 40, 4)
     Pm = _multi_device(t, Q, mixed=True)
     t.close()
     errs = [rel_l2(Pm[:, c], Pd[:, c]) for c in range(64)]
+    errs_cc = [rel_l2(Pc[:, c], Pd[:, c]) for c in range(64)]
+    print("PARITY " + json.dumps({"case": "tcgen05 transforms %d digits" % nd, "max_rel_l2_tc": max(errs),
+                                  "max_rel_l2_cuda_core": max(errs_cc)}))
     assert max(errs) < tol, (int(np.argmax(errs)), max(errs))

@@ -3,8 +3,10 @@ evaluate_complex), through the C ABI:
 
 * against the quasi-periodic Ewald sum at every target
   (oracle.ewald_targets_qp, pinned on the CPU against the periodic sum and for
-  splitting independence), bars 2e-6 / 2e-9 / 2e-12 relative L2 at 6 / 9 / 12
-  digits (the periodic evaluate's bars);
+  splitting independence), bars 2e-6 / 1e-8 / 2e-12 relative L2 at 6 / 9 / 12
+  digits (the periodic evaluate measures 7.7e-9 against the Ewald sum on the
+  same 9-digit cube; the reference's 9-digit bar is 1e-7,
+  cpp/tests/test_nonuniform.cpp:303);
 * the reference's own tests (cpp/tests/test_periodic_dmk_qp.cpp): bloch = 0
   reduces to the periodic evaluate (|Im| and |Re - periodic| < 1e-5 there; on
   a larger case here the real part to 1e-10 relative, the imaginary part at
@@ -40,7 +42,7 @@ def cmax(a, b):
 
 
 @pytest.mark.parametrize("system", ["cube", "clustered_triclinic"])
-@pytest.mark.parametrize("nd,bar", [(6, 2e-6), (9, 2e-9), (12, 2e-12)])
+@pytest.mark.parametrize("nd,bar", [(6, 2e-6), (9, 1e-8), (12, 2e-12)])
 def test_qp_vs_ewald(system, nd, bar):
     if system == "cube":
         cell, pos, q = uniform_system(3000, 81)
@@ -107,7 +109,7 @@ def test_qp_nz_independence():
         t = pd.PeriodicDMKTree(cell, pos, 9, 30, nz, bloch=BLOCH)
         z.append(t.evaluate_complex(q))
         t.close()
-    assert crel(z[0], z[1]) < 2e-9 and crel(z[2], z[1]) < 2e-9
+    assert crel(z[0], z[1]) < 1e-8 and crel(z[2], z[1]) < 1e-8
 
 
 def test_qp_float_tree_and_device_buffers():
@@ -125,7 +127,7 @@ def test_qp_float_tree_and_device_buffers():
     td.evaluate_complex_device(qd.data_ptr(), out.data_ptr())
     torch.cuda.synchronize()
     zdev = out.cpu().numpy().view(np.complex128)
-    assert np.array_equal(zdev, zd)
+    assert crel(zdev, zd) < 1e-13  # the far-field spreading sums with atomics
     # repeated evaluations agree (cpp/tests/test_periodic_dmk_tree.cpp:38-39)
     assert crel(td.evaluate_complex(q), zd) < 1e-12
     td.close()
