@@ -189,6 +189,23 @@ int pdmk_batch_evaluate_float(void* h, const double* charges, float* pot_out);
 int pdmk_batch_info(void* h, int64_t* out4);
 void pdmk_batch_destroy(void* h);
 
+/* Campaign reference files: oracle potentials at M sampled points of an
+ * N-point system, stored with the system in the reference's 'PDMC' format
+ * (cpp/include/pdmk/campaign_ref_io.hpp:13-186, header-only C++ there; the C++
+ * form here is include/pdmk/campaign_ref_io.hpp).  No counterpart in the
+ * reference's C ABI.  cell9 is column-major as cell_3x3 above; pos_3N as
+ * positions_3xN.  pdmk_campaign_read_header: out5 = {config_id, N, M, digits,
+ * prec}; pdmk_campaign_read fills buffers of those sizes.  -1 on an I/O error,
+ * a malformed file or a digest mismatch.  pdmk_sha256: SHA-256 (FIPS 180-4)
+ * of len bytes into out32. */
+int pdmk_sha256(const void* data, uint64_t len, unsigned char* out32);
+int pdmk_campaign_write(const char* path, uint32_t config_id, uint32_t digits, uint32_t prec, uint64_t seed,
+                        const double* cell9, uint32_t N, const double* pos_3N, const double* chg_N, uint32_t M,
+                        const uint32_t* ref_idx, const double* ref_u);
+int pdmk_campaign_read_header(const char* path, uint32_t* out5, uint64_t* seed);
+int pdmk_campaign_read(const char* path, double* cell9, double* pos_3N, double* chg_N, uint32_t* ref_idx,
+                       double* ref_u);
+
 /* Last error message of the calling thread ("" if none). */
 const char* pdmk_last_error(void);
 

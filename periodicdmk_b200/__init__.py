@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_complex_float", "pdmk_evaluate_complex_device_double",
     "pdmk_batch_create", "pdmk_batch_create_double", "pdmk_batch_evaluate", "pdmk_batch_evaluate_float",
     "pdmk_batch_info", "pdmk_batch_destroy",
+    "pdmk_sha256", "pdmk_campaign_write", "pdmk_campaign_read_header", "pdmk_campaign_read",
     "pdmk_last_error",
 ]
 
@@ -132,6 +133,16 @@ def library():
     lib.pdmk_batch_info.restype = ctypes.c_int
     lib.pdmk_batch_destroy.argtypes = [v]
     lib.pdmk_batch_destroy.restype = None
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    lib.pdmk_sha256.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    lib.pdmk_sha256.restype = ctypes.c_int
+    lib.pdmk_campaign_write.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_uint64, _D, ctypes.c_uint32, _D, _D, ctypes.c_uint32, u32p, _D]
+    lib.pdmk_campaign_write.restype = ctypes.c_int
+    lib.pdmk_campaign_read_header.argtypes = [ctypes.c_char_p, u32p, ctypes.POINTER(ctypes.c_uint64)]
+    lib.pdmk_campaign_read_header.restype = ctypes.c_int
+    lib.pdmk_campaign_read.argtypes = [ctypes.c_char_p, _D, _D, _D, u32p, _D]
+    lib.pdmk_campaign_read.restype = ctypes.c_int
     lib.pdmk_last_error.argtypes = []
     lib.pdmk_last_error.restype = ctypes.c_char_p
     _lib = lib

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <complex>
@@ -16,6 +17,7 @@
 #include <vector>
 
 #include "batch.hpp"
+#include "pdmk/campaign_ref_io.hpp"
 #include "impl.hpp"
 #include "pdmk/periodic_dmk.hpp"
 
@@ -452,6 +454,71 @@ int pdmk_evaluate_device_noalloc_double(void* h, const double* q_dev, double* po
         return 0;
     } catch (const std::exception& e) {
         return fail("pdmk_evaluate_device_noalloc_double", e);
+    }
+}
+
+int pdmk_sha256(const void* data, uint64_t len, unsigned char* out32) {
+    if ((!data && len) || !out32) {
+        set_error("pdmk_sha256", "null buffer");
+        return -1;
+    }
+    pdmk::campaign::sha256(static_cast<const uint8_t*>(data), (size_t)len, out32);
+    return 0;
+}
+
+int pdmk_campaign_write(const char* path, uint32_t config_id, uint32_t digits, uint32_t prec, uint64_t seed,
+                        const double* cell9, uint32_t N, const double* pos, const double* chg, uint32_t M,
+                        const uint32_t* ref_idx, const double* ref_u) {
+    try {
+        if (!path || !cell9 || (N && (!pos || !chg)) || (M && (!ref_idx || !ref_u)))
+            throw std::invalid_argument("null argument");
+        if (digits > 255 || prec > 255) throw std::invalid_argument("digits and prec must fit one byte");
+        pdmk::campaign::RefData d{};
+        d.header.config_id = config_id;
+        d.header.N = N;
+        d.header.digits = (uint8_t)digits;
+        d.header.prec = (uint8_t)prec;
+        d.header.seed = seed;
+        std::memcpy(d.cell, cell9, sizeof(d.cell));
+        d.ref_idx.assign(ref_idx, ref_idx + M);
+        d.ref_u.assign(ref_u, ref_u + M);
+        d.pos.assign(pos, pos + 3 * (size_t)N);
+        d.chg.assign(chg, chg + N);
+        pdmk::campaign::write_ref(path, d);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_campaign_write", e);
+    }
+}
+
+int pdmk_campaign_read_header(const char* path, uint32_t* out5, uint64_t* seed) {
+    try {
+        if (!path || !out5) throw std::invalid_argument("null argument");
+        const pdmk::campaign::RefData d = pdmk::campaign::read_ref(path);
+        out5[0] = d.header.config_id;
+        out5[1] = d.header.N;
+        out5[2] = d.header.M;
+        out5[3] = d.header.digits;
+        out5[4] = d.header.prec;
+        if (seed) *seed = d.header.seed;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_campaign_read_header", e);
+    }
+}
+
+int pdmk_campaign_read(const char* path, double* cell9, double* pos, double* chg, uint32_t* ref_idx, double* ref_u) {
+    try {
+        if (!path || !cell9 || !pos || !chg || !ref_idx || !ref_u) throw std::invalid_argument("null argument");
+        const pdmk::campaign::RefData d = pdmk::campaign::read_ref(path);
+        std::memcpy(cell9, d.cell, sizeof(d.cell));
+        std::copy(d.pos.begin(), d.pos.end(), pos);
+        std::copy(d.chg.begin(), d.chg.end(), chg);
+        std::copy(d.ref_idx.begin(), d.ref_idx.end(), ref_idx);
+        std::copy(d.ref_u.begin(), d.ref_u.end(), ref_u);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_campaign_read", e);
     }
 }
 

@@ -24,6 +24,20 @@ def _build():
     return EXE
 
 
+def test_campaign_io_cpp(tmp_path):
+    # include/pdmk/campaign_ref_io.hpp from C++ (host code only: runs on the CPU)
+    if not os.path.exists(pd.library_path()):
+        pytest.skip("libpdmk_b200.so not built")
+    exe = str(tmp_path / "test_campaign_io")
+    lib = pd.library_path()
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(HERE, "cpp", "test_campaign_io.cpp"), "-o", exe, "-L", os.path.dirname(lib),
+                    "-lpdmk_b200", "-Wl,-rpath," + os.path.dirname(lib)], check=True, capture_output=True, text=True)
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=120)
+    print(r.stdout)
+    assert r.returncode == 0 and "0 failures" in r.stdout, r.stdout + r.stderr
+
+
 def test_cpp_api_compiles_and_links():
     if not os.path.exists(pd.library_path()):
         pytest.skip("libpdmk_b200.so not built")
