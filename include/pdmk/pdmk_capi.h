@@ -24,8 +24,10 @@ extern "C" {
 /* ---- reference entry points ------------------------------------------- */
 
 /* Ewald summation reference (replaces cpp/include/pdmk/pdmk_capi.h:23-28;
- * reference implementation cpp/src/ewald_nufft.cpp:445-654).  Host code, not
- * the accelerated path.  s sets the accuracy: erfc(s) ~ exp(-s^2). */
+ * reference implementation cpp/src/ewald_nufft.cpp:445-654, same parameter
+ * choice).  Runs on the current CUDA device: cell-list real-space sum and a
+ * NUFFT reciprocal sum, O(N log N).  s sets the accuracy: erfc(s) ~ exp(-s^2);
+ * the NUFFT tolerance is 1e-12. */
 int pdmk_ewald_nufft(const double* cell_3x3, int N, const double* positions_3xN, const double* charges, double s,
                      double* potentials_out, double* energy_out);
 

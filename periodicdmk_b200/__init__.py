@@ -454,7 +454,8 @@ class PeriodicDMKBatch:
 
 
 def ewald(cell, positions, charges, s=4.8):
-    """Ewald reference through the C ABI (host code).  Returns (potentials, energy)."""
+    """Ewald summation on the GPU through the C ABI (pdmk_ewald_nufft: cell-list
+    real-space sum, NUFFT reciprocal sum).  Returns (potentials, energy)."""
     lib = library()
     pos = np.ascontiguousarray(positions, dtype=np.float64)
     q = np.ascontiguousarray(charges, dtype=np.float64)

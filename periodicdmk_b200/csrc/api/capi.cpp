@@ -16,6 +16,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "../device/ewald.cuh"
 #include "batch.hpp"
 #include "pdmk/campaign_ref_io.hpp"
 #include "impl.hpp"
@@ -548,74 +549,15 @@ int pdmk_tc_peak(int kind, double* tflops) {
 int pdmk_info_float(void* h, int64_t* out) { return info_impl<float>(h, out); }
 
 // ---------------------------------------------------------------------------
-// Ewald reference (host).  Real-space erfc sum over lattice shells within
-// r_cut = s/alpha plus the reciprocal Gaussian sum over |k| <= 2 s alpha, self
-// term -2 alpha/sqrt(pi) q_i and the charged-system energy correction.
+// Ewald summation on the GPU (csrc/device/ewald.cu): cell-list real-space sum
+// within r_cut = s/alpha, NUFFT reciprocal sum over |k| <= 2 s alpha, self term
+// -2 alpha/sqrt(pi) q_i and the charged-system energy correction.
 // ---------------------------------------------------------------------------
 int pdmk_ewald_nufft(const double* cell, int N, const double* pos, const double* q, double s, double* pot,
                      double* energy) {
     try {
         if (!cell || !pos || !q || !pot) throw std::invalid_argument("null buffer");
-        if (N <= 0) throw std::invalid_argument("N must be positive");
-        const double* a[3] = {cell, cell + 3, cell + 6};
-        auto cross = [](const double* u, const double* v, double* w) {
-            w[0] = u[1] * v[2] - u[2] * v[1];
-            w[1] = u[2] * v[0] - u[0] * v[2];
-            w[2] = u[0] * v[1] - u[1] * v[0];
-        };
-        auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
-        double c[3][3];
-        cross(a[1], a[2], c[0]);
-        cross(a[2], a[0], c[1]);
-        cross(a[0], a[1], c[2]);
-        const double V = std::fabs(dot(a[0], c[0]));
-        if (!(V > 0)) throw std::invalid_argument("degenerate cell");
-        const double alpha = std::pow(N * M_PI * M_PI * M_PI / (V * V), 1.0 / 6.0);
-        const double rcut = s / alpha, kmax = 2.0 * s * alpha;
-        int nmax[3], mmax[3];
-        for (int d = 0; d < 3; ++d) {
-            nmax[d] = (int)std::ceil(rcut / (V / std::sqrt(dot(c[d], c[d]))));
-            mmax[d] = (int)std::ceil(kmax * std::sqrt(dot(a[d], a[d])) / (2 * M_PI));
-        }
-        std::vector<double> phi(N, 0.0);
-        for (int i = 0; i < N; ++i)
-            for (int j = 0; j < N; ++j)
-                for (int n0 = -nmax[0]; n0 <= nmax[0]; ++n0)
-                    for (int n1 = -nmax[1]; n1 <= nmax[1]; ++n1)
-                        for (int n2 = -nmax[2]; n2 <= nmax[2]; ++n2) {
-                            if (i == j && !n0 && !n1 && !n2) continue;
-                            double dr[3];
-                            for (int d = 0; d < 3; ++d)
-                                dr[d] = pos[3 * i + d] - pos[3 * j + d] + n0 * a[0][d] + n1 * a[1][d] + n2 * a[2][d];
-                            const double r2 = dot(dr, dr);
-                            if (r2 > rcut * rcut) continue;
-                            const double r = std::sqrt(r2);
-                            phi[i] += q[j] * std::erfc(alpha * r) / r;
-                        }
-        double b[3][3];
-        for (int d = 0; d < 3; ++d)
-            for (int e = 0; e < 3; ++e) b[d][e] = 2 * M_PI * c[d][e] / V;
-        for (int m3 = -mmax[2]; m3 <= mmax[2]; ++m3)
-            for (int m2 = -mmax[1]; m2 <= mmax[1]; ++m2)
-                for (int m1 = -mmax[0]; m1 <= mmax[0]; ++m1) {
-                    if (!m1 && !m2 && !m3) continue;
-                    double kv[3];
-                    for (int d = 0; d < 3; ++d) kv[d] = m1 * b[0][d] + m2 * b[1][d] + m3 * b[2][d];
-                    const double k2 = dot(kv, kv);
-                    if (k2 > kmax * kmax) continue;
-                    const double w = 4 * M_PI / V * std::exp(-k2 / (4 * alpha * alpha)) / k2;
-                    std::complex<double> S(0);
-                    for (int j = 0; j < N; ++j) S += q[j] * std::polar(1.0, -dot(kv, pos + 3 * j));
-                    for (int i = 0; i < N; ++i) phi[i] += w * (S * std::polar(1.0, dot(kv, pos + 3 * i))).real();
-                }
-        double E = 0, Q = 0;
-        for (int i = 0; i < N; ++i) {
-            phi[i] -= 2.0 * alpha / std::sqrt(M_PI) * q[i];
-            pot[i] = phi[i];
-            E += q[i] * phi[i];
-            Q += q[i];
-        }
-        if (energy) *energy = 0.5 * E - M_PI * Q * Q / (2 * V * alpha * alpha);
+        pdmkb::ewald_gpu(cell, N, pos, q, s, pot, energy);
         return 0;
     } catch (const std::exception& e) {
         return fail("pdmk_ewald_nufft", e);

@@ -9,9 +9,8 @@ import re
 import numpy as np
 import pytest
 
-import oracle
 import periodicdmk_b200 as pd
-from conftest import TRICLINIC, rel_l2, uniform_system
+from conftest import TRICLINIC, uniform_system
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -84,22 +83,6 @@ def test_no_cpu_fallback():
     cell, pos, q = uniform_system(200, 1)
     with pytest.raises(RuntimeError, match="CUDA"):
         pd.PeriodicDMKTree(cell, pos, 6, 20, 4)
-
-
-def test_ewald_entry_matches_oracle():
-    cell, pos, q = uniform_system(64, 3, TRICLINIC, charges="uniform")
-    a, ea = pd.ewald(cell, pos, q, 5.5)
-    b, eb = oracle.ewald_direct(cell, pos, q, 5.5)
-    assert rel_l2(a, b) < 1e-10
-    assert abs(ea - eb) < 1e-10 * abs(eb)
-
-
-def test_ewald_entry_madelung():
-    pos = np.array([[0, 0, 0], [.5, .5, 0], [.5, 0, .5], [0, .5, .5], [.5, 0, 0], [0, .5, 0], [0, 0, .5],
-                    [.5, .5, .5]])
-    q = np.array([1, 1, 1, 1, -1, -1, -1, -1.0])
-    _, e = pd.ewald(np.eye(3), pos, q, 5.5)
-    assert abs(-e / 8 - 1.7475645946331822) < 1e-8
 
 
 def test_cubic_cover():
