@@ -259,6 +259,8 @@ void ewald_gpu(const double* cell, int n, const double* pos, const double* q, do
     }
     const int64_t nbins = (int64_t)m[0] * m[1] * m[2];
     if (nbins > (1 << 26)) throw std::invalid_argument("too many real-space bins");
+    if ((int64_t)(2 * R[0] + 1) * (2 * R[1] + 1) * (2 * R[2] + 1) > (1 << 20))
+        throw std::invalid_argument("cell too thin for the real-space cutoff (more than 2^20 image bins per target)");
     std::vector<int> bin(n);
     std::vector<double4> wrapped(n);
     for (int i = 0; i < n; ++i) {
