@@ -208,6 +208,14 @@ int pdmk_campaign_read_header(const char* path, uint32_t* out5, uint64_t* seed);
 int pdmk_campaign_read(const char* path, double* cell9, double* pos_3N, double* chg_N, uint32_t* ref_idx,
                        double* ref_u);
 
+/* Tree construction check: builds the plan of a system with its point steps
+ * on the host (on_device = 0) or on the current CUDA device (1) and writes the
+ * SHA-256 of the plan's point order, image list, box topology and interaction
+ * lists to out32, and the build time to build_ms (may be null).  The two forms
+ * give the same digest. */
+int pdmk_plan_digest(const double* cell_3x3, int N, const double* positions_3xN, int n_digits, int n_per_leaf,
+                     int nz, int on_device, unsigned char* out32, double* build_ms);
+
 /* Last error message of the calling thread ("" if none). */
 const char* pdmk_last_error(void);
 

@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = [
     "pdmk_evaluate_complex_float", "pdmk_evaluate_complex_device_double",
     "pdmk_batch_create", "pdmk_batch_create_double", "pdmk_batch_evaluate", "pdmk_batch_evaluate_float",
     "pdmk_batch_info", "pdmk_batch_destroy",
-    "pdmk_sha256", "pdmk_campaign_write", "pdmk_campaign_read_header", "pdmk_campaign_read",
+    "pdmk_sha256", "pdmk_campaign_write", "pdmk_campaign_read_header", "pdmk_campaign_read", "pdmk_plan_digest",
     "pdmk_last_error",
 ]
 
@@ -143,6 +143,9 @@ def library():
     lib.pdmk_campaign_read_header.restype = ctypes.c_int
     lib.pdmk_campaign_read.argtypes = [ctypes.c_char_p, _D, _D, _D, u32p, _D]
     lib.pdmk_campaign_read.restype = ctypes.c_int
+    lib.pdmk_plan_digest.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p, _D]
+    lib.pdmk_plan_digest.restype = ctypes.c_int
     lib.pdmk_last_error.argtypes = []
     lib.pdmk_last_error.restype = ctypes.c_char_p
     _lib = lib
@@ -466,6 +469,20 @@ def ewald(cell, positions, charges, s=4.8):
     if rc != 0:
         raise RuntimeError("pdmk_ewald_nufft failed: " + _last_error())
     return pot, float(e[0])
+
+
+def plan_digest(cell, positions, n_digits=6, n_per_leaf=300, nz=4, on_device=False):
+    """(SHA-256 hex of the tree plan, build milliseconds) with the point steps of
+    the tree construction on the host or on the GPU; both give the same digest."""
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    c = _cell_colmajor(cell)
+    out = ctypes.create_string_buffer(32)
+    ms = np.zeros(1)
+    rc = library().pdmk_plan_digest(_ptr(c), len(pos), _ptr(pos), int(n_digits), int(n_per_leaf), int(nz),
+                                    1 if on_device else 0, out, _ptr(ms))
+    if rc != 0:
+        raise RuntimeError("pdmk_plan_digest failed: " + _last_error())
+    return out.raw.hex(), float(ms[0])
 
 
 def optimize_cubic_cover(cell, nz=4):

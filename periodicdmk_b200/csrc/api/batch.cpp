@@ -15,6 +15,8 @@
 // autotuner whose choice is cached per batch shape for the process).
 #include "batch.hpp"
 
+#include "../device/tree_build.hpp"
+
 #include <algorithm>
 #include <atomic>
 #include <exception>
@@ -39,18 +41,24 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         if (Ns[i] <= 0) throw std::invalid_argument("every system needs at least one point");
         off_[i + 1] = off_[i] + Ns[i];
     }
-    // host plans in parallel
+    PDMK_CUDA_CHECK(cudaGetDevice(&device_));
+    // plans in parallel on host threads (the point steps of the larger
+    // systems on the GPU)
     std::vector<std::unique_ptr<Plan>> plans(nsys);
     std::atomic<int> next{0};
     std::exception_ptr first_error;
     std::mutex err_mu;
     auto work = [&]() {
+        cudaSetDevice(device_);
         for (;;) {
             const int i = next.fetch_add(1);
             if (i >= nsys) return;
             try {
-                plans[i] = std::make_unique<Plan>(
-                    build_plan(cells + 9 * (size_t)i, Ns[i], positions + 3 * off_[i], n_digits, n_per_leaf, nz));
+                const double* c = cells + 9 * (size_t)i;
+                const double* x = positions + 3 * off_[i];
+                plans[i] = std::make_unique<Plan>(tree_build_on_device(Ns[i], 20000)
+                                                      ? build_plan_device(c, Ns[i], x, n_digits, n_per_leaf, nz)
+                                                      : build_plan(c, Ns[i], x, n_digits, n_per_leaf, nz));
             } catch (...) {
                 std::lock_guard<std::mutex> g(err_mu);
                 if (!first_error) first_error = std::current_exception();
@@ -63,7 +71,6 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
     for (auto& t : pool) t.join();
     if (first_error) std::rethrow_exception(first_error);
     try {
-        PDMK_CUDA_CHECK(cudaGetDevice(&device_));
         // device trees (uploads, cuFFT plans) on host threads too: each system's
         // upload is a sequence of small allocations and copies
         trees_.resize(nsys);

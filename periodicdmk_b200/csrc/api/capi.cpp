@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -17,6 +18,8 @@
 #include <vector>
 
 #include "../device/ewald.cuh"
+#include "../device/tree_build.hpp"
+#include "../host/plan.hpp"
 #include "batch.hpp"
 #include "pdmk/campaign_ref_io.hpp"
 #include "impl.hpp"
@@ -520,6 +523,36 @@ int pdmk_campaign_read(const char* path, double* cell9, double* pos, double* chg
         return 0;
     } catch (const std::exception& e) {
         return fail("pdmk_campaign_read", e);
+    }
+}
+
+int pdmk_plan_digest(const double* cell, int N, const double* pos, int n_digits, int n_per_leaf, int nz,
+                     int on_device, unsigned char* out32, double* build_ms) {
+    try {
+        if (!cell || !pos || !out32) throw std::invalid_argument("null argument");
+        if (N <= 0) throw std::invalid_argument("N must be positive");
+        const auto t0 = std::chrono::steady_clock::now();
+        const pdmkb::Plan P = on_device ? pdmkb::build_plan_device(cell, N, pos, n_digits, n_per_leaf, nz)
+                                        : pdmkb::build_plan(cell, N, pos, n_digits, n_per_leaf, nz);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (build_ms) *build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        std::vector<uint8_t> b;
+        auto put = [&](const void* p, size_t n) {
+            const uint8_t* c = static_cast<const uint8_t*>(p);
+            b.insert(b.end(), c, c + n);
+        };
+        auto vec = [&](const auto& v) { put(v.data(), v.size() * sizeof(v[0])); };
+        const int64_t head[3] = {P.n_all, P.nboxes, P.nlevels};
+        put(head, sizeof(head));
+        vec(P.src_sorted); vec(P.trg_sorted); vec(P.src_perm); vec(P.trg_perm); vec(P.src_charge_idx);
+        vec(P.img_src_idx); vec(P.depth); vec(P.parent); vec(P.nchild); vec(P.children); vec(P.colleagues);
+        vec(P.centers); vec(P.src_start); vec(P.src_count); vec(P.trg_start); vec(P.trg_count);
+        vec(P.list1_start); vec(P.list1); vec(P.ifpwexp); vec(P.iftensprodeval); vec(P.has_proxy_from_children);
+        vec(P.direct_work);
+        pdmk::campaign::sha256(b.data(), b.size(), out32);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail("pdmk_plan_digest", e);
     }
 }
 

@@ -14,6 +14,7 @@
 #include <string>
 
 #include "../device/device_tree.hpp"
+#include "../device/tree_build.hpp"
 #include "../host/plan.hpp"
 #include "impl.hpp"
 
@@ -34,8 +35,12 @@ PeriodicDMKTreeT<Real, DIM>::PeriodicDMKTreeT(const MatND<DIM>& cell, const std:
     if (bloch.has_value())
         for (int d = 0; d < 3; ++d) b[d] = (*bloch)[d];
     qp_ = bloch.has_value();
+    const int n = (int)positions.size();
+    // the point steps of the construction on the GPU for all but small systems
+    const bool on_device = n > 0 && pdmkb::tree_build_on_device(n, 20000);
     p_->plan = std::make_unique<pdmkb::Plan>(
-        pdmkb::build_plan(c, (int)positions.size(), pos.data(), n_digits, n_per_leaf, nz, qp_ ? b : nullptr));
+        on_device ? pdmkb::build_plan_device(c, n, pos.data(), n_digits, n_per_leaf, nz, qp_ ? b : nullptr)
+                  : pdmkb::build_plan(c, n, pos.data(), n_digits, n_per_leaf, nz, qp_ ? b : nullptr));
     p_->single = std::is_same<Real, float>::value;
     p_->dev = std::make_unique<pdmkb::DeviceTree>(*p_->plan, -1, /*fp64_working_set=*/!p_->single);
     n_src_ = p_->plan->n_src;

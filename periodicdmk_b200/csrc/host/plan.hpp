@@ -113,10 +113,14 @@ struct Plan {
     std::string summary() const;
 };
 
+class PointOps;  // points.hpp
+
 // Build a plan.  cell[j*3+i] = component i of lattice vector j; pos[3*i+d].
 // bloch (3 doubles, or null): quasi-periodic plan (see Plan::qp).
+// points: where the point-heavy steps run (null: on the host; the GPU form is
+// build_plan_device, device/tree_build.cu); the plan does not depend on it.
 // Throws std::invalid_argument on bad input.
 Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz,
-                const double* bloch = nullptr);
+                const double* bloch = nullptr, PointOps* points = nullptr);
 
 }  // namespace pdmkb

@@ -9,6 +9,7 @@
 //   2:1 balance                    cpp/src/dmk/pbc_tree.cpp:438-598
 //   flags, lists, work lists       cpp/src/dmk/pbc_tree.cpp:776-1011
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -17,6 +18,7 @@
 #include <stdexcept>
 
 #include "plan.hpp"
+#include "points.hpp"
 
 namespace pdmkb {
 
@@ -96,11 +98,13 @@ void utri_inv(const double* u, double* v) {
 }
 
 // Lattice images of the originals that fall in the extended grid (one rc
-// layer around the inner grid).  Same shift-loop order as the reference so the
-// image list, and hence the sort, is identical.
-void generate_images(const double* umat, double rc, const int* mgrid, const double* xgrid0, int ns,
-                     const double* src, std::vector<double>& img, std::vector<int>& idx) {
-    double lo_ext[3], hi_ext[3], lo[3], hi[3];
+// layer around the inner grid).  The shift loop order is the reference's, so
+// the image list, and hence the sort, is identical: image_shifts lists the
+// candidate shifts in that order, and for each shift every original whose
+// shifted copy lies in [lo_ext, hi_ext] is appended in input order.
+void image_shifts(const double* umat, double rc, const int* mgrid, const double* xgrid0,
+                  std::vector<std::array<double, 3>>& shifts, double* lo_ext, double* hi_ext) {
+    double lo[3], hi[3];
     for (int i = 0; i < 3; ++i) {
         lo_ext[i] = xgrid0[i] - rc;
         hi_ext[i] = xgrid0[i] + (mgrid[i] + 1) * rc;
@@ -109,8 +113,7 @@ void generate_images(const double* umat, double rc, const int* mgrid, const doub
         for (int j = i + 1; j < 3; ++j) w += std::abs(umat[i + j * 3]);
         hi[i] = xgrid0[i] + w;
     }
-    img.clear();
-    idx.clear();
+    shifts.clear();
     const int n3max = (int)((mgrid[2] + 1) * rc / umat[8]) + 1;
     for (int n3 = -n3max; n3 <= n3max; ++n3) {
         const double s3 = umat[8] * n3;
@@ -125,20 +128,154 @@ void generate_images(const double* umat, double rc, const int* mgrid, const doub
                 if (n1 == 0 && n2 == 0 && n3 == 0) continue;
                 const double s1 = umat[0] * n1 + off;
                 if (lo[0] + s1 > hi_ext[0] || hi[0] + s1 < lo_ext[0]) continue;
-                for (int j = 0; j < ns; ++j) {
-                    const double x0 = src[3 * j] + s1, x1 = src[3 * j + 1] + s2, x2 = src[3 * j + 2] + s3;
-                    if (x0 < lo_ext[0] || x0 > hi_ext[0] || x1 < lo_ext[1] || x1 > hi_ext[1] || x2 < lo_ext[2] ||
-                        x2 > hi_ext[2])
-                        continue;
-                    img.push_back(x0);
-                    img.push_back(x1);
-                    img.push_back(x2);
-                    idx.push_back(j);
-                }
+                shifts.push_back({s1, s2, s3});
             }
         }
     }
 }
+
+
+uint64_t spread3(uint32_t v) {  // 10 bits -> every third bit of 30
+    uint64_t x = v & 0x3FF;
+    x = (x | (x << 16)) & 0x030000FF;
+    x = (x | (x << 8)) & 0x0300F00F;
+    x = (x | (x << 4)) & 0x030C30C3;
+    x = (x | (x << 2)) & 0x09249249;
+    return x;
+}
+
+// The point steps on the host.
+class HostPoints final : public PointOps {
+  public:
+    void load(int n, const double* r) override {
+        for (int s = 0; s < 2; ++s) {
+            pos_[s].assign(r, r + 3 * (size_t)n);
+            perm_[s].resize(n);
+            for (int i = 0; i < n; ++i) perm_[s][i] = i;
+        }
+        n_ = n;
+    }
+    std::vector<int> add_images(const std::vector<std::array<double, 3>>& shifts, const double* lo,
+                                const double* hi) override {
+        std::vector<int> idx;
+        std::vector<double>& x = pos_[0];
+        for (const auto& sh : shifts)
+            for (int j = 0; j < n_; ++j) {
+                const double x0 = x[3 * (size_t)j] + sh[0], x1 = x[3 * (size_t)j + 1] + sh[1],
+                             x2 = x[3 * (size_t)j + 2] + sh[2];
+                if (x0 < lo[0] || x0 > hi[0] || x1 < lo[1] || x1 > hi[1] || x2 < lo[2] || x2 > hi[2]) continue;
+                x.insert(x.end(), {x0, x1, x2});
+                idx.push_back(j);
+            }
+        const int na = (int)(x.size() / 3);
+        perm_[0].resize(na);
+        for (int i = 0; i < na; ++i) perm_[0][i] = i;
+        return idx;
+    }
+    std::vector<int> bin0(int s, const double* xelo, double rcinv, const int* m) override {
+        const std::vector<double>& x = pos_[s];
+        const int np = size(s), nb0 = m[0] * m[1] * m[2];
+        std::vector<int> boxof(np), ip(nb0 + 1, 0);
+        for (int i = 0; i < np; ++i) {
+            int ii[3];
+            for (int k = 0; k < 3; ++k) {
+                ii[k] = (int)((x[3 * (size_t)i + k] - xelo[k]) * rcinv);
+                ii[k] = std::min(std::max(ii[k], 0), m[k] - 1);
+            }
+            boxof[i] = ii[2] * m[0] * m[1] + ii[1] * m[0] + ii[0];
+            ip[boxof[i] + 1]++;
+        }
+        for (int b = 0; b < nb0; ++b) ip[b + 1] += ip[b];
+        std::vector<int> fill(ip.begin(), ip.end() - 1), perm(np);
+        for (int i = 0; i < np; ++i) perm[fill[boxof[i]]++] = i;
+        std::vector<double> sorted(3 * (size_t)np);
+        std::vector<int> sp(np);
+        for (int i = 0; i < np; ++i) {
+            for (int d = 0; d < 3; ++d) sorted[3 * (size_t)i + d] = x[3 * (size_t)perm[i] + d];
+            sp[i] = perm_[s][perm[i]];
+        }
+        pos_[s] = std::move(sorted);
+        perm_[s] = std::move(sp);
+        return ip;
+    }
+    std::vector<std::array<int, 8>> partition(int s, const std::vector<Range>& r) override {
+        std::vector<std::array<int, 8>> out(r.size());
+        std::vector<double>& pos = pos_[s];
+        std::vector<int>& perm = perm_[s];
+        for (size_t k = 0; k < r.size(); ++k) {
+            const int start = r[k].start, npts = r[k].count;
+            std::vector<int> oct(npts);
+            std::array<int, 8> cnt{};
+            for (int i = 0; i < npts; ++i) {
+                int o = 0;
+                for (int d = 0; d < 3; ++d)
+                    if (pos[3 * (size_t)(start + i) + d] >= r[k].c[d]) o |= (1 << d);
+                oct[i] = o;
+                cnt[o]++;
+            }
+            int run[8];
+            run[0] = start;
+            for (int c = 1; c < 8; ++c) run[c] = run[c - 1] + cnt[c - 1];
+            std::vector<double> tp(pos.begin() + 3 * (size_t)start, pos.begin() + 3 * (size_t)(start + npts));
+            std::vector<int> tq(perm.begin() + start, perm.begin() + start + npts);
+            for (int i = 0; i < npts; ++i) {
+                const int g = run[oct[i]]++;
+                for (int d = 0; d < 3; ++d) pos[3 * (size_t)g + d] = tp[3 * (size_t)i + d];
+                perm[g] = tq[i];
+            }
+            out[k] = cnt;
+        }
+        return out;
+    }
+    void morton(int s, const std::vector<Leaf>& leaves) override {
+        std::vector<double>& pos = pos_[s];
+        std::vector<int>& perm = perm_[s];
+        for (const Leaf& L : leaves) {
+            const int start = L.start, count = L.count;
+            if (count < 2) continue;
+            std::vector<uint64_t> key(count);
+            std::vector<int> order(count);
+            for (int i = 0; i < count; ++i) {
+                uint64_t k = 0;
+                for (int d = 0; d < 3; ++d) {
+                    const double f = (pos[3 * (size_t)(start + i) + d] - (L.c[d] - L.h)) / (2.0 * L.h);
+                    const int qd = std::min(1023, std::max(0, (int)(f * 1024.0)));
+                    k |= spread3((uint32_t)qd) << d;
+                }
+                key[i] = k;
+                order[i] = i;
+            }
+            std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
+            std::vector<double> tp(pos.begin() + 3 * (size_t)start, pos.begin() + 3 * (size_t)(start + count));
+            std::vector<int> tq(perm.begin() + start, perm.begin() + start + count);
+            for (int i = 0; i < count; ++i) {
+                for (int d = 0; d < 3; ++d) pos[3 * (size_t)(start + i) + d] = tp[3 * (size_t)order[i] + d];
+                perm[start + i] = tq[order[i]];
+            }
+        }
+    }
+    int64_t outside(int s, const std::vector<Leaf>& leaves) override {
+        int64_t bad = 0;
+        for (const Leaf& L : leaves)
+            for (int i = L.start; i < L.start + L.count; ++i)
+                for (int d = 0; d < 3; ++d)
+                    if (std::abs(pos_[s][3 * (size_t)i + d] - L.c[d]) > L.h) {
+                        ++bad;
+                        break;
+                    }
+        return bad;
+    }
+    void fetch(int s, std::vector<double>& pos, std::vector<int>& perm) override {
+        pos = pos_[s];
+        perm = perm_[s];
+    }
+    int size(int s) const override { return (int)perm_[s].size(); }
+
+  private:
+    int n_ = 0;
+    std::vector<double> pos_[2];
+    std::vector<int> perm_[2];
+};
 
 inline int child_sign(int c, int d) { return ((c >> d) & 1) ? 1 : -1; }
 
@@ -149,8 +286,8 @@ struct Builder {
     std::vector<std::array<int, 27>> coll;
     std::vector<double> cen;  // 3 per box
     std::vector<int> sse, tse;  // [start, end] inclusive per box, end = start-1 if empty
-    std::vector<double> spos, tpos;  // sorted positions
-    std::vector<int> sperm, tperm;   // sorted -> input index
+    PointOps* ops = nullptr;    // where the points live
+    std::vector<int> pending;   // split boxes whose points are not yet partitioned
 
     int add_box(int d, int par) {
         const int id = (int)depth.size();
@@ -171,40 +308,8 @@ struct Builder {
     int scount(int b) const { return sse[2 * b + 1] - sse[2 * b] + 1; }
     int tcount(int b) const { return tse[2 * b + 1] - tse[2 * b] + 1; }
 
-    // Stable partition of a parent's sorted range into its children by the
-    // octant of each point relative to the parent centre (>= means upper half).
-    static void split_range(int par, const std::vector<double>& cen, const std::array<int, 8>& ch, int npts,
-                            int start, std::vector<double>& pos, std::vector<int>& perm, std::vector<int>& se) {
-        if (npts <= 0) return;
-        const double* pc = &cen[3 * par];
-        std::vector<int> oct(npts);
-        int cnt[8] = {};
-        for (int i = 0; i < npts; ++i) {
-            int o = 0;
-            for (int d = 0; d < 3; ++d)
-                if (pos[3 * (start + i) + d] >= pc[d]) o |= (1 << d);
-            oct[i] = o;
-            cnt[o]++;
-        }
-        int off[8];
-        off[0] = start;
-        for (int c = 1; c < 8; ++c) off[c] = off[c - 1] + cnt[c - 1];
-        for (int c = 0; c < 8; ++c) {
-            se[2 * ch[c]] = off[c];
-            se[2 * ch[c] + 1] = off[c] + cnt[c] - 1;
-        }
-        std::vector<double> tp(pos.begin() + 3 * start, pos.begin() + 3 * (start + npts));
-        std::vector<int> tq(perm.begin() + start, perm.begin() + start + npts);
-        int run[8];
-        std::memcpy(run, off, sizeof(off));
-        for (int i = 0; i < npts; ++i) {
-            const int g = run[oct[i]]++;
-            for (int d = 0; d < 3; ++d) pos[3 * g + d] = tp[3 * i + d];
-            perm[g] = tq[i];
-        }
-    }
-
-    // Create the 8 children of b (depth L -> L+1), distribute its points.
+    // Create the 8 children of b (depth L -> L+1); their points are
+    // distributed by the next flush.
     void split(int b, int L, double rc) {
         const double bsh = rc / (double)(1 << (L + 2));
         nchild[b] = 8;
@@ -213,9 +318,38 @@ struct Builder {
             children[b][c] = id;
             for (int d = 0; d < 3; ++d) cen[3 * id + d] = cen[3 * b + d] + child_sign(c, d) * bsh;
         }
-        const int ns = scount(b), nt = tcount(b);
-        if (ns > 0) split_range(b, cen, children[b], ns, sse[2 * b], spos, sperm, sse);
-        if (nt > 0) split_range(b, cen, children[b], nt, tse[2 * b], tpos, tperm, tse);
+        pending.push_back(b);
+    }
+
+    // Stable partition of every pending box's points into its children by the
+    // octant relative to the box centre (>= means upper half).  The ranges of
+    // different boxes are disjoint, so one batch gives the same result as
+    // partitioning each box as it splits.
+    void flush() {
+        if (pending.empty()) return;
+        for (int s = 0; s < 2; ++s) {
+            std::vector<int>& se = s == 0 ? sse : tse;
+            std::vector<PointOps::Range> r;
+            std::vector<int> who;
+            for (int b : pending) {
+                const int cnt = se[2 * b + 1] - se[2 * b] + 1;
+                if (cnt <= 0) continue;
+                r.push_back({se[2 * b], cnt, {cen[3 * b], cen[3 * b + 1], cen[3 * b + 2]}});
+                who.push_back(b);
+            }
+            if (r.empty()) continue;
+            const std::vector<std::array<int, 8>> counts = ops->partition(s, r);
+            for (size_t k = 0; k < who.size(); ++k) {
+                int off = r[k].start;
+                for (int c = 0; c < 8; ++c) {
+                    const int ch = children[who[k]][c];
+                    se[2 * ch] = off;
+                    se[2 * ch + 1] = off + counts[k][c] - 1;
+                    off += counts[k][c];
+                }
+            }
+        }
+        pending.clear();
     }
 
     // Colleague list of box nb (depth L+1) from the children of its parent's
@@ -256,7 +390,7 @@ struct Builder {
 }  // namespace
 
 Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int n_per_leaf, int nz,
-                const double* bloch) {
+                const double* bloch, PointOps* points) {
     if (n <= 0) throw std::invalid_argument("number of points must be positive");
     if (n_per_leaf <= 0) throw std::invalid_argument("n_per_leaf must be positive");
     if (nz <= 0) throw std::invalid_argument("nz must be positive (the automatic rc choice is not supported)");
@@ -291,13 +425,17 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
             P.r_user[3 * (size_t)i + j] = s;
         }
 
-    std::vector<double> img;
-    generate_images(P.umat, P.rc, P.mgrid, P.xgrid0, n, P.r_user.data(), img, P.img_src_idx);
+    HostPoints host_points;
+    PointOps& ops = points ? *points : host_points;
+    ops.load(n, P.r_user.data());
+    {
+        std::vector<std::array<double, 3>> shifts;
+        double lo_ext[3], hi_ext[3];
+        image_shifts(P.umat, P.rc, P.mgrid, P.xgrid0, shifts, lo_ext, hi_ext);
+        P.img_src_idx = ops.add_images(shifts, lo_ext, hi_ext);
+    }
     const int nsall = n + (int)P.img_src_idx.size();
     P.n_all = nsall;
-    std::vector<double> srcall(3 * (size_t)nsall);
-    std::copy(P.r_user.begin(), P.r_user.end(), srcall.begin());
-    std::copy(img.begin(), img.end(), srcall.begin() + 3 * (size_t)n);
 
     // ---- level-0 rectangular grid
     const double rc = P.rc;
@@ -331,33 +469,15 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
 
     // ---- stable counting sort into level-0 boxes (bin index truncation as
     // the reference: (int)((x - xelo) / rc) clamped to the grid)
-    auto bin_sort = [&](int np, const double* x, std::vector<double>& sorted, std::vector<int>& perm,
-                        std::vector<int>& se) {
-        const double rcinv = 1.0 / rc;
-        std::vector<int> boxof(np), cnt(nb0, 0);
-        for (int i = 0; i < np; ++i) {
-            int ii[3];
-            for (int k = 0; k < 3; ++k) {
-                ii[k] = (int)((x[3 * (size_t)i + k] - xelo[k]) * rcinv);
-                ii[k] = std::min(std::max(ii[k], 0), mle[k] - 1);
-            }
-            boxof[i] = ii[2] * mle[0] * mle[1] + ii[1] * mle[0] + ii[0];
-            cnt[boxof[i]]++;
-        }
-        std::vector<int> ip(nb0 + 1, 0);
+    B.ops = &ops;
+    for (int s = 0; s < 2; ++s) {
+        const std::vector<int> ip = ops.bin0(s, xelo, 1.0 / rc, mle);
+        std::vector<int>& se = s == 0 ? B.sse : B.tse;
         for (int b = 0; b < nb0; ++b) {
-            ip[b + 1] = ip[b] + cnt[b];
             se[2 * b] = ip[b];
             se[2 * b + 1] = ip[b + 1] - 1;
         }
-        perm.resize(np);
-        for (int i = 0; i < np; ++i) perm[ip[boxof[i]]++] = i;
-        sorted.resize(3 * (size_t)np);
-        for (int i = 0; i < np; ++i)
-            for (int d = 0; d < 3; ++d) sorted[3 * (size_t)i + d] = x[3 * (size_t)perm[i] + d];
-    };
-    bin_sort(nsall, srcall.data(), B.spos, B.sperm, B.sse);
-    bin_sort(n, P.r_user.data(), B.tpos, B.tperm, B.tse);
+    }
 
     // ---- top-down refinement
     double npl_alpha = 1.5;
@@ -374,6 +494,7 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
             any = true;
             B.split(b, level, rc);
         }
+        B.flush();
         if (!any) break;
         max_level = level + 1;
         const double child_bs = rc / (double)(1 << (level + 1));
@@ -388,6 +509,7 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
         while (changed && iter++ < 50) {
             changed = false;
             for (int L = 0; L <= max_level; ++L) {
+                B.flush();  // counts of the boxes split at the previous level
                 const double lvl_bs = rc / (double)(1 << L);
                 const double child_bs = rc / (double)(1 << (L + 1));
                 const double adj_tol = 1.05 * 0.5 * (lvl_bs + child_bs);
@@ -444,6 +566,8 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
         }
     }
 
+    B.flush();
+
     // ---- finalize topology
     const int nb = B.nbox();
     P.nboxes = nb;
@@ -483,63 +607,30 @@ Plan build_plan(const double* cell, int n, const double* pos, int n_digits, int 
         }
     // Every point must sit inside its leaf (the reference logs "misplaced
     // particles" otherwise, pbc_tree.cpp:699-732); treat it as a hard error.
-    for (int b = 0; b < nb; ++b) {
-        if (!P.is_leaf[b]) continue;
-        const double hb = P.boxsize[P.depth[b]] / 2.0 * 1.01;
-        for (int i = P.src_start[b]; i < P.src_start[b] + P.src_count[b]; ++i)
-            for (int d = 0; d < 3; ++d)
-                if (std::abs(B.spos[3 * (size_t)i + d] - P.centers[3 * b + d]) > hb)
-                    throw std::invalid_argument("point outside the cell's covering grid (positions must lie in the cell)");
-    }
-    // Inside each leaf, order the points along a Morton curve of the leaf box:
-    // consecutive points (one GPU warp's targets, one chunk of sources) then
-    // cover a compact sub-box, so the cutoff tests of the near field agree
-    // across a warp.  Sums over a leaf do not depend on the order.
+    // Inside each leaf, the points are then ordered along a Morton curve of
+    // the leaf box: consecutive points (one GPU warp's targets, one chunk of
+    // sources) then cover a compact sub-box, so the cutoff tests of the near
+    // field agree across a warp.  Sums over a leaf do not depend on the order.
     {
-        auto spread3 = [](uint32_t v) {  // 10 bits -> every third bit of 30
-            uint64_t x = v & 0x3FF;
-            x = (x | (x << 16)) & 0x030000FF;
-            x = (x | (x << 8)) & 0x0300F00F;
-            x = (x | (x << 4)) & 0x030C30C3;
-            x = (x | (x << 2)) & 0x09249249;
-            return x;
-        };
-        auto morton_sort = [&](int b, int start, int count, std::vector<double>& pos, std::vector<int>& perm) {
-            if (count < 2) return;
-            const double h = P.boxsize[P.depth[b]] / 2.0;
-            std::vector<uint64_t> key(count);
-            std::vector<int> order(count);
-            for (int i = 0; i < count; ++i) {
-                uint64_t k = 0;
-                for (int d = 0; d < 3; ++d) {
-                    const double f = (pos[3 * (size_t)(start + i) + d] - (P.centers[3 * b + d] - h)) / (2.0 * h);
-                    const int qd = std::min(1023, std::max(0, (int)(f * 1024.0)));
-                    k |= spread3((uint32_t)qd) << d;
-                }
-                key[i] = k;
-                order[i] = i;
-            }
-            std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
-            std::vector<double> tp(pos.begin() + 3 * (size_t)start, pos.begin() + 3 * (size_t)(start + count));
-            std::vector<int> tq(perm.begin() + start, perm.begin() + start + count);
-            for (int i = 0; i < count; ++i) {
-                for (int d = 0; d < 3; ++d) pos[3 * (size_t)(start + i) + d] = tp[3 * (size_t)order[i] + d];
-                perm[start + i] = tq[order[i]];
-            }
-        };
+        std::vector<PointOps::Leaf> inside, ls, lt;
         for (int b = 0; b < nb; ++b) {
             if (!P.is_leaf[b]) continue;
-            if (P.src_count[b] > 1) morton_sort(b, P.src_start[b], P.src_count[b], B.spos, B.sperm);
-            if (P.trg_count[b] > 1) morton_sort(b, P.trg_start[b], P.trg_count[b], B.tpos, B.tperm);
+            const double* c = &P.centers[3 * b];
+            const double h = P.boxsize[P.depth[b]] / 2.0;
+            inside.push_back({P.src_start[b], P.src_count[b], {c[0], c[1], c[2]}, h * 1.01});
+            if (P.src_count[b] > 1) ls.push_back({P.src_start[b], P.src_count[b], {c[0], c[1], c[2]}, h});
+            if (P.trg_count[b] > 1) lt.push_back({P.trg_start[b], P.trg_count[b], {c[0], c[1], c[2]}, h});
         }
+        if (ops.outside(0, inside) > 0)
+            throw std::invalid_argument("point outside the cell's covering grid (positions must lie in the cell)");
+        ops.morton(0, ls);
+        ops.morton(1, lt);
     }
-    P.src_sorted = std::move(B.spos);
-    P.trg_sorted = std::move(B.tpos);
-    P.trg_perm = std::move(B.tperm);
+    ops.fetch(0, P.src_sorted, P.src_perm);
+    ops.fetch(1, P.trg_sorted, P.trg_perm);
     P.src_charge_idx.resize(nsall);
-    P.src_perm = B.sperm;
     for (int i = 0; i < nsall; ++i) {
-        const int j = B.sperm[i];
+        const int j = P.src_perm[i];
         P.src_charge_idx[i] = j < n ? j : P.img_src_idx[j - n];
     }
 

@@ -111,3 +111,13 @@ def test_batch_create_rejects_bad_input_without_compute():
     h = lib.pdmk_batch_create(0, None, None, None, 6, 300, 4)
     assert not h
     assert lib.pdmk_batch_evaluate(None, None, None) == -1
+
+
+def test_plan_digest_host_construction():
+    # the host form of the tree construction (no GPU needed): deterministic,
+    # and sensitive to the build parameters
+    cell, pos, _ = uniform_system(3000, 7, TRICLINIC)
+    d1, _ = pd.plan_digest(cell, pos, 6, 50, 4)
+    d2, _ = pd.plan_digest(cell, pos, 6, 50, 4)
+    d3, _ = pd.plan_digest(cell, pos, 6, 10, 4)
+    assert d1 == d2 and d1 != d3 and len(d1) == 64
