@@ -822,7 +822,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         const double a11 = 1.0 / u[0], a21 = -u[3] / (u[0] * u[4]), a22 = 1.0 / u[4];
         const double a31 = (u[3] * u[7] - u[6] * u[4]) / (u[0] * u[4] * u[8]);
         const double a32 = -u[7] / (u[4] * u[8]), a33 = 1.0 / u[8];
-        Pswf0 pf(P.dp.beta);
+        const Pswf0& pf = Pswf0::get(P.dp.beta);
         const double psi0 = pf(0.0), twopi = 2.0 * M_PI;
         const double dfac = 4.0 * M_PI / (psi0 * P.volume);
         auto inK = [&](int k1, int k2, int k3) {

@@ -2,6 +2,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 
 namespace pdmkb {
@@ -19,7 +22,9 @@ static void legendre_pd(int n, double x, double& p, double& dp) {
     dp = n * (x * p1 - p0) / (x * x - 1.0);
 }
 
-void gauss_legendre(int n, double* x, double* w) {
+namespace {
+
+void gauss_legendre_compute(int n, double* x, double* w) {
     // Newton iteration from the Tricomi initial guess; symmetric fill.
     const int m = (n + 1) / 2;
     for (int i = 0; i < m; ++i) {
@@ -39,6 +44,22 @@ void gauss_legendre(int n, double* x, double* w) {
         w[i] = wt;
     }
     if (n % 2 == 1) x[m - 1] = 0.0;
+}
+
+}  // namespace
+
+void gauss_legendre(int n, double* x, double* w) {
+    static std::mutex mu;
+    static std::map<int, std::pair<std::vector<double>, std::vector<double>>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto& e = cache[n];
+    if (e.first.empty() && n > 0) {
+        e.first.resize(n);
+        e.second.resize(n);
+        gauss_legendre_compute(n, e.first.data(), e.second.data());
+    }
+    std::copy(e.first.begin(), e.first.end(), x);
+    std::copy(e.second.begin(), e.second.end(), w);
 }
 
 // Cyclic Jacobi eigen-decomposition of a dense symmetric matrix (row-major).
@@ -120,6 +141,33 @@ Pswf0::Pswf0(double c) : c_(c) {
     int last = (int)leg_.size() - 1;
     while (last > 0 && std::fabs(leg_[last]) < 1e-18 * std::fabs(leg_[0])) --last;
     leg_.resize(last + 1);
+    // moments on [0,1] with a 200-point rule, as prolate_intvals
+    // (cpp/src/dmk/prolate.cpp:483-511)
+    const int nq = 200;
+    std::vector<double> x(nq), w(nq);
+    gauss_legendre(nq, x.data(), w.data());
+    double s0 = 0, s1 = 0, s2 = 0, s4 = 0;
+    for (int i = 0; i < nq; ++i) {
+        const double t = 0.5 * (x[i] + 1.0), wt = 0.5 * w[i];
+        const double f = (*this)(t);
+        s0 += wt * f;
+        s1 += wt * f * t;
+        s2 += wt * f * t * t;
+        s4 += wt * f * t * t * t * t;
+    }
+    mom_[0] = s0;
+    mom_[1] = s1;
+    mom_[2] = s2 / s0;
+    mom_[3] = s4;
+}
+
+const Pswf0& Pswf0::get(double c) {
+    static std::mutex mu;
+    static std::map<double, std::unique_ptr<Pswf0>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto& p = cache[c];
+    if (!p) p = std::make_unique<Pswf0>(c);
+    return *p;
 }
 
 double Pswf0::operator()(double x) const {
@@ -137,19 +185,10 @@ double Pswf0::operator()(double x) const {
 }
 
 void Pswf0::moments(double& c0, double& c1, double& c2, double& c4) const {
-    const int n = 200;
-    std::vector<double> x(n), w(n);
-    gauss_legendre(n, x.data(), w.data());
-    c0 = c1 = c2 = c4 = 0.0;
-    for (int i = 0; i < n; ++i) {
-        const double t = 0.5 * (x[i] + 1.0), wt = 0.5 * w[i];
-        const double f = (*this)(t);
-        c0 += wt * f;
-        c1 += wt * f * t;
-        c2 += wt * f * t * t;
-        c4 += wt * f * t * t * t * t;
-    }
-    c2 /= c0;
+    c0 = mom_[0];
+    c1 = mom_[1];
+    c2 = mom_[2];
+    c4 = mom_[3];
 }
 
 }  // namespace pdmkb

@@ -13,13 +13,17 @@
 
 namespace pdmkb {
 
-// n-point Gauss-Legendre nodes (ascending) and weights on [-1, 1].
+// n-point Gauss-Legendre nodes (ascending) and weights on [-1, 1] (computed
+// once per n and process; thread-safe).
 void gauss_legendre(int n, double* x, double* w);
 
 class Pswf0 {
   public:
     Pswf0() = default;
     explicit Pswf0(double c);
+    // The function for c, built once per c and process (thread-safe; every
+    // tree of a digit count shares it).
+    static const Pswf0& get(double c);
     // psi_0^c(x) for |x| <= 1 (0 outside: the DMK tables never evaluate there).
     double operator()(double x) const;
     double c() const { return c_; }
@@ -31,6 +35,7 @@ class Pswf0 {
   private:
     double c_ = 0;
     std::vector<double> leg_;  // Legendre coefficients of P_k, k = 0..K
+    double mom_[4] = {0, 0, 0, 0};  // c0, c1, c2, c4 (computed by the constructor)
 };
 
 }  // namespace pdmkb

@@ -50,7 +50,7 @@ std::vector<double> cheb_vinv(int p) {
 void build_tables(Plan& P) {
     const int p = P.p, n = P.n_pw, n2 = P.n_pw2, M = P.n_modes;
     const double beta = P.dp.beta;
-    Pswf0 pf(beta);
+    const Pswf0& pf = Pswf0::get(beta);
     double c0, c1, c2, c4;
     pf.moments(c0, c1, c2, c4);
     const double psi0 = pf(0.0);
