@@ -104,6 +104,7 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         PDMK_CUDA_CHECK(cudaMallocHost(&err_host_, sizeof(int) * nsys));
         graphs_.assign(nsys, nullptr);
         if (single_) {
+            for (auto& t : trees_) t->defer_near_ = true;
             // queue items: every system's near-field leaves, largest work first
             std::vector<std::tuple<int64_t, int, int>> items;
             for (int i = 0; i < nsys; ++i) {
@@ -181,7 +182,7 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
         PDMK_CUDA_CHECK(cudaStreamWaitEvent(ts, ready_, 0));
         auto enqueue = [&]() {
             if (single_)
-                t.enqueue_deferred(q_dev_ + off_[i]);
+                t.enqueue_multi_device(q_dev_ + off_[i], 1, pot_dev_ + off_[i], /*fp32=*/true);
             else
                 t.evaluate_device(q_dev_ + off_[i], pot_dev_ + off_[i], nullptr);
         };

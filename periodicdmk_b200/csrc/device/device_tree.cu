@@ -63,9 +63,6 @@ T* DeviceTree::alloc(size_t n) {
     bytes_ += bytes;
     return static_cast<T*>(p);
 }
-// element types the members defined in multi.cu allocate
-template float* DeviceTree::alloc<float>(size_t);
-template float4* DeviceTree::alloc<float4>(size_t);
 
 template <typename T>
 T* DeviceTree::upload(const std::vector<T>& v) {

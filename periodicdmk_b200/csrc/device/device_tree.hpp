@@ -130,15 +130,13 @@ class DeviceTree {
 
   public:
     bool last_was_multi_ = false;
-    // One charge vector of a system in a batch (batch.cpp): the tree part and
-    // the far field on the single-RHS FP64 kernels (at one RHS they are faster
-    // than the multi-RHS kernels) and the float source charges of the near
-    // field, enqueued on stream(); the near field and the final gather are
-    // left to the batch's queue kernel (batch_near.cu), which reads this
-    // tree's buffers through near_leaf_sys.  Defined in multi.cu.
-    void enqueue_deferred(const double* q_user_d);
-    // Descriptor of this tree's buffers for the batch near-field kernel (after
-    // the first enqueue_deferred); out = this system's potentials in user order.
+    // Set by a batch of systems: single-RHS float evaluates leave out the near
+    // field and the final gather, which the batch's queue kernel does for all
+    // systems in one launch (batch_near.cu).
+    bool defer_near_ = false;
+    // Descriptor of this tree's buffers for the batch near-field kernel (the
+    // single-RHS float state must exist: one deferred evaluate has run);
+    // out = this system's potentials in user order.
     void near_leaf_sys(dev::NearLeafSys& d, double* out) const;
     // Near-field leaves (target leaves) and their estimated work (targets x
     // sources over the leaf's near pairs), host copies.
@@ -296,9 +294,6 @@ class DeviceTree {
     dev::cd* spec_save_ = nullptr;  // far-field spectrum after the multiplier
     dev::cd* spec_tmp_ = nullptr;   // i K_d times it
     dev::GradFrame frame_{};
-    // float split positions and source charges of enqueue_deferred
-    float4 *def_src_hi_ = nullptr, *def_src_lo_ = nullptr, *def_trg_hi_ = nullptr, *def_trg_lo_ = nullptr;
-    float* def_src_q_ = nullptr;
     // quasi-periodic state (qp.cu)
     bool qp_ = false;
     bool qp_run_ = false;               // run_multi_block<double> computes the two QP columns

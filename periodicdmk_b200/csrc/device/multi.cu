@@ -1247,8 +1247,9 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         }
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
-    // near field
-    if (near_.n_leaves > 0) {
+    // near field (left to the batch's queue kernel when deferred)
+    const bool deferred = f32 && defer_near_ && kb == 1;
+    if (near_.n_leaves > 0 && !deferred) {
         dev::NearM a{};
         a.trg_start = near_.trg_start; a.trg_count = near_.trg_count; a.pair_start = near_.pair_start;
         a.pair_src_start = near_.pair_src_start; a.pair_src_count = near_.pair_src_count;
@@ -1336,7 +1337,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
     if (qp) {
         dev::launch_qp_finalize(m.pot, m.far, trg_, trg_perm_, Q, qp_trg_phase_, pot_user, n_, s); ++nl;
-    } else {
+    } else if (!deferred) {
         const int64_t tot = (int64_t)n_ * kvalid;
         dev::k_finalize_m<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m.pot, m.far, trg_, trg_perm_, m.q_t, pot_user,
                                                                         n_, kvalid); ++nl;
@@ -1346,59 +1347,25 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     multi_launches_ += nl;
 }
 
-void DeviceTree::enqueue_deferred(const double* q) {
-    require_periodic("evaluate");
-    PDMK_CUDA_CHECK(cudaSetDevice(device_));
-    ensure_fp64_working_set();
-    cudaStream_t s = stream_;
-    if (!def_src_q_) {
-        def_src_hi_ = alloc<float4>(n_all_);
-        def_src_lo_ = alloc<float4>(n_all_);
-        def_trg_hi_ = alloc<float4>(n_);
-        def_trg_lo_ = alloc<float4>(n_);
-        def_src_q_ = alloc<float>(n_all_);
-        dev::k_split_positions<<<(n_all_ + 255) / 256, 256, 0, s>>>(src_, def_src_hi_, def_src_lo_, n_all_);
-        dev::k_split_positions<<<(n_ + 255) / 256, 256, 0, s>>>(trg_, def_trg_hi_, def_trg_lo_, n_);
-    }
-    int nl = 0;
-    PDMK_CUDA_CHECK(cudaMemsetAsync(pot_sorted_, 0, sizeof(double) * n_, s));
-    nl += run_fp64_tree(q, f64_scratch_, f64_scratch_elems_, s);
-    // float charges per sorted source (one RHS: the user-order vector is its own row-major form)
-    dev::k_gather_src_rows<float><<<(unsigned)((n_all_ + 255) / 256), 256, 0, s>>>(def_src_q_, src_charge_idx_, q,
-                                                                                  n_all_, 1); ++nl;
-    // far field (FP64)
-    dev::launch_nufft_gather_q(trg_perm_, q, q_sorted_, n_, s); ++nl;
-    PDMK_CUDA_CHECK(cudaMemsetAsync(grid_, 0, sizeof(double) * n_grid_, s));
-    dev::launch_spread(nufft_, nufft_max_jk_, nufft_max_ex_, s); ++nl;
-    if (cufftExecD2Z(plan_fwd_, grid_, reinterpret_cast<cufftDoubleComplex*>(spec_)) != CUFFT_SUCCESS)
-        throw std::runtime_error("cuFFT error in the forward far-field transform");
-    dev::launch_multiply(spec_, mult_, n_spec_, s); ++nl;
-    if (cufftExecZ2D(plan_inv_, reinterpret_cast<cufftDoubleComplex*>(spec_), grid_) != CUFFT_SUCCESS)
-        throw std::runtime_error("cuFFT error in the inverse far-field transform");
-    dev::launch_interp(nufft_, s); ++nl;
-    PDMK_CUDA_CHECK(cudaGetLastError());
-    multi_launches_ = nl;
-    last_was_multi_ = false;
-}
-
 void DeviceTree::near_leaf_sys(dev::NearLeafSys& d, double* out) const {
-    if (!def_src_q_) throw std::logic_error("near_leaf_sys: no deferred evaluate has run");
+    const MultiState* m = multi_[1].get();
+    if (!m || m->kb != 1) throw std::logic_error("near_leaf_sys: no single-RHS float state");
     d.trg_start = near_.trg_start;
     d.trg_count = near_.trg_count;
     d.pair_start = near_.pair_start;
     d.pair_src_start = near_.pair_src_start;
     d.pair_src_count = near_.pair_src_count;
     d.pair_bsize = near_.pair_bsize;
-    d.trg_hi = def_trg_hi_;
-    d.trg_lo = def_trg_lo_;
-    d.src_hi = def_src_hi_;
-    d.src_lo = def_src_lo_;
-    d.src_q = def_src_q_;
-    d.pot = pot_sorted_;
-    d.far = far_sorted_;
+    d.trg_hi = m->trg_hi;
+    d.trg_lo = m->trg_lo;
+    d.src_hi = m->src_hi;
+    d.src_lo = m->src_lo;
+    d.src_q = static_cast<const float*>(m->src_q);
+    d.pot = m->pot;
+    d.far = m->far;
     d.trg = trg_;
     d.perm = trg_perm_;
-    d.q_t = q_sorted_;
+    d.q_t = m->q_t;
     d.out = out;
 }
 
