@@ -150,3 +150,29 @@ def test_qp_errors():
     assert lib.pdmk_evaluate_complex_double(None, 0, None, None, None) == -1
     with pytest.raises(RuntimeError):
         pd.PeriodicDMKTree(cell, pos, 6, 30, 4, bloch=[np.nan, 0.0, 0.0]).evaluate_complex(q)
+
+
+def _lattice_q(cell):
+    """Rotation of the lattice-QR frame (columns: the lattice vectors sorted by
+    decreasing length, orthonormalised in that order)."""
+    cell = np.asarray(cell, dtype=np.float64)
+    order = sorted(range(3), key=lambda j: -np.linalg.norm(cell[:, j]))
+    q, r = np.linalg.qr(cell[:, order])
+    return q * np.sign(np.diag(r))
+
+
+def test_qp_rotated_frame():
+    # a cell whose longest lattice vector is not the first: the tree works in a
+    # rotated frame, the Bloch vector is given in it (as the reference takes
+    # it), and bloch_cartesian = Q bloch
+    cell = np.array([[0.8, 0.1, 0.0], [0.0, 1.3, 0.2], [0.0, 0.0, 1.0]])
+    _, pos, q = uniform_system(2000, 87, cell)
+    Q = _lattice_q(cell)
+    assert np.abs(Q - np.eye(3)).max() > 0.1
+    t = pd.PeriodicDMKTree(cell, pos, 6, 25, 4, bloch=BLOCH)
+    u = t.evaluate_complex(q)
+    t.close()
+    ref = oracle.ewald_targets_qp(cell, pos, q, np.arange(len(q)), Q @ BLOCH, s=6.5)
+    e = crel(u, ref)
+    print("PARITY " + json.dumps({"case": "quasi-periodic rotated frame 6 digits", "rel_l2_vs_ewald": e}))
+    assert e < 2e-6

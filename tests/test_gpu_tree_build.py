@@ -66,3 +66,18 @@ def test_device_build_rejects_points_outside():
     for dev in (False, True):
         with pytest.raises(RuntimeError, match="outside"):
             pd.plan_digest(cell, pos, 6, 300, 4, on_device=dev)
+
+
+def test_points_on_cell_faces():
+    # fractional coordinates exactly 0 and just below 1 on every axis: images
+    # and bins at the grid edges agree between the two constructions
+    rng = np.random.default_rng(110)
+    frac = rng.uniform(0, 1, (40000, 3))
+    frac[:5000, 0] = 0.0
+    frac[5000:10000, 1] = np.nextafter(1.0, 0.0)
+    frac[10000:12000, :2] = 0.0  # on an edge of the cell
+    cell = TRICLINIC
+    pos = frac @ cell.T
+    dh, _ = pd.plan_digest(cell, pos, 6, 60, 4, on_device=False)
+    dd, _ = pd.plan_digest(cell, pos, 6, 60, 4, on_device=True)
+    assert dd == dh
