@@ -29,11 +29,21 @@ namespace dev {
 
 namespace {
 
+// squared gap between a chunk's box and a target box (0 when they overlap)
+__device__ __forceinline__ float box_gap2(const float4& lo, const float4& hi, const float* b) {
+    const float gx = fmaxf(0.0f, fmaxf(lo.x - b[3], b[0] - hi.x));
+    const float gy = fmaxf(0.0f, fmaxf(lo.y - b[4], b[1] - hi.y));
+    const float gz = fmaxf(0.0f, fmaxf(lo.z - b[5], b[2] - hi.z));
+    return fmaf(gx, gx, fmaf(gy, gy, gz * gz));
+}
+
 template <int NC, int TPT>
 __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
     __shared__ float4 sh[128], sl[128];
     __shared__ float sq[128];
     __shared__ int s_item;
+    __shared__ float s_wbox[4][6];  // per warp: bounding box of its targets of the pass
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
         __syncthreads();  // the previous item's shared-memory reads are done
         if (threadIdx.x == 0) s_item = atomicAdd(a.head, 1);
@@ -48,46 +58,92 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
         for (int base = 0; base < nt; base += TPT * 128) {
             float4 th[TPT], tl[TPT];
             double acc[TPT];
+            float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
 #pragma unroll
             for (int u = 0; u < TPT; ++u) {
                 const int t = base + threadIdx.x + u * 128;
                 th[u] = t < nt ? S.trg_hi[t0 + t] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
                 tl[u] = t < nt ? S.trg_lo[t0 + t] : make_float4(0.f, 0.f, 0.f, 0.f);
                 acc[u] = 0.0;
+                if (t < nt) {
+                    lo[0] = fminf(lo[0], th[u].x); hi[0] = fmaxf(hi[0], th[u].x);
+                    lo[1] = fminf(lo[1], th[u].y); hi[1] = fmaxf(hi[1], th[u].y);
+                    lo[2] = fminf(lo[2], th[u].z); hi[2] = fmaxf(hi[2], th[u].z);
+                }
+            }
+            // target boxes of the warps and of the pass, widened by the FP32
+            // rounding of the hi-part coordinates (relative 2^-23)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                    hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                }
+            if (lane == 0)
+                for (int d = 0; d < 3; ++d) {
+                    const float pad = 2.5e-7f * fmaxf(fabsf(lo[d]), fabsf(hi[d])) + 1e-30f;
+                    s_wbox[warp][d] = lo[d] - pad;
+                    s_wbox[warp][3 + d] = hi[d] + pad;
+                }
+            __syncthreads();
+            float wbox[6], cbox[6];
+            for (int d = 0; d < 6; ++d) wbox[d] = s_wbox[warp][d];
+            for (int d = 0; d < 3; ++d) {
+                cbox[d] = fminf(fminf(s_wbox[0][d], s_wbox[1][d]), fminf(s_wbox[2][d], s_wbox[3][d]));
+                cbox[3 + d] = fmaxf(fmaxf(s_wbox[0][3 + d], s_wbox[1][3 + d]), fmaxf(s_wbox[2][3 + d], s_wbox[3][3 + d]));
             }
             for (int pr = p0; pr < p1; ++pr) {
                 const int s0 = S.pair_src_start[pr], ns = S.pair_src_count[pr];
                 const double bd = S.pair_bsize[pr];
                 const float d2max = (float)(bd * bd), rsc = (float)(2.0 / bd), cen = (float)(-0.5 * bd);
+                const float keep2 = d2max * 1.00001f;
+                const int cb = S.pair_chunk_base[pr];
                 float part[TPT];
 #pragma unroll
                 for (int u = 0; u < TPT; ++u) part[u] = 0.f;
                 for (int sb = 0; sb < ns; sb += 128) {
+                    // 32-source chunks of this block that come within b of the pass's
+                    // targets (the same answer in every thread: the skip is uniform)
+                    const int nchk = min(4, (ns - sb + 31) / 32);
+                    unsigned need = 0;
+                    for (int k = 0; k < nchk; ++k) {
+                        const int c = cb + (sb >> 5) + k;
+                        if (box_gap2(__ldg(S.chunk_lo + c), __ldg(S.chunk_hi + c), cbox) <= keep2) need |= 1u << k;
+                    }
+                    if (!need) continue;
                     __syncthreads();
                     const int js = sb + threadIdx.x;
-                    if (js < ns) {
+                    if (js < ns && ((need >> (threadIdx.x >> 5)) & 1u)) {
                         sh[threadIdx.x] = S.src_hi[s0 + js];
                         sl[threadIdx.x] = S.src_lo[s0 + js];
                         sq[threadIdx.x] = S.src_q[s0 + js];
                     }
                     __syncthreads();
                     const int m = min(128, ns - sb);
-                    for (int j = 0; j < m; ++j) {
-                        const float4 yh = sh[j], yl = sl[j];
-                        const float qj = sq[j];
+                    for (int k = 0; k < nchk; ++k) {
+                        if (!((need >> k) & 1u)) continue;
+                        const int c = cb + (sb >> 5) + k;
+                        // this warp's targets against the chunk (warp-uniform)
+                        if (box_gap2(__ldg(S.chunk_lo + c), __ldg(S.chunk_hi + c), wbox) > keep2) continue;
+                        const int je = min(m, 32 * k + 32);
+                        for (int j = 32 * k; j < je; ++j) {
+                            const float4 yh = sh[j], yl = sl[j];
+                            const float qj = sq[j];
 #pragma unroll
-                        for (int u = 0; u < TPT; ++u) {
-                            const float dx = (th[u].x - yh.x) + (tl[u].x - yl.x);
-                            const float dy = (th[u].y - yh.y) + (tl[u].y - yl.y);
-                            const float dz = (th[u].z - yh.z) + (tl[u].z - yl.z);
-                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                            if (r2 > 1e-30f && r2 < d2max) {
-                                const float rinv = rsqrtf(r2);
-                                const float x = fmaf(r2, rinv, cen) * rsc;
-                                float pv = a.coef32[NC - 1];
+                            for (int u = 0; u < TPT; ++u) {
+                                const float dx = (th[u].x - yh.x) + (tl[u].x - yl.x);
+                                const float dy = (th[u].y - yh.y) + (tl[u].y - yl.y);
+                                const float dz = (th[u].z - yh.z) + (tl[u].z - yl.z);
+                                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                                if (r2 > 1e-30f && r2 < d2max) {
+                                    const float rinv = rsqrtf(r2);
+                                    const float x = fmaf(r2, rinv, cen) * rsc;
+                                    float pv = a.coef32[NC - 1];
 #pragma unroll
-                                for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, a.coef32[i]);
-                                part[u] = fmaf(pv * rinv, qj, part[u]);
+                                    for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, a.coef32[i]);
+                                    part[u] = fmaf(pv * rinv, qj, part[u]);
+                                }
                             }
                         }
                     }
@@ -104,6 +160,7 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
                     S.out[S.perm[i]] = S.pot[i] + acc[u] + S.far[i] - S.trg[i].w * S.q_t[i];
                 }
             }
+            __syncthreads();  // s_wbox is rewritten by the next pass
         }
     }
 }

@@ -16,6 +16,9 @@ struct NearLeafSys {
     const int* pair_src_start;  // per near pair: sorted source range
     const int* pair_src_count;
     const double* pair_bsize;   // per near pair: cutoff b
+    const int* pair_chunk_base; // per near pair: index of the first 32-source chunk box of its source box
+    const float4* chunk_lo;     // per 32-source chunk: bounding box (rounded outwards)
+    const float4* chunk_hi;
     const float4* trg_hi;       // double-float split positions (tree order)
     const float4* trg_lo;
     const float4* src_hi;

@@ -1356,6 +1356,9 @@ void DeviceTree::near_leaf_sys(dev::NearLeafSys& d, double* out) const {
     d.pair_src_start = near_.pair_src_start;
     d.pair_src_count = near_.pair_src_count;
     d.pair_bsize = near_.pair_bsize;
+    d.pair_chunk_base = near_.pair_chunk_base;
+    d.chunk_lo = near_.chunk_lo;
+    d.chunk_hi = near_.chunk_hi;
     d.trg_hi = m->trg_hi;
     d.trg_lo = m->trg_lo;
     d.src_hi = m->src_hi;
