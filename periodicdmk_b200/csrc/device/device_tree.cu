@@ -11,7 +11,9 @@
 //   far field    real fine grid n1*n2*n3, half spectrum n1*n2*(n3/2+1), multiplier
 // Every index list is built and bounds-checked here, on the host.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
@@ -81,6 +83,19 @@ DeviceTree::DeviceTree(const Plan& P, int device, bool fp64_working_set) {
 }
 
 void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
+    // PDMK_BUILD_PROFILE=1: host milliseconds of every phase below, on stderr
+    const bool prof = std::getenv("PDMK_BUILD_PROFILE") != nullptr;
+    auto t_prev = std::chrono::steady_clock::now();
+    const char* cur = "setup";
+    auto phase = [&](const char* next) {  // closes the current phase, opens the next
+        if (prof) {
+            const auto t = std::chrono::steady_clock::now();
+            std::fprintf(stderr, "device tree %-24s %9.2f ms\n", cur,
+                         std::chrono::duration<double, std::milli>(t - t_prev).count());
+            t_prev = t;
+        }
+        cur = next;
+    };
     if (device < 0) PDMK_CUDA_CHECK(cudaGetDevice(&device));
     device_ = device;
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
@@ -99,6 +114,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     const int p = p_, n = npw_, n2 = npw2_, M = M_;
     const int64_t ncoef = (int64_t)p * p * p;
 
+    phase("far-field bins");
     // ------------------------------------------------------------------ far-field bins
     // NUFFT bins are contiguous ranges of sorted targets inside one leaf.  A leaf
     // whose subgrid would be wider than kMaxEx cells is split by grid blocks,
@@ -199,6 +215,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         }
     }
 
+    phase("points");
     // ------------------------------------------------------------------ points
     {
         std::vector<double4> src(n_all_);
@@ -222,6 +239,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         pot_dev_ = alloc<double>(n_);
     }
 
+    phase("expansions");
     // ------------------------------------------------------------------ expansions
     // Storage only for expansions that some evaluation reads.  The plan (like
     // the reference, cpp/src/dmk/pbc_tree.cpp:983-994 and its outgoing pass)
@@ -344,6 +362,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         }
     }
 
+    phase("tables");
     // ------------------------------------------------------------------ tables
     {
         std::vector<double> c2p((size_t)8 * 3 * p * p);
@@ -378,6 +397,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         }
     }
 
+    phase("upward: proxy moment");
     // ------------------------------------------------------------------ upward: proxy moments
     {
         std::vector<std::vector<int>> by_center(P.nboxes);
@@ -409,6 +429,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         c2x_.src_count = upload(sc);
         launches_ += 1;
     }
+    phase("upward: c2p groups");
     // ------------------------------------------------------------------ upward: c2p groups
     for (int l = P.nlevels - 1; l >= 0; --l) {
         for (int c = 0; c < 8; ++c) {
@@ -430,6 +451,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
             c2p_groups_.push_back(g);
         }
     }
+    phase("outgoing plane waves");
     // ------------------------------------------------------------------ outgoing plane waves
     for (int l = 0; l < P.nlevels; ++l) {
         std::vector<int64_t> in, out;
@@ -447,6 +469,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         g.out_off = upload(out);
         pw_groups_.push_back(g);
     }
+    phase("downward per level");
     // ------------------------------------------------------------------ downward per level
     for (int l = 0; l < P.nlevels; ++l) {
         const double bs = P.boxsize[l];
@@ -501,6 +524,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         }
         eval_levels_.push_back(E);
     }
+    phase("leaf evaluation");
     // ------------------------------------------------------------------ leaf evaluation
     {
         std::vector<int> slot, t0, tc;
@@ -522,6 +546,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         eval_.trg_count = upload(tc);
         eval_.center_scale = upload(cs);
     }
+    phase("FP64 single-RHS pass");
     // ------------------------------------------------------------------ FP64 single-RHS pass by level
     // Same boxes and translations as the lists above, renumbered so that each
     // level's plane waves and downward coefficients live in level-sized
@@ -630,6 +655,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         for (const auto& F : f64_levels_) leaves += F.eval.n_leaves;
         check(leaves == eval_.n_leaves, "leaf evaluation lists by level");
     }
+    phase("near field");
     // ------------------------------------------------------------------ near field
     {
         // Contact-geometry cull of the reference (cpp/include/dmk/tree.hpp:111-220,
@@ -762,6 +788,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         launches_ += 1;
     }
 
+    phase("FP64 transform scrat");
     // ------------------------------------------------------------------ FP64 transform scratch
     // Enough for the largest level in one chunk, capped at PDMK_FP64_SCRATCH_MB
     // (default 1024 MiB); larger levels run in chunks of boxes.
@@ -793,6 +820,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         noalloc_reserve(device_);  // double trees may use the no-allocation evaluate
     }
 
+    phase("far field");
     // ------------------------------------------------------------------ far field
     {
         n_grid_ = (int64_t)ng[0] * ng[1] * ng[2];
@@ -1012,6 +1040,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     }
     launches_ += 2;  // charge gather, final gather
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    phase("");
 }
 
 DeviceTree::~DeviceTree() { release(); }
