@@ -1276,9 +1276,6 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                 // segment length between FP64 drains (tuning: PDMK_NEAR_SEG)
                 t.seg_chunks = 0;
                 if (const char* sg = std::getenv("PDMK_NEAR_SEG")) t.seg_chunks = std::atoi(sg);
-                // residual polynomial by Estrin's scheme (tuning: PDMK_NEAR_ESTRIN)
-                t.estrin = 0;
-                if (const char* es = std::getenv("PDMK_NEAR_ESTRIN")) t.estrin = std::atoi(es) ? 1 : 0;
                 t.withhold_chunk = -1;
                 t.wait_cycles = 4000000000LL;
                 if (const char* w = std::getenv("PDMK_TEST_WITHHOLD_NEAR_CHUNK")) {

@@ -426,28 +426,7 @@ struct NearPair {
     float d2max, rsc, cen;
 };
 
-// sum_i c_i x^i by Estrin's scheme: pairs c_2i + c_2i+1 x, then pairs of
-// those with x^2, x^4, ... (dependency depth about log2(NC) multiply-adds
-// instead of Horner's NC - 1)
 template <int NC>
-__device__ __forceinline__ float poly_estrin(const float (&c)[NC], float x) {
-    constexpr int H = (NC + 1) / 2;
-    float a[H];
-#pragma unroll
-    for (int i = 0; i < NC / 2; ++i) a[i] = fmaf(c[2 * i + 1], x, c[2 * i]);
-    if constexpr (NC % 2 == 1) a[H - 1] = c[NC - 1];
-    float xp = x * x;
-#pragma unroll
-    for (int n = H; n > 1; n = (n + 1) / 2) {
-#pragma unroll
-        for (int i = 0; i < n / 2; ++i) a[i] = fmaf(a[2 * i + 1], xp, a[2 * i]);
-        if (n % 2 == 1) a[n / 2] = a[n - 1];
-        xp = xp * xp;
-    }
-    return a[0];
-}
-
-template <int NC, bool ESTRIN>
 __global__ void __launch_bounds__(kNThreads, 1)
     k_near_tc(NearTc a, const float4* __restrict__ trg_hi, const float4* __restrict__ trg_lo,
               const float4* __restrict__ src_hi, const float4* __restrict__ src_lo, const float* __restrict__ src_q,
@@ -709,14 +688,9 @@ __global__ void __launch_bounds__(kNThreads, 1)
                     const float r2 = r2v[k] > 0.0f ? r2v[k] : 1.0f;
                     const float rinv = rsqrtf(r2);
                     const float x = fmaf(r2, rinv, pr.cen) * pr.rsc;
-                    float pv;
-                    if constexpr (ESTRIN) {
-                        pv = poly_estrin<NC>(cf, x);
-                    } else {
-                        pv = cf[NC - 1];
+                    float pv = cf[NC - 1];
 #pragma unroll
-                        for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, cf[i]);
-                    }
+                    for (int i = NC - 2; i >= 0; --i) pv = fmaf(pv, x, cf[i]);
                     w[k] = r2v[k] > 0.0f ? pv * rinv : 0.0f;
                 }
             }
@@ -797,16 +771,12 @@ void launch_near_tc_nc(const NearTc& a, const float4* th, const float4* tl, cons
     PDMK_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
     if (!configured[dev]) {
-        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_near_tc<NC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNSmem));
-        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_near_tc<NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNSmem));
+        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_near_tc<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNSmem));
         configured[dev] = true;
     }
     const int64_t nblocks = (int64_t)a.n_leaves * ((a.max_trg + 127) / 128);
     if (nblocks > INT32_MAX) throw std::runtime_error("too many near-field tiles for one launch");
-    if (a.estrin)
-        k_near_tc<NC, true><<<(unsigned)nblocks, kNThreads, kNSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
-    else
-        k_near_tc<NC, false><<<(unsigned)nblocks, kNThreads, kNSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
+    k_near_tc<NC><<<(unsigned)nblocks, kNThreads, kNSmem, s>>>(a, th, tl, sh, sl, q, pot, err);
 }
 
 

@@ -52,7 +52,6 @@ struct NearTc {
     // chunks of 32 sources accumulated in tensor memory between two FP64 drains
     // (<= 0: the default, 2)
     int seg_chunks;
-    int estrin;            // 1: residual polynomial by Estrin's scheme (else Horner)
 };
 constexpr int kNearTcMaxPairs = 128;
 constexpr int kNearTcChunk = 32;        // sources per chunk
