@@ -105,41 +105,20 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         graphs_.assign(nsys, nullptr);
         if (single_) {
             for (auto& t : trees_) t->defer_near_ = true;
-            // queue items: every system's near-field leaves, grouped by system
-            // group (consecutive systems in launch order), largest work first
-            // inside a group (PDMK_BATCH_GROUPS: number of groups, default 4)
-            n_groups_ = std::min(nsys, 4);
-            if (const char* gs = std::getenv("PDMK_BATCH_GROUPS")) n_groups_ = std::max(1, std::min(nsys, std::atoi(gs)));
-            group_of_.resize(nsys);
-            group_last_.assign(n_groups_, -1);
-            for (int i = 0; i < nsys; ++i) {
-                group_of_[i] = (int)((int64_t)i * n_groups_ / nsys);
-                group_last_[group_of_[i]] = i;
-            }
-            std::vector<std::tuple<int, int64_t, int, int>> items;
+            // queue items: every system's near-field leaves, largest work first
+            std::vector<std::tuple<int64_t, int, int>> items;
             for (int i = 0; i < nsys; ++i) {
                 const auto& cost = trees_[i]->near_leaf_cost();
-                for (int e = 0; e < trees_[i]->near_leaves(); ++e) items.emplace_back(group_of_[i], -cost[e], i, e);
+                for (int e = 0; e < trees_[i]->near_leaves(); ++e) items.emplace_back(-cost[e], i, e);
             }
             std::stable_sort(items.begin(), items.end());
             std::vector<int2> it(items.size());
-            group_item_.assign(n_groups_ + 1, 0);
-            for (size_t k = 0; k < items.size(); ++k) {
-                it[k] = make_int2(std::get<2>(items[k]), std::get<3>(items[k]));
-                group_item_[std::get<0>(items[k]) + 1]++;
-            }
-            for (int g = 0; g < n_groups_; ++g) group_item_[g + 1] += group_item_[g];
+            for (size_t k = 0; k < items.size(); ++k) it[k] = make_int2(std::get<1>(items[k]), std::get<2>(items[k]));
             n_items_ = (int)it.size();
             PDMK_CUDA_CHECK(cudaMalloc(&items_dev_, sizeof(int2) * std::max<size_t>(it.size(), 1)));
             PDMK_CUDA_CHECK(cudaMemcpy(items_dev_, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
             PDMK_CUDA_CHECK(cudaMalloc(&sys_dev_, sizeof(dev::NearLeafSys) * nsys));
-            PDMK_CUDA_CHECK(cudaMalloc(&head_dev_, sizeof(int) * n_groups_));
-            group_stream_.assign(n_groups_, nullptr);
-            group_done_.assign(n_groups_, nullptr);
-            for (int g = 0; g < n_groups_; ++g) {
-                PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&group_stream_[g], cudaStreamNonBlocking));
-                PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&group_done_[g], cudaEventDisableTiming));
-            }
+            PDMK_CUDA_CHECK(cudaMalloc(&head_dev_, sizeof(int)));
             nc_ = trees_[0]->near_coeffs();
             for (int i = 0; i < nc_; ++i) coef32_[i] = (float)trees_[0]->near_coef()[i];
         }
@@ -167,15 +146,6 @@ void TreeBatch::release() {
     if (pot_dev_) cudaFree(pot_dev_);
     if (potf_dev_) cudaFree(potf_dev_);
     if (sys_dev_) cudaFree(sys_dev_);
-    for (auto& gs : group_stream_)
-        if (gs) {
-            cudaStreamSynchronize(gs);
-            cudaStreamDestroy(gs);
-        }
-    group_stream_.clear();
-    for (auto& ge : group_done_)
-        if (ge) cudaEventDestroy(ge);
-    group_done_.clear();
     if (items_dev_) cudaFree(items_dev_);
     if (head_dev_) cudaFree(head_dev_);
     sys_dev_ = nullptr;
@@ -239,21 +209,9 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
             enqueue();
         }
         PDMK_CUDA_CHECK(cudaEventRecord(done_[i], ts));
-        if (single_) {
-            // the group's queue runs once all of its systems are done (from the
-            // second evaluate on: the first one creates the systems' device
-            // state, which the queue's descriptors point into)
-            const int g = group_of_[i];
-            PDMK_CUDA_CHECK(cudaStreamWaitEvent(group_stream_[g], done_[i], 0));
-            if (queue_built_ && group_last_[g] == (int)i) launch_group(g);
-        } else {
-            PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
-        }
+        PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
     }
-    if (single_ && !queue_built_) {
-        build_queue();
-        for (int g = 0; g < n_groups_; ++g) launch_group(g);
-    }
+    if (single_) run_queue();
     if (pot_float) {
         dev::launch_to_float(pot_dev_, potf_dev_, n, stream_);
         PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, potf_dev_, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_));
@@ -297,18 +255,13 @@ std::mutex g_tune_mu;
 std::map<std::tuple<int, int64_t, int, int>, int> g_tune;
 }  // namespace
 
-void TreeBatch::launch_group(int g) {
-    run_queue(g, group_stream_[g]);
-    PDMK_CUDA_CHECK(cudaEventRecord(group_done_[g], group_stream_[g]));
-    PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, group_done_[g], 0));
-}
-
-void TreeBatch::run_queue(int grp, cudaStream_t qs) {
+void TreeBatch::run_queue() {
+    if (!queue_built_) build_queue();
     dev::BatchNearArgs a{};
     a.sys = sys_dev_;
-    a.items = items_dev_ + group_item_[grp];
-    a.n_items = group_item_[grp + 1] - group_item_[grp];
-    a.head = head_dev_ + grp;
+    a.items = items_dev_;
+    a.n_items = n_items_;
+    a.head = head_dev_;
     for (int i = 0; i < 32; ++i) a.coef32[i] = coef32_[i];
     if (tpt_ == 0) {
         const auto key = std::make_tuple(n_items_, total_points(), nc_, device_);
@@ -318,18 +271,17 @@ void TreeBatch::run_queue(int grp, cudaStream_t qs) {
             if (it != g_tune.end()) tpt_ = it->second;
         }
         if (tpt_ == 0) {
-            // time each candidate once on this group's queue, on its stream
-            // (after its systems; the kernel writes the potentials from inputs
-            // it does not modify, so repeats are harmless)
+            // time each candidate once on this batch (the kernel writes the
+            // potentials from inputs it does not modify, so repeats are harmless)
             cudaEvent_t e0, e1;
             PDMK_CUDA_CHECK(cudaEventCreate(&e0));
             PDMK_CUDA_CHECK(cudaEventCreate(&e1));
             float best = 1e30f;
             for (int tpt : {1, 2, 4}) {
                 const int ctas = dev::batch_near_ctas(nc_, tpt);
-                PDMK_CUDA_CHECK(cudaEventRecord(e0, qs));
-                dev::launch_batch_near(a, nc_, tpt, ctas, qs);
-                PDMK_CUDA_CHECK(cudaEventRecord(e1, qs));
+                PDMK_CUDA_CHECK(cudaEventRecord(e0, stream_));
+                dev::launch_batch_near(a, nc_, tpt, ctas, stream_);
+                PDMK_CUDA_CHECK(cudaEventRecord(e1, stream_));
                 PDMK_CUDA_CHECK(cudaEventSynchronize(e1));
                 float ms = 0;
                 PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
@@ -345,7 +297,7 @@ void TreeBatch::run_queue(int grp, cudaStream_t qs) {
         }
         ctas_ = dev::batch_near_ctas(nc_, tpt_);
     }
-    dev::launch_batch_near(a, nc_, tpt_, ctas_, qs);
+    dev::launch_batch_near(a, nc_, tpt_, ctas_, stream_);
     PDMK_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -44,23 +44,14 @@ class TreeBatch {
     std::vector<cudaGraphExec_t> graphs_;
     int* err_host_ = nullptr;  // pinned, one word per system
     int evaluates_ = 0;
-    // Float trees: the near field and final gather run as persistent launches
-    // over device queues of (system, leaf) items, one per group of systems in
-    // launch order, each as soon as its group's systems are done (so a
-    // group's near field overlaps the later groups' tree passes).
+    // Float trees: the near field and final gather of all systems run as one
+    // persistent launch over a device queue of (system, leaf) items.
     void build_queue();
-    void run_queue(int g, cudaStream_t s);
-    void launch_group(int g);  // group g's queue on its stream; the batch stream waits for it
+    void run_queue();
     dev::NearLeafSys* sys_dev_ = nullptr;
-    int2* items_dev_ = nullptr;  // grouped: group g's items at [group_item_[g], group_item_[g + 1])
-    int* head_dev_ = nullptr;    // one queue head per group
+    int2* items_dev_ = nullptr;
+    int* head_dev_ = nullptr;
     int n_items_ = 0;
-    int n_groups_ = 1;
-    std::vector<int> group_of_;    // system -> group
-    std::vector<int> group_last_;  // group -> last system (launch order)
-    std::vector<int> group_item_;  // group -> first item (size n_groups_ + 1)
-    std::vector<cudaStream_t> group_stream_;
-    std::vector<cudaEvent_t> group_done_;
     int nc_ = 0;
     float coef32_[32] = {};
     bool queue_built_ = false;
