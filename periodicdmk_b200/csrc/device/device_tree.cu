@@ -104,6 +104,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
 
     if (const char* tm = std::getenv("PDMK_TC_MASK")) tc_mask_ = std::atoi(tm) & 15;
     if (const char* dm = std::getenv("PDMK_FP64_DMMA")) fp64_dmma_ = std::atoi(dm) != 0;
+    if (const char* mm = std::getenv("PDMK_MOMENTS_DMMA")) moments_dmma_ = std::atoi(mm) != 0;
     n_ = P.n_src;
     n_digits_ = P.dp.n_digits_tree;
     n_all_ = P.n_all;
@@ -1094,7 +1095,10 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
     int nl = 0;
     PDMK_CUDA_CHECK(cudaMemsetAsync(proxy_up_, 0, sizeof(double) * std::max<int64_t>(n_up_ * ncoef, 1), s));
     dev::launch_gather(src_, src_charge_idx_, q, n_all_, s);
-    dev::launch_c2proxy(c2x_, p, s);
+    if (moments_dmma_ && dev::c2proxy_dmma_supported(p))
+        dev::launch_c2proxy_dmma(c2x_, p, s);
+    else
+        dev::launch_c2proxy(c2x_, p, s);
     nl += 2;
     // child -> parent translation of real (p,p,p) tensors: one fused kernel, or
     // three contractions through scratch in chunks of C.c2p translations

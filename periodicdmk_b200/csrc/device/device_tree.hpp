@@ -152,6 +152,9 @@ class DeviceTree {
     // FP64 child <-> parent translations on the FP64 tensor cores (DMMA)
     // instead of the CUDA cores.  Initialised from PDMK_FP64_DMMA (default 0).
     int fp64_dmma_ = 0;
+    // Proxy moments of the FP64 path at p = 28, 38 on DMMA (dmma.cu) instead of
+    // the register-tiled CUDA-core kernel.  Initialised from PDMK_MOMENTS_DMMA.
+    int moments_dmma_ = 0;
 
   private:
     void init(const Plan& P, int device, bool fp64_working_set);

@@ -126,7 +126,111 @@ void launch_nt(const ContractArgs& a, cudaStream_t s) {
     launch_s<0, NT>(a, s);
 }
 
+// Proxy moments of the FP64 path for the high orders on the FP64 tensor cores:
+// per centre box O[(i,j), k] = sum_s X_i(s) Y_j(s) (q_s Z_k(s)) with X, Y, Z the
+// Chebyshev values at the source's scaled coordinates (cpp/src/dmk/proxy.cpp,
+// charge-to-proxy), a GEMM with M = P^2 rows r = i + P j, N = P columns k and
+// K = the box's sources.  A CTA of 8 warps takes 256 rows (4 row tiles of 8 per
+// warp) and all columns (NT tiles of 8); sources are staged 32 at a time as
+// their three Chebyshev tables (the charge folded into Z); per 4 sources a
+// thread forms its A element X_i Y_j (one product) and NT B elements and the
+// warp issues 4 x NT mma.m8n8k4.f64.  Every coefficient is written once (the
+// children's translations are added afterwards), as the CUDA-core kernel does.
+template <int P>
+__global__ void __launch_bounds__(256) k_c2proxy_dmma(C2ProxyArgs a) {
+    constexpr int TS = 32, NT = (P + 7) / 8, PN = NT * 8, RT = 4, ROWS = 8 * 8 * RT;
+    constexpr int LX = P + 1, LZ = PN + 1;
+    __shared__ double sx[TS][LX], sy[TS][LX], sz[TS][LZ];
+    const int e = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rq = lane >> 2, kq = lane & 3;
+    const int r0 = blockIdx.y * ROWS + warp * 8 * RT;
+    int ai[RT], aj[RT];
+    bool av[RT];
+#pragma unroll
+    for (int t = 0; t < RT; ++t) {
+        const int r = r0 + 8 * t + rq;
+        av[t] = r < P * P;
+        ai[t] = av[t] ? r % P : 0;
+        aj[t] = av[t] ? r / P : 0;
+    }
+    double acc[RT][NT][2];
+#pragma unroll
+    for (int t = 0; t < RT; ++t)
+#pragma unroll
+        for (int c = 0; c < NT; ++c) acc[t][c][0] = acc[t][c][1] = 0.0;
+    const double4 cs = a.center_scale[e];
+    for (int rg = a.rng_start[e]; rg < a.rng_start[e + 1]; ++rg) {
+        const int s0 = a.src_start[rg], ns = a.src_count[rg];
+        for (int base = 0; base < ns; base += TS) {
+            const int nt = min(TS, ns - base);
+            __syncthreads();
+            for (int task = threadIdx.x; task < 3 * TS; task += blockDim.x) {
+                const int si = task % TS, d = task / TS;
+                double* dst = d == 0 ? sx[si] : (d == 1 ? sy[si] : sz[si]);
+                const int len = d == 2 ? PN : P;
+                if (si < nt) {
+                    const double4 pt = a.src[s0 + base + si];
+                    const double x = (d == 0 ? pt.x - cs.x : (d == 1 ? pt.y - cs.y : pt.z - cs.z)) * cs.w;
+                    const double mult = d == 2 ? pt.w : 1.0;  // the charge folded into the z factor
+                    double t0 = 1.0, t1 = x;
+                    dst[0] = mult;
+                    dst[1] = mult * x;
+                    for (int n = 2; n < P; ++n) {
+                        const double t2 = 2.0 * x * t1 - t0;
+                        dst[n] = mult * t2;
+                        t0 = t1;
+                        t1 = t2;
+                    }
+                    for (int n = P; n < len; ++n) dst[n] = 0.0;
+                } else {
+                    for (int n = 0; n < len; ++n) dst[n] = 0.0;
+                }
+            }
+            __syncthreads();
+            const int nks = (nt + 3) / 4;
+            for (int ks = 0; ks < nks; ++ks) {
+                const int s = 4 * ks + kq;
+                double b[NT];
+#pragma unroll
+                for (int c = 0; c < NT; ++c) b[c] = sz[s][8 * c + rq];
+#pragma unroll
+                for (int t = 0; t < RT; ++t) {
+                    const double x = sx[s][ai[t]] * sy[s][aj[t]];
+                    const double av_t = av[t] ? x : 0.0;
+#pragma unroll
+                    for (int c = 0; c < NT; ++c) dmma(acc[t][c][0], acc[t][c][1], av_t, b[c]);
+                }
+            }
+        }
+    }
+    double* out = a.proxy_up + (int64_t)a.slot[e] * (P * P * P);
+#pragma unroll
+    for (int t = 0; t < RT; ++t) {
+        const int r = r0 + 8 * t + rq;
+        if (r >= P * P) continue;
+#pragma unroll
+        for (int c = 0; c < NT; ++c)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = 8 * c + 2 * kq + h;
+                if (k < P) out[r + (int64_t)P * P * k] = acc[t][c][h];
+            }
+    }
+}
+
 }  // namespace
+
+bool c2proxy_dmma_supported(int p) { return p == 28 || p == 38; }
+
+void launch_c2proxy_dmma(const C2ProxyArgs& a, int p, cudaStream_t s) {
+    if (a.n_centers <= 0) return;
+    switch (p) {
+        case 28: k_c2proxy_dmma<28><<<dim3(a.n_centers, (28 * 28 + 255) / 256), 256, 0, s>>>(a); break;
+        case 38: k_c2proxy_dmma<38><<<dim3(a.n_centers, (38 * 38 + 255) / 256), 256, 0, s>>>(a); break;
+        default: throw std::runtime_error("moments order not covered");
+    }
+}
 
 bool translate_dmma_supported(int ni, int na) { return ni > 0 && na > 0 && ni <= 64 && na <= 40; }
 

@@ -13,5 +13,10 @@ namespace dev {
 bool translate_dmma_supported(int ni, int na);
 void launch_translate_dmma(const ContractArgs& a, cudaStream_t s);
 
+// Proxy moments of the FP64 path (launch_c2proxy's sum) on mma.sync.m8n8k4.f64,
+// for the orders of 9 and 12 digits (p = 28, 38).
+bool c2proxy_dmma_supported(int p);
+void launch_c2proxy_dmma(const C2ProxyArgs& a, int p, cudaStream_t s);
+
 }  // namespace dev
 }  // namespace pdmkb

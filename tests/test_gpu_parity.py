@@ -199,3 +199,19 @@ def test_fp64_translations_on_dmma(nd, monkeypatch):
     t = _tree(cell, pos, nd, 40)
     assert rel_l2(t.evaluate(q), ref) < 1e-13
     t.close()
+
+
+@pytest.mark.parametrize("nd", [9, 12])
+def test_fp64_moments_on_dmma(nd, monkeypatch):
+    # PDMK_MOMENTS_DMMA=1 (read when the tree is built) forms the proxy moments
+    # of the orders p = 28, 38 on mma.sync.m8n8k4.f64: the same sums in another
+    # order, so the potentials agree with the CUDA-core kernel to rounding
+    cell, pos, q = clustered_system(20000, 42, TRICLINIC, n_clusters=8, sigma=0.03)
+    monkeypatch.setenv("PDMK_MOMENTS_DMMA", "0")
+    ref_tree = _tree(cell, pos, nd, 40)
+    ref = ref_tree.evaluate(q)
+    ref_tree.close()
+    monkeypatch.setenv("PDMK_MOMENTS_DMMA", "1")
+    t = _tree(cell, pos, nd, 40)
+    assert rel_l2(t.evaluate(q), ref) < 1e-13
+    t.close()
