@@ -105,7 +105,6 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     if (const char* tm = std::getenv("PDMK_TC_MASK")) tc_mask_ = std::atoi(tm) & 15;
     if (const char* dm = std::getenv("PDMK_FP64_DMMA")) fp64_dmma_ = std::atoi(dm) != 0;
     if (const char* mm = std::getenv("PDMK_MOMENTS_DMMA")) moments_dmma_ = std::atoi(mm) != 0;
-    if (const char* ev = std::getenv("PDMK_EVAL_DMMA")) eval_dmma_ = std::atoi(ev) != 0;
     n_ = P.n_src;
     n_digits_ = P.dp.n_digits_tree;
     n_all_ = P.n_all;
@@ -1210,10 +1209,7 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
         if (F.eval.n_leaves) {
             dev::EvalArgs e = F.eval;
             e.proxy_down = down;
-            if (eval_dmma_ && dev::eval_dmma_supported(p))
-                dev::launch_eval_dmma(e, p, s);
-            else
-                dev::launch_eval(e, p, s);
+            dev::launch_eval(e, p, s);
             ++nl;
             if (grad_on_) {
                 dev::launch_eval_grad(e, p, grad_sorted_, n_, s);

@@ -156,9 +156,6 @@ class DeviceTree {
     // the register-tiled CUDA-core kernel.  Initialised from PDMK_MOMENTS_DMMA
     // (default 1: 86 -> 42 ms per 12-digit evaluate of 2e6 clustered points).
     int moments_dmma_ = 1;
-    // Leaf evaluation of the FP64 path at p = 28, 38 on DMMA (dmma.cu) instead
-    // of the register-tiled CUDA-core kernel.  Initialised from PDMK_EVAL_DMMA.
-    int eval_dmma_ = 0;
 
   private:
     void init(const Plan& P, int device, bool fp64_working_set);

@@ -219,115 +219,7 @@ __global__ void __launch_bounds__(256) k_c2proxy_dmma(C2ProxyArgs a) {
     }
 }
 
-// Leaf evaluation of the FP64 path for the high orders on the FP64 tensor
-// cores: per leaf u_t = sum_k Z_k(t) D[t, k], D[t, k] = sum_{(i,j)} X_i(t) Y_j(t)
-// C[i + P j + P^2 k], a GEMM with M = the leaf's targets (64 per pass: one row
-// tile of 8 per warp), N = P columns k (NT tiles of 8) and K = P^2 pairs (i, j),
-// the coefficients streamed through shared memory 64 pairs at a time.  Per 4
-// pairs a thread forms its A element X_i Y_j (one product) and NT B elements.
-template <int P>
-__global__ void __launch_bounds__(256) k_eval_dmma(EvalArgs a) {
-    constexpr int NT = (P + 7) / 8, PN = NT * 8, TPASS = 64, KC = 64, LB = KC + 4;
-    constexpr int P2 = P * P, NKC = (P2 + KC - 1) / KC;
-    constexpr int LT = P + 1;
-    extern __shared__ __align__(16) double sme[];
-    auto sX = reinterpret_cast<double(*)[LT]>(sme);
-    auto sY = reinterpret_cast<double(*)[LT]>(sme + TPASS * LT);
-    auto sZ = reinterpret_cast<double(*)[LT]>(sme + 2 * TPASS * LT);
-    auto sB = reinterpret_cast<double(*)[LB]>(sme + 3 * TPASS * LT);  // [k][pair in chunk]
-    const int e = blockIdx.x;
-    const int t0 = a.trg_start[e], nt = a.trg_count[e];
-    const double4 cs = a.center_scale[e];
-    const double* C = a.proxy_down + (int64_t)a.slot[e] * (P * P * P);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rq = lane >> 2, kq = lane & 3;
-    const int tl = warp * 8 + rq;  // this thread's target row in the pass
-    for (int tbase = 0; tbase < nt; tbase += TPASS) {
-        __syncthreads();  // the previous pass is done with the tables
-        for (int task = threadIdx.x; task < 3 * TPASS; task += blockDim.x) {
-            const int ti = task % TPASS, d = task / TPASS;
-            double* dst = d == 0 ? sX[ti] : (d == 1 ? sY[ti] : sZ[ti]);
-            const int t = tbase + ti;
-            double x = 0.0;
-            if (t < nt) {
-                const double4 pt = a.trg[t0 + t];
-                x = (d == 0 ? pt.x - cs.x : (d == 1 ? pt.y - cs.y : pt.z - cs.z)) * cs.w;
-            }
-            const double m = (t < nt || d != 0) ? 1.0 : 0.0;  // absent targets: zero rows of A
-            double x0 = 1.0, x1 = x;
-            dst[0] = m;
-            dst[1] = m * x;
-            for (int n = 2; n < P; ++n) {
-                const double x2 = 2.0 * x * x1 - x0;
-                dst[n] = m * x2;
-                x0 = x1;
-                x1 = x2;
-            }
-        }
-        double acc[NT][2];
-#pragma unroll
-        for (int c = 0; c < NT; ++c) acc[c][0] = acc[c][1] = 0.0;
-        for (int kc = 0; kc < NKC; ++kc) {
-            const int r0 = kc * KC;
-            __syncthreads();  // tables written / previous chunk consumed
-            for (int idx = threadIdx.x; idx < PN * KC; idx += blockDim.x) {
-                const int k = idx / KC, rl = idx - k * KC;
-                const int r = r0 + rl;
-                sB[k][rl] = (k < P && r < P2) ? C[r + (int64_t)P2 * k] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll 4
-            for (int ks = 0; ks < KC / 4; ++ks) {
-                const int rl = 4 * ks + kq, r = r0 + rl;
-                const int i = r % P, j = r / P;
-                const double av = r < P2 ? sX[tl][i] * sY[tl][j] : 0.0;
-#pragma unroll
-                for (int c = 0; c < NT; ++c) dmma(acc[c][0], acc[c][1], av, sB[8 * c + rq][rl]);
-            }
-        }
-        // u_t = sum_k Z_k(t) D[t, k]: this lane holds columns 2 kq, 2 kq + 1 of each tile
-        double u = 0.0;
-#pragma unroll
-        for (int c = 0; c < NT; ++c)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int k = 8 * c + 2 * kq + h;
-                if (k < P) u = fma(acc[c][h], sZ[tl][k], u);
-            }
-        u += __shfl_xor_sync(0xffffffffu, u, 1);
-        u += __shfl_xor_sync(0xffffffffu, u, 2);
-        const int t = tbase + tl;
-        if (kq == 0 && t < nt) a.pot[t0 + t] += u;
-    }
-}
-
 }  // namespace
-
-bool eval_dmma_supported(int p) { return p == 28 || p == 38; }
-
-template <int P>
-void launch_eval_dmma_p(const EvalArgs& a, cudaStream_t s) {
-    constexpr int NT = (P + 7) / 8, PN = NT * 8;
-    constexpr size_t smem = sizeof(double) * (3 * 64 * (P + 1) + PN * (64 + 4));
-    static bool configured[64] = {};
-    int dev = 0;
-    PDMK_CUDA_CHECK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
-    if (!configured[dev]) {
-        PDMK_CUDA_CHECK(cudaFuncSetAttribute(k_eval_dmma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured[dev] = true;
-    }
-    k_eval_dmma<P><<<a.n_leaves, 256, smem, s>>>(a);
-}
-
-void launch_eval_dmma(const EvalArgs& a, int p, cudaStream_t s) {
-    if (a.n_leaves <= 0) return;
-    switch (p) {
-        case 28: launch_eval_dmma_p<28>(a, s); break;
-        case 38: launch_eval_dmma_p<38>(a, s); break;
-        default: throw std::runtime_error("evaluation order not covered");
-    }
-}
 
 bool c2proxy_dmma_supported(int p) { return p == 28 || p == 38; }
 

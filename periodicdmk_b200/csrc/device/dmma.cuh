@@ -17,10 +17,6 @@ void launch_translate_dmma(const ContractArgs& a, cudaStream_t s);
 // for the orders of 9 and 12 digits (p = 28, 38).
 bool c2proxy_dmma_supported(int p);
 void launch_c2proxy_dmma(const C2ProxyArgs& a, int p, cudaStream_t s);
-// Leaf evaluation of the FP64 path (launch_eval's sum, accumulated into pot)
-// on mma.sync.m8n8k4.f64, for p = 28, 38.
-bool eval_dmma_supported(int p);
-void launch_eval_dmma(const EvalArgs& a, int p, cudaStream_t s);
 
 }  // namespace dev
 }  // namespace pdmkb

@@ -215,18 +215,3 @@ def test_fp64_moments_on_dmma(nd, monkeypatch):
     t = _tree(cell, pos, nd, 40)
     assert rel_l2(t.evaluate(q), ref) < 1e-13
     t.close()
-
-
-@pytest.mark.parametrize("nd", [9, 12])
-def test_fp64_leaf_evaluation_on_dmma(nd, monkeypatch):
-    # PDMK_EVAL_DMMA=1 evaluates the local expansions at the leaf targets of the
-    # orders p = 28, 38 on mma.sync.m8n8k4.f64 (the same sums in another order)
-    cell, pos, q = clustered_system(20000, 43, TRICLINIC, n_clusters=8, sigma=0.03)
-    monkeypatch.setenv("PDMK_EVAL_DMMA", "0")
-    ref_tree = _tree(cell, pos, nd, 40)
-    ref = ref_tree.evaluate(q)
-    ref_tree.close()
-    monkeypatch.setenv("PDMK_EVAL_DMMA", "1")
-    t = _tree(cell, pos, nd, 40)
-    assert rel_l2(t.evaluate(q), ref) < 1e-13
-    t.close()
