@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <stdexcept>
 
 #include "common.cuh"
@@ -45,12 +46,31 @@ __global__ void __launch_bounds__(256) k_translate_dmma(ContractArgs a, int RS, 
     double* out = static_cast<double*>(a.out) + (a.out_off ? a.out_off[e] : (int64_t)e * a.out_stride);
     const double* mat = static_cast<const double*>(a.mat) + (a.mat_off ? a.mat_off[e] : 0);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int r = warp; r < kDRows; r += 8) {
-        const double* row = in + (int64_t)(r0 + r) * K;
-        for (int k = lane; k < 4 * KS; k += 32) sA[r * RS + k] = (r < nr && k < K) ? row[k] : 0.0;
+    // The tile's input rows are contiguous in global memory: asynchronous
+    // 16-byte copies when K is even and the block is 16-byte aligned (the
+    // translation tensors are), element loads otherwise; zero padding after.
+    const bool vec = (K % 2 == 0) && ((reinterpret_cast<uintptr_t>(in + (int64_t)r0 * K) & 15) == 0) && (RS % 2 == 0);
+    if (vec) {
+        const int hk = K / 2, nchunk = nr * hk;
+        const double* src0 = in + (int64_t)r0 * K;
+        for (int c = tid; c < nchunk; c += blockDim.x) {
+            const int r = c / hk, k = 2 * (c - r * hk);
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(sA + r * RS + k);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src0 + (int64_t)r * K + k) : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        for (int r = warp; r < kDRows; r += 8)
+            for (int k = lane; k < 4 * KS; k += 32)
+                if (r >= nr || k >= K) sA[r * RS + k] = 0.0;
+    } else {
+        for (int r = warp; r < kDRows; r += 8) {
+            const double* row = in + (int64_t)(r0 + r) * K;
+            for (int k = lane; k < 4 * KS; k += 32) sA[r * RS + k] = (r < nr && k < K) ? row[k] : 0.0;
+        }
     }
     for (int i = warp; i < 4 * KS; i += 8)
         for (int c = lane; c < 8 * NT; c += 32) sB[i * BS + c] = (i < K && c < N) ? mat[c + (int64_t)N * i] : 0.0;
+    if (vec) asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     double acc[2][NT][2];
 #pragma unroll
