@@ -19,7 +19,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cstdlib>
 #include <stdexcept>
 
 #include "batch_near.cuh"
@@ -38,10 +37,7 @@ __device__ __forceinline__ float box_gap2(const float4& lo, const float4& hi, co
     return fmaf(gx, gx, fmaf(gy, gy, gz * gz));
 }
 
-// LOCAL: coordinates relative to an origin inside the target leaf, rounded to
-// FP32 once per target and per staged source (one subtraction per axis and
-// pair); otherwise double-float differences (three operations per axis).
-template <int NC, int TPT, bool LOCAL>
+template <int NC, int TPT>
 __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
     __shared__ float4 sh[128], sl[128];
     __shared__ float sq[128];
@@ -59,14 +55,6 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
         const int e = w.y;
         const int t0 = S.trg_start[e], nt = S.trg_count[e];
         const int p0 = S.pair_start[e], p1 = S.pair_start[e + 1];
-        // origin of the local coordinates: the leaf's first target
-        double ox = 0.0, oy = 0.0, oz = 0.0;
-        if (LOCAL && nt > 0) {
-            const float4 h0 = S.trg_hi[t0], l0 = S.trg_lo[t0];
-            ox = (double)h0.x + (double)l0.x;
-            oy = (double)h0.y + (double)l0.y;
-            oz = (double)h0.z + (double)l0.z;
-        }
         for (int base = 0; base < nt; base += TPT * 128) {
             float4 th[TPT], tl[TPT];
             double acc[TPT];
@@ -82,14 +70,6 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
                     lo[1] = fminf(lo[1], th[u].y); hi[1] = fmaxf(hi[1], th[u].y);
                     lo[2] = fminf(lo[2], th[u].z); hi[2] = fmaxf(hi[2], th[u].z);
                 }
-            }
-            float4 tloc[TPT];
-#pragma unroll
-            for (int u = 0; u < TPT; ++u) {
-                tloc[u] = make_float4((float)((double)th[u].x - ox + (double)tl[u].x),
-                                      (float)((double)th[u].y - oy + (double)tl[u].y),
-                                      (float)((double)th[u].z - oz + (double)tl[u].z), 0.f);
-                if (th[u].x >= 1e29f) tloc[u] = make_float4(1e30f, 1e30f, 1e30f, 0.f);
             }
             // target boxes of the warps and of the pass, widened by the FP32
             // rounding of the hi-part coordinates (relative 2^-23)
@@ -135,15 +115,8 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
                     __syncthreads();
                     const int js = sb + threadIdx.x;
                     if (js < ns && ((need >> (threadIdx.x >> 5)) & 1u)) {
-                        const float4 yh = S.src_hi[s0 + js], yl = S.src_lo[s0 + js];
-                        if (LOCAL) {
-                            sh[threadIdx.x] = make_float4((float)((double)yh.x - ox + (double)yl.x),
-                                                          (float)((double)yh.y - oy + (double)yl.y),
-                                                          (float)((double)yh.z - oz + (double)yl.z), 0.f);
-                        } else {
-                            sh[threadIdx.x] = yh;
-                            sl[threadIdx.x] = yl;
-                        }
+                        sh[threadIdx.x] = S.src_hi[s0 + js];
+                        sl[threadIdx.x] = S.src_lo[s0 + js];
                         sq[threadIdx.x] = S.src_q[s0 + js];
                     }
                     __syncthreads();
@@ -155,14 +128,13 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
                         if (box_gap2(__ldg(S.chunk_lo + c), __ldg(S.chunk_hi + c), wbox) > keep2) continue;
                         const int je = min(m, 32 * k + 32);
                         for (int j = 32 * k; j < je; ++j) {
-                            const float4 yh = sh[j];
-                            const float4 yl = LOCAL ? make_float4(0.f, 0.f, 0.f, 0.f) : sl[j];
+                            const float4 yh = sh[j], yl = sl[j];
                             const float qj = sq[j];
 #pragma unroll
                             for (int u = 0; u < TPT; ++u) {
-                                const float dx = LOCAL ? tloc[u].x - yh.x : (th[u].x - yh.x) + (tl[u].x - yl.x);
-                                const float dy = LOCAL ? tloc[u].y - yh.y : (th[u].y - yh.y) + (tl[u].y - yl.y);
-                                const float dz = LOCAL ? tloc[u].z - yh.z : (th[u].z - yh.z) + (tl[u].z - yl.z);
+                                const float dx = (th[u].x - yh.x) + (tl[u].x - yl.x);
+                                const float dy = (th[u].y - yh.y) + (tl[u].y - yl.y);
+                                const float dz = (th[u].z - yh.z) + (tl[u].z - yl.z);
                                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                                 if (r2 > 1e-30f && r2 < d2max) {
                                     const float rinv = rsqrtf(r2);
@@ -195,13 +167,9 @@ __global__ void __launch_bounds__(128) k_batch_near(BatchNearArgs a) {
 
 template <int TPT>
 void launch_tpt(const BatchNearArgs& a, int nc, int ctas, cudaStream_t s) {
-    static const bool local = std::getenv("PDMK_BATCH_NEAR_LOCAL") && std::atoi(std::getenv("PDMK_BATCH_NEAR_LOCAL"));
     switch (nc) {
-#define PDMK_BN(NC)                                                              \
-    case NC:                                                                     \
-        if (local) k_batch_near<NC, TPT, true><<<ctas, 128, 0, s>>>(a);          \
-        else k_batch_near<NC, TPT, false><<<ctas, 128, 0, s>>>(a);               \
-        break;
+#define PDMK_BN(NC) \
+    case NC: k_batch_near<NC, TPT><<<ctas, 128, 0, s>>>(a); break;
         PDMK_BN(5) PDMK_BN(6) PDMK_BN(9) PDMK_BN(11) PDMK_BN(12) PDMK_BN(15) PDMK_BN(17) PDMK_BN(18) PDMK_BN(22)
         PDMK_BN(23) PDMK_BN(25)
 #undef PDMK_BN
@@ -215,7 +183,7 @@ int occupancy_tpt(int nc) {
     switch (nc) {
 #define PDMK_BO(NC)                                                                                          \
     case NC:                                                                                                 \
-        PDMK_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch_near<NC, TPT, false>, 128, 0)); \
+        PDMK_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch_near<NC, TPT>, 128, 0)); \
         break;
         PDMK_BO(5) PDMK_BO(6) PDMK_BO(9) PDMK_BO(11) PDMK_BO(12) PDMK_BO(15) PDMK_BO(17) PDMK_BO(18) PDMK_BO(22)
         PDMK_BO(23) PDMK_BO(25)
