@@ -10,6 +10,8 @@ Tolerances (relative L2):
   * total vs Ewald: the reference's own bars (cpp/tests/test_periodic_dmk.cpp:42,67,
     cpp/tests/test_nonuniform.cpp:303) tightened where the method allows.
 """
+import json
+
 import numpy as np
 import pytest
 
@@ -215,3 +217,16 @@ def test_fp64_moments_on_dmma(nd, monkeypatch):
     t = _tree(cell, pos, nd, 40)
     assert rel_l2(t.evaluate(q), ref) < 1e-13
     t.close()
+
+
+def test_float_tree_vs_oracle():
+    # the float tree (mixed precision, one RHS) against the FP64 oracle at 6
+    # digits: the north-star bar for the mixed path, 1e-6 relative L2
+    (cell, pos, q), npl = SYSTEMS["cube_deep"]()
+    tf = _tree(cell, pos, 6, npl, precision="float")
+    b = tf.evaluate(q)
+    tf.close()
+    ref = oracle.evaluate(cell, pos, q, 6, npl, 4)
+    e = rel_l2(b, ref)
+    print("PARITY " + json.dumps({"case": "float tree, one RHS, 6 digits", "rel_l2_vs_oracle": e}))
+    assert e < 1e-6
