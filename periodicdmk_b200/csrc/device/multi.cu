@@ -399,11 +399,22 @@ struct NearM {
     const int* pair_src_start;
     const int* pair_src_count;
     const double* pair_bsize;
+    const int* pair_chunk_base;  // per near pair: first 32-source chunk box of its source box
+    const float4* chunk_lo;      // per 32-source chunk: bounding box (rounded outwards)
+    const float4* chunk_hi;
     double coef[32];
     int n_leaves;
     int64_t N;
     int kb;
 };
+
+// squared gap between a chunk's box and a target box b = (lo xyz, hi xyz)
+__device__ __forceinline__ float chunk_gap2(const float4& lo, const float4& hi, const float* b) {
+    const float gx = fmaxf(0.0f, fmaxf(lo.x - b[3], b[0] - hi.x));
+    const float gy = fmaxf(0.0f, fmaxf(lo.y - b[4], b[1] - hi.y));
+    const float gz = fmaxf(0.0f, fmaxf(lo.z - b[5], b[2] - hi.z));
+    return fmaf(gx, gx, fmaf(gy, gy, gz * gz));
+}
 
 // FP64: positions double4, charges double[s * kb + c]
 template <int NC, int KB>
@@ -486,6 +497,8 @@ __global__ void __launch_bounds__(128) k_near_m32(NearM a, const float4* __restr
     constexpr int TPT = 2;
     __shared__ float4 sh[128], sl[128];
     __shared__ float sq[128][KB];
+    __shared__ float s_wbox[4][6];  // per warp: bounding box of its targets of the pass
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int e = blockIdx.x;
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
     float c[NC];
@@ -495,6 +508,7 @@ __global__ void __launch_bounds__(128) k_near_m32(NearM a, const float4* __restr
         for (int base = 0; base < nt; base += TPT * 128) {
             float4 th[TPT], tl[TPT];
             double acc[TPT][KB];
+            float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
 #pragma unroll
             for (int u = 0; u < TPT; ++u) {
                 const int t = base + threadIdx.x + u * 128;
@@ -502,20 +516,59 @@ __global__ void __launch_bounds__(128) k_near_m32(NearM a, const float4* __restr
                 tl[u] = t < nt ? trg_lo[t0 + t] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                 for (int q = 0; q < KB; ++q) acc[u][q] = 0.0;
+                if (t < nt) {
+                    lo[0] = fminf(lo[0], th[u].x); hi[0] = fmaxf(hi[0], th[u].x);
+                    lo[1] = fminf(lo[1], th[u].y); hi[1] = fmaxf(hi[1], th[u].y);
+                    lo[2] = fminf(lo[2], th[u].z); hi[2] = fmaxf(hi[2], th[u].z);
+                }
+            }
+            // target boxes of the warps and of the pass, widened by the FP32
+            // rounding of the hi-part coordinates (relative 2^-23)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                    hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                }
+            __syncthreads();  // the previous pass is done with s_wbox
+            if (lane == 0)
+                for (int d = 0; d < 3; ++d) {
+                    const float pad = 2.5e-7f * fmaxf(fabsf(lo[d]), fabsf(hi[d])) + 1e-30f;
+                    s_wbox[warp][d] = lo[d] - pad;
+                    s_wbox[warp][3 + d] = hi[d] + pad;
+                }
+            __syncthreads();
+            float wbox[6], cbox[6];
+            for (int d = 0; d < 6; ++d) wbox[d] = s_wbox[warp][d];
+            for (int d = 0; d < 3; ++d) {
+                cbox[d] = fminf(fminf(s_wbox[0][d], s_wbox[1][d]), fminf(s_wbox[2][d], s_wbox[3][d]));
+                cbox[3 + d] = fmaxf(fmaxf(s_wbox[0][3 + d], s_wbox[1][3 + d]), fmaxf(s_wbox[2][3 + d], s_wbox[3][3 + d]));
             }
             for (int pr = a.pair_start[e]; pr < a.pair_start[e + 1]; ++pr) {
                 const int s0 = a.pair_src_start[pr], ns = a.pair_src_count[pr];
                 const double bd = a.pair_bsize[pr];
                 const float d2max = (float)(bd * bd), rsc = (float)(2.0 / bd), cen = (float)(-0.5 * bd);
+                const float keep2 = d2max * 1.00001f;
+                const int cbase = a.pair_chunk_base[pr];
                 float part[TPT][KB];
 #pragma unroll
                 for (int u = 0; u < TPT; ++u)
 #pragma unroll
                     for (int q = 0; q < KB; ++q) part[u][q] = 0.f;
                 for (int sb = 0; sb < ns; sb += 128) {
+                    // 32-source chunks of this block within b of the pass's targets
+                    // (the same answer in every thread: the skip is uniform)
+                    const int nchk = min(4, (ns - sb + 31) / 32);
+                    unsigned need = 0;
+                    for (int k = 0; k < nchk; ++k) {
+                        const int c = cbase + (sb >> 5) + k;
+                        if (chunk_gap2(__ldg(a.chunk_lo + c), __ldg(a.chunk_hi + c), cbox) <= keep2) need |= 1u << k;
+                    }
+                    if (!need) continue;
                     __syncthreads();
                     const int js = sb + threadIdx.x;
-                    if (js < ns) {
+                    if (js < ns && ((need >> (threadIdx.x >> 5)) & 1u)) {
                         sh[threadIdx.x] = src_hi[s0 + js];
                         sl[threadIdx.x] = src_lo[s0 + js];
 #pragma unroll
@@ -524,7 +577,15 @@ __global__ void __launch_bounds__(128) k_near_m32(NearM a, const float4* __restr
                     }
                     __syncthreads();
                     const int m = min(128, ns - sb);
-                    for (int j = 0; j < m; ++j) {
+                    for (int k = 0; k < nchk; ++k) {
+                    if (!((need >> k) & 1u)) continue;
+                    {
+                        const int c = cbase + (sb >> 5) + k;
+                        // this warp's targets against the chunk (warp-uniform)
+                        if (chunk_gap2(__ldg(a.chunk_lo + c), __ldg(a.chunk_hi + c), wbox) > keep2) continue;
+                    }
+                    const int je = min(m, 32 * k + 32);
+                    for (int j = 32 * k; j < je; ++j) {
                         const float4 yh = sh[j], yl = sl[j];
 #pragma unroll
                         for (int u = 0; u < TPT; ++u) {
@@ -543,6 +604,7 @@ __global__ void __launch_bounds__(128) k_near_m32(NearM a, const float4* __restr
                                 for (int q = 0; q < KB; ++q) part[u][q] = fmaf(w, sq[j][q], part[u][q]);
                             }
                         }
+                    }
                     }
                 }
 #pragma unroll
@@ -1254,6 +1316,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         a.trg_start = near_.trg_start; a.trg_count = near_.trg_count; a.pair_start = near_.pair_start;
         a.pair_src_start = near_.pair_src_start; a.pair_src_count = near_.pair_src_count;
         a.pair_bsize = near_.pair_bsize; a.n_leaves = near_.n_leaves; a.N = n_; a.kb = kb;
+        a.pair_chunk_base = near_.pair_chunk_base; a.chunk_lo = near_.chunk_lo; a.chunk_hi = near_.chunk_hi;
         for (int i = 0; i < near_.nc; ++i) a.coef[i] = near_.coef[i];
         bool tc_done = false;
         if constexpr (f32) {
