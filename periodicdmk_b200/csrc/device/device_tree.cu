@@ -105,6 +105,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
     if (const char* tm = std::getenv("PDMK_TC_MASK")) tc_mask_ = std::atoi(tm) & 15;
     if (const char* dm = std::getenv("PDMK_FP64_DMMA")) fp64_dmma_ = std::atoi(dm) != 0;
     if (const char* mm = std::getenv("PDMK_MOMENTS_DMMA")) moments_dmma_ = std::atoi(mm) != 0;
+    if (const char* ov = std::getenv("PDMK_E2E_OVERLAP")) overlap_h2d_ = std::atoi(ov) != 0;
     n_ = P.n_src;
     n_digits_ = P.dp.n_digits_tree;
     n_all_ = P.n_all;

@@ -5,6 +5,7 @@
 #include <cufft.h>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -120,6 +121,20 @@ class DeviceTree {
     MultiState& multi_state(int kb, bool fp32);
     template <typename T>
     void run_multi_block(MultiState& m, const double* Q, int kvalid, double* pot_user);
+    // far field of the columns [c0, c0 + cols) of a multi-RHS block (q_t -> far)
+    int far_columns(MultiState& m, int c0, int cols, bool qp, cufftHandle fwd, cufftHandle inv, cudaStream_t s);
+    // Host-buffer multi-RHS evaluate with the charge upload in column chunks:
+    // upload(c0, cols) enqueues a chunk's copy on stream_; the far field of each
+    // chunk runs on a second stream as soon as it has arrived, the tree passes
+    // after the last chunk.  False when the shape does not allow it (nothing
+    // enqueued then).
+    bool multi_host_overlapped(int k, bool fp32, double* qd, double* pd,
+                               const std::function<void(int, int)>& upload);
+    // run_multi_block leaves the far field (and the target-charge gather) to
+    // the caller, whose work is complete at far_ext_event_
+    bool far_ext_ = false;
+    cudaEvent_t far_ext_event_ = nullptr;
+    int overlap_h2d_ = 1;  // PDMK_E2E_OVERLAP=0 keeps the upload in one copy before the evaluate
     std::unique_ptr<MultiState, MultiStateDeleter> multi_[2];
     StageTimes last_multi_{};
     // device staging of the host-buffer multi-RHS calls (grow-only, freed with the tree)

@@ -929,6 +929,12 @@ struct DeviceTree::MultiState {
     double* grid = nullptr;
     cd* spec = nullptr;
     cufftHandle fwd = 0, inv = 0;
+    // overlapped host evaluates: far field of column chunks on a second stream
+    cudaStream_t far_stream = nullptr;
+    cufftHandle fwd_c = 0, inv_c = 0;  // batched plans over one chunk of columns
+    int chunk_cols = 0;
+    std::vector<cudaEvent_t> ev_chunk;  // chunk c's charges are on the device
+    cudaEvent_t ev_far0 = nullptr, ev_far = nullptr;  // far-stream work begins / is done
     // FP32 copies of tables and positions
     float* c2p = nullptr;
     float* p2c = nullptr;
@@ -954,6 +960,13 @@ struct DeviceTree::MultiState {
     ~MultiState() {
         if (fwd) cufftDestroy(fwd);
         if (inv) cufftDestroy(inv);
+        if (fwd_c) cufftDestroy(fwd_c);
+        if (inv_c) cufftDestroy(inv_c);
+        if (far_stream) cudaStreamSynchronize(far_stream);
+        for (cudaEvent_t e : ev_chunk) cudaEventDestroy(e);
+        if (ev_far0) cudaEventDestroy(ev_far0);
+        if (ev_far) cudaEventDestroy(ev_far);
+        if (far_stream) cudaStreamDestroy(far_stream);
         for (void* p : allocs) cudaFree(p);
     }
 };
@@ -1105,8 +1118,8 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     if (qp_ && !qp) require_periodic("evaluate_multi");
     if (qp && (kb != 2 || kvalid != 1)) throw std::logic_error("quasi-periodic evaluate: two-column state expected");
     int nl = 0;
+    if (far_ext_ && qp) throw std::logic_error("quasi-periodic evaluate with an external far field");
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[0], s));
-    PDMK_CUDA_CHECK(cudaMemsetAsync(m.pot, 0, sizeof(double) * n_ * kb, s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(up, 0, sizeof(T) * std::max<int64_t>(n_up_ * ncoef * kb, 1), s));
     PDMK_CUDA_CHECK(cudaMemsetAsync(down, 0, sizeof(T) * std::max<int64_t>(n_down_ * ncoef * kb, 1), s));
     if (qp) {
@@ -1116,16 +1129,19 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
                                trg_perm_, qp_trg_phase_, n_, Q, s);
         nl += 2;
     } else {
-        // charges to row-major (the far-field output buffer is free until the
-        // interpolation writes it), then one contiguous row per source
+        // charges to row-major (the potential buffer is free until it is zeroed
+        // below), then one contiguous row per source
         const int64_t tot = (int64_t)n_all_ * kb;
         const dim3 tgrid((unsigned)((n_ + 31) / 32), (unsigned)((kb + 31) / 32));
-        dev::k_transpose_q<<<tgrid, dim3(32, 8), 0, s>>>(Q, m.far, n_, kb, kvalid); ++nl;
-        dev::k_gather_src_rows<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src_q, src_charge_idx_, m.far, n_all_,
+        dev::k_transpose_q<<<tgrid, dim3(32, 8), 0, s>>>(Q, m.pot, n_, kb, kvalid); ++nl;
+        dev::k_gather_src_rows<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src_q, src_charge_idx_, m.pot, n_all_,
                                                                                 kb); ++nl;
-        const int64_t tt = (int64_t)n_ * kb;
-        dev::k_gather_trg_m<<<(unsigned)((tt + 255) / 256), 256, 0, s>>>(m.q_t, trg_perm_, Q, n_, kb, kvalid); ++nl;
+        if (!far_ext_) {
+            const int64_t tt = (int64_t)n_ * kb;
+            dev::k_gather_trg_m<<<(unsigned)((tt + 255) / 256), 256, 0, s>>>(m.q_t, trg_perm_, Q, n_, kb, kvalid); ++nl;
+        }
     }
+    PDMK_CUDA_CHECK(cudaMemsetAsync(m.pot, 0, sizeof(double) * n_ * kb, s));
     // proxy moments: tensor-core GEMM (FP32 blocks of >= 16 RHS), else per-RHS CUDA-core kernel
     if (c2x_.n_centers > 0) {
         bool done = false;
@@ -1369,34 +1385,12 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         ++nl;
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[2], s));
-    // far field, FP64, all rhs of the block at once
-    {
-        dev::NufftArgs na = nufft_;
-        na.q_sorted = m.q_t;
-        na.grid = m.grid;
-        na.far = m.far;
-        na.rhs_q_stride = n_;
-        na.rhs_grid_stride = n_grid_;
-        na.rhs_far_stride = n_;
-        PDMK_CUDA_CHECK(cudaMemsetAsync(m.grid, 0, sizeof(double) * n_grid_ * kb, s));
-        // mixed precision: spreading with single-precision taps and partial
-        // sums into the FP64 grid; transforms and interpolation stay FP64
-        // (single-precision interpolation sums lost accuracy for no speed)
-        bool spread32 = false;
-        if constexpr (f32) spread32 = dev::launch_spread_multi_f32(na, m.esw32, kb, s);
-        if (!spread32) dev::launch_spread_multi(na, m.esw, nufft_max_jk_, nufft_max_ex_, kb, s);
-        ++nl;
-        if (cufftExecD2Z(m.fwd, m.grid, reinterpret_cast<cufftDoubleComplex*>(m.spec)) != CUFFT_SUCCESS)
-            throw std::runtime_error("cuFFT error in the batched forward transform");
-        if (qp)
-            dev::launch_qp_combine(m.spec, qp_s_, qp_d_, n_spec_, s);
-        else
-            dev::launch_multiply(m.spec, mult_, n_spec_, s, kb);
-        ++nl;
-        if (cufftExecZ2D(m.inv, reinterpret_cast<cufftDoubleComplex*>(m.spec), m.grid) != CUFFT_SUCCESS)
-            throw std::runtime_error("cuFFT error in the batched inverse transform");
-        dev::launch_interp_multi(na, m.esw, n_, kb, s); ++nl;
-    }
+    // far field, FP64, all rhs of the block at once (or, in an overlapped host
+    // evaluate, already enqueued on the far-field stream by column chunks)
+    if (far_ext_)
+        PDMK_CUDA_CHECK(cudaStreamWaitEvent(s, far_ext_event_, 0));
+    else
+        nl += far_columns(m, 0, kb, qp, m.fwd, m.inv, s);
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
     if (qp) {
         dev::launch_qp_finalize(m.pot, m.far, trg_, trg_perm_, Q, qp_trg_phase_, pot_user, n_, s); ++nl;
@@ -1433,6 +1427,105 @@ void DeviceTree::near_leaf_sys(dev::NearLeafSys& d, double* out) const {
     d.perm = trg_perm_;
     d.q_t = m->q_t;
     d.out = out;
+}
+
+int DeviceTree::far_columns(MultiState& m, int c0, int cols, bool qp, cufftHandle fwd, cufftHandle inv,
+                            cudaStream_t s) {
+    dev::NufftArgs na = nufft_;
+    na.q_sorted = m.q_t + (int64_t)c0 * n_;
+    na.grid = m.grid + (int64_t)c0 * n_grid_;
+    na.far = m.far + (int64_t)c0 * n_;
+    na.rhs_q_stride = n_;
+    na.rhs_grid_stride = n_grid_;
+    na.rhs_far_stride = n_;
+    cd* spec = m.spec + (int64_t)c0 * n_spec_;
+    PDMK_CUDA_CHECK(cudaMemsetAsync(na.grid, 0, sizeof(double) * n_grid_ * cols, s));
+    // mixed precision: spreading with single-precision taps and partial sums
+    // into the FP64 grid; transforms and interpolation stay FP64
+    // (single-precision interpolation sums lost accuracy for no speed)
+    bool spread32 = false;
+    if (m.fp32) spread32 = dev::launch_spread_multi_f32(na, m.esw32, cols, s);
+    if (!spread32) dev::launch_spread_multi(na, m.esw, nufft_max_jk_, nufft_max_ex_, cols, s);
+    if (cufftExecD2Z(fwd, na.grid, reinterpret_cast<cufftDoubleComplex*>(spec)) != CUFFT_SUCCESS)
+        throw std::runtime_error("cuFFT error in the batched forward transform");
+    if (qp)
+        dev::launch_qp_combine(spec, qp_s_, qp_d_, n_spec_, s);
+    else
+        dev::launch_multiply(spec, mult_, n_spec_, s, cols);
+    if (cufftExecZ2D(inv, reinterpret_cast<cufftDoubleComplex*>(spec), na.grid) != CUFFT_SUCCESS)
+        throw std::runtime_error("cuFFT error in the batched inverse transform");
+    dev::launch_interp_multi(na, m.esw, n_, cols, s);
+    return 3;
+}
+
+bool DeviceTree::multi_host_overlapped(int k, bool fp32, double* qd, double* pd,
+                                       const std::function<void(int, int)>& upload) {
+    constexpr int kChunkCols = 8;
+    fp32 = fp32 && mixed_allowed();
+    if (!overlap_h2d_ || qp_ || k < 2 * kChunkCols || k % kChunkCols != 0) return false;
+    if (multi_block(k, fp32) < k) return false;  // one block of k columns only
+    MultiState& m = multi_state(multi_block(k, fp32), fp32);
+    if (!m.far_stream) {
+        PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&m.far_stream, cudaStreamNonBlocking));
+        PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&m.ev_far, cudaEventDisableTiming));
+        PDMK_CUDA_CHECK(cudaEventCreate(&m.ev_far0));
+        int dims[3] = {nufft_.n1, nufft_.n2, nufft_.n3};
+        const cufftResult r1 = cufftPlanMany(&m.fwd_c, 3, dims, nullptr, 1, (int)n_grid_, nullptr, 1, (int)n_spec_,
+                                             CUFFT_D2Z, kChunkCols);
+        const cufftResult r2 = cufftPlanMany(&m.inv_c, 3, dims, nullptr, 1, (int)n_spec_, nullptr, 1, (int)n_grid_,
+                                             CUFFT_Z2D, kChunkCols);
+        if (r1 != CUFFT_SUCCESS || r2 != CUFFT_SUCCESS) throw std::runtime_error("cuFFT error: chunk plan creation failed");
+        cufftSetStream(m.fwd_c, m.far_stream);
+        cufftSetStream(m.inv_c, m.far_stream);
+        m.chunk_cols = kChunkCols;
+    }
+    const int nch = k / m.chunk_cols;
+    while ((int)m.ev_chunk.size() < nch) {
+        cudaEvent_t e;
+        PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        m.ev_chunk.push_back(e);
+    }
+    multi_launches_ = 0;
+    // uploads, in order, on the main stream
+    for (int c = 0; c < nch; ++c) {
+        upload(c * m.chunk_cols, m.chunk_cols);
+        PDMK_CUDA_CHECK(cudaEventRecord(m.ev_chunk[c], stream_));
+    }
+    // the far field of each chunk as soon as it is in
+    cudaStream_t fs = m.far_stream;
+    for (int c = 0; c < nch; ++c) {
+        const int c0 = c * m.chunk_cols, cols = m.chunk_cols;
+        PDMK_CUDA_CHECK(cudaStreamWaitEvent(fs, m.ev_chunk[c], 0));
+        if (c == 0) PDMK_CUDA_CHECK(cudaEventRecord(m.ev_far0, fs));
+        const int64_t tt = (int64_t)n_ * cols;
+        dev::k_gather_trg_m<<<(unsigned)((tt + 255) / 256), 256, 0, fs>>>(m.q_t + (int64_t)c0 * n_, trg_perm_,
+                                                                          qd + (int64_t)c0 * n_, n_, cols, cols);
+        multi_launches_ += 1 + far_columns(m, c0, cols, false, m.fwd_c, m.inv_c, fs);
+    }
+    PDMK_CUDA_CHECK(cudaEventRecord(m.ev_far, fs));
+    // the tree passes, near field and finalize on the main stream
+    struct Ext {
+        DeviceTree& t;
+        Ext(DeviceTree& x, cudaEvent_t e) : t(x) { t.far_ext_ = true; t.far_ext_event_ = e; }
+        ~Ext() { t.far_ext_ = false; t.far_ext_event_ = nullptr; }
+    } ext(*this, m.ev_far);
+    if (fp32)
+        run_multi_block<float>(m, qd, k, pd);
+    else
+        run_multi_block<double>(m, qd, k, pd);
+    StageTimes t = last_times();
+    float far_ms = 0.0f;
+    PDMK_CUDA_CHECK(cudaEventElapsedTime(&far_ms, m.ev_far0, ev_[4]));
+    t.nufft_ms = far_ms;  // far-field stream from its first chunk to the finalize (overlaps the rest)
+    int err = 0;
+    PDMK_CUDA_CHECK(cudaMemcpy(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        PDMK_CUDA_CHECK(cudaMemset(m.err, 0, sizeof(int)));
+        throw std::runtime_error("CUDA error: tensor-core pipeline wait timed out in the multi-RHS evaluate");
+    }
+    last_multi_ = t;
+    last_was_multi_ = true;
+    return true;
 }
 
 void DeviceTree::evaluate_multi_device(const double* Q, int k, double* pot, bool fp32, StageTimes* times) {
@@ -1577,9 +1670,15 @@ void DeviceTree::evaluate_multi_host_f32(const float* Q, int k, float* pot, bool
     // are widened into the charge staging buffer, and the float potentials
     // are narrowed into the charge buffer after the evaluate
     float* qf = reinterpret_cast<float*>(stage_p_) + n;
-    PDMK_CUDA_CHECK(cudaMemcpyAsync(qf, Q, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, stream_));
-    dev::k_to_double_in<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(qf, stage_q_, n);
-    evaluate_multi_device(stage_q_, k, stage_p_, fp32, nullptr);
+    auto upload = [&](int c0, int cols) {
+        const int64_t o = (int64_t)c0 * n_, m = (int64_t)cols * n_;
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(qf + o, Q + o, sizeof(float) * (size_t)m, cudaMemcpyHostToDevice, stream_));
+        dev::k_to_double_in<<<(unsigned)((m + 255) / 256), 256, 0, stream_>>>(qf + o, stage_q_ + o, m);
+    };
+    if (!multi_host_overlapped(k, fp32, stage_q_, stage_p_, upload)) {
+        upload(0, k);
+        evaluate_multi_device(stage_q_, k, stage_p_, fp32, nullptr);
+    }
     float* pf = reinterpret_cast<float*>(stage_q_);
     dev::k_to_float_out<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(stage_p_, pf, n);
     PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pf, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, stream_));
@@ -1595,8 +1694,16 @@ void DeviceTree::evaluate_multi_host(const double* Q, int k, void* pot, bool pot
     ensure_stage(n);
     double* qd = stage_q_;
     double* pd = stage_p_;
-    PDMK_CUDA_CHECK(cudaMemcpyAsync(qd, Q, bytes, cudaMemcpyHostToDevice, stream_));
-    evaluate_multi_device(qd, k, pd, fp32, times);
+    auto upload = [&](int c0, int cols) {
+        const int64_t o = (int64_t)c0 * n_;
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(qd + o, Q + o, sizeof(double) * (size_t)cols * n_, cudaMemcpyHostToDevice,
+                                        stream_));
+    };
+    // stage times asked for: one upload, then the stages in sequence
+    if (times || !multi_host_overlapped(k, fp32, qd, pd, upload)) {
+        upload(0, k);
+        evaluate_multi_device(qd, k, pd, fp32, times);
+    }
     if (pot_float) {
         // reuse the charge buffer for the float copy of the potentials
         float* pf = reinterpret_cast<float*>(qd);

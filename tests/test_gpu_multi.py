@@ -196,3 +196,39 @@ def test_tensor_core_transforms(nd, tol, monkeypatch):
     print("PARITY " + json.dumps({"case": "tcgen05 transforms %d digits" % nd, "max_rel_l2_tc": max(errs),
                                   "max_rel_l2_cuda_core": max(errs_cc)}))
     assert max(errs) < tol, (int(np.argmax(errs)), max(errs))
+
+
+@pytest.mark.parametrize("precision", ["float", "double"])
+def test_overlapped_upload_equals_one_upload(precision, monkeypatch):
+    # Host-buffer calls with k a multiple of 8 (and >= 16) upload the charges in
+    # 8-column chunks and run each chunk's far field on a second stream while
+    # the next chunk is copied; the tree passes start after the last chunk.
+    # Against the same call with one upload and the stages in sequence
+    # (PDMK_E2E_OVERLAP=0): the far field's FFTs run in batches of 8 instead of
+    # k, everything else is the same arithmetic.
+    cell, pos, _ = clustered_system(30000, 61, TRICLINIC, n_clusters=4, sigma=0.02)
+    Q = _charges(len(pos), 24, 62)
+    res = {}
+    for ov in ("0", "1"):
+        monkeypatch.setenv("PDMK_E2E_OVERLAP", ov)
+        t = pd.PeriodicDMKTree(cell, pos, 6, 60, 4, precision=precision)
+        a = t.evaluate_multi(Q)
+        b = t.evaluate_multi(Q)  # a second call reuses the chunk plans and streams
+        f = t.evaluate_multi_f32(Q.astype(np.float32)) if precision == "float" else None
+        res[ov] = (a, b, f)
+        t.close()
+    a0, _, f0 = res["0"]
+    a1, b1, f1 = res["1"]
+    for c in range(Q.shape[1]):
+        assert rel_l2(a1[:, c], a0[:, c]) < 1e-12
+        assert rel_l2(b1[:, c], a1[:, c]) < 1e-12
+        if f0 is not None:
+            assert rel_l2(f1[:, c], f0[:, c]) < 1e-6
+    # a width that is not a multiple of 8 takes the one-upload path
+    monkeypatch.setenv("PDMK_E2E_OVERLAP", "1")
+    t = pd.PeriodicDMKTree(cell, pos, 6, 60, 4, precision=precision)
+    c = t.evaluate_multi(Q[:, :19])
+    t.close()
+    tol = 1e-12 if precision == "double" else 2e-7  # FP32 blocks of another width
+    for j in range(19):
+        assert rel_l2(c[:, j], a0[:, j]) < tol
