@@ -430,15 +430,30 @@ class PeriodicDMKBatch:
         return {"n_systems": int(out[0]), "n_points": int(out[1]), "device_bytes": int(out[2]),
                 "float_trees": bool(out[3])}
 
-    def evaluate(self, charges, out_dtype=np.float64):
-        q = np.ascontiguousarray(np.concatenate([np.asarray(c, dtype=np.float64) for c in charges]))
-        if q.shape != (int(self.offsets[-1]),):
+    def evaluate(self, charges, out_dtype=np.float64, out=None):
+        """charges: a sequence of per-system charge vectors, or one float64 array
+        of all systems' charges concatenated (used without a copy).  out: an
+        optional preallocated array of all potentials (out_dtype, concatenated)
+        that is written in place.  Returns the per-system potentials (views of
+        the concatenated output)."""
+        total = int(self.offsets[-1])
+        if isinstance(charges, np.ndarray) and charges.ndim == 1:
+            q = np.ascontiguousarray(charges, dtype=np.float64)
+        else:
+            q = np.ascontiguousarray(np.concatenate([np.asarray(c, dtype=np.float64) for c in charges]))
+        if q.shape != (total,):
             raise ValueError("charges must match the systems' point counts")
+        out_dtype = np.dtype(out_dtype)
+        if out_dtype not in (np.dtype(np.float32), np.dtype(np.float64)):
+            raise ValueError("out_dtype must be float32 or float64")
+        if out is None:
+            out = np.empty(total, dtype=out_dtype)
+        elif (not isinstance(out, np.ndarray) or out.shape != (total,) or out.dtype != out_dtype
+              or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError("out must be a writeable contiguous (total,) array of out_dtype")
         if out_dtype == np.float32:
-            out = np.empty(q.shape[0], dtype=np.float32)
             rc = self._lib.pdmk_batch_evaluate_float(self._h, _ptr(q), _ptr(out, _F))
         else:
-            out = np.empty(q.shape[0], dtype=np.float64)
             rc = self._lib.pdmk_batch_evaluate(self._h, _ptr(q), _ptr(out))
         if rc != 0:
             raise RuntimeError("pdmk_batch_evaluate failed (code %d): %s" % (rc, _last_error()))

@@ -7,6 +7,9 @@
 // copy of all charges, every system's evaluate enqueued on its own stream
 // after that copy (replayed from a CUDA graph from the second evaluate on), one
 // device->host copy of all potentials after every system has finished.
+// Pageable host buffers pass through pinned staging buffers, filled and
+// drained by up to 8 host threads (a pageable cudaMemcpy moves 3-10 GB/s);
+// page-locked ones are copied directly.
 // Float trees (one charge vector per system) leave their near field and final
 // gather out of the per-system sequences: after all systems' other stages one
 // persistent kernel pulls (system, leaf) items from a device queue, largest
@@ -19,6 +22,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
 #include <exception>
 #include <map>
 #include <mutex>
@@ -95,6 +101,9 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         if (first_error) std::rethrow_exception(first_error);
         PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
+        profile_ = std::getenv("PDMK_BATCH_PROFILE") != nullptr;
+        if (profile_)
+            for (auto& e : prof_) PDMK_CUDA_CHECK(cudaEventCreate(&e));
         done_.assign(nsys, nullptr);
         for (auto& e : done_) PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         const size_t n = (size_t)total_points();
@@ -102,6 +111,8 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         PDMK_CUDA_CHECK(cudaMalloc(&pot_dev_, sizeof(double) * n));
         PDMK_CUDA_CHECK(cudaMalloc(&potf_dev_, sizeof(float) * n));
         PDMK_CUDA_CHECK(cudaMallocHost(&err_host_, sizeof(int) * nsys));
+        PDMK_CUDA_CHECK(cudaMallocHost(&q_pin_, sizeof(double) * n));
+        PDMK_CUDA_CHECK(cudaMallocHost(&p_pin_, sizeof(double) * n));
         graphs_.assign(nsys, nullptr);
         if (single_) {
             for (auto& t : trees_) t->defer_near_ = true;
@@ -136,11 +147,16 @@ void TreeBatch::release() {
     graphs_.clear();
     if (err_host_) cudaFreeHost(err_host_);
     err_host_ = nullptr;
+    if (q_pin_) cudaFreeHost(q_pin_);
+    if (p_pin_) cudaFreeHost(p_pin_);
+    q_pin_ = p_pin_ = nullptr;
     trees_.clear();
     for (auto& e : done_)
         if (e) cudaEventDestroy(e);
     done_.clear();
     if (ready_) cudaEventDestroy(ready_);
+    for (auto& e : prof_)
+        if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
     if (q_dev_) cudaFree(q_dev_);
     if (pot_dev_) cudaFree(pot_dev_);
@@ -165,12 +181,54 @@ size_t TreeBatch::device_bytes() const {
     return b;
 }
 
+namespace {
+// page-locked (or device-registered) host memory: copied by DMA directly
+bool pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy on up to 8 host threads (pageable <-> pinned staging)
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>({8, hw, std::max<size_t>(1, bytes >> 22)});
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nt; ++t) {
+        const size_t o = t * part;
+        if (o >= bytes) break;
+        const size_t b = std::min(part, bytes - o);
+        th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, b); });
+    }
+    for (auto& x : th) x.join();
+}
+}  // namespace
+
 void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
     if (!charges || !pot) throw std::invalid_argument("null charges or output");
     PDMK_CUDA_CHECK(cudaSetDevice(device_));
     const int64_t n = total_points();
-    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, charges, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    const auto h0 = std::chrono::steady_clock::now();
+    if (profile_) PDMK_CUDA_CHECK(cudaEventRecord(prof_[0], stream_));
+    // pageable buffers go through the pinned staging: a host-threaded copy
+    // and one DMA transfer each way (a pageable cudaMemcpy is far slower)
+    const bool q_pinned = pinned(charges), p_pinned = pinned(pot);
+    const double* q_src = charges;
+    if (!q_pinned) {
+        parallel_copy(q_pin_, charges, sizeof(double) * n);
+        q_src = q_pin_;
+    }
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, q_src, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     PDMK_CUDA_CHECK(cudaEventRecord(ready_, stream_));
+    if (profile_) PDMK_CUDA_CHECK(cudaEventRecord(prof_[1], stream_));
     // The first evaluate runs the systems directly (it creates their multi-RHS
     // state); the second captures each system's launch sequence into a CUDA
     // graph (device buffers and tables are fixed per system), later ones
@@ -211,12 +269,18 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
         PDMK_CUDA_CHECK(cudaEventRecord(done_[i], ts));
         PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
     }
+    const auto h1 = std::chrono::steady_clock::now();
+    const bool prof = profile_;
+    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[2], stream_));
     if (single_) run_queue();
+    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[3], stream_));
+    const size_t pbytes = (pot_float ? sizeof(float) : sizeof(double)) * (size_t)n;
+    void* p_dst = p_pinned ? pot : static_cast<void*>(p_pin_);
     if (pot_float) {
         dev::launch_to_float(pot_dev_, potf_dev_, n, stream_);
-        PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, potf_dev_, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_));
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(p_dst, potf_dev_, pbytes, cudaMemcpyDeviceToHost, stream_));
     } else {
-        PDMK_CUDA_CHECK(cudaMemcpyAsync(pot, pot_dev_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(p_dst, pot_dev_, pbytes, cudaMemcpyDeviceToHost, stream_));
     }
     // error words of the tensor-core kernels: one asynchronous copy each, one wait
     int n_err = 0;
@@ -230,8 +294,19 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
             }
         }
     }
+    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[4], stream_));
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
     PDMK_CUDA_CHECK(cudaGetLastError());
+    const auto h2 = std::chrono::steady_clock::now();
+    if (!p_pinned) parallel_copy(pot, p_pin_, pbytes);
+    if (prof) {
+        float ms[4];
+        for (int i = 0; i < 4; ++i) PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms[i], prof_[i], prof_[i + 1]));
+        const double enq = std::chrono::duration<double, std::milli>(h1 - h0).count();
+        const double out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h2).count();
+        std::fprintf(stderr, "pdmk batch: upload %.2f ms, systems %.2f ms (host staging + enqueue %.2f ms), queue %.2f ms, "
+                             "download %.2f ms + host copy %.2f ms\n", ms[0], ms[1], enq, ms[2], ms[3], out);
+    }
     ++evaluates_;
     if (n_err)
         for (size_t i = 0; i < trees_.size(); ++i)

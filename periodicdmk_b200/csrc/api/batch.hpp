@@ -36,10 +36,16 @@ class TreeBatch {
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ready_ = nullptr;
+    // PDMK_BATCH_PROFILE: per-evaluate phase times on stderr (upload, systems, queue, download)
+    bool profile_ = false;
+    cudaEvent_t prof_[5]{};
     std::vector<cudaEvent_t> done_;
     double* q_dev_ = nullptr;
     double* pot_dev_ = nullptr;
     float* potf_dev_ = nullptr;
+    // pinned staging of pageable host buffers (filled and drained by host threads)
+    double* q_pin_ = nullptr;
+    double* p_pin_ = nullptr;
     // after the first evaluate, each system's evaluate is replayed from a CUDA graph
     std::vector<cudaGraphExec_t> graphs_;
     int* err_host_ = nullptr;  // pinned, one word per system

@@ -30,6 +30,23 @@ def test_mixed_batch_matches_single_trees():
     again = b.evaluate(qs)
     for u, v in zip(out, again):
         assert rel_l2(v, u) < 1e-12
+    # concatenated charges and a preallocated output (written in place)
+    flat = np.concatenate(qs)
+    buf = np.full(flat.shape[0], np.nan)
+    views = b.evaluate(flat, out=buf)
+    assert np.all(np.isfinite(buf))
+    for u, v in zip(out, views):
+        assert rel_l2(v, u) < 1e-12
+    # page-locked host buffers are copied by DMA directly (no staging)
+    import torch
+
+    qp = torch.from_numpy(flat).pin_memory()
+    pp = torch.empty(flat.shape[0], dtype=torch.float64).pin_memory()
+    b.evaluate(qp.numpy(), out=pp.numpy())
+    for i, u in enumerate(out):
+        assert rel_l2(pp.numpy()[b.offsets[i]:b.offsets[i + 1]], u) < 1e-12
+    with pytest.raises(ValueError):
+        b.evaluate(flat, out=np.empty(flat.shape[0], dtype=np.float32))
     b.close()
 
 
