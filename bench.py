@@ -476,6 +476,24 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
 
+    if args.batch_only:
+        dev = torch.device("cuda", local)
+
+        def max_over_b(x):
+            if dist is None:
+                return x
+            tt = torch.tensor([x], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            return float(tt.item())
+
+        out = run_batch(pd, args, world, rank, (dist.barrier if dist is not None else (lambda: None)), max_over_b)
+        if rank == 0:
+            print(json.dumps({"batch": out, "n_gpus": world, "steps": args.steps, "warmup": args.warmup}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
     n, k = args.n, args.rhs
     cell, pos, q = make_system(n, seed=1)
     rng = np.random.default_rng(7)
@@ -716,6 +734,8 @@ def main():
                     help="time only the CPU oracle on bounded samples of every workload (JSON line)")
     ap.add_argument("--clustered-only", action="store_true",
                     help="run only the clustered triclinic FP64 measurement (its JSON fragment alone)")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run only the many-systems measurement of --batch-systems systems (its JSON fragment alone)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
