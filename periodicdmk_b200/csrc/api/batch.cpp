@@ -129,6 +129,20 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
             PDMK_CUDA_CHECK(cudaMalloc(&items_dev_, sizeof(int2) * std::max<size_t>(it.size(), 1)));
             PDMK_CUDA_CHECK(cudaMemcpy(items_dev_, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
             PDMK_CUDA_CHECK(cudaMalloc(&sys_dev_, sizeof(dev::NearLeafSys) * nsys));
+            // leaf-evaluation items: every system's evaluated leaves, most targets first
+            std::vector<std::tuple<int, int, int>> ev;
+            for (int i = 0; i < nsys; ++i) {
+                const auto& nt = trees_[i]->eval_leaf_targets();
+                for (int e = 0; e < trees_[i]->eval_leaves(); ++e) ev.emplace_back(-nt[e], i, e);
+            }
+            std::stable_sort(ev.begin(), ev.end());
+            std::vector<int2> ei(ev.size());
+            for (size_t k = 0; k < ev.size(); ++k) ei[k] = make_int2(std::get<1>(ev[k]), std::get<2>(ev[k]));
+            n_eitems_ = (int)ei.size();
+            PDMK_CUDA_CHECK(cudaMalloc(&eitems_dev_, sizeof(int2) * std::max<size_t>(ei.size(), 1)));
+            PDMK_CUDA_CHECK(cudaMemcpy(eitems_dev_, ei.data(), sizeof(int2) * ei.size(), cudaMemcpyHostToDevice));
+            PDMK_CUDA_CHECK(cudaMalloc(&esys_dev_, sizeof(dev::EvalLeafSys) * nsys));
+            p_ = trees_[0]->expansion_order();
             PDMK_CUDA_CHECK(cudaMalloc(&head_dev_, sizeof(int)));
             nc_ = trees_[0]->near_coeffs();
             for (int i = 0; i < nc_; ++i) coef32_[i] = (float)trees_[0]->near_coef()[i];
@@ -162,6 +176,10 @@ void TreeBatch::release() {
     if (pot_dev_) cudaFree(pot_dev_);
     if (potf_dev_) cudaFree(potf_dev_);
     if (sys_dev_) cudaFree(sys_dev_);
+    if (esys_dev_) cudaFree(esys_dev_);
+    if (eitems_dev_) cudaFree(eitems_dev_);
+    esys_dev_ = nullptr;
+    eitems_dev_ = nullptr;
     if (items_dev_) cudaFree(items_dev_);
     if (head_dev_) cudaFree(head_dev_);
     sys_dev_ = nullptr;
@@ -272,8 +290,15 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
     const auto h1 = std::chrono::steady_clock::now();
     const bool prof = profile_;
     if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[2], stream_));
-    if (single_) run_queue();
-    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[3], stream_));
+    if (single_) {
+        if (!queue_built_) build_queue();
+        dev::launch_batch_eval(esys_dev_, eitems_dev_, n_eitems_, p_, stream_);
+        if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[3], stream_));
+        run_queue();
+    } else if (prof) {
+        PDMK_CUDA_CHECK(cudaEventRecord(prof_[3], stream_));
+    }
+    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[4], stream_));
     const size_t pbytes = (pot_float ? sizeof(float) : sizeof(double)) * (size_t)n;
     void* p_dst = p_pinned ? pot : static_cast<void*>(p_pin_);
     if (pot_float) {
@@ -294,18 +319,19 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
             }
         }
     }
-    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[4], stream_));
+    if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[5], stream_));
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
     PDMK_CUDA_CHECK(cudaGetLastError());
     const auto h2 = std::chrono::steady_clock::now();
     if (!p_pinned) parallel_copy(pot, p_pin_, pbytes);
     if (prof) {
-        float ms[4];
-        for (int i = 0; i < 4; ++i) PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms[i], prof_[i], prof_[i + 1]));
+        float ms[5];
+        for (int i = 0; i < 5; ++i) PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms[i], prof_[i], prof_[i + 1]));
         const double enq = std::chrono::duration<double, std::milli>(h1 - h0).count();
         const double out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h2).count();
-        std::fprintf(stderr, "pdmk batch: upload %.2f ms, systems %.2f ms (host staging + enqueue %.2f ms), queue %.2f ms, "
-                             "download %.2f ms + host copy %.2f ms\n", ms[0], ms[1], enq, ms[2], ms[3], out);
+        std::fprintf(stderr, "pdmk batch: upload %.2f ms, systems %.2f ms (host staging + enqueue %.2f ms), leaf "
+                             "evaluation %.2f ms, queue %.2f ms, download %.2f ms + host copy %.2f ms\n",
+                     ms[0], ms[1], enq, ms[2], ms[3], ms[4], out);
     }
     ++evaluates_;
     if (n_err)
@@ -317,9 +343,15 @@ void TreeBatch::build_queue() {
     // descriptors of every system's buffers (its single-RHS float state exists
     // after the first deferred evaluate)
     std::vector<dev::NearLeafSys> d(trees_.size());
-    for (size_t i = 0; i < trees_.size(); ++i) trees_[i]->near_leaf_sys(d[i], pot_dev_ + off_[i]);
+    std::vector<dev::EvalLeafSys> ed(trees_.size());
+    for (size_t i = 0; i < trees_.size(); ++i) {
+        trees_[i]->near_leaf_sys(d[i], pot_dev_ + off_[i]);
+        trees_[i]->eval_leaf_sys(ed[i]);
+    }
     PDMK_CUDA_CHECK(cudaMemcpyAsync(sys_dev_, d.data(), sizeof(dev::NearLeafSys) * d.size(), cudaMemcpyHostToDevice,
                                     stream_));
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(esys_dev_, ed.data(), sizeof(dev::EvalLeafSys) * ed.size(),
+                                    cudaMemcpyHostToDevice, stream_));
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
     queue_built_ = true;
 }

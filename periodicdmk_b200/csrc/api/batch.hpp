@@ -36,9 +36,9 @@ class TreeBatch {
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ready_ = nullptr;
-    // PDMK_BATCH_PROFILE: per-evaluate phase times on stderr (upload, systems, queue, download)
+    // PDMK_BATCH_PROFILE: per-evaluate phase times on stderr (upload, systems, leaf evaluation, queue, download)
     bool profile_ = false;
-    cudaEvent_t prof_[5]{};
+    cudaEvent_t prof_[6]{};
     std::vector<cudaEvent_t> done_;
     double* q_dev_ = nullptr;
     double* pot_dev_ = nullptr;
@@ -55,6 +55,12 @@ class TreeBatch {
     void build_queue();
     void run_queue();
     dev::NearLeafSys* sys_dev_ = nullptr;
+    // the leaf evaluations of all systems in one launch: descriptors and
+    // (system, leaf) items, most targets first
+    dev::EvalLeafSys* esys_dev_ = nullptr;
+    int2* eitems_dev_ = nullptr;
+    int n_eitems_ = 0;
+    int p_ = 0;
     int2* items_dev_ = nullptr;
     int* head_dev_ = nullptr;
     int n_items_ = 0;

@@ -5,6 +5,8 @@
 
 #include <cstdint>
 
+#include "kernels.cuh"
+
 namespace pdmkb {
 namespace dev {
 
@@ -39,6 +41,18 @@ struct BatchNearArgs {
     int* head;          // queue head (reset to 0 by the launcher)
     float coef32[32];   // residual polynomial (same digit count for every system)
 };
+
+// One system's leaf-evaluation inputs (float tree, one RHS): the leaves,
+// their proxy potentials (FP32, one RHS) and the tree-order potentials the
+// evaluation adds to.
+struct EvalLeafSys {
+    EvalArgs a;              // trg, slot, trg_start, trg_count, center_scale
+    const float* proxy_down;
+    double* pot;
+};
+// Leaf evaluation of many systems in one launch: one CTA per (system, leaf)
+// item (defined with the single-system kernel in multi.cu).
+void launch_batch_eval(const EvalLeafSys* sys, const int2* items, int n_items, int p, cudaStream_t s);
 
 // CTAs that fill the GPU at full occupancy for tpt targets per thread.
 int batch_near_ctas(int nc, int tpt);

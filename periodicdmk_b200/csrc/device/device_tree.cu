@@ -546,6 +546,7 @@ void DeviceTree::init(const Plan& P, int device, bool fp64_working_set) {
         eval_.slot = upload(slot);
         eval_.trg_start = upload(t0);
         eval_.trg_count = upload(tc);
+        eval_leaf_trg_ = tc;
         eval_.center_scale = upload(cs);
     }
     phase("FP64 single-RHS pass");

@@ -145,10 +145,16 @@ class DeviceTree {
 
   public:
     bool last_was_multi_ = false;
-    // Set by a batch of systems: single-RHS float evaluates leave out the near
-    // field and the final gather, which the batch's queue kernel does for all
-    // systems in one launch (batch_near.cu).
+    // Set by a batch of systems: single-RHS float evaluates leave out the leaf
+    // evaluation, the near field and the final gather, which the batch does for
+    // all systems in one launch each (multi.cu, batch_near.cu).
     bool defer_near_ = false;
+    // Descriptor of this tree's leaf-evaluation inputs for the batch's launch
+    // (the single-RHS float state must exist).
+    void eval_leaf_sys(dev::EvalLeafSys& d) const;
+    int eval_leaves() const { return eval_.n_leaves; }
+    int expansion_order() const { return p_; }
+    const std::vector<int>& eval_leaf_targets() const { return eval_leaf_trg_; }
     // Descriptor of this tree's buffers for the batch near-field kernel (the
     // single-RHS float state must exist: one deferred evaluate has run);
     // out = this system's potentials in user order.
@@ -206,6 +212,7 @@ class DeviceTree {
     int near_max_trg_ = 0, near_max_pairs_ = 0;  // largest target count / source-box count of a near-field leaf
     int near_max_chunks_ = 0;                     // largest number of 32-source chunks of a near-field leaf
     std::vector<int64_t> near_leaf_cost_;         // per near-field leaf: targets x near sources
+    std::vector<int> eval_leaf_trg_;              // per evaluated leaf: targets
     int* near_pair_chunk_base_ = nullptr;         // per near pair: first chunk bounding box of its source box
     float4* near_chunk_lo_ = nullptr;
     float4* near_chunk_hi_ = nullptr;

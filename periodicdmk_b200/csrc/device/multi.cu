@@ -823,10 +823,8 @@ template void launch_sep3<double>(const Sep3&, int, int, cudaStream_t);
 // proxy -> leaf targets, TPT targets per thread: grid (leaves, 1, rhs)
 // ---------------------------------------------------------------------------
 template <typename T, int P, int TPT>
-__global__ void __launch_bounds__(128)
-    k_eval_g(EvalArgs a, const T* __restrict__ proxy_down, double* __restrict__ pot, int64_t N, int kb) {
-    __shared__ T slab[P * P];
-    const int e = blockIdx.x, c = blockIdx.z;
+__device__ __forceinline__ void eval_leaf_g(const EvalArgs& a, int e, int c, const T* __restrict__ proxy_down,
+                                            double* __restrict__ pot, int64_t N, int kb, T* slab) {
     const int t0 = a.trg_start[e], nt = a.trg_count[e];
     const double4 cs = a.center_scale[e];
     const T* C = proxy_down + ((int64_t)a.slot[e] * kb + c) * (P * P * P);
@@ -899,6 +897,35 @@ __global__ void __launch_bounds__(128)
             if (t < nt) potc[t0 + t] += (double)acc[u];
         }
     }
+}
+
+template <typename T, int P, int TPT>
+__global__ void __launch_bounds__(128)
+    k_eval_g(EvalArgs a, const T* __restrict__ proxy_down, double* __restrict__ pot, int64_t N, int kb) {
+    __shared__ T slab[P * P];
+    eval_leaf_g<T, P, TPT>(a, blockIdx.x, blockIdx.z, proxy_down, pot, N, kb, slab);
+}
+
+// many systems' leaves in one grid (float trees, one RHS): item = (system, leaf)
+template <int P, int TPT>
+__global__ void __launch_bounds__(128) k_eval_batch(const EvalLeafSys* __restrict__ sys, const int2* __restrict__ items) {
+    __shared__ float slab[P * P];
+    const int2 it = items[blockIdx.x];
+    const EvalLeafSys& S = sys[it.x];
+    eval_leaf_g<float, P, TPT>(S.a, it.y, 0, S.proxy_down, S.pot, 0, 1, slab);
+}
+
+void launch_batch_eval(const EvalLeafSys* sys, const int2* items, int n_items, int p, cudaStream_t s) {
+    if (n_items <= 0) return;
+    // one target per thread, 64 threads per leaf: the batch's leaves are small
+    // (a 64-thread CTA with 4 targets per thread left most lanes idle: 13.5
+    // against 6.6 ms for the 512-system batch at p = 18)
+    switch (p) {
+        case 9: k_eval_batch<9, 1><<<n_items, 64, 0, s>>>(sys, items); break;
+        case 18: k_eval_batch<18, 1><<<n_items, 64, 0, s>>>(sys, items); break;
+        default: throw std::runtime_error("batched leaf evaluation: float trees have p = 9 or 18");
+    }
+    PDMK_CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace dev
@@ -1314,7 +1341,10 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
             if (eval_done) ++nl;
         }
     }
-    if (eval_.n_leaves > 0 && !eval_done) {
+    // leaf evaluation and near field are left to the batch's launches over
+    // all systems when deferred (float trees of a batch, one RHS)
+    const bool deferred = f32 && defer_near_ && kb == 1;
+    if (eval_.n_leaves > 0 && !eval_done && !deferred) {
         const dim3 grid(eval_.n_leaves, 1, kb);
         switch (p) {
             case 9: dev::k_eval_g<T, 9, 4><<<grid, 64, 0, s>>>(eval_, down, m.pot, n_, kb); ++nl; break;
@@ -1326,7 +1356,6 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     }
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[1], s));
     // near field (left to the batch's queue kernel when deferred)
-    const bool deferred = f32 && defer_near_ && kb == 1;
     if (near_.n_leaves > 0 && !deferred) {
         dev::NearM a{};
         a.trg_start = near_.trg_start; a.trg_count = near_.trg_count; a.pair_start = near_.pair_start;
@@ -1402,6 +1431,14 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[4], s));
     PDMK_CUDA_CHECK(cudaGetLastError());
     multi_launches_ += nl;
+}
+
+void DeviceTree::eval_leaf_sys(dev::EvalLeafSys& d) const {
+    const MultiState* m = multi_[1].get();
+    if (!m || m->kb != 1) throw std::logic_error("eval_leaf_sys: no single-RHS float state");
+    d.a = eval_;
+    d.proxy_down = static_cast<const float*>(m->proxy_down);
+    d.pot = m->pot;
 }
 
 void DeviceTree::near_leaf_sys(dev::NearLeafSys& d, double* out) const {
