@@ -8,8 +8,11 @@
 // after that copy (replayed from a CUDA graph from the second evaluate on), one
 // device->host copy of all potentials after every system has finished.
 // Pageable host buffers pass through pinned staging buffers, filled and
-// drained by up to 8 host threads (a pageable cudaMemcpy moves 3-10 GB/s);
-// page-locked ones are copied directly.
+// drained by up to 8 persistent host threads (a pageable cudaMemcpy moves
+// 3-10 GB/s); page-locked ones are copied directly.  Both transfers run in
+// about 8 chunks of whole systems: a chunk's systems start as soon as its
+// charges are on the device, and a chunk of potentials is copied out of the
+// staging while the later chunks are still in flight.
 // Float trees (one charge vector per system) leave their near field and final
 // gather out of the per-system sequences: after all systems' other stages one
 // persistent kernel pulls (system, leaf) items from a device queue, largest
@@ -23,6 +26,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -100,12 +104,23 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
         for (auto& t : up) t.join();
         if (first_error) std::rethrow_exception(first_error);
         PDMK_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
         profile_ = std::getenv("PDMK_BATCH_PROFILE") != nullptr;
         if (profile_)
             for (auto& e : prof_) PDMK_CUDA_CHECK(cudaEventCreate(&e));
         done_.assign(nsys, nullptr);
         for (auto& e : done_) PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        // transfer chunks: about 8 of equal points, at system boundaries
+        {
+            const int64_t tot = off_.back(), want = std::max<int64_t>(1, (tot + 7) / 8);
+            chunk_sys_.assign(1, 0);
+            for (int i = 1; i <= nsys; ++i)
+                if (i == nsys || off_[i] - off_[chunk_sys_.back()] >= want) chunk_sys_.push_back(i);
+            const size_t nch = chunk_sys_.size() - 1;
+            ev_up_.assign(nch, nullptr);
+            ev_dn_.assign(nch, nullptr);
+            for (auto& e : ev_up_) PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            for (auto& e : ev_dn_) PDMK_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
         const size_t n = (size_t)total_points();
         PDMK_CUDA_CHECK(cudaMalloc(&q_dev_, sizeof(double) * n));
         PDMK_CUDA_CHECK(cudaMalloc(&pot_dev_, sizeof(double) * n));
@@ -168,7 +183,13 @@ void TreeBatch::release() {
     for (auto& e : done_)
         if (e) cudaEventDestroy(e);
     done_.clear();
-    if (ready_) cudaEventDestroy(ready_);
+    for (auto& e : ev_up_)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ev_dn_)
+        if (e) cudaEventDestroy(e);
+    ev_up_.clear();
+    ev_dn_.clear();
+    pool_.reset();
     for (auto& e : prof_)
         if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
@@ -185,7 +206,6 @@ void TreeBatch::release() {
     sys_dev_ = nullptr;
     items_dev_ = nullptr;
     head_dev_ = nullptr;
-    ready_ = nullptr;
     stream_ = nullptr;
     q_dev_ = pot_dev_ = nullptr;
     potf_dev_ = nullptr;
@@ -210,25 +230,69 @@ bool pinned(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
-// memcpy on up to 8 host threads (pageable <-> pinned staging)
-void parallel_copy(void* dst, const void* src, size_t bytes) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t nt = std::min<size_t>({8, hw, std::max<size_t>(1, bytes >> 22)});
-    if (nt <= 1) {
-        std::memcpy(dst, src, bytes);
-        return;
-    }
-    const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
-    std::vector<std::thread> th;
-    for (size_t t = 0; t < nt; ++t) {
-        const size_t o = t * part;
-        if (o >= bytes) break;
-        const size_t b = std::min(part, bytes - o);
-        th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, b); });
-    }
-    for (auto& x : th) x.join();
-}
 }  // namespace
+
+// memcpy split over persistent host threads (pageable <-> pinned staging)
+class CopyPool {
+  public:
+    explicit CopyPool(int n) {
+        for (int i = 0; i < n; ++i) workers_.emplace_back([this, i] { run(i); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& w : workers_) w.join();
+    }
+    void copy(void* dst, const void* src, size_t bytes) {
+        if (bytes < ((size_t)1 << 20) || workers_.empty()) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        std::unique_lock<std::mutex> lk(mu_);
+        dst_ = static_cast<char*>(dst);
+        src_ = static_cast<const char*>(src);
+        bytes_ = bytes;
+        pending_ = (int)workers_.size();
+        ++gen_;
+        cv_.notify_all();
+        done_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+  private:
+    void run(int id) {
+        uint64_t seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (stop_) return;
+            const size_t nw = workers_.size();
+            const size_t part = ((bytes_ + nw - 1) / nw + 63) & ~(size_t)63;
+            const size_t o = std::min(bytes_, part * (size_t)id), b = std::min(part, bytes_ - o);
+            char* d = dst_;
+            const char* sp = src_;
+            lk.unlock();
+            if (b) std::memcpy(d + o, sp + o, b);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t bytes_ = 0;
+    int pending_ = 0;
+};
+
+void CopyPoolDeleter::operator()(CopyPool* p) const { delete p; }
 
 void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
     if (!charges || !pot) throw std::invalid_argument("null charges or output");
@@ -236,57 +300,69 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
     const int64_t n = total_points();
     const auto h0 = std::chrono::steady_clock::now();
     if (profile_) PDMK_CUDA_CHECK(cudaEventRecord(prof_[0], stream_));
-    // pageable buffers go through the pinned staging: a host-threaded copy
-    // and one DMA transfer each way (a pageable cudaMemcpy is far slower)
+    // Pageable buffers go through the pinned staging (a pageable cudaMemcpy
+    // moves 3-10 GB/s): host threads fill it chunk by chunk, each chunk's DMA
+    // starts as soon as it is staged and the systems of that chunk start once
+    // their charges are on the device.
     const bool q_pinned = pinned(charges), p_pinned = pinned(pot);
-    const double* q_src = charges;
-    if (!q_pinned) {
-        parallel_copy(q_pin_, charges, sizeof(double) * n);
-        q_src = q_pin_;
-    }
-    PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_, q_src, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
-    PDMK_CUDA_CHECK(cudaEventRecord(ready_, stream_));
-    if (profile_) PDMK_CUDA_CHECK(cudaEventRecord(prof_[1], stream_));
+    if ((!q_pinned || !p_pinned) && !pool_)
+        pool_.reset(new CopyPool((int)std::min(8u, std::max(1u, std::thread::hardware_concurrency()))));
     // The first evaluate runs the systems directly (it creates their multi-RHS
     // state); the second captures each system's launch sequence into a CUDA
     // graph (device buffers and tables are fixed per system), later ones
     // replay the graphs.
     const bool capture = evaluates_ == 1;
-    for (size_t i = 0; i < trees_.size(); ++i) {
-        DeviceTree& t = *trees_[i];
-        cudaStream_t ts = t.stream();
-        PDMK_CUDA_CHECK(cudaStreamWaitEvent(ts, ready_, 0));
-        auto enqueue = [&]() {
-            if (single_)
-                t.enqueue_multi_device(q_dev_ + off_[i], 1, pot_dev_ + off_[i], /*fp32=*/true);
-            else
-                t.evaluate_device(q_dev_ + off_[i], pot_dev_ + off_[i], nullptr);
-        };
-        if (graphs_[i]) {
-            PDMK_CUDA_CHECK(cudaGraphLaunch(graphs_[i], ts));
-        } else if (capture) {
-            cudaGraph_t g = nullptr;
-            PDMK_CUDA_CHECK(cudaStreamBeginCapture(ts, cudaStreamCaptureModeThreadLocal));
-            try {
-                enqueue();
-            } catch (...) {
-                cudaStreamEndCapture(ts, &g);
-                if (g) cudaGraphDestroy(g);
-                throw;
-            }
-            PDMK_CUDA_CHECK(cudaStreamEndCapture(ts, &g));
-            cudaGraphExec_t ge = nullptr;
-            const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
-            cudaGraphDestroy(g);
-            PDMK_CUDA_CHECK(ie);
-            graphs_[i] = ge;
-            PDMK_CUDA_CHECK(cudaGraphLaunch(ge, ts));
-        } else {
-            enqueue();
+    const int nch = (int)chunk_sys_.size() - 1;
+    for (int c = 0; c < nch; ++c) {
+        const int s0 = chunk_sys_[c], s1 = chunk_sys_[c + 1];
+        const int64_t o0 = off_[s0], cnt = off_[s1] - o0;
+        const double* src = charges + o0;
+        if (!q_pinned) {
+            pool_->copy(q_pin_ + o0, charges + o0, sizeof(double) * (size_t)cnt);
+            src = q_pin_ + o0;
         }
-        PDMK_CUDA_CHECK(cudaEventRecord(done_[i], ts));
-        PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(q_dev_ + o0, src, sizeof(double) * (size_t)cnt, cudaMemcpyHostToDevice,
+                                        stream_));
+        PDMK_CUDA_CHECK(cudaEventRecord(ev_up_[c], stream_));
+        for (int i = s0; i < s1; ++i) {
+            DeviceTree& t = *trees_[i];
+            cudaStream_t ts = t.stream();
+            PDMK_CUDA_CHECK(cudaStreamWaitEvent(ts, ev_up_[c], 0));
+            auto enqueue = [&]() {
+                if (single_)
+                    t.enqueue_multi_device(q_dev_ + off_[i], 1, pot_dev_ + off_[i], /*fp32=*/true);
+                else
+                    t.evaluate_device(q_dev_ + off_[i], pot_dev_ + off_[i], nullptr);
+            };
+            if (graphs_[i]) {
+                PDMK_CUDA_CHECK(cudaGraphLaunch(graphs_[i], ts));
+            } else if (capture) {
+                cudaGraph_t g = nullptr;
+                PDMK_CUDA_CHECK(cudaStreamBeginCapture(ts, cudaStreamCaptureModeThreadLocal));
+                try {
+                    enqueue();
+                } catch (...) {
+                    cudaStreamEndCapture(ts, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                PDMK_CUDA_CHECK(cudaStreamEndCapture(ts, &g));
+                cudaGraphExec_t ge = nullptr;
+                const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+                cudaGraphDestroy(g);
+                PDMK_CUDA_CHECK(ie);
+                graphs_[i] = ge;
+                PDMK_CUDA_CHECK(cudaGraphLaunch(ge, ts));
+            } else {
+                enqueue();
+            }
+            PDMK_CUDA_CHECK(cudaEventRecord(done_[i], ts));
+        }
     }
+    if (profile_) PDMK_CUDA_CHECK(cudaEventRecord(prof_[1], stream_));
+    // the main stream joins every system (after all uploads are enqueued, so
+    // that no upload waits for a system)
+    for (size_t i = 0; i < trees_.size(); ++i) PDMK_CUDA_CHECK(cudaStreamWaitEvent(stream_, done_[i], 0));
     const auto h1 = std::chrono::steady_clock::now();
     const bool prof = profile_;
     if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[2], stream_));
@@ -299,13 +375,15 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
         PDMK_CUDA_CHECK(cudaEventRecord(prof_[3], stream_));
     }
     if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[4], stream_));
-    const size_t pbytes = (pot_float ? sizeof(float) : sizeof(double)) * (size_t)n;
-    void* p_dst = p_pinned ? pot : static_cast<void*>(p_pin_);
-    if (pot_float) {
-        dev::launch_to_float(pot_dev_, potf_dev_, n, stream_);
-        PDMK_CUDA_CHECK(cudaMemcpyAsync(p_dst, potf_dev_, pbytes, cudaMemcpyDeviceToHost, stream_));
-    } else {
-        PDMK_CUDA_CHECK(cudaMemcpyAsync(p_dst, pot_dev_, pbytes, cudaMemcpyDeviceToHost, stream_));
+    const size_t es = pot_float ? sizeof(float) : sizeof(double);
+    char* p_dst = static_cast<char*>(p_pinned ? pot : static_cast<void*>(p_pin_));
+    if (pot_float) dev::launch_to_float(pot_dev_, potf_dev_, n, stream_);
+    const char* p_src = pot_float ? reinterpret_cast<const char*>(potf_dev_) : reinterpret_cast<const char*>(pot_dev_);
+    for (int c = 0; c < nch; ++c) {
+        const int64_t o0 = off_[chunk_sys_[c]], cnt = off_[chunk_sys_[c + 1]] - o0;
+        PDMK_CUDA_CHECK(cudaMemcpyAsync(p_dst + es * o0, p_src + es * o0, es * (size_t)cnt, cudaMemcpyDeviceToHost,
+                                        stream_));
+        PDMK_CUDA_CHECK(cudaEventRecord(ev_dn_[c], stream_));
     }
     // error words of the tensor-core kernels: one asynchronous copy each, one wait
     int n_err = 0;
@@ -320,18 +398,25 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
         }
     }
     if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[5], stream_));
+    // drain each chunk of the staging as soon as its DMA is done
+    double out_ms = 0.0;  // host copy time (profile)
+    if (!p_pinned)
+        for (int c = 0; c < nch; ++c) {
+            const int64_t o0 = off_[chunk_sys_[c]], cnt = off_[chunk_sys_[c + 1]] - o0;
+            PDMK_CUDA_CHECK(cudaEventSynchronize(ev_dn_[c]));
+            const auto c0 = std::chrono::steady_clock::now();
+            pool_->copy(static_cast<char*>(pot) + es * o0, p_dst + es * o0, es * (size_t)cnt);
+            out_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
+        }
     PDMK_CUDA_CHECK(cudaStreamSynchronize(stream_));
     PDMK_CUDA_CHECK(cudaGetLastError());
-    const auto h2 = std::chrono::steady_clock::now();
-    if (!p_pinned) parallel_copy(pot, p_pin_, pbytes);
     if (prof) {
         float ms[5];
         for (int i = 0; i < 5; ++i) PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms[i], prof_[i], prof_[i + 1]));
         const double enq = std::chrono::duration<double, std::milli>(h1 - h0).count();
-        const double out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h2).count();
         std::fprintf(stderr, "pdmk batch: upload %.2f ms, systems %.2f ms (host staging + enqueue %.2f ms), leaf "
                              "evaluation %.2f ms, queue %.2f ms, download %.2f ms + host copy %.2f ms\n",
-                     ms[0], ms[1], enq, ms[2], ms[3], ms[4], out);
+                     ms[0], ms[1], enq, ms[2], ms[3], ms[4], out_ms);
     }
     ++evaluates_;
     if (n_err)

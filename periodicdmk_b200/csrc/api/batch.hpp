@@ -11,6 +11,11 @@
 
 namespace pdmkb {
 
+class CopyPool;  // host threads copying between pageable and pinned buffers (batch.cpp)
+struct CopyPoolDeleter {
+    void operator()(CopyPool* p) const;
+};
+
 class TreeBatch {
   public:
     // cells: nsys x 9 (column-major 3x3 each); positions: 3 x Ns[i] blocks in order.
@@ -35,7 +40,6 @@ class TreeBatch {
     bool single_ = false;
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
-    cudaEvent_t ready_ = nullptr;
     // PDMK_BATCH_PROFILE: per-evaluate phase times on stderr (upload, systems, leaf evaluation, queue, download)
     bool profile_ = false;
     cudaEvent_t prof_[6]{};
@@ -46,6 +50,11 @@ class TreeBatch {
     // pinned staging of pageable host buffers (filled and drained by host threads)
     double* q_pin_ = nullptr;
     double* p_pin_ = nullptr;
+    std::unique_ptr<CopyPool, CopyPoolDeleter> pool_;
+    // transfers in chunks of whole systems: chunk c = systems chunk_sys_[c] ..
+    // chunk_sys_[c + 1] - 1; its upload / download is complete at ev_up_[c] / ev_dn_[c]
+    std::vector<int> chunk_sys_;
+    std::vector<cudaEvent_t> ev_up_, ev_dn_;
     // after the first evaluate, each system's evaluate is replayed from a CUDA graph
     std::vector<cudaGraphExec_t> graphs_;
     int* err_host_ = nullptr;  // pinned, one word per system
