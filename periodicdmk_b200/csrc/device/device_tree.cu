@@ -1126,7 +1126,8 @@ int DeviceTree::run_fp64_tree(const double* q, cd* scratch, int64_t cap, cudaStr
             a.mode = dev::kStore; a.structure = structure;
             // FP64 tensor cores (DMMA) when selected, else the CUDA-core contraction
             auto rrr = [&](const dev::ContractArgs& c) {
-                if (fp64_dmma_ && dev::translate_dmma_supported(c.ni, c.na)) dev::launch_translate_dmma(c, s);
+                const bool dm = fp64_dmma_ < 0 ? p_ == 28 : fp64_dmma_ != 0;
+                if (dm && dev::translate_dmma_supported(c.ni, c.na)) dev::launch_translate_dmma(c, s);
                 else dev::launch_contract(c, dev::kRRR, s);
             };
             rrr(a);

@@ -172,7 +172,7 @@ class DeviceTree {
     int tc_mask_ = 7;
     // FP64 child <-> parent translations on the FP64 tensor cores (DMMA)
     // instead of the CUDA cores.  Initialised from PDMK_FP64_DMMA (default 0).
-    int fp64_dmma_ = 0;
+    int fp64_dmma_ = -1;  // translations on DMMA: 1 on, 0 off, -1 at p = 28 only (measured faster there)
     // Proxy moments of the FP64 path at p = 28, 38 on DMMA (dmma.cu) instead of
     // the register-tiled CUDA-core kernel.  Initialised from PDMK_MOMENTS_DMMA
     // (default 1: 86 -> 42 ms per 12-digit evaluate of 2e6 clustered points).

@@ -190,10 +190,11 @@ def test_errors_on_device_tree():
 @pytest.mark.parametrize("nd", [9, 12])
 def test_fp64_translations_on_dmma(nd, monkeypatch):
     # PDMK_FP64_DMMA=1 (read when the tree is built) runs the child <-> parent
-    # translations on mma.sync.m8n8k4.f64; same arithmetic up to the order of
-    # the FP64 sums, so it agrees with the CUDA-core path to rounding and with
-    # the oracle as before
+    # translations on mma.sync.m8n8k4.f64 (the default at 9 digits), 0 on the
+    # CUDA cores (the default at 12); same arithmetic up to the order of the
+    # FP64 sums, so the two agree to rounding
     cell, pos, q = clustered_system(20000, 41, TRICLINIC, n_clusters=8, sigma=0.03)
+    monkeypatch.setenv("PDMK_FP64_DMMA", "0")
     ref_tree = _tree(cell, pos, nd, 40)
     ref = ref_tree.evaluate(q)
     ref_tree.close()
