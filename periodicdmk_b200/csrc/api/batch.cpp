@@ -158,6 +158,15 @@ TreeBatch::TreeBatch(int nsys, const double* cells, const int* Ns, const double*
             PDMK_CUDA_CHECK(cudaMemcpy(eitems_dev_, ei.data(), sizeof(int2) * ei.size(), cudaMemcpyHostToDevice));
             PDMK_CUDA_CHECK(cudaMalloc(&esys_dev_, sizeof(dev::EvalLeafSys) * nsys));
             p_ = trees_[0]->expansion_order();
+            // interpolation items: 128-target blocks of every system
+            std::vector<int2> ii;
+            for (int i = 0; i < nsys; ++i)
+                for (int64_t b = 0; b * 128 < off_[i + 1] - off_[i]; ++b) ii.push_back(make_int2(i, (int)b));
+            n_iitems_ = (int)ii.size();
+            PDMK_CUDA_CHECK(cudaMalloc(&iitems_dev_, sizeof(int2) * std::max<size_t>(ii.size(), 1)));
+            PDMK_CUDA_CHECK(cudaMemcpy(iitems_dev_, ii.data(), sizeof(int2) * ii.size(), cudaMemcpyHostToDevice));
+            PDMK_CUDA_CHECK(cudaMalloc(&isys_dev_, sizeof(dev::InterpSys) * nsys));
+            w_ = trees_[0]->nufft_width();
             PDMK_CUDA_CHECK(cudaMalloc(&head_dev_, sizeof(int)));
             nc_ = trees_[0]->near_coeffs();
             for (int i = 0; i < nc_; ++i) coef32_[i] = (float)trees_[0]->near_coef()[i];
@@ -199,8 +208,12 @@ void TreeBatch::release() {
     if (sys_dev_) cudaFree(sys_dev_);
     if (esys_dev_) cudaFree(esys_dev_);
     if (eitems_dev_) cudaFree(eitems_dev_);
+    if (isys_dev_) cudaFree(isys_dev_);
+    if (iitems_dev_) cudaFree(iitems_dev_);
     esys_dev_ = nullptr;
     eitems_dev_ = nullptr;
+    isys_dev_ = nullptr;
+    iitems_dev_ = nullptr;
     if (items_dev_) cudaFree(items_dev_);
     if (head_dev_) cudaFree(head_dev_);
     sys_dev_ = nullptr;
@@ -369,6 +382,7 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
     if (single_) {
         if (!queue_built_) build_queue();
         dev::launch_batch_eval(esys_dev_, eitems_dev_, n_eitems_, p_, stream_);
+        dev::launch_batch_interp(isys_dev_, iitems_dev_, n_iitems_, w_, stream_);
         if (prof) PDMK_CUDA_CHECK(cudaEventRecord(prof_[3], stream_));
         run_queue();
     } else if (prof) {
@@ -415,7 +429,7 @@ void TreeBatch::evaluate(const double* charges, void* pot, bool pot_float) {
         for (int i = 0; i < 5; ++i) PDMK_CUDA_CHECK(cudaEventElapsedTime(&ms[i], prof_[i], prof_[i + 1]));
         const double enq = std::chrono::duration<double, std::milli>(h1 - h0).count();
         std::fprintf(stderr, "pdmk batch: upload %.2f ms, systems %.2f ms (host staging + enqueue %.2f ms), leaf "
-                             "evaluation %.2f ms, queue %.2f ms, download %.2f ms + host copy %.2f ms\n",
+                             "evaluation + interpolation %.2f ms, queue %.2f ms, download %.2f ms + host copy %.2f ms\n",
                      ms[0], ms[1], enq, ms[2], ms[3], ms[4], out_ms);
     }
     ++evaluates_;
@@ -429,10 +443,15 @@ void TreeBatch::build_queue() {
     // after the first deferred evaluate)
     std::vector<dev::NearLeafSys> d(trees_.size());
     std::vector<dev::EvalLeafSys> ed(trees_.size());
+    std::vector<dev::InterpSys> id(trees_.size());
     for (size_t i = 0; i < trees_.size(); ++i) {
         trees_[i]->near_leaf_sys(d[i], pot_dev_ + off_[i]);
         trees_[i]->eval_leaf_sys(ed[i]);
+        trees_[i]->interp_sys(id[i]);
+        if (trees_[i]->nufft_width() != w_) throw std::logic_error("batch systems with different NUFFT widths");
     }
+    PDMK_CUDA_CHECK(cudaMemcpyAsync(isys_dev_, id.data(), sizeof(dev::InterpSys) * id.size(), cudaMemcpyHostToDevice,
+                                    stream_));
     PDMK_CUDA_CHECK(cudaMemcpyAsync(sys_dev_, d.data(), sizeof(dev::NearLeafSys) * d.size(), cudaMemcpyHostToDevice,
                                     stream_));
     PDMK_CUDA_CHECK(cudaMemcpyAsync(esys_dev_, ed.data(), sizeof(dev::EvalLeafSys) * ed.size(),

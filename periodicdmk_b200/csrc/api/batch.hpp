@@ -40,7 +40,8 @@ class TreeBatch {
     bool single_ = false;
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
-    // PDMK_BATCH_PROFILE: per-evaluate phase times on stderr (upload, systems, leaf evaluation, queue, download)
+    // PDMK_BATCH_PROFILE: per-evaluate phase times on stderr (upload, systems, leaf evaluation and
+    // interpolation, queue, download)
     bool profile_ = false;
     cudaEvent_t prof_[6]{};
     std::vector<cudaEvent_t> done_;
@@ -70,6 +71,12 @@ class TreeBatch {
     int2* eitems_dev_ = nullptr;
     int n_eitems_ = 0;
     int p_ = 0;
+    // the far-field interpolations of all systems in one launch: descriptors
+    // and (system, block of 128 targets) items
+    dev::InterpSys* isys_dev_ = nullptr;
+    int2* iitems_dev_ = nullptr;
+    int n_iitems_ = 0;
+    int w_ = 0;
     int2* items_dev_ = nullptr;
     int* head_dev_ = nullptr;
     int n_items_ = 0;

@@ -54,6 +54,18 @@ struct EvalLeafSys {
 // item (defined with the single-system kernel in multi.cu).
 void launch_batch_eval(const EvalLeafSys* sys, const int2* items, int n_items, int p, cudaStream_t s);
 
+// One system's far-field interpolation inputs (one RHS): its transformed
+// grid, its targets' window taps and the far-field output (tree order).
+struct InterpSys {
+    NufftArgs a;        // grid, far, pt_l0, grid sizes, width, visit order
+    const double* esw;  // per target: 3 x W taps
+    int64_t n;          // targets
+};
+// Interpolation of many systems in one launch: one CTA per (system, block of
+// 128 targets) item; every system has the kernel width w (defined with the
+// single-system kernels in nufft_multi.cu).
+void launch_batch_interp(const InterpSys* sys, const int2* items, int n_items, int w, cudaStream_t s);
+
 // CTAs that fill the GPU at full occupancy for tpt targets per thread.
 int batch_near_ctas(int nc, int tpt);
 // tpt: targets per thread (1, 2 or 4); ctas: persistent grid size.

@@ -122,7 +122,8 @@ class DeviceTree {
     template <typename T>
     void run_multi_block(MultiState& m, const double* Q, int kvalid, double* pot_user);
     // far field of the columns [c0, c0 + cols) of a multi-RHS block (q_t -> far)
-    int far_columns(MultiState& m, int c0, int cols, bool qp, cufftHandle fwd, cufftHandle inv, cudaStream_t s);
+    int far_columns(MultiState& m, int c0, int cols, bool qp, cufftHandle fwd, cufftHandle inv, cudaStream_t s,
+                    bool interp = true);
     // Host-buffer multi-RHS evaluate with the charge upload in column chunks:
     // upload(c0, cols) enqueues a chunk's copy on stream_; the far field of each
     // chunk runs on a second stream as soon as it has arrived, the tree passes
@@ -146,13 +147,18 @@ class DeviceTree {
   public:
     bool last_was_multi_ = false;
     // Set by a batch of systems: single-RHS float evaluates leave out the leaf
-    // evaluation, the near field and the final gather, which the batch does for
-    // all systems in one launch each (multi.cu, batch_near.cu).
+    // evaluation, the far-field interpolation, the near field and the final
+    // gather, which the batch does for all systems in one launch each
+    // (multi.cu, nufft_multi.cu, batch_near.cu).
     bool defer_near_ = false;
     // Descriptor of this tree's leaf-evaluation inputs for the batch's launch
     // (the single-RHS float state must exist).
     void eval_leaf_sys(dev::EvalLeafSys& d) const;
     int eval_leaves() const { return eval_.n_leaves; }
+    // Descriptor of this tree's far-field interpolation for the batch's launch
+    // (the single-RHS float state must exist).
+    void interp_sys(dev::InterpSys& d) const;
+    int nufft_width() const { return nufft_.w; }
     int expansion_order() const { return p_; }
     const std::vector<int>& eval_leaf_targets() const { return eval_leaf_trg_; }
     // Descriptor of this tree's buffers for the batch near-field kernel (the

@@ -1419,7 +1419,7 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     if (far_ext_)
         PDMK_CUDA_CHECK(cudaStreamWaitEvent(s, far_ext_event_, 0));
     else
-        nl += far_columns(m, 0, kb, qp, m.fwd, m.inv, s);
+        nl += far_columns(m, 0, kb, qp, m.fwd, m.inv, s, /*interp=*/!deferred);
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[3], s));
     if (qp) {
         dev::launch_qp_finalize(m.pot, m.far, trg_, trg_perm_, Q, qp_trg_phase_, pot_user, n_, s); ++nl;
@@ -1431,6 +1431,20 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
     PDMK_CUDA_CHECK(cudaEventRecord(ev_[4], s));
     PDMK_CUDA_CHECK(cudaGetLastError());
     multi_launches_ += nl;
+}
+
+void DeviceTree::interp_sys(dev::InterpSys& d) const {
+    const MultiState* m = multi_[1].get();
+    if (!m || m->kb != 1) throw std::logic_error("interp_sys: no single-RHS float state");
+    d.a = nufft_;
+    d.a.q_sorted = m->q_t;
+    d.a.grid = m->grid;
+    d.a.far = m->far;
+    d.a.rhs_q_stride = n_;
+    d.a.rhs_grid_stride = n_grid_;
+    d.a.rhs_far_stride = n_;
+    d.esw = m->esw;
+    d.n = n_;
 }
 
 void DeviceTree::eval_leaf_sys(dev::EvalLeafSys& d) const {
@@ -1467,7 +1481,7 @@ void DeviceTree::near_leaf_sys(dev::NearLeafSys& d, double* out) const {
 }
 
 int DeviceTree::far_columns(MultiState& m, int c0, int cols, bool qp, cufftHandle fwd, cufftHandle inv,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool interp) {
     dev::NufftArgs na = nufft_;
     na.q_sorted = m.q_t + (int64_t)c0 * n_;
     na.grid = m.grid + (int64_t)c0 * n_grid_;
@@ -1491,6 +1505,7 @@ int DeviceTree::far_columns(MultiState& m, int c0, int cols, bool qp, cufftHandl
         dev::launch_multiply(spec, mult_, n_spec_, s, cols);
     if (cufftExecZ2D(inv, reinterpret_cast<cufftDoubleComplex*>(spec), na.grid) != CUFFT_SUCCESS)
         throw std::runtime_error("cuFFT error in the batched inverse transform");
+    if (!interp) return 2;
     dev::launch_interp_multi(na, m.esw, n_, cols, s);
     return 3;
 }

@@ -9,6 +9,8 @@
 // Grid layout (cuFFT batched real input): grid[c * rhs_grid_stride + (x*n2 + y)*n3 + z].
 #include <stdexcept>
 
+#include "batch_near.cuh"
+#include "common.cuh"
 #include "kernels.cuh"
 #include "nufft_multi.cuh"
 
@@ -229,12 +231,10 @@ __global__ void __launch_bounds__((W * W + 31) / 32 * 32) k_spread_r(NufftArgs a
     }
 }
 
+// interpolation of the it-th target of the visit order, RHS c0 .. c0 + CB - 1
 template <int W, int CB>
-__global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __restrict__ esw, int64_t n) {
-    const int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (it >= n) return;
+__device__ __forceinline__ void interp_target(const NufftArgs& a, const double* __restrict__ esw, int64_t it, int c0) {
     const int64_t t = a.interp_order ? a.interp_order[it] : it;
-    const int c0 = blockIdx.y * CB;
     const int4 l0 = a.pt_l0[t];
     const double* wt = esw + t * 3 * W;
     double wy[W], wz[W];
@@ -270,6 +270,23 @@ __global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __r
     }
 #pragma unroll
     for (int c = 0; c < CB; ++c) a.far[(int64_t)(c0 + c) * a.rhs_far_stride + t] = u[c];
+}
+
+template <int W, int CB>
+__global__ void __launch_bounds__(128) k_interp_m(NufftArgs a, const double* __restrict__ esw, int64_t n) {
+    const int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n) return;
+    interp_target<W, CB>(a, esw, it, blockIdx.y * CB);
+}
+
+// many systems' interpolations in one grid (one RHS): item = (system, block of 128 targets)
+template <int W>
+__global__ void __launch_bounds__(128) k_interp_batch(const InterpSys* __restrict__ sys, const int2* __restrict__ items) {
+    const int2 w = items[blockIdx.x];
+    const InterpSys& S = sys[w.x];
+    const int64_t it = (int64_t)w.y * 128 + threadIdx.x;
+    if (it >= S.n) return;
+    interp_target<W, 1>(S.a, S.esw, it, 0);
 }
 
 // Interpolation from each bin's subgrid in shared memory: one CTA per bin,
@@ -567,6 +584,14 @@ void launch_interp_multi(const NufftArgs& a, const double* esw, int64_t n, int n
 #define PDMK_INW(W) interp_w<W>(a, esw, n, nrhs, s)
     PDMK_NUFFT_W_SWITCH(a.w, PDMK_INW)
 #undef PDMK_INW
+}
+
+void launch_batch_interp(const InterpSys* sys, const int2* items, int n_items, int w, cudaStream_t s) {
+    if (n_items <= 0) return;
+#define PDMK_IB(W) k_interp_batch<W><<<n_items, 128, 0, s>>>(sys, items)
+    PDMK_NUFFT_W_SWITCH(w, PDMK_IB)
+#undef PDMK_IB
+    PDMK_CUDA_CHECK(cudaGetLastError());
 }
 
 bool launch_spread_multi_f32(const NufftArgs& a, const float* esw32, int nrhs, cudaStream_t s) {
