@@ -153,7 +153,7 @@ def lpt_partition(costs, parts):
 
 
 def run_batch(pd, args, world, rank, barrier, max_over_ranks):
-    """512 independent systems (cfg5 form) through pdmk_batch_evaluate, host
+    """512 independent triclinic systems (N log-uniform in [1e3, 1e5]) through pdmk_batch_evaluate, host
     buffers in and out; systems split across ranks by LPT on their point
     counts.  Returns the JSON fragment for the bench line."""
     cells, pos, qs = batch_systems(args.batch_systems, seed=11)

@@ -24,7 +24,7 @@ pytestmark = pytest.mark.gpu
 SYSTEMS = {
     "cube_deep": lambda: (uniform_system(3000, 21), 30),
     "triclinic_clustered": lambda: (clustered_system(3000, 22, TRICLINIC, n_clusters=4, sigma=0.02), 25),
-    "cube_cfg1": lambda: (uniform_system(20000, 1), 300),
+    "cube_2e4": lambda: (uniform_system(20000, 1), 300),
 }
 
 
@@ -48,11 +48,11 @@ def test_parts_match_oracle(name, nd):
     t.close()
 
 
-def test_cfg1_matches_oracle_and_ewald():
+def test_cube_2e4_matches_oracle_and_ewald():
     # N = 20,000 cube, +-1 charges, 6 digits, npl 300: the reference's own
     # CPU-runnable case.  Against the DMK oracle (same algorithm) and against
     # an Ewald sum at every target (the physics): the drop-in bar is 2e-6.
-    (cell, pos, q), npl = SYSTEMS["cube_cfg1"]()
+    (cell, pos, q), npl = SYSTEMS["cube_2e4"]()
     t = _tree(cell, pos, 6, npl)
     info = t.info()
     assert info["n_boxes"] == 216 and info["n_levels"] == 1

@@ -145,7 +145,7 @@ def test_oracle_linearity_and_charge_flip():
 
 
 def test_plan_sizes_uniform_cube():
-    # cfg1: N=20000 uniform cube, 6 digits, npl 300, nz 4: one level of 6^3 boxes,
+    # N=20000 uniform cube, 6 digits, npl 300, nz 4: one level of 6^3 boxes,
     # 64 inner leaves, 18^3 far-field modes.
     cell, pos, _ = uniform_system(20000, 1)
     st = oracle.plan_stats(cell, pos, 6, 300, 4)
