@@ -439,6 +439,50 @@ def run_reference(args):
     return 0
 
 
+def run_digits3(pd, cell, pos, q, Q, args, world, dev, flush, barrier, max_over_ranks):
+    """The same cube at 3 digits: plain FP64 evaluate of one RHS and the
+    mixed-precision batched evaluate of the k RHS (device buffers, L2 flushed
+    between steps), with the mixed result's rel L2 against the plain one on
+    RHS 0.  Returns the JSON fragment."""
+    import torch
+
+    n, k = len(q), Q.shape[1]
+    td = pd.PeriodicDMKTree(cell, pos, n_digits=3, n_per_leaf=300, nz=4, precision="double")
+    tf = pd.PeriodicDMKTree(cell, pos, n_digits=3, n_per_leaf=300, nz=4, precision="float")
+    q_d = torch.from_numpy(q).to(dev)
+    p_d = torch.empty(n, dtype=torch.float64, device=dev)
+    Qc = torch.from_numpy(np.ascontiguousarray(Q.T)).to(dev)
+    Pc = torch.empty_like(Qc)
+    out = {}
+    for name, run, rhs in (("plain_fp64_single_rhs", lambda: td.evaluate_device(q_d.data_ptr(), p_d.data_ptr()), 1),
+                           ("mixed_batched", lambda: tf.evaluate_multi_device(k, Qc.data_ptr(), Pc.data_ptr()), k)):
+        tree = td if rhs == 1 else tf
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        sts = []
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            run()
+            sts.append(tree.stage_times())
+        torch.cuda.synchronize()
+        barrier()
+        t = max_over_ranks(sum(s["total_ms"] for s in sts) / 1e3) / args.steps
+        out[name] = {"value": world * n * rhs / t / 1e6, "unit": "Mpts*RHS/s", "ms_per_step": t * 1e3,
+                     "stage_ms_median": {kk: statistics.median(s[kk] for s in sts)
+                                         for kk in ("dmk_ms", "near_ms", "nufft_ms", "total_ms")}}
+    ref = p_d.cpu().numpy()
+    mixed0 = Pc.cpu().numpy()[0]
+    td.close()
+    tf.close()
+    out["mixed_vs_plain_fp64"] = out["mixed_batched"]["value"] / out["plain_fp64_single_rhs"]["value"]
+    out["rel_l2_mixed_vs_plain_rhs0"] = float(np.linalg.norm(mixed0 - ref) / np.linalg.norm(ref))
+    out["workload"] = "the headline cube (N=%d) at 3 digits, npl 300, nz 4; %d RHS for the batched form" % (n, k)
+    return out
+
+
 def run_ours(args):
     import ctypes
 
@@ -694,6 +738,8 @@ def run_ours(args):
             "roofline": roofline, "measured_peaks": measured_peaks, "clocks": clk2.summary()}
     tree_d.close()
     tree_f.close()
+    if not args.no_digits3:
+        line["digits_3"] = run_digits3(pd, cell, pos, q, Q, args, world, dev, flush, barrier, max_over_ranks)
     if args.batch_systems > 0:
         line["batch"] = run_batch(pd, args, world, rank, barrier, max_over_ranks)
     if args.clustered_digits.strip():
@@ -734,6 +780,8 @@ def main():
                     help="time only the CPU oracle on bounded samples of every workload (JSON line)")
     ap.add_argument("--clustered-only", action="store_true",
                     help="run only the clustered triclinic FP64 measurement (its JSON fragment alone)")
+    ap.add_argument("--no-digits3", action="store_true",
+                    help="skip the 3-digit measurement of the headline cube")
     ap.add_argument("--batch-only", action="store_true",
                     help="run only the many-systems measurement of --batch-systems systems (its JSON fragment alone)")
     args = ap.parse_args()
