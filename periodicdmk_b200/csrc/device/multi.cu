@@ -1279,10 +1279,19 @@ void DeviceTree::run_multi_block(MultiState& m, const double* Q, int kvalid, dou
         for (int b0 = 0; b0 < E.n; b0 += Cb) {
             const int nb = std::min(Cb, E.n - b0);
             {
-                const dim3 grid(nb, (M + 255) / 256, (kb + 3) / 4);
-                dev::k_shift_m<T, 4><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
-                                                       static_cast<C*>(m.pw_in), M, E.term_start, E.term_slot,
-                                                       E.term_stencil, kb, b0); ++nl;
+                // eight RHS per thread for wide blocks (each shift weight feeds
+                // more products: 85.45 -> 84.95 ms per 64-RHS evaluate), four otherwise
+                if (kb >= 8) {
+                    const dim3 grid(nb, (M + 255) / 256, (kb + 7) / 8);
+                    dev::k_shift_m<T, 8><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
+                                                           static_cast<C*>(m.pw_in), M, E.term_start, E.term_slot,
+                                                           E.term_stencil, kb, b0); ++nl;
+                } else {
+                    const dim3 grid(nb, (M + 255) / 256, (kb + 3) / 4);
+                    dev::k_shift_m<T, 4><<<grid, 256, 0, s>>>(pw, static_cast<const T*>(levtab(E.level, 4)),
+                                                           static_cast<C*>(m.pw_in), M, E.term_start, E.term_slot,
+                                                           E.term_stencil, kb, b0); ++nl;
+                }
             }
             if (pw_fused) {
                 dev::PwFused f{};
